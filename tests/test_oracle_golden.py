@@ -1,0 +1,186 @@
+"""Pin the CPU oracle against the reference's own published known answers
+(tests/golden/known_answers.json, extracted by make_known_answers.py)."""
+import json
+import pathlib
+
+import numpy as np
+import pytest
+
+from oracle.mesh import block_tree_mesh
+from oracle.operator import PoissonOperator
+from oracle.multigrid import MultigridOptions, TreeGeometricMultigrid, jacobi_weight
+from oracle.krylov import solve
+
+GOLD = json.loads((pathlib.Path(__file__).parent / "golden" / "known_answers.json").read_text())
+
+
+def two_level(bs):
+    return block_tree_mesh(block_size=(bs, bs), max_level=2,
+                           refine=lambda k, o, e: k[0] == 0 or (k[0] == 1 and k[1] == 0 and k[2] == 0))
+
+
+@pytest.mark.parametrize("row", GOLD["manufactured_periodic_two_level"]["rows"], ids=lambda r: f"b{r['block']}")
+def test_manufactured_errors_match_published_table(row):
+    """docs/src/poisson.md:253-257: the L2/Linf errors (4 significant digits)
+    pin the composite operator, including the non-diagonal AMR face metric."""
+    mesh = two_level(row["block"])
+    assert mesh.ncells == row["cells"]
+    op = PoissonOperator(mesh)
+    mg = TreeGeometricMultigrid(op, MultigridOptions(coarse_size=8))
+    x, y = mesh.cell_centers()
+    exact = np.sin(2 * np.pi * x) * np.cos(2 * np.pi * y)
+    p, st = solve(op, mg, 8 * np.pi ** 2 * exact, rtol=1e-10, max_cycles=60)
+    assert st.converged
+    v = mesh.cell_volumes()
+    err = np.abs(p - exact)
+    l2 = np.sqrt(np.sum(v * err ** 2) / np.sum(v))
+    assert float(f"{l2:.3e}") == row["l2"]
+    assert float(f"{err.max():.3e}") == row["linf"]
+    # The published PCG counts are not asserted by the reference's own test
+    # (which checks a spread <= 3); this restatement takes at most two more.
+    assert row["pcg_iterations"] <= st.cycles <= row["pcg_iterations"] + 2
+
+
+def test_iteration_spread_and_second_order():
+    """test/operators/poisson.jl:820-831: spread <= 3, rates > 1.7."""
+    res = []
+    for bs in (4, 8, 16):
+        mesh = two_level(bs)
+        op = PoissonOperator(mesh)
+        mg = TreeGeometricMultigrid(op, MultigridOptions(coarse_size=8))
+        x, y = mesh.cell_centers()
+        exact = np.sin(2 * np.pi * x) * np.cos(2 * np.pi * y)
+        p, st = solve(op, mg, 8 * np.pi ** 2 * exact, rtol=1e-10, max_cycles=60)
+        v = mesh.cell_volumes()
+        err = np.abs(p - exact)
+        res.append((st.cycles, np.sqrt(np.sum(v * err ** 2) / np.sum(v)), err.max()))
+    cycles = [r[0] for r in res]
+    assert max(cycles) - min(cycles) <= 3
+    for k in (1, 2):
+        e = np.array([r[k] for r in res])
+        assert np.all(np.diff(e) < 0)
+        assert np.min(np.log2(e[:2] / e[1:])) > 1.7
+
+
+@pytest.mark.parametrize("periodic", [(True, True), (True, False), (False, True), (False, False)])
+def test_root_block_hierarchy(periodic):
+    g = GOLD["root_block_hierarchy"]
+    mesh = block_tree_mesh(base_mesh=tuple(g["base_mesh"]), block_size=tuple(g["block_size"]),
+                           origin=(-1.0, 0.25), extent=(2.0, 1.5), periodic=periodic)
+    coef = 3.0 + 0.1 * mesh.face_center[:, 0] + 0.2 * mesh.face_center[:, 1] + 0.3 * mesh.face_axis
+    op = PoissonOperator(mesh, coef)
+    mg = TreeGeometricMultigrid(op, MultigridOptions(coarse_size=g["coarse_size"]))
+    assert [list(o.mesh.base_mesh) for o in mg.operators] == g["expected_bases"]
+    assert mg.level_sizes == g["expected_sizes"]
+    for k, o in enumerate(mg.operators):
+        cm = o.mesh
+        assert abs(np.sum(o.volumes) - 3.0) <= 128 * np.finfo(float).eps * 3
+        expected = 3.0 + 0.1 * cm.face_center[:, 0] + 0.2 * cm.face_center[:, 1] + 0.3 * cm.face_axis
+        assert np.allclose(o.face_coefficient, expected, rtol=128 * np.finfo(float).eps, atol=0)
+        assert np.max(np.abs(o.matrix @ np.ones(cm.ncells))) <= 1024 * np.finfo(float).eps * max(
+            np.max(np.asarray(abs(o.matrix).sum(axis=1))), 1.0)
+        for axis in (1, 2):
+            tangential = cm.base_mesh[2 - axis]
+            assert np.sum(cm.bface_axis == axis) == (0 if periodic[axis - 1] else 2 * tangential)
+        if k + 1 < len(mg.operators):
+            P = mg.prolongations[k]
+            assert np.allclose(P @ np.ones(P.shape[1]), 1.0, atol=128 * np.finfo(float).eps, rtol=0)
+
+
+@pytest.mark.parametrize("case", GOLD["root_block_hierarchy"]["layout_cases"], ids=str)
+def test_isotropic_agglomeration(case):
+    layout, expected = case
+    mesh = block_tree_mesh(base_mesh=(layout[0] * 4, layout[1] * 4), block_size=(4, 4), periodic=(True, False))
+    mg = TreeGeometricMultigrid(PoissonOperator(mesh), MultigridOptions(coarse_size=1))
+    assert [list(o.mesh.tree.layout) for o in mg.operators] == expected
+    assert mg.level_sizes == [16 * r[0] * r[1] for r in expected]
+
+
+@pytest.mark.parametrize("case", GOLD["root_block_hierarchy"]["stopping_cases"], ids=str)
+def test_stopping_rules(case):
+    coarse_size, max_levels, expected = case
+    mesh = block_tree_mesh(base_mesh=(16, 16), block_size=(4, 4))
+    mg = TreeGeometricMultigrid(PoissonOperator(mesh), MultigridOptions(coarse_size=coarse_size, max_levels=max_levels))
+    assert mg.level_sizes == expected
+
+
+def test_mixed_pruning_sizes():
+    g = GOLD["root_block_hierarchy"]["mixed_pruning"]
+    mesh = block_tree_mesh(base_mesh=(8, 8), block_size=(4, 4), max_level=1,
+                           refine=lambda k, o, e: k == (0, 0, 0))
+    mg = TreeGeometricMultigrid(PoissonOperator(mesh), MultigridOptions(coarse_size=g["coarse_size"]))
+    assert mg.level_sizes == g["sizes"]
+
+
+@pytest.mark.parametrize("case", GOLD["periodic_floor"]["cases"], ids=str)
+def test_periodic_axes_keep_four_cells(case):
+    base, periodic, expected = case
+    mesh = block_tree_mesh(base_mesh=tuple(base), block_size=(2, 2), periodic=tuple(periodic))
+    mg = TreeGeometricMultigrid(PoissonOperator(mesh), MultigridOptions(coarse_size=1))
+    assert [list(o.mesh.base_mesh) for o in mg.operators] == expected
+
+
+def test_jacobi_weight_policies():
+    g = GOLD["jacobi_weight"]
+    s = g["skip_case"]
+    inv, w = jacobi_weight(np.array(s["diagonal"]), np.array(s["row_sums"]),
+                           skip_nonpositive=True, clamp=False, zero_weight=0.0)
+    assert list(inv) == s["inverse"] and w == s["weight"]
+    with pytest.raises(ValueError):
+        jacobi_weight(np.array([2.0, 0.0]), np.array([1.0, 0.0]))
+    for d, r, expected in g["clamped"]:
+        assert jacobi_weight(np.array(d), np.array(r))[1] == expected
+    assert jacobi_weight(np.array([2.0]), np.array([0.0]), skip_nonpositive=True,
+                         clamp=False, zero_weight=0.0)[1] == 0.0
+
+
+def test_factorized_action_matches_assembled_and_nullspace():
+    """test/operators/poisson.jl:255-298 and :758-818 (symmetry, A*1 = 0)."""
+    mesh = two_level(4)
+    coef = 1 + 0.3 * np.sin(np.arange(mesh.nfaces) + 1.0)
+    op = PoissonOperator(mesh, coef)
+    x = np.sin(0.7 * (np.arange(mesh.ncells) + 1))
+    y = np.cos(0.3 * (np.arange(mesh.ncells) + 1))
+    ax = op.apply(x)
+    assert np.allclose(ax, op.matrix @ x, rtol=64 * np.finfo(float).eps, atol=64 * np.finfo(float).eps * 10)
+    assert abs(x @ op.apply(y) - ax @ y) <= 128 * np.finfo(float).eps * abs(ax @ y) + 1e-14
+    assert np.max(np.abs(op.apply(np.ones(mesh.ncells)))) <= 64 * np.finfo(float).eps * 10
+    w = np.linalg.eigvalsh(op.matrix.toarray())
+    tol = 5e-12 * w.max()
+    assert w[0] >= -tol and np.sum(np.abs(w) <= tol) == 1
+
+
+def test_block_partition_independence():
+    """test/operators/poisson.jl:884-919: one block, four blocks and four roots
+    give the same solution to 2e-12."""
+    meshes = [block_tree_mesh(block_size=(16, 16)),
+              block_tree_mesh(block_size=(8, 8), max_level=1, refine=lambda k, o, e: True),
+              block_tree_mesh(base_mesh=(16, 16), block_size=(8, 8))]
+    sols = []
+    for mesh in meshes:
+        op = PoissonOperator(mesh)
+        mg = TreeGeometricMultigrid(op, MultigridOptions(coarse_size=8))
+        x, y = mesh.cell_centers()
+        p, st = solve(op, mg, 8 * np.pi ** 2 * np.sin(2 * np.pi * x) * np.cos(2 * np.pi * y), rtol=2e-12)
+        assert st.converged
+        sols.append(dict(zip(zip(np.round(x, 12), np.round(y, 12)), p)))
+    for other in sols[1:]:
+        assert other.keys() == sols[0].keys()
+        assert max(abs(other[k] - sols[0][k]) for k in sols[0]) <= 2e-12
+
+
+def test_periodic_nullspace_convention():
+    """test/operators/poisson.jl:921-933."""
+    mesh = block_tree_mesh(block_size=(8, 8))
+    op = PoissonOperator(mesh)
+    mg = TreeGeometricMultigrid(op, MultigridOptions(coarse_size=4))
+    rhs = np.full(mesh.ncells, 3.0)
+    with pytest.raises(ValueError):
+        solve(op, mg, rhs, compatibility="error")
+    with pytest.raises(ValueError):
+        solve(op, mg, rhs, compatibility="invalid")
+    p, st = solve(op, mg, rhs, x0=np.full(mesh.ncells, 7.0))
+    assert st.converged
+    assert abs(st.removed_rhs_mean - 3) < 1e-12
+    assert abs(np.sum(p * op.volumes)) <= 16 * np.finfo(float).eps
+    assert np.max(np.abs(p)) <= 16 * np.finfo(float).eps
