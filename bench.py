@@ -1,0 +1,270 @@
+"""Benchmark of the B200 pressure solve (one JSON line on rank 0).
+
+Workload: the two-phase droplet pressure solve on an adaptive tree (unit
+square, free-slip walls, 4x4 blocks of 16x16 cells refined 4 levels to
+h = 1/1024 in a band of 8 finest cells around the circle |x - (0.5, 0.6)| =
+0.15; density 1000 inside, 1 outside; CGFM surface-tension RHS plus N(0, 1)
+noise), solved to relative residual 1e-10 (strong L-infinity, the reference's
+`solve!(...; rtol=1e-10)`).  A step is one complete solve.
+
+metric: cell-updates/s = fine cells x CG iterations / time, for the mixed
+precision (FP32 V-cycle inside FP64 CG) solve; the FP64 solve on the same mesh
+is reported beside it.  Inputs are resident in HBM for `value`; `e2e` goes
+through the public C-ABI (`tpa_solve`) with pinned host buffers, host<->device
+copies inside the timed region.  The L2 is flushed (a 256 MiB write) between
+timed steps because the working set (~20 MB) fits in L2.
+
+`--impl reference` times the CPU restatement of the reference solve (the
+reference is Julia and does not run here) on the same workload.
+"""
+import argparse
+import json
+import os
+import pathlib
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path[:0] = [str(ROOT), str(ROOT / "twophaseamr.jl_b200")]
+
+RTOL = 1e-10
+HBM_FALLBACK = 6650.0
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return HBM_FALLBACK, "fallback"
+
+
+def workload(levels=4):
+    from tpagmg import workloads as W
+    return W.droplet_spec(levels=levels)
+
+
+def reference_arm(args):
+    """CPU restatement of the reference solve, on this host's cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import cgmg
+    res = cgmg.bench_droplet(steps=args.steps, warmup=args.warmup, levels=args.levels)
+    line = {
+        "impl": "reference", "metric": "cell-updates/s to rel. residual 1e-10 (droplet AMR pressure solve)",
+        "value": res["cell_updates_per_s"], "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Philox)",
+        "config": {"workload": f"droplet_amr levels={args.levels}", "fine_cells": res["cells"],
+                   "cg_iterations": res["iterations"], "threads": res["threads"]},
+        "cpu_baseline": {"value": res["cell_updates_per_s"], "unit": "cell-updates/s", "cores": res["threads"],
+                         "kind": "port", "sample": f"{args.steps} full solves of the droplet workload"},
+        "e2e": {"value": res["cell_updates_per_s"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in self.path.read_text().strip().splitlines() if r.strip()]
+            sm = [float(r[0]) for r in rows]
+            reasons = set()
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for r in rows:
+                for k, n in enumerate(names):
+                    if "Active" in r[3 + k] and "Not" not in r[3 + k]:
+                        reasons.add(n)
+            return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][1]), "reasons": sorted(reasons),
+                    "samples": len(rows)}
+        except Exception as e:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "error": str(e)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--levels", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import ctypes as C
+    import torch
+    import torch.distributed as dist
+    from tpagmg import EllipticSolver, PoissonOperator, BlockTreeMesh
+    from tpagmg import workloads as W
+    from tpagmg import _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    spec = workload(args.levels)
+    mesh = BlockTreeMesh(**spec)
+    frac, kappa, psi = W.droplet_inputs(mesh)
+    solver = EllipticSolver(PoissonOperator(mesh, kappa), device=local)
+    stream = torch.cuda.current_stream()
+    solver.ctx.call("tpa_set_stream", C.c_void_p(stream.cuda_stream))
+    rhs_h = W.droplet_rhs(mesh, solver.apply(psi))
+    n = mesh.ncells
+    rhs_d = torch.from_numpy(rhs_h).cuda()
+    x_d = torch.zeros(n, dtype=torch.float64, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
+
+    def device_solve(precision):
+        x_d.zero_()
+        return solver.solve_device(rhs_d.data_ptr(), x_d.data_ptr(), rtol=RTOL, precision=precision)
+
+    for _ in range(args.warmup):
+        device_solve("mixed")
+        device_solve("fp64")
+    barrier()
+
+    def timed(precision, steps):
+        ms, its, launches = [], [], 0
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = device_solve(precision)
+            e1.record(stream)
+            e1.synchronize()
+            assert st.converged, st
+            ms.append(e0.elapsed_time(e1))
+            its.append(st.cycles)
+            launches += st.kernel_launches
+        return float(np.mean(ms)), float(np.mean(its)), launches, ms
+
+    with ClockSampler(local) as clk:
+        barrier()
+        mixed_ms, mixed_it, mixed_launches, _ = timed("mixed", args.steps)
+        barrier()
+    fp64_ms, fp64_it, _, _ = timed("fp64", args.steps)
+    x_mixed = x_d.clone()
+    device_solve("fp64")
+    x_ref = x_d.clone()
+    mixed_err = float((x_mixed - x_ref).abs().max() / x_ref.abs().max())
+
+    # max over ranks
+    t = torch.tensor([mixed_ms, fp64_ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    mixed_ms, fp64_ms = (float(v) for v in t.cpu())
+
+    # end to end through the public C-ABI with pinned host buffers
+    rhs_pin = torch.from_numpy(rhs_h).pin_memory()
+    x_pin = torch.zeros(n, dtype=torch.float64).pin_memory()
+    e2e_ms = []
+    for k in range(args.steps + 1):
+        x_pin.zero_()
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = _lib.StatsC()
+        solver.ctx.call("tpa_solve", _lib.ptr(rhs_pin.numpy(), C.c_double), _lib.ptr(x_pin.numpy(), C.c_double),
+                        RTOL, 0.0, 100, 0, 1, C.byref(st))
+        dt = (time.perf_counter() - t0) * 1e3
+        if k:
+            e2e_ms.append(dt)
+        e2e_it = st.cycles
+    e2e_ms_mean = float(np.mean(e2e_ms))
+
+    # roofline: fine-level smoothing sweep of the mixed cycle, timed alone
+    sweep = C.c_double()
+    solver.ctx.call("tpa_time_kernel", 0, 0, 1, 200, C.byref(sweep))
+    sweep64 = C.c_double()
+    solver.ctx.call("tpa_time_kernel", 0, 0, 0, 200, C.byref(sweep64))
+    # algorithmic bytes of one damped-Jacobi sweep with variable coefficients:
+    # read x, b and two face coefficients per cell, write x (3 s + 2 s_kappa)
+    alg32 = n * (3 * 4 + 2 * 4)
+    alg64 = n * (3 * 8 + 2 * 8)
+    peak, peak_kind = measured_peaks()
+    achieved = alg32 / (sweep.value * 1e-3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import cgmg
+        res = cgmg.bench_droplet(steps=1, warmup=0, levels=args.levels, threads=os.cpu_count())
+        cpu = {"value": res["cell_updates_per_s"], "unit": "cell-updates/s", "cores": res["threads"],
+               "kind": "port", "sample": "1 full solve of the same droplet workload (setup excluded)"}
+
+    cells_updates = n * mixed_it
+    value = world * cells_updates / (mixed_ms * 1e-3)
+    line = {
+        "metric": "cell-updates/s to rel. residual 1e-10 (droplet AMR pressure solve, mixed FP32/FP64 GMG)",
+        "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": mixed_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32/f64", "data": "synthetic (seeded Philox)",
+        "config": {"workload": f"droplet_amr levels={args.levels} (unit square, 4x4 roots of 16x16, circle band)",
+                   "fine_cells": n, "levels": solver.level_sizes(), "parallelism": "replicas" if world > 1 else "1 GPU",
+                   "l2": "flushed between steps (256 MiB write)"},
+        "time_to_tolerance_ms": {"mixed": mixed_ms, "fp64": fp64_ms, "speedup_mixed_over_fp64": fp64_ms / mixed_ms},
+        "cg_iterations": {"mixed": mixed_it, "fp64": fp64_it},
+        "fp64_value": world * n * fp64_it / (fp64_ms * 1e-3),
+        "mixed_error_vs_fp64": mixed_err,
+        "e2e": {"value": world * n * e2e_it / (e2e_ms_mean * 1e-3), "unit": "cell-updates/s",
+                "ms_per_step": e2e_ms_mean, "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": mixed_launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "damped-Jacobi sweep, finest level, FP32",
+                     "kernel_ms": sweep.value, "kernel_ms_fp64": sweep64.value,
+                     "algorithmic_bytes": alg32, "peak_kind": peak_kind},
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,155 @@
+/*
+ * tpagmg.h - C-ABI of the B200 pressure-projection solver for TwoPhaseAMR.jl.
+ *
+ * The library replaces the reference's one-velocity pressure solve: Krylov CG
+ * preconditioned by the tree geometric multigrid over the block quadtree, with
+ * the variable-coefficient operator -div(kappa grad p) (kappa = 1/rho_f).  All
+ * paths cited below are inside ronaldremmerswaal/TwoPhaseAMR.jl.
+ *
+ * Conventions: indices are 0-based int32 (the reference's are 1-based Int64);
+ * cell index = block * nx * ny + j * nx + i with blocks sorted by
+ * (level, j, i) (src/mesh/topology/mesh.jl:28-30, 759-773).  The caller owns
+ * every host array; the library copies what it needs during the call and keeps
+ * no host pointers.  Every call returns a tpa_status; no C++ exception crosses
+ * this boundary.  Calls on one context must be serialised by the caller.
+ */
+#ifndef TPAGMG_H
+#define TPAGMG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t tpa_status;
+#define TPA_OK 0
+#define TPA_ERR_INVALID_ARG 1 /* bad sizes, values or call order (ArgumentError)  */
+#define TPA_ERR_CUDA 2        /* CUDA runtime failure or no usable device          */
+#define TPA_ERR_TIMEOUT 3     /* a bounded device wait gave up                     */
+#define TPA_ERR_NONFINITE 4   /* non-finite input                                  */
+#define TPA_ERR_UNSUPPORTED 5 /* outside the supported configuration              */
+#define TPA_ERR_STATE 7       /* call made before the state it needs exists        */
+
+#define TPA_PRECISION_FP64 0  /* V-cycle in FP64                                   */
+#define TPA_PRECISION_MIXED 1 /* V-cycle in FP32 inside the FP64 CG                */
+
+#define TPA_COMPATIBILITY_PROJECT 0
+#define TPA_COMPATIBILITY_ERROR 1
+
+typedef struct tpa_context tpa_context;
+
+/* MultigridOptions (src/solvers/multigrid/options.jl:14-48). */
+typedef struct {
+    int32_t coarse_size; /* default 64 */
+    int32_t pre_sweeps;  /* default 2  */
+    int32_t post_sweeps; /* default 2  */
+    int32_t max_levels;  /* default 32 */
+} tpa_multigrid_options;
+
+/* LinearSolverStats (src/solvers/multigrid/stats.jl:15-30) plus device timing. */
+typedef struct {
+    int32_t cycles;
+    int32_t converged;
+    int32_t compatible;
+    int32_t restarts;
+    double initial_l2;
+    double initial_linf;
+    double final_l2;
+    double final_linf;
+    double target_linf;
+    double residual_scale;
+    double removed_rhs_mean;
+    double device_ms;       /* CUDA-event time of the solve on the solver stream   */
+    int32_t kernel_launches; /* kernels this call launched                         */
+    int32_t precision;
+} tpa_stats;
+
+/* Create a context for CUDA device `device`.  No CUDA call is made until the
+ * first device operation.  Replaces the Julia-side EllipticSolver state. */
+tpa_status tpa_create(tpa_context** out, int32_t device);
+void tpa_destroy(tpa_context* ctx);
+/* Message of the last failed call on ctx (valid until the next call). */
+const char* tpa_last_error(const tpa_context* ctx);
+
+/* BlockTreeMesh(; base_mesh, block_size, origin, extent, periodic) from its
+ * leaf keys (src/mesh/topology/mesh.jl:1059-1121): the library restores 2:1
+ * grading (`_balance!`, mesh.jl:673-714), sorts the blocks and builds the face
+ * schedules.  leaf_keys holds (level, i, j) per leaf. */
+tpa_status tpa_set_mesh(tpa_context* ctx, const int32_t base_mesh[2], const int32_t block_size[2],
+                        const int32_t periodic[2], const double origin[2], const double extent[2], int64_t nleaves,
+                        const int32_t* leaf_keys);
+/* out = {nblocks, ncells, ninterior_faces, nboundary_faces, finest_level}. */
+tpa_status tpa_mesh_sizes(const tpa_context* ctx, int64_t out[5]);
+/* Sorted leaf keys (3 per block) and geometry (origin x, origin y, spacing x,
+ * spacing y, volume per block); either pointer may be NULL
+ * (mesh.blocks, mesh.jl:12-19, 759-773). */
+tpa_status tpa_mesh_blocks(const tpa_context* ctx, int32_t* keys, double* geometry);
+/* Interior faces in schedule order (mesh.faces, mesh.jl:32-38, 874-927):
+ * minus cell, plus cell, axis (1 or 2), area.  Any pointer may be NULL. */
+tpa_status tpa_mesh_faces(const tpa_context* ctx, int32_t* minus, int32_t* plus, int8_t* axis, double* area);
+/* Boundary faces (mesh.boundary_faces, mesh.jl:40-46). */
+tpa_status tpa_mesh_boundary_faces(const tpa_context* ctx, int32_t* cell, int8_t* axis, int8_t* side,
+                                   double* area);
+
+/* PoissonOperator(mesh; face_coefficient) (src/operators/elliptic.jl:969-980):
+ * one nonnegative coefficient per interior face (kappa = 1/rho_f for the
+ * two-phase operator, two_phase/forces.jl:113-140). */
+tpa_status tpa_set_operator(tpa_context* ctx, const double* face_coefficient);
+/* Number of stored off-diagonal inverse-metric entries (0 when K is diagonal),
+ * operators/gradient.jl:369-393. */
+tpa_status tpa_metric_offdiagonal_count(const tpa_context* ctx, int64_t* count);
+
+/* TreeGeometricMultigridPreconditioner(operator; multigrid) with pruning=:all
+ * (src/solvers/multigrid/geometric_preconditioner.jl:171-442); opts may be NULL
+ * for the defaults.  Host set-up only. */
+tpa_status tpa_build_hierarchy(tpa_context* ctx, const tpa_multigrid_options* opts);
+/* Number of levels and the cell count of each (hierarchy.operators). */
+tpa_status tpa_hierarchy_sizes(const tpa_context* ctx, int32_t* nlevels, int64_t* sizes, int32_t capacity);
+/* Tentative owners of level `level` (fine cell -> coarse cell of level+1),
+ * `_tree_cell_prolongation` (tree_coarsening.jl:228-252). */
+tpa_status tpa_level_owners(const tpa_context* ctx, int32_t level, int32_t* owners);
+/* Level scalars: smoother weight, transfer weight, number of ungauged components. */
+tpa_status tpa_level_info(const tpa_context* ctx, int32_t level, double* smoother_weight, double* transfer_weight,
+                          int32_t* components);
+/* Restricted face coefficients of level `level` (tree_coarsening.jl:538-555). */
+tpa_status tpa_level_face_coefficients(const tpa_context* ctx, int32_t level, double* kappa);
+
+/* `_refresh_geometric_multigrid!` (geometric_preconditioner.jl:483-594): new
+ * fine face coefficients on the fixed topology; refreshes every level. */
+tpa_status tpa_refresh(tpa_context* ctx, const double* face_coefficient);
+
+/* solve!(solution, solver, rhs; rtol, atol, max_cycles, compatibility)
+ * (src/solvers/multigrid/elliptic_solver.jl:628-675).  rhs is the strong-form
+ * right-hand side, x the initial guess on entry and the solution on return,
+ * both host arrays in cell order. */
+tpa_status tpa_solve(tpa_context* ctx, const double* rhs, double* x, double rtol, double atol, int32_t max_cycles,
+                     int32_t compatibility, int32_t precision, tpa_stats* stats);
+/* Same with device pointers (cell order, on the context's device). */
+tpa_status tpa_solve_device(tpa_context* ctx, const double* rhs, double* x, double rtol, double atol,
+                            int32_t max_cycles, int32_t compatibility, int32_t precision, tpa_stats* stats);
+
+/* y = S x, the integrated pressure operator on the finest level
+ * (FactorizedEllipticOperator mul!, elliptic.jl:1125-1180).  Host arrays. */
+tpa_status tpa_apply(tpa_context* ctx, const double* x, double* y);
+/* z = one V-cycle applied to the integrated residual r (ldiv!, cycles.jl:262-283). */
+tpa_status tpa_vcycle(tpa_context* ctx, const double* r, double* z, int32_t precision);
+/* Wait for the context's stream. */
+tpa_status tpa_synchronize(tpa_context* ctx);
+/* Run subsequent device work on the caller's CUDA stream (a cudaStream_t
+ * passed as void*; NULL restores the context's own stream).  Replaces nothing
+ * in the reference (it has no device); it lets a caller order the solve with
+ * its own device work and time it with events on that stream. */
+tpa_status tpa_set_stream(tpa_context* ctx, void* stream);
+/* Average device time in ms of `iters` back-to-back launches of one kernel on
+ * level `level`: which = 0 smoothing sweep, 1 residual + restriction,
+ * 2 prolongation, 3 CG operator product (finest level, FP64).  Measurement
+ * support for the roofline; it overwrites the level's work vectors. */
+tpa_status tpa_time_kernel(tpa_context* ctx, int32_t which, int32_t level, int32_t precision, int32_t iters,
+                           double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TPAGMG_H */

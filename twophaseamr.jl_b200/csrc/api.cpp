@@ -1,0 +1,393 @@
+// C-ABI of the B200 pressure solver (declared in include/tpagmg.h).
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/tpagmg.h"
+#include "device.cuh"
+#include "host.hpp"
+
+struct tpa_context {
+    int device = 0;
+    std::string error;
+    bool have_mesh = false, have_operator = false, have_hierarchy = false, uploaded = false;
+    tpa::Mesh mesh;
+    tpa::LevelOperator op;  // fine operator before the hierarchy takes it
+    tpa::Hierarchy hier;
+    std::unique_ptr<tpa::DeviceSolver> dev;
+    tpa::DevArray<double> d_rhs, d_x, d_y;
+    void* user_stream = nullptr;
+};
+
+namespace {
+
+template <typename F>
+tpa_status guard(tpa_context* ctx, F&& f) {
+    if (!ctx) return TPA_ERR_INVALID_ARG;
+    try {
+        ctx->error.clear();
+        f();
+        return TPA_OK;
+    } catch (const tpa::Error& e) {
+        ctx->error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        ctx->error = "host allocation failed";
+        return TPA_ERR_INVALID_ARG;
+    } catch (const std::exception& e) {
+        ctx->error = e.what();
+        return TPA_ERR_INVALID_ARG;
+    }
+}
+
+const tpa::LevelOperator& fine_op(const tpa_context* ctx) {
+    if (ctx->have_hierarchy) return ctx->hier.levels[0].op;
+    if (!ctx->have_operator) throw tpa::Error(TPA_ERR_STATE, "no operator: call tpa_set_operator first");
+    return ctx->op;
+}
+
+void ensure_device(tpa_context* ctx) {
+    if (!ctx->have_hierarchy) throw tpa::Error(TPA_ERR_STATE, "no hierarchy: call tpa_build_hierarchy first");
+    if (ctx->uploaded) return;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count <= ctx->device)
+        throw tpa::Error(TPA_ERR_CUDA, "no usable CUDA device for the B200 solver");
+    if (!ctx->dev) ctx->dev.reset(new tpa::DeviceSolver(ctx->device));
+    ctx->dev->set_stream(static_cast<cudaStream_t>(ctx->user_stream));
+    ctx->dev->upload(ctx->hier);
+    size_t n = size_t(ctx->dev->ncells());
+    ctx->d_rhs.alloc(n);
+    ctx->d_x.alloc(n);
+    ctx->d_y.alloc(n);
+    ctx->uploaded = true;
+}
+
+void fill_stats(const tpa::SolveStats& s, int precision, int launches, tpa_stats* out) {
+    if (!out) return;
+    std::memset(out, 0, sizeof(*out));
+    out->cycles = s.cycles;
+    out->converged = s.converged;
+    out->compatible = 1;
+    out->restarts = s.restarts;
+    out->initial_l2 = s.initial_l2;
+    out->initial_linf = s.initial_linf;
+    out->final_l2 = s.final_l2;
+    out->final_linf = s.final_linf;
+    out->target_linf = s.target_linf;
+    out->residual_scale = s.residual_scale;
+    out->removed_rhs_mean = s.removed_rhs_mean;
+    out->device_ms = s.ms_total;
+    out->kernel_launches = launches;
+    out->precision = precision;
+}
+
+}  // namespace
+
+extern "C" {
+
+tpa_status tpa_create(tpa_context** out, int32_t device) {
+    if (!out || device < 0) return TPA_ERR_INVALID_ARG;
+    try {
+        *out = new tpa_context();
+        (*out)->device = device;
+        return TPA_OK;
+    } catch (...) {
+        return TPA_ERR_INVALID_ARG;
+    }
+}
+
+void tpa_destroy(tpa_context* ctx) {
+    if (!ctx) return;
+    try {
+        ctx->d_rhs.free();
+        ctx->d_x.free();
+        ctx->d_y.free();
+        ctx->dev.reset();
+    } catch (...) {
+    }
+    delete ctx;
+}
+
+const char* tpa_last_error(const tpa_context* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
+
+tpa_status tpa_set_mesh(tpa_context* ctx, const int32_t base_mesh[2], const int32_t block_size[2],
+                        const int32_t periodic[2], const double origin[2], const double extent[2], int64_t nleaves,
+                        const int32_t* leaf_keys) {
+    return guard(ctx, [&] {
+        if (!base_mesh || !block_size || !periodic || !origin || !extent || (nleaves > 0 && !leaf_keys) ||
+            nleaves < 0)
+            throw tpa::Error(TPA_ERR_INVALID_ARG, "null argument");
+        int base[2] = {base_mesh[0], base_mesh[1]}, bs[2] = {block_size[0], block_size[1]};
+        bool per[2] = {periodic[0] != 0, periodic[1] != 0};
+        for (int a = 0; a < 2; ++a)
+            if (!std::isfinite(origin[a]) || !std::isfinite(extent[a]))
+                throw tpa::Error(TPA_ERR_NONFINITE, "domain origin and extent must be finite");
+        std::vector<uint64_t> leaves;
+        if (nleaves == 0) {
+            for (int j = 0; j < base[1] / std::max(bs[1], 1); ++j)
+                for (int i = 0; i < base[0] / std::max(bs[0], 1); ++i) leaves.push_back(tpa::pack_key(0, i, j));
+        } else {
+            for (int64_t k = 0; k < nleaves; ++k) {
+                const int32_t* kk = leaf_keys + 3 * k;
+                if (kk[0] < 0 || kk[1] < 0 || kk[2] < 0) throw tpa::Error(TPA_ERR_INVALID_ARG, "negative leaf key");
+                leaves.push_back(tpa::pack_key(kk[0], kk[1], kk[2]));
+            }
+        }
+        ctx->mesh = tpa::build_mesh(base, bs, per, origin, extent, leaves);
+        ctx->have_mesh = true;
+        ctx->have_operator = ctx->have_hierarchy = ctx->uploaded = false;
+    });
+}
+
+tpa_status tpa_mesh_sizes(const tpa_context* cctx, int64_t out[5]) {
+    auto* ctx = const_cast<tpa_context*>(cctx);
+    return guard(ctx, [&] {
+        if (!ctx->have_mesh) throw tpa::Error(TPA_ERR_STATE, "no mesh");
+        const tpa::Mesh& m = ctx->have_hierarchy ? ctx->hier.levels[0].op.mesh : ctx->mesh;
+        out[0] = m.nblocks();
+        out[1] = m.ncells();
+        out[2] = m.nfaces();
+        out[3] = int64_t(m.bcell.size());
+        out[4] = m.active;
+    });
+}
+
+static const tpa::Mesh& cur_mesh(const tpa_context* ctx) {
+    if (!ctx->have_mesh) throw tpa::Error(TPA_ERR_STATE, "no mesh");
+    return ctx->have_hierarchy ? ctx->hier.levels[0].op.mesh : (ctx->have_operator ? ctx->op.mesh : ctx->mesh);
+}
+
+tpa_status tpa_mesh_blocks(const tpa_context* cctx, int32_t* keys, double* geometry) {
+    auto* ctx = const_cast<tpa_context*>(cctx);
+    return guard(ctx, [&] {
+        const tpa::Mesh& m = cur_mesh(ctx);
+        for (int64_t b = 0; b < m.nblocks(); ++b) {
+            uint64_t k = m.keys[size_t(b)];
+            if (keys) {
+                keys[3 * b] = tpa::key_level(k);
+                keys[3 * b + 1] = int32_t(tpa::key_i(k));
+                keys[3 * b + 2] = int32_t(tpa::key_j(k));
+            }
+            if (geometry) {
+                geometry[5 * b] = m.box[size_t(b)];
+                geometry[5 * b + 1] = m.boy[size_t(b)];
+                geometry[5 * b + 2] = m.bsx[size_t(b)];
+                geometry[5 * b + 3] = m.bsy[size_t(b)];
+                geometry[5 * b + 4] = m.bvol[size_t(b)];
+            }
+        }
+    });
+}
+
+tpa_status tpa_mesh_faces(const tpa_context* cctx, int32_t* minus, int32_t* plus, int8_t* axis, double* area) {
+    auto* ctx = const_cast<tpa_context*>(cctx);
+    return guard(ctx, [&] {
+        const tpa::Mesh& m = cur_mesh(ctx);
+        size_t nf = m.fm.size();
+        if (minus) std::memcpy(minus, m.fm.data(), nf * sizeof(int32_t));
+        if (plus) std::memcpy(plus, m.fp.data(), nf * sizeof(int32_t));
+        if (axis) std::memcpy(axis, m.fax.data(), nf);
+        if (area) std::memcpy(area, m.farea.data(), nf * sizeof(double));
+    });
+}
+
+tpa_status tpa_mesh_boundary_faces(const tpa_context* cctx, int32_t* cell, int8_t* axis, int8_t* side,
+                                   double* area) {
+    auto* ctx = const_cast<tpa_context*>(cctx);
+    return guard(ctx, [&] {
+        const tpa::Mesh& m = cur_mesh(ctx);
+        size_t nb = m.bcell.size();
+        if (cell) std::memcpy(cell, m.bcell.data(), nb * sizeof(int32_t));
+        if (axis) std::memcpy(axis, m.bax.data(), nb);
+        if (side) std::memcpy(side, m.bside.data(), nb);
+        if (area) std::memcpy(area, m.barea.data(), nb * sizeof(double));
+    });
+}
+
+tpa_status tpa_set_operator(tpa_context* ctx, const double* face_coefficient) {
+    return guard(ctx, [&] {
+        if (!ctx->have_mesh) throw tpa::Error(TPA_ERR_STATE, "no mesh: call tpa_set_mesh first");
+        if (!face_coefficient) throw tpa::Error(TPA_ERR_INVALID_ARG, "null face coefficients");
+        tpa::LevelOperator op;
+        op.mesh = ctx->have_hierarchy ? ctx->hier.levels[0].op.mesh : (ctx->have_operator ? ctx->op.mesh : ctx->mesh);
+        size_t nf = op.mesh.fm.size();
+        for (size_t f = 0; f < nf; ++f)
+            if (!std::isfinite(face_coefficient[f])) throw tpa::Error(TPA_ERR_NONFINITE, "face coefficients must be finite");
+        op.kappa.assign(face_coefficient, face_coefficient + nf);
+        op.metric = tpa::assemble_metric(op.mesh);
+        tpa::assemble_operator(op);
+        ctx->op = std::move(op);
+        ctx->have_operator = true;
+        ctx->have_hierarchy = ctx->uploaded = false;
+    });
+}
+
+tpa_status tpa_metric_offdiagonal_count(const tpa_context* cctx, int64_t* count) {
+    auto* ctx = const_cast<tpa_context*>(cctx);
+    return guard(ctx, [&] { *count = int64_t(fine_op(ctx).metric.off_val.size()); });
+}
+
+tpa_status tpa_build_hierarchy(tpa_context* ctx, const tpa_multigrid_options* opts) {
+    return guard(ctx, [&] {
+        if (!ctx->have_operator && !ctx->have_hierarchy)
+            throw tpa::Error(TPA_ERR_STATE, "no operator: call tpa_set_operator first");
+        tpa::HierarchyOptions o;
+        if (opts) {
+            o.coarse_size = opts->coarse_size;
+            o.pre_sweeps = opts->pre_sweeps;
+            o.post_sweeps = opts->post_sweeps;
+            o.max_levels = opts->max_levels;
+        }
+        if (o.pre_sweeps != o.post_sweeps)
+            throw tpa::Error(TPA_ERR_INVALID_ARG,
+                             "CG requires equal pre_sweeps and post_sweeps for a geometric multigrid preconditioner");
+        tpa::LevelOperator fine = ctx->have_hierarchy ? ctx->hier.levels[0].op : std::move(ctx->op);
+        ctx->have_hierarchy = false;
+        ctx->hier = tpa::build_hierarchy(std::move(fine), o);
+        ctx->op = tpa::LevelOperator();
+        ctx->have_hierarchy = true;
+        ctx->have_operator = true;
+        ctx->uploaded = false;
+    });
+}
+
+tpa_status tpa_hierarchy_sizes(const tpa_context* cctx, int32_t* nlevels, int64_t* sizes, int32_t capacity) {
+    auto* ctx = const_cast<tpa_context*>(cctx);
+    return guard(ctx, [&] {
+        if (!ctx->have_hierarchy) throw tpa::Error(TPA_ERR_STATE, "no hierarchy");
+        int32_t nl = int32_t(ctx->hier.levels.size());
+        if (nlevels) *nlevels = nl;
+        for (int32_t l = 0; sizes && l < nl && l < capacity; ++l) sizes[l] = ctx->hier.levels[size_t(l)].op.A.n;
+    });
+}
+
+static const tpa::HostLevel& level_of(const tpa_context* ctx, int32_t level) {
+    if (!ctx->have_hierarchy) throw tpa::Error(TPA_ERR_STATE, "no hierarchy");
+    if (level < 0 || size_t(level) >= ctx->hier.levels.size()) throw tpa::Error(TPA_ERR_INVALID_ARG, "bad level");
+    return ctx->hier.levels[size_t(level)];
+}
+
+tpa_status tpa_level_owners(const tpa_context* cctx, int32_t level, int32_t* owners) {
+    auto* ctx = const_cast<tpa_context*>(cctx);
+    return guard(ctx, [&] {
+        const tpa::HostLevel& l = level_of(ctx, level);
+        if (l.owner.empty()) throw tpa::Error(TPA_ERR_INVALID_ARG, "the coarsest level has no transfer");
+        std::memcpy(owners, l.owner.data(), l.owner.size() * sizeof(int32_t));
+    });
+}
+
+tpa_status tpa_level_info(const tpa_context* cctx, int32_t level, double* sw, double* tw, int32_t* comps) {
+    auto* ctx = const_cast<tpa_context*>(cctx);
+    return guard(ctx, [&] {
+        const tpa::HostLevel& l = level_of(ctx, level);
+        if (sw) *sw = l.weight;
+        if (tw) *tw = l.transfer_weight;
+        if (comps) *comps = l.op.singular ? int32_t(l.op.comp.volume.size()) : 0;
+    });
+}
+
+tpa_status tpa_level_face_coefficients(const tpa_context* cctx, int32_t level, double* kappa) {
+    auto* ctx = const_cast<tpa_context*>(cctx);
+    return guard(ctx, [&] {
+        const tpa::HostLevel& l = level_of(ctx, level);
+        std::memcpy(kappa, l.op.kappa.data(), l.op.kappa.size() * sizeof(double));
+    });
+}
+
+tpa_status tpa_refresh(tpa_context* ctx, const double* face_coefficient) {
+    return guard(ctx, [&] {
+        if (!ctx->have_hierarchy) throw tpa::Error(TPA_ERR_STATE, "no hierarchy");
+        size_t nf = ctx->hier.levels[0].op.kappa.size();
+        for (size_t f = 0; f < nf; ++f)
+            if (!std::isfinite(face_coefficient[f]) || face_coefficient[f] < 0)
+                throw tpa::Error(TPA_ERR_INVALID_ARG, "face coefficients must be finite and nonnegative");
+        tpa::refresh_hierarchy(ctx->hier, std::vector<double>(face_coefficient, face_coefficient + nf));
+        if (ctx->uploaded) {
+            ctx->dev->upload(ctx->hier);
+        }
+    });
+}
+
+tpa_status tpa_solve_device(tpa_context* ctx, const double* rhs, double* x, double rtol, double atol,
+                            int32_t max_cycles, int32_t compatibility, int32_t precision, tpa_stats* stats) {
+    return guard(ctx, [&] {
+        ensure_device(ctx);
+        tpa::SolveStats st;
+        ctx->dev->reset_launches();
+        ctx->dev->solve(rhs, x, rtol, atol, max_cycles, compatibility, precision, st);
+        fill_stats(st, precision, ctx->dev->kernel_launches(), stats);
+    });
+}
+
+tpa_status tpa_solve(tpa_context* ctx, const double* rhs, double* x, double rtol, double atol, int32_t max_cycles,
+                     int32_t compatibility, int32_t precision, tpa_stats* stats) {
+    return guard(ctx, [&] {
+        if (!rhs || !x) throw tpa::Error(TPA_ERR_INVALID_ARG, "null rhs or solution");
+        ensure_device(ctx);
+        size_t n = size_t(ctx->dev->ncells());
+        for (size_t i = 0; i < n; ++i)
+            if (!std::isfinite(rhs[i])) throw tpa::Error(TPA_ERR_NONFINITE, "right-hand side must be finite");
+        cudaStream_t s = ctx->dev->stream();
+        TPA_CUDA(cudaMemcpyAsync(ctx->d_rhs.p, rhs, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        TPA_CUDA(cudaMemcpyAsync(ctx->d_x.p, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        tpa::SolveStats st;
+        ctx->dev->reset_launches();
+        ctx->dev->solve(ctx->d_rhs.p, ctx->d_x.p, rtol, atol, max_cycles, compatibility, precision, st);
+        TPA_CUDA(cudaMemcpyAsync(x, ctx->d_x.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        TPA_CUDA(cudaStreamSynchronize(s));
+        fill_stats(st, precision, ctx->dev->kernel_launches(), stats);
+    });
+}
+
+tpa_status tpa_apply(tpa_context* ctx, const double* x, double* y) {
+    return guard(ctx, [&] {
+        ensure_device(ctx);
+        size_t n = size_t(ctx->dev->ncells());
+        cudaStream_t s = ctx->dev->stream();
+        TPA_CUDA(cudaMemcpyAsync(ctx->d_x.p, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        ctx->dev->apply(ctx->d_x.p, ctx->d_y.p);
+        TPA_CUDA(cudaMemcpyAsync(y, ctx->d_y.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        TPA_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+tpa_status tpa_vcycle(tpa_context* ctx, const double* r, double* z, int32_t precision) {
+    return guard(ctx, [&] {
+        if (precision != 0 && precision != 1) throw tpa::Error(TPA_ERR_INVALID_ARG, "bad precision");
+        ensure_device(ctx);
+        size_t n = size_t(ctx->dev->ncells());
+        cudaStream_t s = ctx->dev->stream();
+        TPA_CUDA(cudaMemcpyAsync(ctx->d_x.p, r, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        ctx->dev->vcycle(ctx->d_x.p, ctx->d_y.p, precision);
+        TPA_CUDA(cudaMemcpyAsync(z, ctx->d_y.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        TPA_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+tpa_status tpa_set_stream(tpa_context* ctx, void* stream) {
+    return guard(ctx, [&] {
+        if (ctx->dev) TPA_CUDA(cudaStreamSynchronize(ctx->dev->stream()));
+        ctx->user_stream = stream;
+        if (ctx->dev) ctx->dev->set_stream(static_cast<cudaStream_t>(stream));
+    });
+}
+
+tpa_status tpa_time_kernel(tpa_context* ctx, int32_t which, int32_t level, int32_t precision, int32_t iters,
+                           double* ms) {
+    return guard(ctx, [&] {
+        if (which < 0 || which > 3 || iters <= 0 || !ms || (precision != 0 && precision != 1))
+            throw tpa::Error(TPA_ERR_INVALID_ARG, "bad kernel timing request");
+        ensure_device(ctx);
+        *ms = ctx->dev->time_kernel(which, level, precision, iters);
+    });
+}
+
+tpa_status tpa_synchronize(tpa_context* ctx) {
+    return guard(ctx, [&] {
+        if (ctx->dev) TPA_CUDA(cudaStreamSynchronize(ctx->dev->stream()));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,147 @@
+// Device-resident tree hierarchy and the B200 solve (V-cycle + PCG).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "host.hpp"
+
+namespace tpa {
+
+constexpr int kMaxComponents = 16;
+constexpr int kReduceBlocks = 296;   // 2 CTAs per SM on 148 SMs; fixed => deterministic sums
+constexpr int kThreads = 256;
+
+#define TPA_CUDA(call)                                                                    \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            throw ::tpa::Error(2, std::string(#call) + ": " + cudaGetErrorString(e_));    \
+    } while (0)
+
+template <typename T>
+struct DevArray {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        free();
+        n = count;
+        if (count) TPA_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    }
+    void upload(const T* h, size_t count, cudaStream_t s) {
+        if (count != n) alloc(count);
+        if (count) TPA_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void free() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevArray() { free(); }
+    DevArray() = default;
+    DevArray(const DevArray&) = delete;
+    DevArray& operator=(const DevArray&) = delete;
+    DevArray(DevArray&& o) noexcept : p(o.p), n(o.n) {
+        o.p = nullptr;
+        o.n = 0;
+    }
+    DevArray& operator=(DevArray&& o) noexcept {
+        if (this != &o) {
+            free();
+            p = o.p;
+            n = o.n;
+            o.p = nullptr;
+            o.n = 0;
+        }
+        return *this;
+    }
+};
+
+// Level data in one precision T (double for the FP64 cycle, float for the
+// mixed-precision cycle).
+template <typename T>
+struct DevLevelT {
+    DevArray<T> val, dinv, tinv, vol;
+    DevArray<T> x, y, b, r, s;   // work vectors
+    T w = 1, tw = 0;             // smoother weight, transfer weight
+};
+
+struct DevLevel {
+    int n = 0, nc = 0;           // cells here, cells on the next coarser level
+    int64_t nnz = 0;
+    int ncomp = 0;               // ungauged components (0: nonsingular)
+    DevArray<int> rowptr, col, owner, child_ptr, child, slot;
+    std::vector<double> comp_volume;
+    DevLevelT<double> d;
+    DevLevelT<float> f;
+};
+
+// PCG scalars kept on the device between kernels.
+struct CgScalars {
+    double gamma, gamma_next, pAp, alpha, beta, pnorm2;
+    double strong_max, target, rnorm;
+    int flags;    // bit0: user exit (strong residual <= target), bit1: zero curvature, bit2: machine/solved
+    int iter;
+};
+
+struct SolveStats {
+    int cycles = 0, converged = 0;
+    double initial_l2 = 0, initial_linf = 0, final_l2 = 0, final_linf = 0, target_linf = 0;
+    double residual_scale = 1, removed_rhs_mean = 0;
+    double ms_total = 0;
+    int restarts = 0;
+};
+
+class DeviceSolver {
+public:
+    explicit DeviceSolver(int device);
+    ~DeviceSolver();
+    void upload(const Hierarchy& h);
+    int ncells() const { return levels_.empty() ? 0 : levels_[0].n; }
+    int nlevels() const { return int(levels_.size()); }
+    cudaStream_t stream() const { return stream_; }
+    // Run on a caller-owned stream (nullptr: the solver's own stream).
+    void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
+    // Average time (ms) of `iters` launches of one kernel family on level `level`:
+    // 0 = smoothing sweep, 1 = residual+restriction, 2 = prolongation, 3 = CG operator.
+    double time_kernel(int which, int level, int precision, int iters);
+
+    // y = A x on the finest level (FP64), device pointers.
+    void apply(const double* x, double* y);
+    // z = V-cycle(r), device pointers; precision 0 = FP64, 1 = FP32 cycle.
+    void vcycle(const double* r, double* z, int precision);
+    // `solve!`: rhs (strong form) and x (initial guess in, solution out) are
+    // device pointers in cell order.
+    void solve(const double* rhs, double* x, double rtol, double atol, int max_cycles, int compatibility,
+               int precision, SolveStats& st);
+
+    int kernel_launches() const { return launches_; }
+    void reset_launches() { launches_ = 0; }
+
+private:
+    template <typename T> DevLevelT<T>& lv(int l);
+    template <typename T> void vcycle_t(int l);
+    template <typename T> void project_rhs(int l, T* b);
+    template <typename T> void remove_means(int l, T* x);
+    void strong_max(const double* r, double* out_dev);
+    double read_scalar(const double* dev);
+
+    int device_;
+    cudaStream_t stream_ = nullptr, own_stream_ = nullptr;
+    std::vector<DevLevel> levels_;
+    DevArray<double> coarse_inv_, coarse_b_, coarse_x_;
+    int coarse_n_ = 0;
+    int pre_ = 2, post_ = 2;
+    // fine-level FP64 PCG workspace
+    DevArray<double> b_, r_, p_, ap_, z_, tmp_, partial_;
+    DevArray<CgScalars> sc_;
+    DevArray<double> sums_;   // component sums scratch
+    CgScalars* host_sc_ = nullptr;
+    double* host_d_ = nullptr;
+    int launches_ = 0;
+};
+
+}  // namespace tpa

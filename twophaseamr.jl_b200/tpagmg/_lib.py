@@ -1,0 +1,130 @@
+"""ctypes binding of `libtpagmg.so` (the C-ABI declared in include/tpagmg.h).
+
+The library is loaded from `tpagmg/_lib/` inside the source tree.  There is no
+CPU fallback: if the library is missing, importing the solver raises, and every
+device entry point returns TPA_ERR_CUDA on a machine without a CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+
+import numpy as np
+
+LIB_PATH = pathlib.Path(__file__).resolve().parent / "_lib" / "libtpagmg.so"
+
+TPA_OK = 0
+TPA_ERR_INVALID_ARG = 1
+TPA_ERR_CUDA = 2
+TPA_ERR_TIMEOUT = 3
+TPA_ERR_NONFINITE = 4
+TPA_ERR_UNSUPPORTED = 5
+TPA_ERR_STATE = 7
+
+
+class TpaError(RuntimeError):
+    """A failed library call; `code` is the tpa_status."""
+
+    def __init__(self, code, message):
+        super().__init__(f"[tpa_status {code}] {message}")
+        self.code = code
+
+
+class MultigridOptionsC(C.Structure):
+    _fields_ = [("coarse_size", C.c_int32), ("pre_sweeps", C.c_int32),
+                ("post_sweeps", C.c_int32), ("max_levels", C.c_int32)]
+
+
+class StatsC(C.Structure):
+    _fields_ = [("cycles", C.c_int32), ("converged", C.c_int32), ("compatible", C.c_int32),
+                ("restarts", C.c_int32), ("initial_l2", C.c_double), ("initial_linf", C.c_double),
+                ("final_l2", C.c_double), ("final_linf", C.c_double), ("target_linf", C.c_double),
+                ("residual_scale", C.c_double), ("removed_rhs_mean", C.c_double),
+                ("device_ms", C.c_double), ("kernel_launches", C.c_int32), ("precision", C.c_int32)]
+
+
+P = C.c_void_p
+i32p = C.POINTER(C.c_int32)
+i64p = C.POINTER(C.c_int64)
+f64p = C.POINTER(C.c_double)
+i8p = C.POINTER(C.c_int8)
+
+SIGNATURES = {
+    "tpa_create": (C.c_int32, [C.POINTER(P), C.c_int32]),
+    "tpa_destroy": (None, [P]),
+    "tpa_last_error": (C.c_char_p, [P]),
+    "tpa_set_mesh": (C.c_int32, [P, i32p, i32p, i32p, f64p, f64p, C.c_int64, i32p]),
+    "tpa_mesh_sizes": (C.c_int32, [P, i64p]),
+    "tpa_mesh_blocks": (C.c_int32, [P, i32p, f64p]),
+    "tpa_mesh_faces": (C.c_int32, [P, i32p, i32p, i8p, f64p]),
+    "tpa_mesh_boundary_faces": (C.c_int32, [P, i32p, i8p, i8p, f64p]),
+    "tpa_set_operator": (C.c_int32, [P, f64p]),
+    "tpa_metric_offdiagonal_count": (C.c_int32, [P, i64p]),
+    "tpa_build_hierarchy": (C.c_int32, [P, C.POINTER(MultigridOptionsC)]),
+    "tpa_hierarchy_sizes": (C.c_int32, [P, i32p, i64p, C.c_int32]),
+    "tpa_level_owners": (C.c_int32, [P, C.c_int32, i32p]),
+    "tpa_level_info": (C.c_int32, [P, C.c_int32, f64p, f64p, i32p]),
+    "tpa_level_face_coefficients": (C.c_int32, [P, C.c_int32, f64p]),
+    "tpa_refresh": (C.c_int32, [P, f64p]),
+    "tpa_solve": (C.c_int32, [P, f64p, f64p, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int32,
+                              C.POINTER(StatsC)]),
+    "tpa_solve_device": (C.c_int32, [P, P, P, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int32,
+                                     C.POINTER(StatsC)]),
+    "tpa_apply": (C.c_int32, [P, f64p, f64p]),
+    "tpa_vcycle": (C.c_int32, [P, f64p, f64p, C.c_int32]),
+    "tpa_synchronize": (C.c_int32, [P]),
+    "tpa_set_stream": (C.c_int32, [P, P]),
+    "tpa_time_kernel": (C.c_int32, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, f64p]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load the library once; raise if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"libtpagmg.so not built: run `python twophaseamr.jl_b200/build.py` ({LIB_PATH})")
+        handle = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def ptr(a, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype)) if a is not None else None
+
+
+class Context:
+    """Owns one `tpa_context`."""
+
+    def __init__(self, device=0):
+        self.handle = P()
+        self._check(lib().tpa_create(C.byref(self.handle), int(device)), "tpa_create")
+
+    def _check(self, status, what):
+        if status != TPA_OK:
+            msg = lib().tpa_last_error(self.handle).decode() if self.handle else what
+            raise TpaError(status, f"{what}: {msg}")
+
+    def call(self, name, *args):
+        self._check(getattr(lib(), name)(self.handle, *args), name)
+
+    def close(self):
+        if self.handle:
+            lib().tpa_destroy(self.handle)
+            self.handle = P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)

@@ -1,0 +1,183 @@
+"""`EllipticSolver` and `solve` (the reference's `solve!`) on the B200.
+
+Mirrors (ronaldremmerswaal/TwoPhaseAMR.jl):
+  src/solvers/multigrid/elliptic_solver.jl:211-302  EllipticSolver(operator; krylov,
+        preconditioner, preconditioner_options, multigrid)
+  src/solvers/multigrid/elliptic_solver.jl:614-675  solve!(solution, solver, rhs;
+        rtol=1e-10, atol=0, max_cycles=100, compatibility=:project)
+  src/solvers/multigrid/stats.jl:100-135            LinearSolverStats
+  src/solvers/multigrid/cycles.jl:328-340           CG needs equal pre/post sweeps
+
+The hierarchy is built on the host by the library; every solve runs on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from .options import LinearSolverOptions, MultigridOptions
+
+_PRECISION = {"fp64": 0, "mixed": 1}
+
+
+@dataclass
+class LinearSolverStats:
+    """Convergence statistics of the latest solve (stats.jl:113-135)."""
+
+    cycles: int = 0
+    converged: bool = False
+    compatible: bool = True
+    initial_l2: float = float("inf")
+    initial_linf: float = float("inf")
+    final_l2: float = float("inf")
+    final_linf: float = float("inf")
+    target_linf: float = float("inf")
+    residual_scale: float = 1.0
+    removed_rhs_mean: float = 0.0
+    removed_rhs_component_means: list = field(default_factory=list)
+    removed_rhs_component_anchors: list = field(default_factory=list)
+    method: str = "cg"
+    preconditioner: str = "gpu_tree_geometric_multigrid"
+    device_ms: float = 0.0
+    restarts: int = 0
+    kernel_launches: int = 0
+    precision: str = "fp64"
+
+
+class EllipticSolver:
+    """Krylov CG + tree geometric multigrid on one B200 for a `PoissonOperator`."""
+
+    def __init__(self, operator, *, krylov=None, krylov_options=None, preconditioner="gpu_tree_geometric",
+                 preconditioner_options=None, multigrid=None, coarse_size=None, pre_sweeps=None,
+                 post_sweeps=None, max_levels=None, device=0, options=None):
+        if options is not None:
+            if not isinstance(options, LinearSolverOptions):
+                raise TypeError("options must be LinearSolverOptions")
+            krylov, krylov_options = options.krylov, options.krylov_options
+            preconditioner, preconditioner_options = options.preconditioner, options.preconditioner_options
+        if preconditioner == "auto":
+            preconditioner = "gpu_tree_geometric"
+        if preconditioner not in ("geometric", "tree_geometric", "gpu_tree_geometric"):
+            raise ValueError("the B200 solver implements the tree geometric multigrid preconditioner only")
+        if krylov not in (None, "cg", "CG"):
+            raise ValueError("the B200 solver implements CG only")
+        mg = multigrid or MultigridOptions()
+        mg = MultigridOptions(coarse_size=mg.coarse_size if coarse_size is None else coarse_size,
+                              pre_sweeps=mg.pre_sweeps if pre_sweeps is None else pre_sweeps,
+                              post_sweeps=mg.post_sweeps if post_sweeps is None else post_sweeps,
+                              max_levels=mg.max_levels if max_levels is None else max_levels)
+        if mg.pre_sweeps != mg.post_sweeps:
+            raise ValueError(f"CG requires equal pre_sweeps and post_sweeps for a geometric multigrid "
+                             f"preconditioner; got {mg.pre_sweeps} and {mg.post_sweeps}")
+        popts = dict(preconditioner_options or {})
+        precision = popts.pop("precision", "fp64")
+        if precision not in _PRECISION:
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        if popts:
+            raise ValueError(f"unsupported preconditioner_options: {sorted(popts)}")
+        self.operator = operator
+        self.multigrid = mg
+        self.precision = precision
+        mesh = operator.mesh
+        self.ctx = _lib.Context(device)
+        self.ctx.call("tpa_set_mesh", *mesh._mesh_args())
+        self._kappa = _lib.f64(operator.face_coefficient)
+        self.ctx.call("tpa_set_operator", _lib.ptr(self._kappa, C.c_double))
+        o = _lib.MultigridOptionsC(mg.coarse_size, mg.pre_sweeps, mg.post_sweeps, mg.max_levels)
+        self.ctx.call("tpa_build_hierarchy", C.byref(o))
+        self.stats = LinearSolverStats(precision=precision)
+
+    # -- hierarchy queries (parity tests) -------------------------------------
+    def level_sizes(self):
+        n = C.c_int32()
+        self.ctx.call("tpa_hierarchy_sizes", C.byref(n), None, 0)
+        sizes = np.zeros(n.value, dtype=np.int64)
+        self.ctx.call("tpa_hierarchy_sizes", C.byref(n), _lib.ptr(sizes, C.c_int64), n.value)
+        return [int(s) for s in sizes]
+
+    def level_owners(self, level):
+        out = np.zeros(self.level_sizes()[level], dtype=np.int32)
+        self.ctx.call("tpa_level_owners", int(level), _lib.ptr(out, C.c_int32))
+        return out
+
+    def level_info(self, level):
+        sw, tw, nc = C.c_double(), C.c_double(), C.c_int32()
+        self.ctx.call("tpa_level_info", int(level), C.byref(sw), C.byref(tw), C.byref(nc))
+        return sw.value, tw.value, nc.value
+
+    def level_face_coefficients(self, level, nfaces):
+        out = np.zeros(nfaces, dtype=np.float64)
+        self.ctx.call("tpa_level_face_coefficients", int(level), _lib.ptr(out, C.c_double))
+        return out
+
+    # -- device operations --------------------------------------------------
+    def refresh(self, face_coefficient):
+        """`_refresh_geometric_multigrid!` after a coefficient change."""
+        self._kappa = _lib.f64(face_coefficient)
+        self.ctx.call("tpa_refresh", _lib.ptr(self._kappa, C.c_double))
+        self.operator.face_coefficient = self._kappa.copy()
+
+    def apply(self, x):
+        x = _lib.f64(x)
+        y = np.empty_like(x)
+        self.ctx.call("tpa_apply", _lib.ptr(x, C.c_double), _lib.ptr(y, C.c_double))
+        return y
+
+    def vcycle(self, r, precision=None):
+        r = _lib.f64(r)
+        z = np.empty_like(r)
+        self.ctx.call("tpa_vcycle", _lib.ptr(r, C.c_double), _lib.ptr(z, C.c_double),
+                      _PRECISION[precision or self.precision])
+        return z
+
+    def _stats_from(self, st):
+        s = self.stats
+        s.cycles, s.converged, s.compatible = st.cycles, bool(st.converged), bool(st.compatible)
+        s.initial_l2, s.initial_linf = st.initial_l2, st.initial_linf
+        s.final_l2, s.final_linf, s.target_linf = st.final_l2, st.final_linf, st.target_linf
+        s.residual_scale, s.removed_rhs_mean = st.residual_scale, st.removed_rhs_mean
+        s.device_ms, s.restarts, s.kernel_launches = st.device_ms, st.restarts, st.kernel_launches
+        return s
+
+    def solve_device(self, rhs_ptr, x_ptr, *, rtol=1e-10, atol=0.0, max_cycles=100, compatibility="project",
+                     precision=None):
+        """`solve!` on device arrays (raw CUDA pointers, cell order)."""
+        st = _lib.StatsC()
+        self.ctx.call("tpa_solve_device", C.c_void_p(rhs_ptr), C.c_void_p(x_ptr), float(rtol), float(atol),
+                      int(max_cycles), _compat(compatibility), _PRECISION[precision or self.precision], C.byref(st))
+        return self._stats_from(st)
+
+
+def _compat(compatibility):
+    if compatibility not in ("project", "error"):
+        raise ValueError("compatibility must be :project or :error")
+    return 0 if compatibility == "project" else 1
+
+
+def solve(solution, solver, rhs, *, rtol=1e-10, atol=0.0, max_cycles=100, compatibility="project", precision=None):
+    """`solve!(solution, solver, rhs)`: solve L(solution) = rhs in place.
+
+    `rhs` is the strong-form right-hand side and `solution` the initial guess,
+    both float64 arrays in cell order; `solution` is overwritten.  Returns the
+    solver's `LinearSolverStats`.
+    """
+    if not 0 <= rtol < 1:
+        raise ValueError("rtol must lie in [0, 1)")
+    if atol < 0:
+        raise ValueError("atol must be nonnegative")
+    if max_cycles < 0:
+        raise ValueError("max_cycles must be nonnegative")
+    comp = _compat(compatibility)
+    if not (isinstance(solution, np.ndarray) and solution.dtype == np.float64 and solution.flags.c_contiguous):
+        raise TypeError("solution must be a contiguous float64 array")
+    n = solver.operator.mesh.ncells
+    if solution.shape != (n,) or np.shape(rhs) != (n,):
+        raise ValueError("fields and multigrid solver must share a mesh")
+    b = _lib.f64(rhs)
+    st = _lib.StatsC()
+    solver.ctx.call("tpa_solve", _lib.ptr(b, C.c_double), _lib.ptr(solution, C.c_double), float(rtol), float(atol),
+                    int(max_cycles), comp, _PRECISION[precision or solver.precision], C.byref(st))
+    return solver._stats_from(st)
