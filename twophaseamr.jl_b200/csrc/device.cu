@@ -412,6 +412,7 @@ DeviceSolver::DeviceSolver(int device) : device_(device) {
 DeviceSolver::~DeviceSolver() {
     cudaSetDevice(device_);
     if (stream_) cudaStreamSynchronize(stream_);
+    destroy_graphs();
     levels_.clear();
     if (host_sc_) cudaFreeHost(host_sc_);
     if (host_d_) cudaFreeHost(host_d_);
@@ -482,6 +483,7 @@ void DeviceSolver::upload(const Hierarchy& h) {
     const size_t n = size_t(levels_[0].n);
     for (auto* a : {&b_, &r_, &p_, &ap_, &z_, &tmp_}) a->alloc(n);
     TPA_CUDA(cudaStreamSynchronize(stream_));
+    build_views();
 }
 
 void DeviceSolver::apply(const double* x, double* y) {
@@ -596,6 +598,10 @@ void DeviceSolver::vcycle_t(int /*unused*/) {
 
 void DeviceSolver::vcycle(const double* r, double* z, int precision) {
     const int n = levels_[0].n;
+    if (fused_ok_) {
+        vcycle_fused(r, z, precision);
+        return;
+    }
     if (precision == 0) {
         TPA_CUDA(cudaMemcpyAsync(levels_[0].d.b.p, r, sizeof(double) * size_t(n), cudaMemcpyDeviceToDevice, stream_));
         vcycle_t<double>(0);
@@ -609,6 +615,7 @@ void DeviceSolver::vcycle(const double* r, double* z, int precision) {
 }
 
 double DeviceSolver::time_kernel(int which, int level, int precision, int iters) {
+    if (fused_ok_) return time_fused(which, level, precision, iters);
     if (level < 0 || level >= int(levels_.size())) throw Error(1, "bad level");
     if (which != 3 && level == int(levels_.size()) - 1) throw Error(1, "the coarsest level has no such kernel");
     if (which == 3 && level != 0) throw Error(1, "the CG operator lives on the finest level");
@@ -680,8 +687,11 @@ void DeviceSolver::strong_max(const double* r, double* out) {
     launches_ += 2;
 }
 
-void DeviceSolver::solve(const double* rhs, double* x, double rtol, double atol, int max_cycles, int compatibility,
-                         int precision, SolveStats& st) {
+void DeviceSolver::solve(const double* rhs, double* x_user, double rtol, double atol, int max_cycles,
+                         int compatibility, int precision, SolveStats& st) {
+    // The solve works on an internal copy of the iterate so that the captured
+    // CG graph always sees the same addresses.
+    double* x = xw_.p;
     TPA_CUDA(cudaSetDevice(device_));
     if (!(rtol >= 0 && rtol < 1)) throw Error(1, "rtol must lie in [0, 1)");
     if (!(atol >= 0)) throw Error(1, "atol must be nonnegative");
@@ -698,6 +708,7 @@ void DeviceSolver::solve(const double* rhs, double* x, double rtol, double atol,
     TPA_CUDA(cudaEventCreate(&e1));
     TPA_CUDA(cudaEventRecord(e0, stream_));
     st = SolveStats();
+    TPA_CUDA(cudaMemcpyAsync(x, x_user, sizeof(double) * size_t(n), cudaMemcpyDeviceToDevice, stream_));
     k_scale_rhs<<<g, kThreads, 0, stream_>>>(n, rhs, vol, b_.p, x);
     ++launches_;
     double removed = 0;
@@ -762,7 +773,20 @@ void DeviceSolver::solve(const double* rhs, double* x, double rtol, double atol,
     double target = std::max(atol, std::max(rtol * std::max(init_linf, eps), floor));
     int total = 0;
     if (init_linf > target) {
-        while (total < max_cycles) {
+        while (total < max_cycles && fused_ok_) {
+            int niter = 0, flags = 0;
+            cg_fused(precision, target, max_cycles - total, niter, flags);
+            total += niter;
+            if (L.ncomp) remove_means<double>(0, x);
+            residual(x, r_.p);
+            strong_max(r_.p, sums_.p + 53);
+            double final_linf = read_scalar(sums_.p + 53);
+            double eff = guarded(x, target, init_linf, final_linf);
+            ++st.restarts;
+            if (final_linf <= eff) break;
+            if (!std::isfinite(final_linf) || niter == 0) break;
+        }
+        while (total < max_cycles && !fused_ok_) {
             // Krylov.jl cg! warm-started at x: r = b - A x, z = M r, p = z, gamma = r'z
             residual(x, r_.p);
             vcycle(r_.p, z_.p, precision);
@@ -808,6 +832,7 @@ void DeviceSolver::solve(const double* rhs, double* x, double rtol, double atol,
     double fin_l2, fin_linf;
     norms(r_.p, fin_l2, fin_linf);
     target = guarded(x, target, init_linf, fin_linf);
+    TPA_CUDA(cudaMemcpyAsync(x_user, x, sizeof(double) * size_t(n), cudaMemcpyDeviceToDevice, stream_));
     TPA_CUDA(cudaEventRecord(e1, stream_));
     TPA_CUDA(cudaEventSynchronize(e1));
     float ms = 0;

@@ -7,6 +7,7 @@
 #include <string>
 #include <vector>
 
+#include "fused.cuh"
 #include "host.hpp"
 
 namespace tpa {
@@ -66,6 +67,7 @@ template <typename T>
 struct DevLevelT {
     DevArray<T> val, dinv, tinv, vol;
     DevArray<T> x, y, b, r, s;   // work vectors
+    DevArray<T> bp;              // projected right-hand side (fused cycle)
     T w = 1, tw = 0;             // smoother weight, transfer weight
 };
 
@@ -142,6 +144,33 @@ private:
     CgScalars* host_sc_ = nullptr;
     double* host_d_ = nullptr;
     int launches_ = 0;
+
+    // ---- fused cycle (default options) and the graph-captured CG loop ----
+public:
+    bool fused() const { return fused_ok_; }
+    int tail_first() const { return tail_first_; }
+
+private:
+    void build_views();
+    template <typename T> void enqueue_vcycle(const double* r, const double* rsum, double* mean_out);
+    // CG from the current xw_/b_: returns iterations and flags (Krylov.jl cg! loop)
+    void cg_fused(int precision, double target, int itmax, int& niter, int& flags);
+    void vcycle_fused(const double* r, double* z, int precision);
+    void destroy_graphs();
+    cudaGraphExec_t cg_graph(int precision);
+    double time_fused(int which, int level, int precision, int iters);
+
+    bool fused_ok_ = false;
+    int tail_first_ = 0;
+    std::vector<LevelView<double>> vd_;
+    std::vector<LevelView<float>> vf_;
+    DevArray<LevelView<double>> vd_dev_;
+    DevArray<LevelView<float>> vf_dev_;
+    DevArray<double> fpartial_, fpartial2_, lsum_, xw_;
+    DevArray<unsigned> counters_;
+    DevArray<char> cgs_;  // CgState
+    cudaGraphExec_t cg_exec_[2] = {nullptr, nullptr};
+    int graph_body_launches_[2] = {0, 0};
 };
 
 }  // namespace tpa

@@ -1,0 +1,332 @@
+// Fused V-cycle and PCG kernels for the default cycle (two pre- and two
+// post-sweeps, at most one ungauged component per level).
+//
+// Each kernel removes one or more grid-wide dependencies of the plain cycle of
+// src/solvers/multigrid/cycles.jl:8-77 (ronaldremmerswaal/TwoPhaseAMR.jl):
+//   k_pre2          both pre-sweeps from x = 0: the first sweep is pointwise,
+//                   x1 = w D^-1 b, so the second one evaluates x1 at the
+//                   neighbours on the fly; the RHS projection of the level
+//                   (`_multigrid_project_component_rhs!`) is applied inline
+//   k_residual, k_restrict  r = b - A x, s = Dt^-1 r, then b_c = P_tent.(r - wt A s)
+//                   with the coarse RHS sum folded in the same launch
+//   k_prolong       x += e - wt Dt^-1 A e with e = P_tent x_c, in place (it
+//                   reads no neighbouring fine value)
+//   k_tail          every level with at most kTailCells cells in one CTA
+// Reductions fold their per-block partials in the last block to finish (a
+// fixed-order fold: results do not depend on block scheduling).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace tpa {
+
+// Levels at or below this many cells run inside one CTA (tunable: TPAGMG_TAIL_CELLS).
+constexpr int kTailCellsDefault = 2048;
+constexpr int kTailThreads = 1024;
+
+// Pointers of one level in precision T, read by the fused kernels.
+template <typename T>
+struct LevelView {
+    int n, nc;
+    const int* rp;
+    const int* ci;
+    const T* val;
+    const T* dinv;
+    const T* tinv;
+    const T* vol;
+    const int* owner;
+    const int* cptr;
+    const int* child;
+    T w, tw;
+    int singular;      // ungauged component present (one)
+    double cvol_inv;   // 1 / component volume
+    T* b;              // restricted right-hand side (raw)
+    T* bp;             // projected right-hand side
+    T* x;              // iterate
+    T* y;              // second iterate buffer
+    T* r;              // residual
+    T* s;              // Dt^-1 r
+};
+
+// fold partial[0..count) in fixed order by one block; returns the sum in thread 0
+__device__ __forceinline__ double fold_partials(const double* partial, int count) {
+    __shared__ double sh[32];
+    double acc = 0;
+    for (int i = threadIdx.x; i < count; i += blockDim.x) acc += ((volatile const double*)partial)[i];
+    for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (!lane) sh[wid] = acc;
+    __syncthreads();
+    acc = 0;
+    if (threadIdx.x < (blockDim.x >> 5)) acc = sh[threadIdx.x];
+    if (wid == 0)
+        for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    return acc;
+}
+
+__device__ __forceinline__ double fold_partials_max(const double* partial, int count) {
+    __shared__ double sh[32];
+    __shared__ int nan_seen;
+    double m = 0;
+    bool nan = false;
+    for (int i = threadIdx.x; i < count; i += blockDim.x) {
+        double q = ((volatile const double*)partial)[i];
+        if (q != q) nan = true;
+        m = fmax(m, q);
+    }
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (threadIdx.x == 0) nan_seen = 0;
+    if (!lane) sh[wid] = m;
+    __syncthreads();
+    if (nan) nan_seen = 1;
+    m = 0;
+    if (threadIdx.x < (blockDim.x >> 5)) m = sh[threadIdx.x];
+    if (wid == 0)
+        for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    __syncthreads();
+    return nan_seen ? NAN : m;
+}
+
+__device__ __forceinline__ double block_sum_all(double v) {
+    __shared__ double sh[32];
+    for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (!lane) sh[wid] = v;
+    __syncthreads();
+    v = 0;
+    if (threadIdx.x < (blockDim.x >> 5)) v = sh[threadIdx.x];
+    if (wid == 0)
+        for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Write this block's partial, and return true in the block that finishes last.
+__device__ __forceinline__ bool publish_partial(double v, double* partial, unsigned* counter) {
+    __shared__ bool last;
+    v = block_sum_all(v);
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = v;
+        __threadfence();
+        unsigned t = atomicAdd(counter, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    return last;
+}
+
+template <typename T>
+__device__ __forceinline__ T rowdot(const LevelView<T>& L, const T* v, int i) {
+    T acc = T(0);
+    for (int k = L.rp[i]; k < L.rp[i + 1]; ++k) acc += L.val[k] * v[L.ci[k]];
+    return acc;
+}
+
+// ---------------------------------------------------------------------------------
+// Per-level phases as device functions over a cell, shared by the multi-CTA
+// kernels and the single-CTA tail.
+
+// projected RHS value at cell j (in FP64 arithmetic)
+template <typename T, typename TB>
+__device__ __forceinline__ T proj_b(const LevelView<T>& L, const TB* b, double mean, int j) {
+    double v = double(b[j]);
+    if (L.singular) v -= double(L.vol[j]) * mean;
+    return T(v);
+}
+
+template <typename T, typename TB>
+__device__ __forceinline__ void pre2_cell(const LevelView<T>& L, const TB* b, double mean, int i) {
+    T bi = proj_b<T, TB>(L, b, mean, i);
+    T acc = T(0);
+    for (int k = L.rp[i]; k < L.rp[i + 1]; ++k) {
+        int j = L.ci[k];
+        T bj = j == i ? bi : proj_b<T, TB>(L, b, mean, j);
+        acc += L.val[k] * (L.w * L.dinv[j] * bj);
+    }
+    T x1 = L.w * L.dinv[i] * bi;
+    L.x[i] = x1 + L.w * L.dinv[i] * (bi - acc);
+    L.bp[i] = bi;
+}
+
+template <typename T>
+__device__ __forceinline__ void residual_cell(const LevelView<T>& L, int i) {
+    T ri = L.bp[i] - rowdot(L, L.x, i);
+    L.r[i] = ri;
+    L.s[i] = L.tinv[i] * ri;
+}
+
+template <typename T>
+__device__ __forceinline__ T restrict_cell(const LevelView<T>& L, int J) {
+    T acc = T(0);
+    for (int k = L.cptr[J]; k < L.cptr[J + 1]; ++k) {
+        int i = L.child[k];
+        acc += L.r[i] - L.tw * rowdot(L, L.s, i);
+    }
+    return acc;
+}
+
+// x += e - wt Dt^-1 A e, e = xc[owner(.)]
+template <typename T>
+__device__ __forceinline__ void prolong_cell(const LevelView<T>& L, const T* xc, int i) {
+    T ae = T(0);
+    for (int k = L.rp[i]; k < L.rp[i + 1]; ++k) ae += L.val[k] * xc[L.owner[L.ci[k]]];
+    L.x[i] += xc[L.owner[i]] - L.tw * L.tinv[i] * ae;
+}
+
+template <typename T>
+__device__ __forceinline__ void sweep_cell(const LevelView<T>& L, const T* in, T* out, int i) {
+    out[i] = in[i] + L.w * L.dinv[i] * (L.bp[i] - rowdot(L, in, i));
+}
+
+// ---------------------------------------------------------------------------------
+// multi-CTA kernels
+
+// `level_sum` (may be null): the RHS sum of this level, folded by the kernel
+// that produced b; mean = sum * cvol_inv.
+template <typename T, typename TB>
+__global__ void k_pre2(LevelView<T> L, const TB* __restrict__ b, const double* level_sum) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
+    if (i < L.n) pre2_cell<T, TB>(L, b, mean, i);
+}
+
+template <typename T>
+__global__ void k_residual(LevelView<T> L) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < L.n) residual_cell(L, i);
+}
+
+// b_c = P_tent'(r - wt A s); coarse RHS sum folded into `coarse_sum` when non-null.
+template <typename T>
+__global__ void k_restrict(LevelView<T> L, T* __restrict__ bc, double* partial, unsigned* counter, double* coarse_sum) {
+    int J = blockIdx.x * blockDim.x + threadIdx.x;
+    T v = T(0);
+    if (J < L.nc) {
+        v = restrict_cell(L, J);
+        bc[J] = v;
+    }
+    if (coarse_sum) {
+        if (publish_partial(double(v), partial, counter)) {
+            double s = fold_partials(partial, gridDim.x);
+            if (threadIdx.x == 0) {
+                *coarse_sum = s;
+                *counter = 0;
+            }
+        }
+    }
+}
+
+template <typename T>
+__global__ void k_prolong(LevelView<T> L, const T* __restrict__ xc) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < L.n) prolong_cell(L, xc, i);
+}
+
+// first post-sweep: y = sweep(x)
+template <typename T>
+__global__ void k_post1(LevelView<T> L) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < L.n) sweep_cell(L, L.x, L.y, i);
+}
+
+// second post-sweep x = sweep(y); with `mean_out`, also the volume-weighted mean
+template <typename T>
+__global__ void k_post2(LevelView<T> L, double* partial, unsigned* counter, double* mean_out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0;
+    if (i < L.n) {
+        sweep_cell(L, L.y, L.x, i);
+        v = double(L.vol[i]) * double(L.x[i]);
+    }
+    if (mean_out) {
+        if (publish_partial(v, partial, counter)) {
+            double s = fold_partials(partial, gridDim.x);
+            if (threadIdx.x == 0) {
+                *mean_out = s * L.cvol_inv;
+                *counter = 0;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// single-CTA tail: levels first..nl-1
+
+template <typename T>
+__device__ double tail_sum(const T* v, const T* w, int n) {
+    double acc = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += w ? double(w[i]) * double(v[i]) : double(v[i]);
+    __syncthreads();
+    double s = block_sum_all(acc);
+    __shared__ double total;
+    if (threadIdx.x == 0) total = s;
+    __syncthreads();
+    return total;
+}
+
+// `top_b`: RHS of level 0 (type TB), used only when first == 0
+template <typename T, typename TB>
+__global__ void __launch_bounds__(kTailThreads) k_tail(const LevelView<T>* __restrict__ levels, int first, int nl,
+                                                       const TB* top_b, const double* __restrict__ G, int gn,
+                                                       double* mean_out) {
+    for (int l = first; l < nl; ++l) {
+        LevelView<T> L = levels[l];
+        const bool top = (l == 0);  // only the finest level reads the caller's RHS
+        double mean = 0;
+        if (L.singular) {
+            double s = top ? tail_sum(top_b, (const TB*)nullptr, L.n) : tail_sum(L.b, (const T*)nullptr, L.n);
+            mean = s * L.cvol_inv;
+        }
+        if (l == nl - 1) {
+            // projected RHS, then the dense (augmented) coarse solve in FP64
+            for (int i = threadIdx.x; i < L.n; i += blockDim.x)
+                L.bp[i] = top ? proj_b<T, TB>(L, top_b, mean, i) : proj_b<T, T>(L, L.b, mean, i);
+            __syncthreads();
+            // one warp per row, lanes striding the row: coalesced reads of G
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+            for (int i = warp; i < gn; i += nwarps) {
+                const double* row = G + size_t(i) * gn;
+                double acc = 0;
+                for (int k = lane; k < gn; k += 32) acc += row[k] * double(L.bp[k]);
+                for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+                if (!lane) L.x[i] = T(acc);
+            }
+            __syncthreads();
+            break;
+        }
+        for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+            if (top) pre2_cell<T, TB>(L, top_b, mean, i);
+            else pre2_cell<T, T>(L, L.b, mean, i);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < L.n; i += blockDim.x) residual_cell(L, i);
+        __syncthreads();
+        T* bc = levels[l + 1].b;
+        for (int J = threadIdx.x; J < L.nc; J += blockDim.x) bc[J] = restrict_cell(L, J);
+        __syncthreads();
+    }
+    for (int l = nl - 2; l >= first; --l) {
+        LevelView<T> L = levels[l];
+        const T* xc = levels[l + 1].x;
+        for (int i = threadIdx.x; i < L.n; i += blockDim.x) prolong_cell(L, xc, i);
+        __syncthreads();
+        for (int i = threadIdx.x; i < L.n; i += blockDim.x) sweep_cell(L, L.x, L.y, i);
+        __syncthreads();
+        for (int i = threadIdx.x; i < L.n; i += blockDim.x) sweep_cell(L, L.y, L.x, i);
+        __syncthreads();
+    }
+    if (mean_out && first == 0) {
+        LevelView<T> L = levels[0];
+        if (L.singular) {
+            double s = tail_sum(L.x, L.vol, L.n);
+            if (threadIdx.x == 0) *mean_out = s * L.cvol_inv;
+        } else if (threadIdx.x == 0) {
+            *mean_out = 0;
+        }
+    }
+}
+
+}  // namespace tpa

@@ -1,0 +1,491 @@
+// Fused V-cycle launches and the PCG loop captured as one CUDA graph.
+//
+// One conjugate-gradient iteration (Krylov.jl 0.10 `cg!` with M = the V-cycle,
+// ldiv = true, as called by `_run_krylov!`, src/solvers/multigrid/
+// elliptic_solver.jl:403-464 in ronaldremmerswaal/TwoPhaseAMR.jl) is the body
+// of a graph WHILE node; the last kernel of the body evaluates the stopping
+// rules on the device (machine stop sqrt(r'z) + 1 <= 1, iteration limit, zero
+// curvature, and the strong-residual callback max|r_i|/V_i <= target) and sets
+// the loop condition, so a whole Krylov run is one graph launch.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <type_traits>
+
+#include "device.cuh"
+
+namespace tpa {
+namespace {
+
+struct CgState {
+    double gamma, pAp, alpha, beta, pnorm2, strong_max, target, rsum, rnorm;
+    int flags;  // 1 user exit, 2 zero curvature, 4 machine stop, 8 zero initial residual
+    int iter, itmax;
+};
+
+enum Counter { kRestrictSum = 0, kPostMean = 1, kCgAp = 2, kCgUpdate = 3, kCgZ = 4, kCgRes = 5, kRsum = 6 };
+
+inline int blocks_for(int64_t n) {
+    int64_t g = (n + kThreads - 1) / kThreads;
+    return int(g < 1 ? 1 : g);
+}
+
+// r = b - A x, folds sum(r) into s->rsum
+__global__ void k_cg_residual(LevelView<double> A, const double* __restrict__ b, const double* __restrict__ x,
+                              double* __restrict__ r, double* partial, unsigned* counter, CgState* s) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0;
+    if (i < A.n) {
+        v = b[i] - rowdot(A, x, i);
+        r[i] = v;
+    }
+    if (publish_partial(v, partial, counter)) {
+        double t = fold_partials(partial, gridDim.x);
+        if (threadIdx.x == 0) {
+            s->rsum = t;
+            *counter = 0;
+        }
+    }
+}
+
+__global__ void k_sum_into(int n, const double* __restrict__ v, double* partial, unsigned* counter, double* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (publish_partial(i < n ? v[i] : 0.0, partial, counter)) {
+        double t = fold_partials(partial, gridDim.x);
+        if (threadIdx.x == 0) {
+            *out = t;
+            *counter = 0;
+        }
+    }
+}
+
+// Ap = A p and alpha = gamma / p'Ap with the zero-curvature guard
+__global__ void k_cg_ap(LevelView<double> A, const double* __restrict__ p, double* __restrict__ ap, double* partial,
+                        unsigned* counter, CgState* s) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0;
+    if (i < A.n) {
+        double y = rowdot(A, p, i);
+        ap[i] = y;
+        v = p[i] * y;
+    }
+    if (publish_partial(v, partial, counter)) {
+        double pAp = fold_partials(partial, gridDim.x);
+        if (threadIdx.x == 0) {
+            const double eps = 2.220446049250313e-16;
+            s->pAp = pAp;
+            if (pAp <= eps * s->pnorm2 && fabs(pAp) <= eps * s->pnorm2) {
+                s->flags |= 2;
+                s->alpha = 0;
+            } else {
+                s->alpha = s->gamma / pAp;
+            }
+            *counter = 0;
+        }
+    }
+}
+
+// x += alpha p, r -= alpha Ap; folds max|r_i|/V_i and sum(r)
+__global__ void k_cg_update(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+                            const double* __restrict__ ap, const double* __restrict__ vol, double* pmax, double* psum,
+                            unsigned* counter, CgState* s) {
+    __shared__ bool last;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool skip = s->flags & 2;
+    const double alpha = s->alpha;
+    double m = 0, sum = 0;
+    if (i < n) {
+        double ri = r[i];
+        if (!skip) {
+            x[i] += alpha * p[i];
+            ri -= alpha * ap[i];
+            r[i] = ri;
+        }
+        double V = vol[i];
+        if (V > 0) m = fabs(ri) / V;
+        sum = ri;
+    }
+    // block max (NaN propagating) and block sum
+    __shared__ double shm[32], shs[32];
+    __shared__ int nan_seen;
+    if (threadIdx.x == 0) nan_seen = 0;
+    __syncthreads();
+    if (m != m) nan_seen = 1;
+    double mm = m, ss = sum;
+    for (int o = 16; o; o >>= 1) {
+        mm = fmax(mm, __shfl_down_sync(0xffffffffu, mm, o));
+        ss += __shfl_down_sync(0xffffffffu, ss, o);
+    }
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (!lane) {
+        shm[wid] = mm;
+        shs[wid] = ss;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double bm = 0, bs = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            bm = fmax(bm, shm[w]);
+            bs += shs[w];
+        }
+        pmax[blockIdx.x] = nan_seen ? NAN : bm;
+        psum[blockIdx.x] = bs;
+        __threadfence();
+        unsigned t = atomicAdd(counter, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last) {
+        double mx = fold_partials_max(pmax, gridDim.x);
+        double sm = fold_partials(psum, gridDim.x);
+        if (threadIdx.x == 0) {
+            s->strong_max = mx;
+            s->rsum = sm;
+            *counter = 0;
+        }
+    }
+}
+
+// z = x0 - mean, gamma_next = r'z and the stopping rules; `init` starts a run
+// (p = z, gamma = r'z).  With `set_cond`, sets the graph loop condition.
+template <typename T>
+__global__ void k_cg_z(int n, const T* __restrict__ xv, const double* mean, const double* __restrict__ r,
+                       double* __restrict__ z, double* __restrict__ p, double* partial, unsigned* counter, CgState* s,
+                       int init, cudaGraphConditionalHandle handle, int set_cond) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double m = mean ? *mean : 0.0;
+    double v = 0;
+    if (i < n) {
+        double zi = double(xv[i]) - m;
+        z[i] = zi;
+        if (init) p[i] = zi;
+        v = r[i] * zi;
+    }
+    if (publish_partial(v, partial, counter)) {
+        double g = fold_partials(partial, gridDim.x);
+        if (threadIdx.x == 0) {
+            *counter = 0;
+            bool stop;
+            if (init) {
+                s->gamma = g;
+                s->pnorm2 = g;
+                s->rnorm = sqrt(g);
+                s->beta = 0;
+                s->iter = 0;
+                s->flags = g == 0 ? 8 : 0;
+                stop = g == 0 || s->itmax <= 0;
+            } else if (s->flags & 2) {
+                stop = true;  // zero curvature: the iteration is abandoned
+            } else {
+                double rnorm = sqrt(g);
+                s->rnorm = rnorm;
+                bool solved = rnorm + 1.0 <= 1.0;
+                if (!solved) {
+                    double beta = g / s->gamma;
+                    s->beta = beta;
+                    s->pnorm2 = g + beta * beta * s->pnorm2;
+                    s->gamma = g;
+                } else {
+                    s->flags |= 4;
+                }
+                s->iter += 1;
+                if (s->strong_max <= s->target) s->flags |= 1;
+                stop = solved || s->iter >= s->itmax || (s->flags & 1);
+            }
+            if (set_cond) cudaGraphSetConditional(handle, stop ? 0u : 1u);
+        }
+    }
+}
+
+__global__ void k_cg_p(int n, double* __restrict__ p, const double* __restrict__ z, const CgState* s) {
+    if (s->flags & 6) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = z[i] + s->beta * p[i];
+}
+
+__global__ void k_cg_set(CgState* s, double target, int itmax) {
+    s->target = target;
+    s->itmax = itmax;
+    s->flags = 0;
+    s->iter = 0;
+}
+
+__global__ void k_z_out(int n, const float* __restrict__ xf, const double* __restrict__ xd, const double* mean,
+                        double* __restrict__ z) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double m = mean ? *mean : 0.0;
+    z[i] = (xf ? double(xf[i]) : xd[i]) - m;
+}
+
+}  // namespace
+
+void DeviceSolver::build_views() {
+    fused_ok_ = (pre_ == 2 && post_ == 2);
+    for (auto& L : levels_)
+        if (L.ncomp > 1) fused_ok_ = false;
+    const int nl = int(levels_.size());
+    vd_.assign(size_t(nl), LevelView<double>{});
+    vf_.assign(size_t(nl), LevelView<float>{});
+    int tail_cells = kTailCellsDefault;
+    if (const char* env = std::getenv("TPAGMG_TAIL_CELLS")) tail_cells = std::max(0, std::atoi(env));
+    tail_first_ = nl - 1;  // the coarsest level always runs in the tail (dense solve)
+    for (int l = nl - 1; l >= 0; --l)
+        if (levels_[size_t(l)].n <= tail_cells) tail_first_ = l;
+        else break;
+    int64_t maxgrid = 1;
+    for (int l = 0; l < nl; ++l) {
+        DevLevel& L = levels_[size_t(l)];
+        L.d.bp.alloc(size_t(L.n));
+        L.f.bp.alloc(size_t(L.n));
+        maxgrid = std::max<int64_t>(maxgrid, blocks_for(L.n));
+        auto fill = [&](auto& v, auto& D) {
+            v.n = L.n;
+            v.nc = L.nc;
+            v.rp = L.rowptr.p;
+            v.ci = L.col.p;
+            v.val = D.val.p;
+            v.dinv = D.dinv.p;
+            v.tinv = D.tinv.p;
+            v.vol = D.vol.p;
+            v.owner = L.owner.p;
+            v.cptr = L.child_ptr.p;
+            v.child = L.child.p;
+            v.w = D.w;
+            v.tw = D.tw;
+            v.singular = L.ncomp == 1;
+            v.cvol_inv = L.ncomp == 1 ? 1.0 / L.comp_volume[0] : 0.0;
+            v.b = D.b.p;
+            v.bp = D.bp.p;
+            v.x = D.x.p;
+            v.y = D.y.p;
+            v.r = D.r.p;
+            v.s = D.s.p;
+        };
+        fill(vd_[size_t(l)], L.d);
+        fill(vf_[size_t(l)], L.f);
+    }
+    vd_dev_.upload(vd_.data(), vd_.size(), stream_);
+    vf_dev_.upload(vf_.data(), vf_.size(), stream_);
+    fpartial_.alloc(size_t(maxgrid));
+    fpartial2_.alloc(size_t(maxgrid));
+    lsum_.alloc(size_t(nl + 2));
+    xw_.alloc(size_t(levels_[0].n));
+    counters_.alloc(16);
+    TPA_CUDA(cudaMemsetAsync(counters_.p, 0, 16 * sizeof(unsigned), stream_));
+    TPA_CUDA(cudaMemsetAsync(lsum_.p, 0, size_t(nl + 2) * sizeof(double), stream_));
+    cgs_.alloc(sizeof(CgState));
+    TPA_CUDA(cudaMemsetAsync(cgs_.p, 0, sizeof(CgState), stream_));
+    TPA_CUDA(cudaStreamSynchronize(stream_));
+    destroy_graphs();
+}
+
+void DeviceSolver::destroy_graphs() {
+    for (auto& g : cg_exec_)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+// V-cycle on r (FP64, integrated residual) with level-0 RHS sum `rsum`
+// (device pointer); result in view 0's x, level-0 mean in *mean_out.
+template <typename T>
+void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* mean_out) {
+    const int nl = int(levels_.size());
+    const int t = tail_first_;
+    const std::vector<LevelView<T>>* Vp;
+    const LevelView<T>* Vdev;
+    if constexpr (std::is_same<T, double>::value) {
+        Vp = &vd_;
+        Vdev = vd_dev_.p;
+    } else {
+        Vp = &vf_;
+        Vdev = vf_dev_.p;
+    }
+    const std::vector<LevelView<T>>& V = *Vp;
+    for (int l = 0; l < t; ++l) {
+        const LevelView<T>& L = V[size_t(l)];
+        if (l == 0) k_pre2<T, double><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, r, rsum);
+        else k_pre2<T, T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, L.b, lsum_.p + l);
+        const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
+        k_residual<T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L);
+        k_restrict<T><<<blocks_for(L.nc), kThreads, 0, stream_>>>(L, V[size_t(l + 1)].b, fpartial_.p,
+                                                                  counters_.p + kRestrictSum,
+                                                                  next_sum ? lsum_.p + l + 1 : nullptr);
+        launches_ += 3;
+    }
+    k_tail<T, double><<<1, kTailThreads, 0, stream_>>>(Vdev, t, nl, t == 0 ? r : nullptr, coarse_inv_.p, coarse_n_,
+                                                         t == 0 && V[0].singular ? mean_out : nullptr);
+    ++launches_;
+    for (int l = t - 1; l >= 0; --l) {
+        const LevelView<T>& L = V[size_t(l)];
+        k_prolong<T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, V[size_t(l + 1)].x);
+        k_post1<T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L);
+        const bool want_mean = (l == 0) && L.singular;
+        k_post2<T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, fpartial_.p, counters_.p + kPostMean,
+                                                              want_mean ? mean_out : nullptr);
+        launches_ += 3;
+    }
+    if (!V[0].singular) TPA_CUDA(cudaMemsetAsync(mean_out, 0, sizeof(double), stream_));
+    TPA_CUDA(cudaGetLastError());
+}
+
+template void DeviceSolver::enqueue_vcycle<double>(const double*, const double*, double*);
+template void DeviceSolver::enqueue_vcycle<float>(const double*, const double*, double*);
+
+void DeviceSolver::vcycle_fused(const double* r, double* z, int precision) {
+    const int n = levels_[0].n;
+    const int nl = int(levels_.size());
+    double* rsum = lsum_.p;  // slot 0: level-0 RHS sum
+    double* mean = lsum_.p + nl;
+    k_sum_into<<<blocks_for(n), kThreads, 0, stream_>>>(n, r, fpartial_.p, counters_.p + kRsum, rsum);
+    ++launches_;
+    if (precision == 0) enqueue_vcycle<double>(r, rsum, mean);
+    else enqueue_vcycle<float>(r, rsum, mean);
+    k_z_out<<<blocks_for(n), kThreads, 0, stream_>>>(n, precision ? vf_[0].x : nullptr,
+                                                      precision ? nullptr : vd_[0].x, mean, z);
+    ++launches_;
+    TPA_CUDA(cudaGetLastError());
+}
+
+cudaGraphExec_t DeviceSolver::cg_graph(int precision) {
+    if (cg_exec_[precision]) return cg_exec_[precision];
+    const int n = levels_[0].n;
+    const int nl = int(levels_.size());
+    CgState* s = reinterpret_cast<CgState*>(cgs_.p);
+    double* mean = lsum_.p + nl;
+    cudaGraph_t g;
+    TPA_CUDA(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle handle;
+    TPA_CUDA(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
+    alignas(cudaGraphNodeParams) unsigned char cp_storage[sizeof(cudaGraphNodeParams)];
+    std::memset(cp_storage, 0, sizeof(cp_storage));
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_storage);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    TPA_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    cudaStream_t saved = stream_;
+    stream_ = own_stream_;
+    const int saved_launches = launches_;
+    TPA_CUDA(cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    const LevelView<double>& A = vd_[0];
+    k_cg_ap<<<blocks_for(n), kThreads, 0, stream_>>>(A, p_.p, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
+    k_cg_update<<<blocks_for(n), kThreads, 0, stream_>>>(n, xw_.p, r_.p, p_.p, ap_.p, A.vol, fpartial_.p,
+                                                          fpartial2_.p, counters_.p + kCgUpdate, s);
+    if (precision == 0) {
+        enqueue_vcycle<double>(r_.p, &s->rsum, mean);
+        k_cg_z<double><<<blocks_for(n), kThreads, 0, stream_>>>(n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+                                                                counters_.p + kCgZ, s, 0, handle, 1);
+    } else {
+        enqueue_vcycle<float>(r_.p, &s->rsum, mean);
+        k_cg_z<float><<<blocks_for(n), kThreads, 0, stream_>>>(n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+                                                               counters_.p + kCgZ, s, 0, handle, 1);
+    }
+    k_cg_p<<<blocks_for(n), kThreads, 0, stream_>>>(n, p_.p, z_.p, s);
+    cudaGraph_t captured;
+    cudaError_t ce = cudaStreamEndCapture(stream_, &captured);
+    stream_ = saved;
+    graph_body_launches_[precision] = launches_ - saved_launches + 5;
+    launches_ = saved_launches;
+    if (ce != cudaSuccess) {
+        cudaGraphDestroy(g);
+        throw Error(2, std::string("graph capture failed: ") + cudaGetErrorString(ce));
+    }
+    cudaGraphExec_t exec;
+    cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) throw Error(2, std::string("graph instantiation failed: ") + cudaGetErrorString(ie));
+    cg_exec_[precision] = exec;
+    return exec;
+}
+
+void DeviceSolver::cg_fused(int precision, double target, int itmax, int& niter, int& flags) {
+    const int n = levels_[0].n;
+    const int nl = int(levels_.size());
+    CgState* s = reinterpret_cast<CgState*>(cgs_.p);
+    double* mean = lsum_.p + nl;
+    cudaGraphExec_t exec = cg_graph(precision);
+    k_cg_set<<<1, 1, 0, stream_>>>(s, target, itmax);
+    k_cg_residual<<<blocks_for(n), kThreads, 0, stream_>>>(vd_[0], b_.p, xw_.p, r_.p, fpartial_.p,
+                                                            counters_.p + kCgRes, s);
+    launches_ += 2;
+    if (precision == 0) {
+        enqueue_vcycle<double>(r_.p, &s->rsum, mean);
+        k_cg_z<double><<<blocks_for(n), kThreads, 0, stream_>>>(n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+                                                                counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(),
+                                                                0);
+    } else {
+        enqueue_vcycle<float>(r_.p, &s->rsum, mean);
+        k_cg_z<float><<<blocks_for(n), kThreads, 0, stream_>>>(n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+                                                               counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(),
+                                                               0);
+    }
+    ++launches_;
+    CgState hs;
+    TPA_CUDA(cudaMemcpyAsync(&hs, s, sizeof(CgState), cudaMemcpyDeviceToHost, stream_));
+    TPA_CUDA(cudaStreamSynchronize(stream_));
+    if (!(hs.flags & 8) && itmax > 0) {
+        TPA_CUDA(cudaGraphLaunch(exec, stream_));
+        TPA_CUDA(cudaMemcpyAsync(&hs, s, sizeof(CgState), cudaMemcpyDeviceToHost, stream_));
+        TPA_CUDA(cudaStreamSynchronize(stream_));
+        // every started body ran its kernels; zero curvature ends one early
+        int bodies = hs.iter + ((hs.flags & 2) ? 1 : 0);
+        launches_ += bodies * graph_body_launches_[precision];
+    }
+    TPA_CUDA(cudaGetLastError());
+    niter = hs.iter;
+    flags = hs.flags;
+}
+
+double DeviceSolver::time_fused(int which, int level, int precision, int iters) {
+    if (level < 0 || level >= tail_first_) throw Error(1, "level is handled by the single-CTA tail");
+    cudaEvent_t e0, e1;
+    TPA_CUDA(cudaEventCreate(&e0));
+    TPA_CUDA(cudaEventCreate(&e1));
+    auto one = [&](const auto& V, auto tag) {
+        using T = decltype(tag);
+        const LevelView<T>& L = V[size_t(level)];
+        switch (which) {
+            case 0: k_post2<T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, fpartial_.p, counters_.p, nullptr); break;
+            case 1:
+                k_restrict<T><<<blocks_for(L.nc), kThreads, 0, stream_>>>(L, V[size_t(level + 1)].b, fpartial_.p,
+                                                                          counters_.p, nullptr);
+                break;
+            case 2: k_prolong<T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, V[size_t(level + 1)].x); break;
+            case 4: k_pre2<T, T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, L.b, nullptr); break;
+            case 5: k_residual<T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L); break;
+            default: throw Error(1, "unknown kernel");
+        }
+    };
+    auto launch = [&]() {
+        if (which == 3) {
+            if (precision != 0 || level != 0) throw Error(1, "the CG operator runs in FP64 on the finest level");
+            CgState* s = reinterpret_cast<CgState*>(cgs_.p);
+            k_cg_ap<<<blocks_for(vd_[0].n), kThreads, 0, stream_>>>(vd_[0], p_.p, ap_.p, fpartial_.p,
+                                                                     counters_.p + kCgAp, s);
+        } else if (precision == 0) {
+            one(vd_, double(0));
+        } else {
+            one(vf_, float(0));
+        }
+    };
+    launch();
+    TPA_CUDA(cudaEventRecord(e0, stream_));
+    for (int k = 0; k < iters; ++k) launch();
+    TPA_CUDA(cudaEventRecord(e1, stream_));
+    TPA_CUDA(cudaEventSynchronize(e1));
+    TPA_CUDA(cudaGetLastError());
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return double(ms) / iters;
+}
+
+}  // namespace tpa
