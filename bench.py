@@ -125,6 +125,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--levels", type=int, default=4)
+    ap.add_argument("--workload", default="droplet_amr", choices=["droplet_amr", "uniform_2048"])
+    ap.add_argument("--size", type=int, default=2048, help="cells per side of the uniform workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true", help="only W warm-up and K mixed solves (for ncu)")
     args = ap.parse_args()
@@ -151,13 +153,20 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    spec = workload(args.levels)
-    mesh = BlockTreeMesh(**spec)
-    frac, kappa, psi = W.droplet_inputs(mesh)
+    if args.workload == "droplet_amr":
+        spec = workload(args.levels)
+        mesh = BlockTreeMesh(**spec)
+        frac, kappa, psi = W.droplet_inputs(mesh)
+    else:  # uniform_2048: 128x128 periodic roots of 16x16, kappa = 1
+        mesh = BlockTreeMesh(**W.uniform_spec(args.size))
+        kappa = np.ones(mesh.nfaces)
     solver = EllipticSolver(PoissonOperator(mesh, kappa), device=local)
     stream = torch.cuda.current_stream()
     solver.ctx.call("tpa_set_stream", C.c_void_p(stream.cuda_stream))
-    rhs_h = W.droplet_rhs(mesh, solver.apply(psi))
+    if args.workload == "droplet_amr":
+        rhs_h = W.droplet_rhs(mesh, solver.apply(psi))
+    else:
+        rhs_h = W.gaussian_rhs(mesh, W.SEEDS["uniform_2048"])
     n = mesh.ncells
     rhs_d = torch.from_numpy(rhs_h).cuda()
     x_d = torch.zeros(n, dtype=torch.float64, device="cuda")
@@ -242,10 +251,11 @@ def main():
     solver.ctx.call("tpa_time_kernel", 0, 0, 1, 200, C.byref(sweep))
     sweep64 = C.c_double()
     solver.ctx.call("tpa_time_kernel", 0, 0, 0, 200, C.byref(sweep64))
-    # algorithmic bytes of one damped-Jacobi sweep with variable coefficients:
-    # read x, b and two face coefficients per cell, write x (3 s + 2 s_kappa)
-    alg32 = n * (3 * 4 + 2 * 4)
-    alg64 = n * (3 * 8 + 2 * 8)
+    # algorithmic bytes of one damped-Jacobi sweep: read x and b, write x, plus
+    # two face coefficients per cell when they vary (3 s + 2 s_kappa)
+    skappa = 0 if args.workload == "uniform_2048" else 1
+    alg32 = n * (3 * 4 + 2 * 4 * skappa)
+    alg64 = n * (3 * 8 + 2 * 8 * skappa)
     peak, peak_kind = measured_peaks()
     achieved = alg32 / (sweep.value * 1e-3) / 1e9
 
@@ -265,7 +275,7 @@ def main():
         "dtype": "f32/f64", "data": "synthetic (seeded Philox)",
         "config": {"workload": f"droplet_amr levels={args.levels} (unit square, 4x4 roots of 16x16, circle band)",
                    "fine_cells": n, "levels": solver.level_sizes(), "parallelism": "replicas" if world > 1 else "1 GPU",
-                   "l2": "flushed between steps (256 MiB write)"},
+                   "l2": "flushed between steps (256 MiB write)", "device_layout": solver.device_info()},
         "time_to_tolerance_ms": {"mixed": mixed_ms, "fp64": fp64_ms, "speedup_mixed_over_fp64": fp64_ms / mixed_ms},
         "cg_iterations": {"mixed": mixed_it, "fp64": fp64_it},
         "fp64_value": world * n * fp64_it / (fp64_ms * 1e-3),

@@ -136,6 +136,11 @@ tpa_status tpa_apply(tpa_context* ctx, const double* x, double* y);
 tpa_status tpa_vcycle(tpa_context* ctx, const double* r, double* z, int32_t precision);
 /* Wait for the context's stream. */
 tpa_status tpa_synchronize(tpa_context* ctx);
+/* Device layout of the uploaded hierarchy: out = {levels on the block-
+ * structured stencil path, exception (CSR) rows on those levels, first level
+ * of the single-CTA coarse tail, 1 if the fused default cycle is used}.
+ * Uploads the hierarchy if needed. */
+tpa_status tpa_device_info(tpa_context* ctx, int64_t out[4]);
 /* Run subsequent device work on the caller's CUDA stream (a cudaStream_t
  * passed as void*; NULL restores the context's own stream).  Replaces nothing
  * in the reference (it has no device); it lets a caller order the solve with

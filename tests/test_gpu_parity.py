@@ -136,6 +136,29 @@ def test_balanced_force_cgfm():
         assert np.max(np.abs(d)) <= 1e-8 * np.max(np.abs(psi))
 
 
+@pytest.mark.parametrize("name", ["taylor_green_128", "droplet_l2"])
+def test_structured_levels_match_csr_levels(name, monkeypatch):
+    """The block-structured stencil path (with CSR exception rows at coarse-fine
+    edges) gives the same V-cycle as the plain CSR path."""
+    monkeypatch.setenv("TPAGMG_STRUCTURED", "all")
+    m, s, oo, mg = build(name)
+    info = s.device_info()
+    assert info["structured_levels"] >= 1 and info["fused_cycle"]
+    if name == "droplet_l2":
+        assert info["exception_rows"] > 0
+    rng = np.random.default_rng(3)
+    r = rng.standard_normal(m.ncells) * oo.volumes
+    r -= oo.volumes * np.sum(r) / np.sum(oo.volumes)
+    z = s.vcycle(r, precision="fp64")
+    monkeypatch.setenv("TPAGMG_NO_STRUCTURED", "1")
+    spec, coarse, coef = CASES[name]
+    s2 = EllipticSolver(PoissonOperator(m, s.operator.face_coefficient), multigrid=MultigridOptions(coarse_size=coarse))
+    assert s2.device_info()["structured_levels"] == 0
+    z2 = s2.vcycle(r, precision="fp64")
+    assert np.max(np.abs(z - z2)) <= 1e-12 * np.max(np.abs(z2))
+    assert np.max(np.abs(s.apply(r) - s2.apply(r))) <= 1e-13 * np.max(np.abs(s2.apply(r)))
+
+
 def test_solves_are_bitwise_repeatable():
     m, s, oo, mg = build("droplet_l2")
     rhs = W.gaussian_rhs(m, 3)

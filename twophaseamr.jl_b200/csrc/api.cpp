@@ -384,6 +384,16 @@ tpa_status tpa_time_kernel(tpa_context* ctx, int32_t which, int32_t level, int32
     });
 }
 
+tpa_status tpa_device_info(tpa_context* ctx, int64_t out[4]) {
+    return guard(ctx, [&] {
+        ensure_device(ctx);
+        out[0] = ctx->dev->structured_levels();
+        out[1] = ctx->dev->exception_rows();
+        out[2] = ctx->dev->tail_first();
+        out[3] = ctx->dev->fused() ? 1 : 0;
+    });
+}
+
 tpa_status tpa_synchronize(tpa_context* ctx) {
     return guard(ctx, [&] {
         if (ctx->dev) TPA_CUDA(cudaStreamSynchronize(ctx->dev->stream()));

@@ -484,6 +484,7 @@ void DeviceSolver::upload(const Hierarchy& h) {
     for (auto* a : {&b_, &r_, &p_, &ap_, &z_, &tmp_}) a->alloc(n);
     TPA_CUDA(cudaStreamSynchronize(stream_));
     build_views();
+    upload_structured(h);
 }
 
 void DeviceSolver::apply(const double* x, double* y) {

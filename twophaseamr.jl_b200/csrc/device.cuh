@@ -9,6 +9,8 @@
 
 #include "fused.cuh"
 #include "host.hpp"
+#include "stencil.cuh"
+#include "structure.hpp"
 
 namespace tpa {
 
@@ -171,6 +173,25 @@ private:
     DevArray<char> cgs_;  // CgState
     cudaGraphExec_t cg_exec_[2] = {nullptr, nullptr};
     int graph_body_launches_[2] = {0, 0};
+
+    // block-structured level data (stencil + exception rows)
+    struct StructDev {
+        bool on = false;
+        DevArray<int> nbr, ex, ex_ptr, ex_col, map;
+        DevArray<double> cx_d, cy_d, exv_d;
+        DevArray<float> cx_f, cy_f, exv_f;
+        int64_t nex = 0;
+        bool const_coef = false, const_diag = false;
+    };
+    std::vector<StructDev> sdev_;
+    std::vector<SView<double>> sd_;
+    std::vector<SView<float>> sf_;
+    void upload_structured(const Hierarchy& h);
+
+public:
+    // Levels on the block-structured path and their exception-row counts.
+    int structured_levels() const;
+    int64_t exception_rows() const;
 };
 
 }  // namespace tpa

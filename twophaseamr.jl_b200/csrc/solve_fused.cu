@@ -86,6 +86,39 @@ __global__ void k_cg_ap(LevelView<double> A, const double* __restrict__ p, doubl
     }
 }
 
+__device__ __forceinline__ void alpha_from(double pAp, CgState* s) {
+    const double eps = 2.220446049250313e-16;
+    s->pAp = pAp;
+    if (pAp <= eps * s->pnorm2 && fabs(pAp) <= eps * s->pnorm2) {
+        s->flags |= 2;
+        s->alpha = 0;
+    } else {
+        s->alpha = s->gamma / pAp;
+    }
+}
+
+// block-structured finest level: Ap = A p and alpha
+__global__ void s_cg_ap(SView<double> L, const double* __restrict__ p, double* __restrict__ ap, double* partial,
+                        unsigned* counter, CgState* s) {
+    s_apply_dot(L, p, ap, partial, counter, [&](double pAp) { alpha_from(pAp, s); });
+}
+
+// block-structured finest level: r = b - A x, folds sum(r) into s->rsum
+__global__ void s_cg_residual(SView<double> L, const double* __restrict__ b, const double* __restrict__ x,
+                              double* __restrict__ r, double* partial, unsigned* counter, CgState* s) {
+    const int bk = blockIdx.x, t = threadIdx.x;
+    const int i = t % L.nx, j = t / L.nx, c = bk * L.cpb + t;
+    double v = b[c] - s_apply(L, bk, i, j, c, [&](int q) { return x[q]; });
+    r[c] = v;
+    if (publish_partial(v, partial, counter)) {
+        double tt = fold_partials(partial, gridDim.x);
+        if (threadIdx.x == 0) {
+            s->rsum = tt;
+            *counter = 0;
+        }
+    }
+}
+
 // x += alpha p, r -= alpha Ap; folds max|r_i|/V_i and sum(r)
 __global__ void k_cg_update(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
                             const double* __restrict__ ap, const double* __restrict__ vol, double* pmax, double* psum,
@@ -305,8 +338,24 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
         Vdev = vf_dev_.p;
     }
     const std::vector<LevelView<T>>& V = *Vp;
+    const std::vector<SView<T>>* Sp;
+    if constexpr (std::is_same<T, double>::value) Sp = &sd_;
+    else Sp = &sf_;
     for (int l = 0; l < t; ++l) {
         const LevelView<T>& L = V[size_t(l)];
+        if (sdev_[size_t(l)].on) {
+            const SView<T>& S = (*Sp)[size_t(l)];
+            const int g = S.nblocks, th = S.cpb;
+            if (l == 0) s_pre2<T, double><<<g, th, 0, stream_>>>(S, r, rsum);
+            else s_pre2<T, T><<<g, th, 0, stream_>>>(S, S.b, lsum_.p + l);
+            const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
+            s_residual<T><<<g, th, 0, stream_>>>(S);
+            s_restrict<T><<<g, th, th * sizeof(T), stream_>>>(S, V[size_t(l + 1)].b, fpartial_.p,
+                                                               counters_.p + kRestrictSum,
+                                                               next_sum ? lsum_.p + l + 1 : nullptr);
+            launches_ += 3;
+            continue;
+        }
         if (l == 0) k_pre2<T, double><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, r, rsum);
         else k_pre2<T, T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, L.b, lsum_.p + l);
         const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
@@ -321,6 +370,16 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
     ++launches_;
     for (int l = t - 1; l >= 0; --l) {
         const LevelView<T>& L = V[size_t(l)];
+        if (sdev_[size_t(l)].on) {
+            const SView<T>& S = (*Sp)[size_t(l)];
+            const int g = S.nblocks, th = S.cpb;
+            s_prolong<T><<<g, th, 0, stream_>>>(S, V[size_t(l + 1)].x);
+            s_post1<T><<<g, th, 0, stream_>>>(S);
+            const bool want_mean = (l == 0) && L.singular;
+            s_post2<T><<<g, th, 0, stream_>>>(S, fpartial_.p, counters_.p + kPostMean, want_mean ? mean_out : nullptr);
+            launches_ += 3;
+            continue;
+        }
         k_prolong<T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, V[size_t(l + 1)].x);
         k_post1<T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L);
         const bool want_mean = (l == 0) && L.singular;
@@ -375,7 +434,10 @@ cudaGraphExec_t DeviceSolver::cg_graph(int precision) {
     const int saved_launches = launches_;
     TPA_CUDA(cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     const LevelView<double>& A = vd_[0];
-    k_cg_ap<<<blocks_for(n), kThreads, 0, stream_>>>(A, p_.p, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
+    if (sdev_[0].on)
+        s_cg_ap<<<sd_[0].nblocks, sd_[0].cpb, 0, stream_>>>(sd_[0], p_.p, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
+    else
+        k_cg_ap<<<blocks_for(n), kThreads, 0, stream_>>>(A, p_.p, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
     k_cg_update<<<blocks_for(n), kThreads, 0, stream_>>>(n, xw_.p, r_.p, p_.p, ap_.p, A.vol, fpartial_.p,
                                                           fpartial2_.p, counters_.p + kCgUpdate, s);
     if (precision == 0) {
@@ -412,8 +474,12 @@ void DeviceSolver::cg_fused(int precision, double target, int itmax, int& niter,
     double* mean = lsum_.p + nl;
     cudaGraphExec_t exec = cg_graph(precision);
     k_cg_set<<<1, 1, 0, stream_>>>(s, target, itmax);
-    k_cg_residual<<<blocks_for(n), kThreads, 0, stream_>>>(vd_[0], b_.p, xw_.p, r_.p, fpartial_.p,
-                                                            counters_.p + kCgRes, s);
+    if (sdev_[0].on)
+        s_cg_residual<<<sd_[0].nblocks, sd_[0].cpb, 0, stream_>>>(sd_[0], b_.p, xw_.p, r_.p, fpartial_.p,
+                                                                  counters_.p + kCgRes, s);
+    else
+        k_cg_residual<<<blocks_for(n), kThreads, 0, stream_>>>(vd_[0], b_.p, xw_.p, r_.p, fpartial_.p,
+                                                                counters_.p + kCgRes, s);
     launches_ += 2;
     if (precision == 0) {
         enqueue_vcycle<double>(r_.p, &s->rsum, mean);
@@ -463,12 +529,39 @@ double DeviceSolver::time_fused(int which, int level, int precision, int iters) 
             default: throw Error(1, "unknown kernel");
         }
     };
+    auto one_s = [&](const auto& S, auto tag) {
+        using T = decltype(tag);
+        const SView<T>& L = S[size_t(level)];
+        const int g = L.nblocks, th = L.cpb;
+        switch (which) {
+            case 0: s_post2<T><<<g, th, 0, stream_>>>(L, fpartial_.p, counters_.p, nullptr); break;
+            case 1:
+                s_restrict<T><<<g, th, th * sizeof(T), stream_>>>(L, (sizeof(T) == 8 ? (T*)vd_[size_t(level + 1)].b
+                                                                                     : (T*)vf_[size_t(level + 1)].b),
+                                                                  fpartial_.p, counters_.p, nullptr);
+                break;
+            case 2:
+                s_prolong<T><<<g, th, 0, stream_>>>(L, (sizeof(T) == 8 ? (const T*)vd_[size_t(level + 1)].x
+                                                                      : (const T*)vf_[size_t(level + 1)].x));
+                break;
+            case 4: s_pre2<T, T><<<g, th, 0, stream_>>>(L, L.b, nullptr); break;
+            case 5: s_residual<T><<<g, th, 0, stream_>>>(L); break;
+            default: throw Error(1, "unknown kernel");
+        }
+    };
     auto launch = [&]() {
         if (which == 3) {
             if (precision != 0 || level != 0) throw Error(1, "the CG operator runs in FP64 on the finest level");
             CgState* s = reinterpret_cast<CgState*>(cgs_.p);
-            k_cg_ap<<<blocks_for(vd_[0].n), kThreads, 0, stream_>>>(vd_[0], p_.p, ap_.p, fpartial_.p,
-                                                                     counters_.p + kCgAp, s);
+            if (sdev_[0].on)
+                s_cg_ap<<<sd_[0].nblocks, sd_[0].cpb, 0, stream_>>>(sd_[0], p_.p, ap_.p, fpartial_.p,
+                                                                    counters_.p + kCgAp, s);
+            else
+                k_cg_ap<<<blocks_for(vd_[0].n), kThreads, 0, stream_>>>(vd_[0], p_.p, ap_.p, fpartial_.p,
+                                                                         counters_.p + kCgAp, s);
+        } else if (sdev_[size_t(level)].on) {
+            if (precision == 0) one_s(sd_, double(0));
+            else one_s(sf_, float(0));
         } else if (precision == 0) {
             one(vd_, double(0));
         } else {
@@ -486,6 +579,110 @@ double DeviceSolver::time_fused(int which, int level, int precision, int iters) 
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return double(ms) / iters;
+}
+
+}  // namespace tpa
+
+namespace tpa {
+
+// Block-structured copies of every level that qualifies: 16x16-style blocks
+// (32 to 1024 cells, a multiple of 32), a valid block map of the transfer and
+// the transfer's inverse diagonal equal to the smoother's.
+void DeviceSolver::upload_structured(const Hierarchy& h) {
+    const int nl = int(levels_.size());
+    sdev_.clear();
+    sdev_.resize(size_t(nl));
+    sd_.assign(size_t(nl), SView<double>{});
+    sf_.assign(size_t(nl), SView<float>{});
+    const bool disabled = std::getenv("TPAGMG_NO_STRUCTURED") != nullptr;
+    for (int l = 0; l < nl; ++l) {
+        const HostLevel& hl = h.levels[size_t(l)];
+        const int cpb = hl.op.mesh.bs[0] * hl.op.mesh.bs[1];
+        if (disabled || l >= tail_first_ || l + 1 >= nl || cpb < 32 || cpb > 1024 || cpb % 32) continue;
+        StructLevel st = build_struct(hl, &h.levels[size_t(l + 1)].op.mesh);
+        if (!st.has_map || !st.tinv_same) continue;
+        // Variable-coefficient levels with coarse-fine exception rows are small and
+        // latency-bound; the CSR kernels (one index chain per row, no divergence
+        // between stencil and exception rows) are faster there.  Force the stencil
+        // path on every level with TPAGMG_STRUCTURED=all.
+        const char* policy = std::getenv("TPAGMG_STRUCTURED");
+        const bool all = policy && std::string(policy) == "all";
+        if (!all && !(st.const_coef && st.nex == 0)) continue;
+        StructDev& D = sdev_[size_t(l)];
+        D.on = true;
+        D.nex = st.nex;
+        D.const_coef = st.const_coef;
+        D.const_diag = st.const_diag;
+        D.nbr.upload(st.nbr.data(), st.nbr.size(), stream_);
+        D.map.upload(st.map.data(), st.map.size(), stream_);
+        std::vector<float> f;
+        if (!st.const_coef) {
+            D.cx_d.upload(st.cx.data(), st.cx.size(), stream_);
+            D.cy_d.upload(st.cy.data(), st.cy.size(), stream_);
+            f.assign(st.cx.begin(), st.cx.end());
+            D.cx_f.upload(f.data(), f.size(), stream_);
+            std::vector<float> g(st.cy.begin(), st.cy.end());
+            D.cy_f.upload(g.data(), g.size(), stream_);
+            TPA_CUDA(cudaStreamSynchronize(stream_));
+        }
+        if (st.nex) {
+            std::vector<int> ptr(st.ex_ptr.begin(), st.ex_ptr.end());
+            D.ex.upload(st.ex.data(), st.ex.size(), stream_);
+            D.ex_ptr.upload(ptr.data(), ptr.size(), stream_);
+            D.ex_col.upload(st.ex_col.data(), st.ex_col.size(), stream_);
+            D.exv_d.upload(st.ex_val.data(), st.ex_val.size(), stream_);
+            std::vector<float> g(st.ex_val.begin(), st.ex_val.end());
+            D.exv_f.upload(g.data(), g.size(), stream_);
+            TPA_CUDA(cudaStreamSynchronize(stream_));
+        }
+        DevLevel& L = levels_[size_t(l)];
+        auto fill = [&](auto& v, auto& DL, auto* cx, auto* cy, auto* exv, auto cast) {
+            v.nx = hl.op.mesh.bs[0];
+            v.ny = hl.op.mesh.bs[1];
+            v.cpb = cpb;
+            v.nblocks = int(hl.op.mesh.nblocks());
+            v.n = L.n;
+            v.nbr = D.nbr.p;
+            v.cx = st.const_coef ? nullptr : cx;
+            v.cy = st.const_coef ? nullptr : cy;
+            v.c0 = cast(st.c0);
+            v.dinv = st.const_diag ? nullptr : DL.dinv.p;
+            v.dinv0 = cast(st.dinv.empty() ? 0.0 : st.dinv[0]);
+            v.ex = st.nex ? D.ex.p : nullptr;
+            v.ex_ptr = D.ex_ptr.p;
+            v.ex_col = D.ex_col.p;
+            v.ex_val = exv;
+            v.map = D.map.p;
+            v.vol = DL.vol.p;
+            v.w = DL.w;
+            v.tw = DL.tw;
+            v.singular = L.ncomp == 1;
+            v.cvol_inv = L.ncomp == 1 ? 1.0 / L.comp_volume[0] : 0.0;
+            v.b = DL.b.p;
+            v.bp = DL.bp.p;
+            v.x = DL.x.p;
+            v.y = DL.y.p;
+            v.r = DL.r.p;
+            v.s = DL.s.p;
+            v.ccpb = cpb;
+        };
+        fill(sd_[size_t(l)], L.d, D.cx_d.p, D.cy_d.p, D.exv_d.p, [](double v) { return v; });
+        fill(sf_[size_t(l)], L.f, D.cx_f.p, D.cy_f.p, D.exv_f.p, [](double v) { return float(v); });
+    }
+    TPA_CUDA(cudaStreamSynchronize(stream_));
+    destroy_graphs();
+}
+
+int DeviceSolver::structured_levels() const {
+    int k = 0;
+    for (const auto& d : sdev_) k += d.on ? 1 : 0;
+    return k;
+}
+
+int64_t DeviceSolver::exception_rows() const {
+    int64_t k = 0;
+    for (const auto& d : sdev_) k += d.on ? d.nex : 0;
+    return k;
 }
 
 }  // namespace tpa

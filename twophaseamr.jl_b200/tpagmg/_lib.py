@@ -74,6 +74,7 @@ SIGNATURES = {
     "tpa_vcycle": (C.c_int32, [P, f64p, f64p, C.c_int32]),
     "tpa_synchronize": (C.c_int32, [P]),
     "tpa_set_stream": (C.c_int32, [P, P]),
+    "tpa_device_info": (C.c_int32, [P, i64p]),
     "tpa_time_kernel": (C.c_int32, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, f64p]),
 }
 

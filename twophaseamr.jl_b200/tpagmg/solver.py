@@ -113,6 +113,13 @@ class EllipticSolver:
         self.ctx.call("tpa_level_face_coefficients", int(level), _lib.ptr(out, C.c_double))
         return out
 
+    def device_info(self):
+        """Device layout: structured levels, exception rows, tail start, fused cycle."""
+        out = np.zeros(4, dtype=np.int64)
+        self.ctx.call("tpa_device_info", _lib.ptr(out, C.c_int64))
+        return {"structured_levels": int(out[0]), "exception_rows": int(out[1]),
+                "tail_first_level": int(out[2]), "fused_cycle": bool(out[3])}
+
     # -- device operations --------------------------------------------------
     def refresh(self, face_coefficient):
         """`_refresh_geometric_multigrid!` after a coefficient change."""
