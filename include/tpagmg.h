@@ -136,6 +136,13 @@ tpa_status tpa_apply(tpa_context* ctx, const double* x, double* y);
 tpa_status tpa_vcycle(tpa_context* ctx, const double* r, double* z, int32_t precision);
 /* Wait for the context's stream. */
 tpa_status tpa_synchronize(tpa_context* ctx);
+/* `_integrated_residual_norms(r, volumes)` (src/solvers/multigrid/cycles.jl:
+ * 210-221, the norms `residual_norms(solver)` reports, elliptic_solver.jl:
+ * 677-679) of an integrated residual r on the finest level (device pointer,
+ * cell order): out[0] = sqrt(sum_V V (r/V)^2 / sum_V V), out[1] = max |r_i|/V_i
+ * over cells of positive volume.  Uses the context's device scratch; out is a
+ * host array. */
+tpa_status tpa_residual_norms(tpa_context* ctx, const double* r, double out[2]);
 /* Device layout of the uploaded hierarchy: out = {levels on the block-
  * structured stencil path, exception (CSR) rows on those levels, first level
  * of the single-CTA coarse tail, 1 if the fused default cycle is used}.

@@ -159,6 +159,19 @@ def test_structured_levels_match_csr_levels(name, monkeypatch):
     assert np.max(np.abs(s.apply(r) - s2.apply(r))) <= 1e-13 * np.max(np.abs(s2.apply(r)))
 
 
+def test_residual_norms_match_oracle():
+    """`_integrated_residual_norms` (cycles.jl:210-221) on the device."""
+    import torch
+    from oracle.krylov import integrated_norms
+    m, s, oo, mg = build("droplet_l2")
+    r = np.random.default_rng(9).standard_normal(m.ncells) * oo.volumes
+    r[5] = -40 * oo.volumes[5]
+    rd = torch.from_numpy(r).cuda()
+    l2, linf = s.residual_norms_device(rd.data_ptr())
+    ol2, olinf = integrated_norms(r, oo.volumes)
+    assert l2 == pytest.approx(ol2, rel=1e-12) and linf == pytest.approx(olinf, rel=1e-15)
+
+
 def test_solves_are_bitwise_repeatable():
     m, s, oo, mg = build("droplet_l2")
     rhs = W.gaussian_rhs(m, 3)

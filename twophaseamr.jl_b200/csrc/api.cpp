@@ -384,6 +384,14 @@ tpa_status tpa_time_kernel(tpa_context* ctx, int32_t which, int32_t level, int32
     });
 }
 
+tpa_status tpa_residual_norms(tpa_context* ctx, const double* r, double out[2]) {
+    return guard(ctx, [&] {
+        if (!r || !out) throw tpa::Error(TPA_ERR_INVALID_ARG, "null residual or output");
+        ensure_device(ctx);
+        ctx->dev->residual_norms(r, out);
+    });
+}
+
 tpa_status tpa_device_info(tpa_context* ctx, int64_t out[4]) {
     return guard(ctx, [&] {
         ensure_device(ctx);

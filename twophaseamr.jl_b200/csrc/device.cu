@@ -675,6 +675,20 @@ double DeviceSolver::time_kernel(int which, int level, int precision, int iters)
     return double(ms) / iters;
 }
 
+void DeviceSolver::residual_norms(const double* r, double out[2]) {
+    DevLevel& L = levels_[0];
+    const double* vol = L.d.vol.p;
+    k_l2_terms<<<kReduceBlocks, kThreads, 0, stream_>>>(L.n, r, vol, partial_.p);
+    k_fold_sum<<<1, kThreads, 0, stream_>>>(partial_.p, kReduceBlocks, sums_.p + 56);
+    k_fold_sum<<<1, kThreads, 0, stream_>>>(partial_.p + kReduceBlocks, kReduceBlocks, sums_.p + 57);
+    launches_ += 3;
+    strong_max(r, sums_.p + 58);
+    TPA_CUDA(cudaMemcpyAsync(host_d_, sums_.p + 56, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    TPA_CUDA(cudaStreamSynchronize(stream_));
+    out[0] = std::sqrt(host_d_[0] / host_d_[1]);
+    out[1] = host_d_[2];
+}
+
 double DeviceSolver::read_scalar(const double* dev) {
     TPA_CUDA(cudaMemcpyAsync(host_d_, dev, sizeof(double), cudaMemcpyDeviceToHost, stream_));
     TPA_CUDA(cudaStreamSynchronize(stream_));

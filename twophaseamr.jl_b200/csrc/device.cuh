@@ -122,6 +122,10 @@ public:
     void solve(const double* rhs, double* x, double rtol, double atol, int max_cycles, int compatibility,
                int precision, SolveStats& st);
 
+    // `_integrated_residual_norms` of a finest-level integrated residual
+    // (device pointer): out = {L2 of the strong residual, strong L-infinity}.
+    void residual_norms(const double* r, double out[2]);
+
     int kernel_launches() const { return launches_; }
     void reset_launches() { launches_ = 0; }
 

@@ -120,6 +120,13 @@ class EllipticSolver:
         return {"structured_levels": int(out[0]), "exception_rows": int(out[1]),
                 "tail_first_level": int(out[2]), "fused_cycle": bool(out[3])}
 
+    def residual_norms_device(self, r_ptr):
+        """`_integrated_residual_norms` of an integrated residual held on the
+        device (raw CUDA pointer, cell order): (L2, strong L-infinity)."""
+        out = np.zeros(2)
+        self.ctx.call("tpa_residual_norms", C.c_void_p(r_ptr), _lib.ptr(out, C.c_double))
+        return float(out[0]), float(out[1])
+
     # -- device operations --------------------------------------------------
     def refresh(self, face_coefficient):
         """`_refresh_geometric_multigrid!` after a coefficient change."""
