@@ -20,6 +20,10 @@ struct tpa_context {
     void* user_stream = nullptr;
 };
 
+namespace tpa {
+void set_context_error(tpa_context* ctx, const std::string& msg) { ctx->error = msg; }
+}  // namespace tpa
+
 namespace {
 
 template <typename F>
