@@ -164,6 +164,7 @@ private:
     void vcycle_fused(const double* r, double* z, int precision);
     void destroy_graphs();
     cudaGraphExec_t cg_graph(int precision);
+    void enqueue_cg_body(int precision, cudaGraphConditionalHandle handle, int set_cond);
     double time_fused(int which, int level, int precision, int iters);
 
     bool fused_ok_ = false;

@@ -31,14 +31,18 @@ inline int blocks_for(int64_t n) {
     return int(g < 1 ? 1 : g);
 }
 
+constexpr int kMaxGrid = 1184;  // 8 CTAs on each of 148 SMs: bounds the partials every fold reads
+inline int reduce_grid(int64_t n) { return int(std::min<int64_t>(blocks_for(n), kMaxGrid)); }
+#define TPA_GRID_STRIDE(i, n) for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += gridDim.x * blockDim.x)
+
 // r = b - A x, folds sum(r) into s->rsum
 __global__ void k_cg_residual(LevelView<double> A, const double* __restrict__ b, const double* __restrict__ x,
                               double* __restrict__ r, double* partial, unsigned* counter, CgState* s) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v = 0;
-    if (i < A.n) {
-        v = b[i] - rowdot(A, x, i);
-        r[i] = v;
+    TPA_GRID_STRIDE(i, A.n) {
+        double ri = b[i] - rowdot(A, x, i);
+        r[i] = ri;
+        v += ri;
     }
     if (publish_partial(v, partial, counter)) {
         double t = fold_partials(partial, gridDim.x);
@@ -50,37 +54,12 @@ __global__ void k_cg_residual(LevelView<double> A, const double* __restrict__ b,
 }
 
 __global__ void k_sum_into(int n, const double* __restrict__ v, double* partial, unsigned* counter, double* out) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (publish_partial(i < n ? v[i] : 0.0, partial, counter)) {
+    double acc = 0;
+    TPA_GRID_STRIDE(i, n) acc += v[i];
+    if (publish_partial(acc, partial, counter)) {
         double t = fold_partials(partial, gridDim.x);
         if (threadIdx.x == 0) {
             *out = t;
-            *counter = 0;
-        }
-    }
-}
-
-// Ap = A p and alpha = gamma / p'Ap with the zero-curvature guard
-__global__ void k_cg_ap(LevelView<double> A, const double* __restrict__ p, double* __restrict__ ap, double* partial,
-                        unsigned* counter, CgState* s) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double v = 0;
-    if (i < A.n) {
-        double y = rowdot(A, p, i);
-        ap[i] = y;
-        v = p[i] * y;
-    }
-    if (publish_partial(v, partial, counter)) {
-        double pAp = fold_partials(partial, gridDim.x);
-        if (threadIdx.x == 0) {
-            const double eps = 2.220446049250313e-16;
-            s->pAp = pAp;
-            if (pAp <= eps * s->pnorm2 && fabs(pAp) <= eps * s->pnorm2) {
-                s->flags |= 2;
-                s->alpha = 0;
-            } else {
-                s->alpha = s->gamma / pAp;
-            }
             *counter = 0;
         }
     }
@@ -97,23 +76,19 @@ __device__ __forceinline__ void alpha_from(double pAp, CgState* s) {
     }
 }
 
-// block-structured finest level: Ap = A p and alpha
-__global__ void s_cg_ap(SView<double> L, const double* __restrict__ p, double* __restrict__ ap, double* partial,
+// Ap = A p and alpha = gamma / p'Ap with the zero-curvature guard
+__global__ void k_cg_ap(LevelView<double> A, const double* __restrict__ p, double* __restrict__ ap, double* partial,
                         unsigned* counter, CgState* s) {
-    s_apply_dot(L, p, ap, partial, counter, [&](double pAp) { alpha_from(pAp, s); });
-}
-
-// block-structured finest level: r = b - A x, folds sum(r) into s->rsum
-__global__ void s_cg_residual(SView<double> L, const double* __restrict__ b, const double* __restrict__ x,
-                              double* __restrict__ r, double* partial, unsigned* counter, CgState* s) {
-    const int bk = blockIdx.x, t = threadIdx.x;
-    const int i = t % L.nx, j = t / L.nx, c = bk * L.cpb + t;
-    double v = b[c] - s_apply(L, bk, i, j, c, [&](int q) { return x[q]; });
-    r[c] = v;
+    double v = 0;
+    TPA_GRID_STRIDE(i, A.n) {
+        double y = rowdot(A, p, i);
+        ap[i] = y;
+        v += p[i] * y;
+    }
     if (publish_partial(v, partial, counter)) {
-        double tt = fold_partials(partial, gridDim.x);
+        double pAp = fold_partials(partial, gridDim.x);
         if (threadIdx.x == 0) {
-            s->rsum = tt;
+            alpha_from(pAp, s);
             *counter = 0;
         }
     }
@@ -124,11 +99,11 @@ __global__ void k_cg_update(int n, double* __restrict__ x, double* __restrict__ 
                             const double* __restrict__ ap, const double* __restrict__ vol, double* pmax, double* psum,
                             unsigned* counter, CgState* s) {
     __shared__ bool last;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool skip = s->flags & 2;
     const double alpha = s->alpha;
     double m = 0, sum = 0;
-    if (i < n) {
+    bool nan = false;
+    TPA_GRID_STRIDE(i, n) {
         double ri = r[i];
         if (!skip) {
             x[i] += alpha * p[i];
@@ -136,15 +111,19 @@ __global__ void k_cg_update(int n, double* __restrict__ x, double* __restrict__ 
             r[i] = ri;
         }
         double V = vol[i];
-        if (V > 0) m = fabs(ri) / V;
-        sum = ri;
+        if (V > 0) {
+            double q = fabs(ri) / V;
+            if (q != q) nan = true;
+            m = fmax(m, q);
+        }
+        sum += ri;
     }
     // block max (NaN propagating) and block sum
     __shared__ double shm[32], shs[32];
     __shared__ int nan_seen;
     if (threadIdx.x == 0) nan_seen = 0;
     __syncthreads();
-    if (m != m) nan_seen = 1;
+    if (nan) nan_seen = 1;
     double mm = m, ss = sum;
     for (int o = 16; o; o >>= 1) {
         mm = fmax(mm, __shfl_down_sync(0xffffffffu, mm, o));
@@ -180,20 +159,53 @@ __global__ void k_cg_update(int n, double* __restrict__ x, double* __restrict__ 
     }
 }
 
+// block-structured finest level: Ap = A p and alpha
+template <int NXC>
+__global__ void s_cg_ap(SView<double> L, const double* __restrict__ p, double* __restrict__ ap, double* partial,
+                        unsigned* counter, CgState* s) {
+    s_apply_dot<double, NXC>(L, p, ap, partial, counter, [&](double pAp) { alpha_from(pAp, s); });
+}
+
+// block-structured finest level: r = b - A x, folds sum(r) into s->rsum
+template <int NXC>
+__global__ void s_cg_residual(SView<double> L, const double* __restrict__ b, const double* __restrict__ x,
+                              double* __restrict__ r, double* partial, unsigned* counter, CgState* s) {
+    double part = 0;
+    for (int bk = blockIdx.x; bk < L.nblocks; bk += gridDim.x) {
+        const int t = threadIdx.x;
+        const int i = t % Blk<NXC>::nx(L), j = t / Blk<NXC>::nx(L), c = bk * Blk<NXC>::cpb(L) + t;
+        double v = b[c] - s_apply<NXC>(L, bk, i, j, c, [&](int q) { return x[q]; });
+        r[c] = v;
+        part += v;
+    }
+    if (publish_partial(part, partial, counter)) {
+        double tt = fold_partials(partial, gridDim.x);
+        if (threadIdx.x == 0) {
+            s->rsum = tt;
+            *counter = 0;
+        }
+    }
+}
+
+template <typename T, typename F>
+void with_nxc(const SView<T>& S, F f) {
+    if (S.nx == 16 && S.ny == 16) f(std::integral_constant<int, 16>{});
+    else f(std::integral_constant<int, 0>{});
+}
+
 // z = x0 - mean, gamma_next = r'z and the stopping rules; `init` starts a run
 // (p = z, gamma = r'z).  With `set_cond`, sets the graph loop condition.
 template <typename T>
 __global__ void k_cg_z(int n, const T* __restrict__ xv, const double* mean, const double* __restrict__ r,
                        double* __restrict__ z, double* __restrict__ p, double* partial, unsigned* counter, CgState* s,
                        int init, cudaGraphConditionalHandle handle, int set_cond) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
     const double m = mean ? *mean : 0.0;
     double v = 0;
-    if (i < n) {
+    TPA_GRID_STRIDE(i, n) {
         double zi = double(xv[i]) - m;
         z[i] = zi;
         if (init) p[i] = zi;
-        v = r[i] * zi;
+        v += r[i] * zi;
     }
     if (publish_partial(v, partial, counter)) {
         double g = fold_partials(partial, gridDim.x);
@@ -346,13 +358,16 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
         if (sdev_[size_t(l)].on) {
             const SView<T>& S = (*Sp)[size_t(l)];
             const int g = S.nblocks, th = S.cpb;
-            if (l == 0) s_pre2<T, double><<<g, th, 0, stream_>>>(S, r, rsum);
-            else s_pre2<T, T><<<g, th, 0, stream_>>>(S, S.b, lsum_.p + l);
             const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
-            s_residual<T><<<g, th, 0, stream_>>>(S);
-            s_restrict<T><<<g, th, th * sizeof(T), stream_>>>(S, V[size_t(l + 1)].b, fpartial_.p,
-                                                               counters_.p + kRestrictSum,
-                                                               next_sum ? lsum_.p + l + 1 : nullptr);
+            with_nxc(S, [&](auto nxc) {
+                constexpr int N = decltype(nxc)::value;
+                if (l == 0) s_pre2<T, double, N><<<g, th, 0, stream_>>>(S, r, rsum);
+                else s_pre2<T, T, N><<<g, th, 0, stream_>>>(S, S.b, lsum_.p + l);
+                s_residual<T, N><<<g, th, 0, stream_>>>(S);
+                s_restrict<T, N><<<next_sum ? std::min(g, kMaxGrid) : g, th, th * sizeof(T), stream_>>>(
+                    S, V[size_t(l + 1)].b, fpartial_.p, counters_.p + kRestrictSum,
+                    next_sum ? lsum_.p + l + 1 : nullptr);
+            });
             launches_ += 3;
             continue;
         }
@@ -373,10 +388,14 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
         if (sdev_[size_t(l)].on) {
             const SView<T>& S = (*Sp)[size_t(l)];
             const int g = S.nblocks, th = S.cpb;
-            s_prolong<T><<<g, th, 0, stream_>>>(S, V[size_t(l + 1)].x);
-            s_post1<T><<<g, th, 0, stream_>>>(S);
             const bool want_mean = (l == 0) && L.singular;
-            s_post2<T><<<g, th, 0, stream_>>>(S, fpartial_.p, counters_.p + kPostMean, want_mean ? mean_out : nullptr);
+            with_nxc(S, [&](auto nxc) {
+                constexpr int N = decltype(nxc)::value;
+                s_prolong<T, N><<<g, th, 0, stream_>>>(S, V[size_t(l + 1)].x);
+                s_post1<T, N><<<g, th, 0, stream_>>>(S);
+                s_post2<T, N><<<want_mean ? std::min(g, kMaxGrid) : g, th, 0, stream_>>>(
+                    S, fpartial_.p, counters_.p + kPostMean, want_mean ? mean_out : nullptr);
+            });
             launches_ += 3;
             continue;
         }
@@ -399,13 +418,44 @@ void DeviceSolver::vcycle_fused(const double* r, double* z, int precision) {
     const int nl = int(levels_.size());
     double* rsum = lsum_.p;  // slot 0: level-0 RHS sum
     double* mean = lsum_.p + nl;
-    k_sum_into<<<blocks_for(n), kThreads, 0, stream_>>>(n, r, fpartial_.p, counters_.p + kRsum, rsum);
+    k_sum_into<<<reduce_grid(n), kThreads, 0, stream_>>>(n, r, fpartial_.p, counters_.p + kRsum, rsum);
     ++launches_;
     if (precision == 0) enqueue_vcycle<double>(r, rsum, mean);
     else enqueue_vcycle<float>(r, rsum, mean);
     k_z_out<<<blocks_for(n), kThreads, 0, stream_>>>(n, precision ? vf_[0].x : nullptr,
                                                       precision ? nullptr : vd_[0].x, mean, z);
     ++launches_;
+    TPA_CUDA(cudaGetLastError());
+}
+
+// One CG iteration: Ap and alpha, the x / r update, the V-cycle, z and the
+// stopping rules (which set the loop condition when `set_cond`), p = z + beta p.
+void DeviceSolver::enqueue_cg_body(int precision, cudaGraphConditionalHandle handle, int set_cond) {
+    const int n = levels_[0].n;
+    const int nl = int(levels_.size());
+    CgState* s = reinterpret_cast<CgState*>(cgs_.p);
+    double* mean = lsum_.p + nl;
+    const LevelView<double>& A = vd_[0];
+    if (sdev_[0].on)
+        with_nxc(sd_[0], [&](auto nxc) {
+            constexpr int N = decltype(nxc)::value;
+            s_cg_ap<N><<<std::min(sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, stream_>>>(sd_[0], p_.p, ap_.p,
+                                                                                       fpartial_.p, counters_.p + kCgAp, s);
+        });
+    else
+        k_cg_ap<<<reduce_grid(n), kThreads, 0, stream_>>>(A, p_.p, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
+    k_cg_update<<<reduce_grid(n), kThreads, 0, stream_>>>(n, xw_.p, r_.p, p_.p, ap_.p, A.vol, fpartial_.p,
+                                                          fpartial2_.p, counters_.p + kCgUpdate, s);
+    if (precision == 0) {
+        enqueue_vcycle<double>(r_.p, &s->rsum, mean);
+        k_cg_z<double><<<reduce_grid(n), kThreads, 0, stream_>>>(n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+                                                                counters_.p + kCgZ, s, 0, handle, set_cond);
+    } else {
+        enqueue_vcycle<float>(r_.p, &s->rsum, mean);
+        k_cg_z<float><<<reduce_grid(n), kThreads, 0, stream_>>>(n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+                                                               counters_.p + kCgZ, s, 0, handle, set_cond);
+    }
+    k_cg_p<<<blocks_for(n), kThreads, 0, stream_>>>(n, p_.p, z_.p, s);
     TPA_CUDA(cudaGetLastError());
 }
 
@@ -433,23 +483,7 @@ cudaGraphExec_t DeviceSolver::cg_graph(int precision) {
     stream_ = own_stream_;
     const int saved_launches = launches_;
     TPA_CUDA(cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    const LevelView<double>& A = vd_[0];
-    if (sdev_[0].on)
-        s_cg_ap<<<sd_[0].nblocks, sd_[0].cpb, 0, stream_>>>(sd_[0], p_.p, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
-    else
-        k_cg_ap<<<blocks_for(n), kThreads, 0, stream_>>>(A, p_.p, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
-    k_cg_update<<<blocks_for(n), kThreads, 0, stream_>>>(n, xw_.p, r_.p, p_.p, ap_.p, A.vol, fpartial_.p,
-                                                          fpartial2_.p, counters_.p + kCgUpdate, s);
-    if (precision == 0) {
-        enqueue_vcycle<double>(r_.p, &s->rsum, mean);
-        k_cg_z<double><<<blocks_for(n), kThreads, 0, stream_>>>(n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
-                                                                counters_.p + kCgZ, s, 0, handle, 1);
-    } else {
-        enqueue_vcycle<float>(r_.p, &s->rsum, mean);
-        k_cg_z<float><<<blocks_for(n), kThreads, 0, stream_>>>(n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
-                                                               counters_.p + kCgZ, s, 0, handle, 1);
-    }
-    k_cg_p<<<blocks_for(n), kThreads, 0, stream_>>>(n, p_.p, z_.p, s);
+    enqueue_cg_body(precision, handle, 1);
     cudaGraph_t captured;
     cudaError_t ce = cudaStreamEndCapture(stream_, &captured);
     stream_ = saved;
@@ -475,20 +509,23 @@ void DeviceSolver::cg_fused(int precision, double target, int itmax, int& niter,
     cudaGraphExec_t exec = cg_graph(precision);
     k_cg_set<<<1, 1, 0, stream_>>>(s, target, itmax);
     if (sdev_[0].on)
-        s_cg_residual<<<sd_[0].nblocks, sd_[0].cpb, 0, stream_>>>(sd_[0], b_.p, xw_.p, r_.p, fpartial_.p,
-                                                                  counters_.p + kCgRes, s);
+        with_nxc(sd_[0], [&](auto nxc) {
+            constexpr int N = decltype(nxc)::value;
+            s_cg_residual<N><<<std::min(sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, stream_>>>(
+                sd_[0], b_.p, xw_.p, r_.p, fpartial_.p, counters_.p + kCgRes, s);
+        });
     else
-        k_cg_residual<<<blocks_for(n), kThreads, 0, stream_>>>(vd_[0], b_.p, xw_.p, r_.p, fpartial_.p,
+        k_cg_residual<<<reduce_grid(n), kThreads, 0, stream_>>>(vd_[0], b_.p, xw_.p, r_.p, fpartial_.p,
                                                                 counters_.p + kCgRes, s);
     launches_ += 2;
     if (precision == 0) {
         enqueue_vcycle<double>(r_.p, &s->rsum, mean);
-        k_cg_z<double><<<blocks_for(n), kThreads, 0, stream_>>>(n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+        k_cg_z<double><<<reduce_grid(n), kThreads, 0, stream_>>>(n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
                                                                 counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(),
                                                                 0);
     } else {
         enqueue_vcycle<float>(r_.p, &s->rsum, mean);
-        k_cg_z<float><<<blocks_for(n), kThreads, 0, stream_>>>(n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+        k_cg_z<float><<<reduce_grid(n), kThreads, 0, stream_>>>(n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
                                                                counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(),
                                                                0);
     }
@@ -496,7 +533,19 @@ void DeviceSolver::cg_fused(int precision, double target, int itmax, int& niter,
     CgState hs;
     TPA_CUDA(cudaMemcpyAsync(&hs, s, sizeof(CgState), cudaMemcpyDeviceToHost, stream_));
     TPA_CUDA(cudaStreamSynchronize(stream_));
-    if (!(hs.flags & 8) && itmax > 0) {
+    if (!(hs.flags & 8) && itmax > 0 && std::getenv("TPAGMG_NO_GRAPH")) {
+        // the same iteration launched kernel by kernel, stopping rules read on
+        // the host after each one (profiling and diagnosis)
+        bool stop = false;
+        while (!stop) {
+            const int before = launches_;
+            enqueue_cg_body(precision, cudaGraphConditionalHandle(), 0);
+            launches_ = before + graph_body_launches_[precision];
+            TPA_CUDA(cudaMemcpyAsync(&hs, s, sizeof(CgState), cudaMemcpyDeviceToHost, stream_));
+            TPA_CUDA(cudaStreamSynchronize(stream_));
+            stop = (hs.flags & 7) || hs.iter >= hs.itmax;
+        }
+    } else if (!(hs.flags & 8) && itmax > 0) {
         TPA_CUDA(cudaGraphLaunch(exec, stream_));
         TPA_CUDA(cudaMemcpyAsync(&hs, s, sizeof(CgState), cudaMemcpyDeviceToHost, stream_));
         TPA_CUDA(cudaStreamSynchronize(stream_));
@@ -533,31 +582,32 @@ double DeviceSolver::time_fused(int which, int level, int precision, int iters) 
         using T = decltype(tag);
         const SView<T>& L = S[size_t(level)];
         const int g = L.nblocks, th = L.cpb;
-        switch (which) {
-            case 0: s_post2<T><<<g, th, 0, stream_>>>(L, fpartial_.p, counters_.p, nullptr); break;
-            case 1:
-                s_restrict<T><<<g, th, th * sizeof(T), stream_>>>(L, (sizeof(T) == 8 ? (T*)vd_[size_t(level + 1)].b
-                                                                                     : (T*)vf_[size_t(level + 1)].b),
-                                                                  fpartial_.p, counters_.p, nullptr);
-                break;
-            case 2:
-                s_prolong<T><<<g, th, 0, stream_>>>(L, (sizeof(T) == 8 ? (const T*)vd_[size_t(level + 1)].x
-                                                                      : (const T*)vf_[size_t(level + 1)].x));
-                break;
-            case 4: s_pre2<T, T><<<g, th, 0, stream_>>>(L, L.b, nullptr); break;
-            case 5: s_residual<T><<<g, th, 0, stream_>>>(L); break;
-            default: throw Error(1, "unknown kernel");
-        }
+        T* bc = sizeof(T) == 8 ? (T*)vd_[size_t(level + 1)].b : (T*)vf_[size_t(level + 1)].b;
+        const T* xc = sizeof(T) == 8 ? (const T*)vd_[size_t(level + 1)].x : (const T*)vf_[size_t(level + 1)].x;
+        with_nxc(L, [&](auto nxc) {
+            constexpr int N = decltype(nxc)::value;
+            switch (which) {
+                case 0: s_post2<T, N><<<g, th, 0, stream_>>>(L, fpartial_.p, counters_.p, nullptr); break;
+                case 1: s_restrict<T, N><<<g, th, th * sizeof(T), stream_>>>(L, bc, fpartial_.p, counters_.p, nullptr); break;
+                case 2: s_prolong<T, N><<<g, th, 0, stream_>>>(L, xc); break;
+                case 4: s_pre2<T, T, N><<<g, th, 0, stream_>>>(L, L.b, nullptr); break;
+                case 5: s_residual<T, N><<<g, th, 0, stream_>>>(L); break;
+                default: throw Error(1, "unknown kernel");
+            }
+        });
     };
     auto launch = [&]() {
         if (which == 3) {
             if (precision != 0 || level != 0) throw Error(1, "the CG operator runs in FP64 on the finest level");
             CgState* s = reinterpret_cast<CgState*>(cgs_.p);
             if (sdev_[0].on)
-                s_cg_ap<<<sd_[0].nblocks, sd_[0].cpb, 0, stream_>>>(sd_[0], p_.p, ap_.p, fpartial_.p,
-                                                                    counters_.p + kCgAp, s);
+                with_nxc(sd_[0], [&](auto nxc) {
+            constexpr int N = decltype(nxc)::value;
+            s_cg_ap<N><<<std::min(sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, stream_>>>(sd_[0], p_.p, ap_.p,
+                                                                                       fpartial_.p, counters_.p + kCgAp, s);
+        });
             else
-                k_cg_ap<<<blocks_for(vd_[0].n), kThreads, 0, stream_>>>(vd_[0], p_.p, ap_.p, fpartial_.p,
+                k_cg_ap<<<reduce_grid(vd_[0].n), kThreads, 0, stream_>>>(vd_[0], p_.p, ap_.p, fpartial_.p,
                                                                          counters_.p + kCgAp, s);
         } else if (sdev_[size_t(level)].on) {
             if (precision == 0) one_s(sd_, double(0));

@@ -1,7 +1,10 @@
-// Block-structured level kernels: one CTA per nx x ny leaf block, one thread
-// per cell, neighbours found by index arithmetic (inside the block, or in the
-// same-size neighbour block across an edge); rows next to a coarse-fine edge
-// use their exact assembled CSR row (see structure.cpp).
+// Block-structured level kernels: one CTA per nx x ny leaf block (or a capped
+// grid that strides over blocks when the kernel also folds a reduction), one
+// thread per cell, neighbours found by index arithmetic (inside the block, or
+// in the same-size neighbour block across an edge); rows next to a coarse-fine
+// edge use their exact assembled CSR row (see structure.cpp).  The block size
+// is a template parameter (NXC = 16 for 16 x 16 blocks, 0 = read at run time),
+// so the usual case indexes with shifts and masks.
 //
 // The phases are those of fused.cuh (the default V-cycle of
 // src/solvers/multigrid/cycles.jl:46-77, ronaldremmerswaal/TwoPhaseAMR.jl):
@@ -37,22 +40,34 @@ struct SView {
     int ccpb;        // cells per block on the coarser level (== cpb)
 };
 
+// compile-time block dimensions when NXC > 0
+template <int NXC>
+struct Blk {
+    template <typename T>
+    __device__ __forceinline__ static int nx(const SView<T>& L) { return NXC ? NXC : L.nx; }
+    template <typename T>
+    __device__ __forceinline__ static int ny(const SView<T>& L) { return NXC ? NXC : L.ny; }
+    template <typename T>
+    __device__ __forceinline__ static int cpb(const SView<T>& L) { return NXC ? NXC * NXC : L.cpb; }
+};
+
 template <typename T>
 __device__ __forceinline__ T s_dinv(const SView<T>& L, int c) {
     return L.dinv ? L.dinv[c] : L.dinv0;
 }
 
 // Neighbour cell indices (W, E, S, N) of cell c = b * cpb + j * nx + i, -1 if none.
-template <typename T>
+template <int NXC, typename T>
 __device__ __forceinline__ void s_neighbours(const SView<T>& L, int b, int i, int j, int c, int nb[4]) {
-    nb[0] = i > 0 ? c - 1 : (L.nbr[4 * b] >= 0 ? L.nbr[4 * b] * L.cpb + j * L.nx + (L.nx - 1) : -1);
-    nb[1] = i < L.nx - 1 ? c + 1 : (L.nbr[4 * b + 1] >= 0 ? L.nbr[4 * b + 1] * L.cpb + j * L.nx : -1);
-    nb[2] = j > 0 ? c - L.nx : (L.nbr[4 * b + 2] >= 0 ? L.nbr[4 * b + 2] * L.cpb + (L.ny - 1) * L.nx + i : -1);
-    nb[3] = j < L.ny - 1 ? c + L.nx : (L.nbr[4 * b + 3] >= 0 ? L.nbr[4 * b + 3] * L.cpb + i : -1);
+    const int nx = Blk<NXC>::nx(L), ny = Blk<NXC>::ny(L), cpb = Blk<NXC>::cpb(L);
+    nb[0] = i > 0 ? c - 1 : (L.nbr[4 * b] >= 0 ? L.nbr[4 * b] * cpb + j * nx + (nx - 1) : -1);
+    nb[1] = i < nx - 1 ? c + 1 : (L.nbr[4 * b + 1] >= 0 ? L.nbr[4 * b + 1] * cpb + j * nx : -1);
+    nb[2] = j > 0 ? c - nx : (L.nbr[4 * b + 2] >= 0 ? L.nbr[4 * b + 2] * cpb + (ny - 1) * nx + i : -1);
+    nb[3] = j < ny - 1 ? c + nx : (L.nbr[4 * b + 3] >= 0 ? L.nbr[4 * b + 3] * cpb + i : -1);
 }
 
 // (A v)_c through a value functor f(q) (the stencil, or the exception row)
-template <typename T, typename F>
+template <int NXC, typename T, typename F>
 __device__ __forceinline__ T s_apply(const SView<T>& L, int b, int i, int j, int c, F f) {
     if (L.ex) {
         int e = L.ex[c];
@@ -63,7 +78,7 @@ __device__ __forceinline__ T s_apply(const SView<T>& L, int b, int i, int j, int
         }
     }
     int nb[4];
-    s_neighbours(L, b, i, j, c, nb);
+    s_neighbours<NXC>(L, b, i, j, c, nb);
     T coef[4];
     if (L.cx) {
         coef[0] = nb[0] >= 0 ? L.cx[nb[0]] : T(0);
@@ -83,23 +98,25 @@ __device__ __forceinline__ T s_apply(const SView<T>& L, int b, int i, int j, int
 }
 
 // coarse cell that owns fine cell q (tentative transfer, block map)
-template <typename T>
+template <int NXC, typename T>
 __device__ __forceinline__ int s_owner(const SView<T>& L, int q) {
-    int b = q / L.cpb, r = q - b * L.cpb;
-    int i = r % L.nx, j = r / L.nx;
+    const int nx = Blk<NXC>::nx(L), cpb = Blk<NXC>::cpb(L);
+    int b = q / cpb, r = q - b * cpb;
+    int i = r % nx, j = r / nx;
     const int* m = L.map + 4 * b;
     int sc = m[3];
-    return m[0] * L.ccpb + (m[2] + j / sc) * L.nx + (m[1] + i / sc);
+    return m[0] * cpb + (m[2] + j / sc) * nx + (m[1] + i / sc);
 }
 
-#define TPA_S_CELL()                                  \
-    const int b = blockIdx.x, t = threadIdx.x;        \
-    const int i = t % L.nx, j = t / L.nx;             \
-    const int c = b * L.cpb + t;
+#define TPA_S_CELL(bk)                                       \
+    const int t = threadIdx.x;                               \
+    const int i = t % Blk<NXC>::nx(L), j = t / Blk<NXC>::nx(L); \
+    const int c = (bk) * Blk<NXC>::cpb(L) + t;
 
-template <typename T, typename TB>
+template <typename T, typename TB, int NXC>
 __global__ void s_pre2(SView<T> L, const TB* __restrict__ bin, const double* level_sum) {
-    TPA_S_CELL();
+    const int b = blockIdx.x;
+    TPA_S_CELL(b);
     const double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
     auto pb = [&](int q) {
         double v = double(bin[q]);
@@ -108,42 +125,48 @@ __global__ void s_pre2(SView<T> L, const TB* __restrict__ bin, const double* lev
     };
     auto x1 = [&](int q) { return L.w * s_dinv(L, q) * pb(q); };
     T bi = pb(c);
-    T ax = s_apply(L, b, i, j, c, x1);
+    T ax = s_apply<NXC>(L, b, i, j, c, x1);
     L.x[c] = x1(c) + L.w * s_dinv(L, c) * (bi - ax);
     L.bp[c] = bi;
 }
 
-template <typename T>
+template <typename T, int NXC>
 __global__ void s_residual(SView<T> L) {
-    TPA_S_CELL();
+    const int b = blockIdx.x;
+    TPA_S_CELL(b);
     const T* x = L.x;
-    T ri = L.bp[c] - s_apply(L, b, i, j, c, [&](int q) { return x[q]; });
+    T ri = L.bp[c] - s_apply<NXC>(L, b, i, j, c, [&](int q) { return x[q]; });
     L.r[c] = ri;
     L.s[c] = s_dinv(L, c) * ri;
 }
 
 // t = r - wt A s per fine cell, aggregated over the 2x2 (or 1x1) children into
-// the coarse block quadrant; optional fold of the coarse RHS sum.
-template <typename T>
+// the coarse block quadrant; optional fold of the coarse RHS sum.  Strides over
+// blocks so that the fold reads at most gridDim.x partials.
+template <typename T, int NXC>
 __global__ void s_restrict(SView<T> L, T* __restrict__ bc, double* partial, unsigned* counter, double* coarse_sum) {
-    TPA_S_CELL();
     extern __shared__ unsigned char smem_raw[];
     T* tile = reinterpret_cast<T*>(smem_raw);
     const T* sv = L.s;
-    tile[t] = L.r[c] - L.tw * s_apply(L, b, i, j, c, [&](int q) { return sv[q]; });
-    __syncthreads();
-    const int* m = L.map + 4 * b;
-    const int cb = m[0], ox = m[1], oy = m[2], sc = m[3];
+    const int nx = Blk<NXC>::nx(L), ny = Blk<NXC>::ny(L), cpb = Blk<NXC>::cpb(L);
     double part = 0;
-    if (sc == 1) {
-        T v = tile[t];
-        bc[cb * L.ccpb + t] = v;
-        part = double(v);
-    } else if (i < L.nx / 2 && j < L.ny / 2) {
-        const int f = 2 * j * L.nx + 2 * i;
-        T v = tile[f] + tile[f + 1] + tile[f + L.nx] + tile[f + L.nx + 1];
-        bc[cb * L.ccpb + (oy + j) * L.nx + (ox + i)] = v;
-        part = double(v);
+    for (int b = blockIdx.x; b < L.nblocks; b += gridDim.x) {
+        TPA_S_CELL(b);
+        __syncthreads();
+        tile[t] = L.r[c] - L.tw * s_apply<NXC>(L, b, i, j, c, [&](int q) { return sv[q]; });
+        __syncthreads();
+        const int* m = L.map + 4 * b;
+        const int cb = m[0], ox = m[1], oy = m[2], sc = m[3];
+        if (sc == 1) {
+            T v = tile[t];
+            bc[cb * cpb + t] = v;
+            part += double(v);
+        } else if (i < nx / 2 && j < ny / 2) {
+            const int f = 2 * j * nx + 2 * i;
+            T v = tile[f] + tile[f + 1] + tile[f + nx] + tile[f + nx + 1];
+            bc[cb * cpb + (oy + j) * nx + (ox + i)] = v;
+            part += double(v);
+        }
     }
     if (coarse_sum) {
         if (publish_partial(part, partial, counter)) {
@@ -157,29 +180,35 @@ __global__ void s_restrict(SView<T> L, T* __restrict__ bc, double* partial, unsi
 }
 
 // x += e - wt Dt^-1 A e with e = x_c[owner(.)], in place
-template <typename T>
+template <typename T, int NXC>
 __global__ void s_prolong(SView<T> L, const T* __restrict__ xc) {
-    TPA_S_CELL();
-    auto e = [&](int q) { return xc[s_owner(L, q)]; };
-    T ae = s_apply(L, b, i, j, c, e);
+    const int b = blockIdx.x;
+    TPA_S_CELL(b);
+    auto e = [&](int q) { return xc[s_owner<NXC>(L, q)]; };
+    T ae = s_apply<NXC>(L, b, i, j, c, e);
     L.x[c] += e(c) - L.tw * s_dinv(L, c) * ae;
 }
 
-template <typename T>
+template <typename T, int NXC>
 __global__ void s_post1(SView<T> L) {
-    TPA_S_CELL();
+    const int b = blockIdx.x;
+    TPA_S_CELL(b);
     const T* x = L.x;
-    L.y[c] = x[c] + L.w * s_dinv(L, c) * (L.bp[c] - s_apply(L, b, i, j, c, [&](int q) { return x[q]; }));
+    L.y[c] = x[c] + L.w * s_dinv(L, c) * (L.bp[c] - s_apply<NXC>(L, b, i, j, c, [&](int q) { return x[q]; }));
 }
 
-template <typename T>
+template <typename T, int NXC>
 __global__ void s_post2(SView<T> L, double* partial, unsigned* counter, double* mean_out) {
-    TPA_S_CELL();
     const T* y = L.y;
-    T v = y[c] + L.w * s_dinv(L, c) * (L.bp[c] - s_apply(L, b, i, j, c, [&](int q) { return y[q]; }));
-    L.x[c] = v;
+    double part = 0;
+    for (int b = blockIdx.x; b < L.nblocks; b += gridDim.x) {
+        TPA_S_CELL(b);
+        T v = y[c] + L.w * s_dinv(L, c) * (L.bp[c] - s_apply<NXC>(L, b, i, j, c, [&](int q) { return y[q]; }));
+        L.x[c] = v;
+        part += double(L.vol[c]) * double(v);
+    }
     if (mean_out) {
-        if (publish_partial(double(L.vol[c]) * double(v), partial, counter)) {
+        if (publish_partial(part, partial, counter)) {
             double s = fold_partials(partial, gridDim.x);
             if (threadIdx.x == 0) {
                 *mean_out = s * L.cvol_inv;
@@ -189,15 +218,19 @@ __global__ void s_post2(SView<T> L, double* partial, unsigned* counter, double* 
     }
 }
 
-// y = A x on the finest level, with the partial x'y (CG operator product) folded
-// by `fold` (called in the last block with the sum).
-template <typename T, typename Fold>
+// y = A x on the finest level with the partial x'y, folded by `fold(sum)` in the
+// last block (CG operator product)
+template <typename T, int NXC, typename Fold>
 __device__ __forceinline__ void s_apply_dot(const SView<T>& L, const T* x, T* y, double* partial, unsigned* counter,
                                             Fold fold) {
-    TPA_S_CELL();
-    T v = s_apply(L, b, i, j, c, [&](int q) { return x[q]; });
-    y[c] = v;
-    if (publish_partial(double(x[c]) * double(v), partial, counter)) {
+    double part = 0;
+    for (int b = blockIdx.x; b < L.nblocks; b += gridDim.x) {
+        TPA_S_CELL(b);
+        T v = s_apply<NXC>(L, b, i, j, c, [&](int q) { return x[q]; });
+        y[c] = v;
+        part += double(x[c]) * double(v);
+    }
+    if (publish_partial(part, partial, counter)) {
         double s = fold_partials(partial, gridDim.x);
         if (threadIdx.x == 0) {
             fold(s);
