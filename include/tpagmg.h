@@ -129,6 +129,50 @@ tpa_status tpa_solve(tpa_context* ctx, const double* rhs, double* x, double rtol
 tpa_status tpa_solve_device(tpa_context* ctx, const double* rhs, double* x, double rtol, double atol,
                             int32_t max_cycles, int32_t compatibility, int32_t precision, tpa_stats* stats);
 
+/* Batched uneven solves: solve!(x[k], solver_k, rhs[k]) for `count`
+ * independent problems, each with its own context (its own mesh, hierarchy
+ * and CUDA stream; contexts must be distinct).  The reference runs such
+ * solves one after another (one EllipticSolver per problem, elliptic_solver.jl:
+ * 628-675); here up to `workers` host threads (<= 0: 32) keep that many
+ * problems in flight on the GPU at once, each problem's CG loop a captured
+ * graph on its own stream.  rhs[k] and x[k] are host arrays in the cell order
+ * of problem k; stats and statuses (either may be NULL) receive one entry per
+ * problem.  All contexts must use one device.  device_ms (may be NULL)
+ * receives the device time from a start event, which every problem's stream
+ * waits on, to the completion of the last problem.  Returns TPA_OK when every
+ * problem succeeded, else the status of the first failed problem (its
+ * message: tpa_last_error(ctxs[k])); the other problems are still solved. */
+tpa_status tpa_solve_batched(tpa_context* const* ctxs, int32_t count, const double* const* rhs, double* const* x,
+                             double rtol, double atol, int32_t max_cycles, int32_t compatibility, int32_t precision,
+                             int32_t workers, tpa_stats* stats, tpa_status* statuses, double* device_ms);
+/* Same with device pointers (rhs[k], x[k] on the contexts' device). */
+tpa_status tpa_solve_batched_device(tpa_context* const* ctxs, int32_t count, const double* const* rhs,
+                                    double* const* x, double rtol, double atol, int32_t max_cycles,
+                                    int32_t compatibility, int32_t precision, int32_t workers, tpa_stats* stats,
+                                    tpa_status* statuses, double* device_ms);
+
+/* Reverse-mode derivative of tpa_solve (the rrule a Julia caller registers
+ * with ChainRulesCore for solve!; the reference differentiates nothing, so
+ * the forward map is that of solve!, elliptic_solver.jl:628-675, with
+ * compatibility :project).  Given the forward solution p and the cotangent
+ * pbar = dJ/dp (host arrays, cell order), it solves the adjoint system (the
+ * same symmetric operator, strong right-hand side pbar / V) and returns
+ * rhs_bar = dJ/d(strong rhs) = V lam (cells) and kappa_bar = dJ/d(face
+ * coefficient) = -lam' (dS/dkappa_f) p (interior faces, tpa_mesh_faces
+ * order).  Either output may be NULL.  rtol, atol, max_cycles and precision
+ * apply to the adjoint solve; stats describes it.  kappa_bar needs kappa > 0
+ * on faces of hanging-vertex patches (TPA_ERR_INVALID_ARG otherwise). */
+tpa_status tpa_adjoint(tpa_context* ctx, const double* p, const double* pbar, double* rhs_bar, double* kappa_bar,
+                       double rtol, double atol, int32_t max_cycles, int32_t precision, tpa_stats* stats);
+/* Same with device pointers (cell and face order, on the context's device). */
+tpa_status tpa_adjoint_device(tpa_context* ctx, const double* p, const double* pbar, double* rhs_bar,
+                              double* kappa_bar, double rtol, double atol, int32_t max_cycles, int32_t precision,
+                              tpa_stats* stats);
+/* grad_f = -lam' (dS/dkappa_f) p for given cell vectors p and lam (host
+ * arrays): the face kernel of tpa_adjoint on its own.  S is the operator of
+ * src/operators/elliptic.jl:157-257 (J' sqrt(k) K sqrt(k) J). */
+tpa_status tpa_face_coefficient_gradient(tpa_context* ctx, const double* p, const double* lam, double* grad);
+
 /* y = S x, the integrated pressure operator on the finest level
  * (FactorizedEllipticOperator mul!, elliptic.jl:1125-1180).  Host arrays. */
 tpa_status tpa_apply(tpa_context* ctx, const double* x, double* y);

@@ -1,0 +1,76 @@
+"""Batched uneven solves (256 independent two-phase problems of tree depth
+2..6) through `tpa_solve_batched`: every batched solution is bitwise the one
+its own `solve!` gives, the small problems match the oracle, and a failing
+problem is reported without stopping the others.
+
+Tolerances: batched vs single solve bit-exact (same context, deterministic
+kernels); mixed precision vs the FP64 oracle 1e-9 relative.
+"""
+import numpy as np
+import pytest
+
+from oracle.mesh import block_tree_mesh
+from oracle.operator import PoissonOperator as OOp
+from oracle.multigrid import MultigridOptions as OMG, TreeGeometricMultigrid
+from oracle.krylov import solve as osolve
+
+pytestmark = pytest.mark.gpu
+
+from tpagmg import BlockTreeMesh, EllipticSolver, PoissonOperator, solve, solve_batched  # noqa: E402
+from tpagmg import workloads as W  # noqa: E402
+from tpagmg._lib import TpaError  # noqa: E402
+
+
+def make(problems, precision="mixed"):
+    out = []
+    for p in problems:
+        m = BlockTreeMesh(**W.batch_spec(p))
+        kappa, rhs = W.batch_inputs(m, p)
+        s = EllipticSolver(PoissonOperator(m, kappa), preconditioner_options={"precision": precision})
+        out.append((p, m, kappa, rhs, s))
+    return out
+
+
+def small(count):
+    return [p for p in W.batch_problems() if p["depth"] <= 3][:count]
+
+
+def test_batched_equals_single_solves_bitwise():
+    probs = make(small(6) + [p for p in W.batch_problems() if p["depth"] == 5][:2])
+    xs = [np.zeros(m.ncells) for _, m, *_ in probs]
+    stats = solve_batched(xs, [s for *_, s in probs], [r for _, _, _, r, _ in probs], rtol=1e-10, workers=4)
+    for (p, m, kappa, rhs, s), x, st in zip(probs, xs, stats):
+        assert st.converged
+        y = np.zeros(m.ncells)
+        st1 = solve(y, s, rhs, rtol=1e-10)
+        assert st1.cycles == st.cycles
+        assert np.array_equal(x, y)
+
+
+def test_batched_small_problems_match_oracle():
+    probs = make(small(3))
+    xs = [np.zeros(m.ncells) for _, m, *_ in probs]
+    solve_batched(xs, [s for *_, s in probs], [r for _, _, _, r, _ in probs], rtol=1e-10)
+    for (p, m, kappa, rhs, s), x in zip(probs, xs):
+        oo = OOp(block_tree_mesh(**W.batch_spec(p)), kappa)
+        po, so = osolve(oo, TreeGeometricMultigrid(oo, OMG()), rhs, rtol=1e-12)
+        assert so.converged
+        assert np.max(np.abs(x - po)) <= 1e-9 * np.max(np.abs(po))
+
+
+def test_batched_reports_failed_problem_and_solves_the_rest():
+    probs = make(small(4))
+    xs = [np.zeros(m.ncells) for _, m, *_ in probs]
+    rhs = [r.copy() for _, _, _, r, _ in probs]
+    rhs[2][5] = np.nan
+    with pytest.raises(TpaError, match="problem 2"):
+        solve_batched(xs, [s for *_, s in probs], rhs, rtol=1e-10)
+    for k in (0, 1, 3):
+        assert np.any(xs[k] != 0)
+
+
+def test_batched_rejects_shared_solver():
+    probs = make(small(1))
+    _, m, _, rhs, s = probs[0]
+    with pytest.raises(ValueError):
+        solve_batched([np.zeros(m.ncells), np.zeros(m.ncells)], [s, s], [rhs, rhs])

@@ -1,8 +1,12 @@
 // C-ABI of the B200 pressure solver (declared in include/tpagmg.h).
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "../../include/tpagmg.h"
 #include "device.cuh"
@@ -16,7 +20,7 @@ struct tpa_context {
     tpa::LevelOperator op;  // fine operator before the hierarchy takes it
     tpa::Hierarchy hier;
     std::unique_ptr<tpa::DeviceSolver> dev;
-    tpa::DevArray<double> d_rhs, d_x, d_y;
+    tpa::DevArray<double> d_rhs, d_x, d_y, d_aux, d_face;
     void* user_stream = nullptr;
 };
 
@@ -61,11 +65,20 @@ void ensure_device(tpa_context* ctx) {
     if (!ctx->dev) ctx->dev.reset(new tpa::DeviceSolver(ctx->device));
     ctx->dev->set_stream(static_cast<cudaStream_t>(ctx->user_stream));
     ctx->dev->upload(ctx->hier);
+    ctx->dev->invalidate_faces();
     size_t n = size_t(ctx->dev->ncells());
     ctx->d_rhs.alloc(n);
     ctx->d_x.alloc(n);
     ctx->d_y.alloc(n);
     ctx->uploaded = true;
+}
+
+void ensure_faces(tpa_context* ctx) {
+    ensure_device(ctx);
+    if (!ctx->dev->faces_ready()) {
+        const tpa::LevelOperator& op = ctx->hier.levels[0].op;
+        ctx->dev->upload_faces(op.mesh, op.metric, op.kappa);
+    }
 }
 
 void fill_stats(const tpa::SolveStats& s, int precision, int launches, tpa_stats* out) {
@@ -85,6 +98,107 @@ void fill_stats(const tpa::SolveStats& s, int precision, int launches, tpa_stats
     out->device_ms = s.ms_total;
     out->kernel_launches = launches;
     out->precision = precision;
+}
+
+void solve_host_body(tpa_context* ctx, const double* rhs, double* x, double rtol, double atol, int32_t max_cycles,
+                     int32_t compatibility, int32_t precision, tpa_stats* stats) {
+    if (!rhs || !x) throw tpa::Error(TPA_ERR_INVALID_ARG, "null rhs or solution");
+    ensure_device(ctx);
+    size_t n = size_t(ctx->dev->ncells());
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(rhs[i])) throw tpa::Error(TPA_ERR_NONFINITE, "right-hand side must be finite");
+    cudaStream_t s = ctx->dev->stream();
+    TPA_CUDA(cudaMemcpyAsync(ctx->d_rhs.p, rhs, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    TPA_CUDA(cudaMemcpyAsync(ctx->d_x.p, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    tpa::SolveStats st;
+    ctx->dev->reset_launches();
+    ctx->dev->solve(ctx->d_rhs.p, ctx->d_x.p, rtol, atol, max_cycles, compatibility, precision, st);
+    TPA_CUDA(cudaMemcpyAsync(x, ctx->d_x.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    TPA_CUDA(cudaStreamSynchronize(s));
+    fill_stats(st, precision, ctx->dev->kernel_launches(), stats);
+}
+
+void solve_device_body(tpa_context* ctx, const double* rhs, double* x, double rtol, double atol, int32_t max_cycles,
+                       int32_t compatibility, int32_t precision, tpa_stats* stats) {
+    if (!rhs || !x) throw tpa::Error(TPA_ERR_INVALID_ARG, "null rhs or solution");
+    ensure_device(ctx);
+    tpa::SolveStats st;
+    ctx->dev->reset_launches();
+    ctx->dev->solve(rhs, x, rtol, atol, max_cycles, compatibility, precision, st);
+    fill_stats(st, precision, ctx->dev->kernel_launches(), stats);
+}
+
+// Independent problems on a pool of host threads, one context (and stream) per
+// problem.  device_ms: the device-time span from a start event that every
+// problem's stream waits on to the last problem's completion event.
+template <typename F>
+tpa_status run_batched(tpa_context* const* ctxs, int32_t count, int32_t workers, tpa_status* statuses,
+                       double* device_ms, F solve_one) {
+    if (count < 0 || (count > 0 && !ctxs)) return TPA_ERR_INVALID_ARG;
+    for (int32_t k = 0; k < count; ++k)
+        if (!ctxs[k] || ctxs[k]->device != ctxs[0]->device) return TPA_ERR_INVALID_ARG;
+    {
+        std::vector<tpa_context*> sorted(ctxs, ctxs + count);
+        std::sort(sorted.begin(), sorted.end());
+        if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end()) return TPA_ERR_INVALID_ARG;
+    }
+    if (device_ms) *device_ms = 0;
+    if (count == 0) return TPA_OK;
+    if (workers <= 0) workers = 32;
+    workers = std::min(workers, count);
+    const int dev = ctxs[0]->device;
+    cudaEvent_t start = nullptr;
+    std::vector<cudaEvent_t> done(size_t(count), nullptr);
+    if (device_ms) {
+        if (cudaSetDevice(dev) != cudaSuccess || cudaEventCreate(&start) != cudaSuccess ||
+            cudaEventRecord(start, nullptr) != cudaSuccess)
+            return TPA_ERR_CUDA;
+    }
+    std::vector<tpa_status> st(size_t(count), TPA_OK);
+    std::atomic<int32_t> next{0};
+    auto run = [&] {
+        cudaSetDevice(dev);
+        for (int32_t k = next++; k < count; k = next++) {
+            tpa_context* ctx = ctxs[k];
+            st[size_t(k)] = guard(ctx, [&] {
+                ensure_device(ctx);
+                cudaStream_t s = ctx->dev->stream();
+                if (start) TPA_CUDA(cudaStreamWaitEvent(s, start, 0));
+                solve_one(ctx, k);
+                if (start) {
+                    TPA_CUDA(cudaEventCreate(&done[size_t(k)]));
+                    TPA_CUDA(cudaEventRecord(done[size_t(k)], s));
+                }
+            });
+        }
+    };
+    std::vector<std::thread> pool;
+    try {
+        for (int32_t w = 1; w < workers; ++w) pool.emplace_back(run);
+    } catch (...) {
+        // fewer threads than asked: the workers that started (and this thread) take every problem
+    }
+    run();
+    for (auto& t : pool) t.join();
+    tpa_status first = TPA_OK;
+    for (int32_t k = 0; k < count; ++k) {
+        if (statuses) statuses[k] = st[size_t(k)];
+        if (first == TPA_OK) first = st[size_t(k)];
+    }
+    if (start) {
+        float span = 0;
+        for (int32_t k = 0; k < count; ++k) {
+            cudaEvent_t e = done[size_t(k)];
+            if (!e) continue;
+            float ms = 0;
+            if (cudaEventSynchronize(e) == cudaSuccess && cudaEventElapsedTime(&ms, start, e) == cudaSuccess)
+                span = std::max(span, ms);
+            cudaEventDestroy(e);
+        }
+        cudaEventDestroy(start);
+        *device_ms = span;
+    }
+    return first;
 }
 
 }  // namespace
@@ -108,6 +222,8 @@ void tpa_destroy(tpa_context* ctx) {
         ctx->d_rhs.free();
         ctx->d_x.free();
         ctx->d_y.free();
+        ctx->d_aux.free();
+        ctx->d_face.free();
         ctx->dev.reset();
     } catch (...) {
     }
@@ -310,38 +426,39 @@ tpa_status tpa_refresh(tpa_context* ctx, const double* face_coefficient) {
         tpa::refresh_hierarchy(ctx->hier, std::vector<double>(face_coefficient, face_coefficient + nf));
         if (ctx->uploaded) {
             ctx->dev->upload(ctx->hier);
+            ctx->dev->invalidate_faces();
         }
     });
 }
 
 tpa_status tpa_solve_device(tpa_context* ctx, const double* rhs, double* x, double rtol, double atol,
                             int32_t max_cycles, int32_t compatibility, int32_t precision, tpa_stats* stats) {
-    return guard(ctx, [&] {
-        ensure_device(ctx);
-        tpa::SolveStats st;
-        ctx->dev->reset_launches();
-        ctx->dev->solve(rhs, x, rtol, atol, max_cycles, compatibility, precision, st);
-        fill_stats(st, precision, ctx->dev->kernel_launches(), stats);
-    });
+    return guard(ctx, [&] { solve_device_body(ctx, rhs, x, rtol, atol, max_cycles, compatibility, precision, stats); });
 }
 
 tpa_status tpa_solve(tpa_context* ctx, const double* rhs, double* x, double rtol, double atol, int32_t max_cycles,
                      int32_t compatibility, int32_t precision, tpa_stats* stats) {
-    return guard(ctx, [&] {
-        if (!rhs || !x) throw tpa::Error(TPA_ERR_INVALID_ARG, "null rhs or solution");
-        ensure_device(ctx);
-        size_t n = size_t(ctx->dev->ncells());
-        for (size_t i = 0; i < n; ++i)
-            if (!std::isfinite(rhs[i])) throw tpa::Error(TPA_ERR_NONFINITE, "right-hand side must be finite");
-        cudaStream_t s = ctx->dev->stream();
-        TPA_CUDA(cudaMemcpyAsync(ctx->d_rhs.p, rhs, n * sizeof(double), cudaMemcpyHostToDevice, s));
-        TPA_CUDA(cudaMemcpyAsync(ctx->d_x.p, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
-        tpa::SolveStats st;
-        ctx->dev->reset_launches();
-        ctx->dev->solve(ctx->d_rhs.p, ctx->d_x.p, rtol, atol, max_cycles, compatibility, precision, st);
-        TPA_CUDA(cudaMemcpyAsync(x, ctx->d_x.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-        TPA_CUDA(cudaStreamSynchronize(s));
-        fill_stats(st, precision, ctx->dev->kernel_launches(), stats);
+    return guard(ctx, [&] { solve_host_body(ctx, rhs, x, rtol, atol, max_cycles, compatibility, precision, stats); });
+}
+
+tpa_status tpa_solve_batched(tpa_context* const* ctxs, int32_t count, const double* const* rhs, double* const* x,
+                             double rtol, double atol, int32_t max_cycles, int32_t compatibility, int32_t precision,
+                             int32_t workers, tpa_stats* stats, tpa_status* statuses, double* device_ms) {
+    if (count > 0 && (!rhs || !x)) return TPA_ERR_INVALID_ARG;
+    return run_batched(ctxs, count, workers, statuses, device_ms, [&](tpa_context* ctx, int32_t k) {
+        solve_host_body(ctx, rhs[k], x[k], rtol, atol, max_cycles, compatibility, precision,
+                        stats ? stats + k : nullptr);
+    });
+}
+
+tpa_status tpa_solve_batched_device(tpa_context* const* ctxs, int32_t count, const double* const* rhs,
+                                    double* const* x, double rtol, double atol, int32_t max_cycles,
+                                    int32_t compatibility, int32_t precision, int32_t workers, tpa_stats* stats,
+                                    tpa_status* statuses, double* device_ms) {
+    if (count > 0 && (!rhs || !x)) return TPA_ERR_INVALID_ARG;
+    return run_batched(ctxs, count, workers, statuses, device_ms, [&](tpa_context* ctx, int32_t k) {
+        solve_device_body(ctx, rhs[k], x[k], rtol, atol, max_cycles, compatibility, precision,
+                          stats ? stats + k : nullptr);
     });
 }
 
@@ -366,6 +483,71 @@ tpa_status tpa_vcycle(tpa_context* ctx, const double* r, double* z, int32_t prec
         TPA_CUDA(cudaMemcpyAsync(ctx->d_x.p, r, n * sizeof(double), cudaMemcpyHostToDevice, s));
         ctx->dev->vcycle(ctx->d_x.p, ctx->d_y.p, precision);
         TPA_CUDA(cudaMemcpyAsync(z, ctx->d_y.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        TPA_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+tpa_status tpa_face_coefficient_gradient(tpa_context* ctx, const double* p, const double* lam, double* grad) {
+    return guard(ctx, [&] {
+        if (!p || !lam || !grad) throw tpa::Error(TPA_ERR_INVALID_ARG, "null argument");
+        ensure_faces(ctx);
+        size_t n = size_t(ctx->dev->ncells()), nf = size_t(ctx->dev->nfaces());
+        if (ctx->d_face.n != nf) ctx->d_face.alloc(nf);
+        cudaStream_t s = ctx->dev->stream();
+        TPA_CUDA(cudaMemcpyAsync(ctx->d_x.p, p, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        TPA_CUDA(cudaMemcpyAsync(ctx->d_y.p, lam, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        ctx->dev->face_gradient(ctx->d_x.p, ctx->d_y.p, ctx->d_face.p);
+        TPA_CUDA(cudaMemcpyAsync(grad, ctx->d_face.p, nf * sizeof(double), cudaMemcpyDeviceToHost, s));
+        TPA_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+static void adjoint_on_device(tpa_context* ctx, const double* p, const double* pbar, double* rhs_bar,
+                              double* kappa_bar, double rtol, double atol, int32_t max_cycles, int32_t precision,
+                              tpa_stats* stats) {
+    ensure_faces(ctx);
+    tpa::DeviceSolver& d = *ctx->dev;
+    size_t n = size_t(d.ncells());
+    if (ctx->d_aux.n != n) ctx->d_aux.alloc(n);
+    cudaStream_t s = d.stream();
+    d.reset_launches();
+    // strong right-hand side pbar / V, zero initial adjoint state
+    d.scale_by_volume(pbar, ctx->d_rhs.p, true);
+    TPA_CUDA(cudaMemsetAsync(ctx->d_aux.p, 0, n * sizeof(double), s));
+    tpa::SolveStats st;
+    d.solve(ctx->d_rhs.p, ctx->d_aux.p, rtol, atol, max_cycles, 0, precision, st);
+    if (rhs_bar) d.scale_by_volume(ctx->d_aux.p, rhs_bar, false);
+    if (kappa_bar) d.face_gradient(p, ctx->d_aux.p, kappa_bar);
+    fill_stats(st, precision, d.kernel_launches(), stats);
+}
+
+tpa_status tpa_adjoint_device(tpa_context* ctx, const double* p, const double* pbar, double* rhs_bar,
+                              double* kappa_bar, double rtol, double atol, int32_t max_cycles, int32_t precision,
+                              tpa_stats* stats) {
+    return guard(ctx, [&] {
+        if (!p || !pbar) throw tpa::Error(TPA_ERR_INVALID_ARG, "null solution or cotangent");
+        adjoint_on_device(ctx, p, pbar, rhs_bar, kappa_bar, rtol, atol, max_cycles, precision, stats);
+    });
+}
+
+tpa_status tpa_adjoint(tpa_context* ctx, const double* p, const double* pbar, double* rhs_bar, double* kappa_bar,
+                       double rtol, double atol, int32_t max_cycles, int32_t precision, tpa_stats* stats) {
+    return guard(ctx, [&] {
+        if (!p || !pbar) throw tpa::Error(TPA_ERR_INVALID_ARG, "null solution or cotangent");
+        ensure_faces(ctx);
+        size_t n = size_t(ctx->dev->ncells()), nf = size_t(ctx->dev->nfaces());
+        for (size_t i = 0; i < n; ++i)
+            if (!std::isfinite(pbar[i]) || !std::isfinite(p[i]))
+                throw tpa::Error(TPA_ERR_NONFINITE, "solution and cotangent must be finite");
+        if (ctx->d_face.n != nf) ctx->d_face.alloc(nf);
+        cudaStream_t s = ctx->dev->stream();
+        TPA_CUDA(cudaMemcpyAsync(ctx->d_x.p, p, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        TPA_CUDA(cudaMemcpyAsync(ctx->d_y.p, pbar, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        adjoint_on_device(ctx, ctx->d_x.p, ctx->d_y.p, rhs_bar ? ctx->d_y.p : nullptr,
+                          kappa_bar ? ctx->d_face.p : nullptr, rtol, atol, max_cycles, precision, stats);
+        if (rhs_bar) TPA_CUDA(cudaMemcpyAsync(rhs_bar, ctx->d_y.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (kappa_bar)
+            TPA_CUDA(cudaMemcpyAsync(kappa_bar, ctx->d_face.p, nf * sizeof(double), cudaMemcpyDeviceToHost, s));
         TPA_CUDA(cudaStreamSynchronize(s));
     });
 }

@@ -197,6 +197,23 @@ public:
     // Levels on the block-structured path and their exception-row counts.
     int structured_levels() const;
     int64_t exception_rows() const;
+
+    // ---- adjoint (csrc/adjoint.cu) ----
+    // Finest-level faces, the inverse face metric K as CSR rows (diagonal
+    // first) and sqrt(kappa); uploaded on first use and after every refresh.
+    void upload_faces(const Mesh& mesh, const Metric& metric, const std::vector<double>& kappa);
+    bool faces_ready() const { return nfaces_ >= 0; }
+    void invalidate_faces() { nfaces_ = -1; }
+    int64_t nfaces() const { return nfaces_; }
+    // g_f = -lam' (dS/dkappa_f) p for cell vectors p, lam (device pointers).
+    void face_gradient(const double* p, const double* lam, double* g);
+    // out = in / V (invert = true) or out = in * V on the finest level.
+    void scale_by_volume(const double* in, double* out, bool invert);
+
+private:
+    int64_t nfaces_ = -1;
+    DevArray<int> f_minus_, f_plus_, k_ptr_, k_col_;
+    DevArray<double> f_area_, k_val_, f_sqrtk_;
 };
 
 }  // namespace tpa

@@ -16,7 +16,7 @@ Every solve runs on the GPU through `libtpagmg.so`; there is no CPU path.
 from .mesh import BlockTreeMesh
 from .options import LinearSolverOptions, MultigridOptions
 from .operator import PoissonOperator, mixture_density, surface_tension_jumps
-from .solver import EllipticSolver, LinearSolverStats, solve
+from .solver import EllipticSolver, LinearSolverStats, solve, solve_batched
 
 __all__ = ["BlockTreeMesh", "PoissonOperator", "MultigridOptions", "LinearSolverOptions", "EllipticSolver",
-           "LinearSolverStats", "solve", "mixture_density", "surface_tension_jumps"]
+           "LinearSolverStats", "solve", "solve_batched", "mixture_density", "surface_tension_jumps"]

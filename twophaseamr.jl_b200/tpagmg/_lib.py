@@ -70,6 +70,17 @@ SIGNATURES = {
                               C.POINTER(StatsC)]),
     "tpa_solve_device": (C.c_int32, [P, P, P, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int32,
                                      C.POINTER(StatsC)]),
+    "tpa_solve_batched": (C.c_int32, [C.POINTER(P), C.c_int32, C.POINTER(f64p), C.POINTER(f64p), C.c_double,
+                                      C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(StatsC),
+                                      i32p, f64p]),
+    "tpa_solve_batched_device": (C.c_int32, [C.POINTER(P), C.c_int32, C.POINTER(P), C.POINTER(P), C.c_double,
+                                             C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                             C.POINTER(StatsC), i32p, f64p]),
+    "tpa_adjoint": (C.c_int32, [P, f64p, f64p, f64p, f64p, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                C.POINTER(StatsC)]),
+    "tpa_adjoint_device": (C.c_int32, [P, P, P, P, P, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                                       C.POINTER(StatsC)]),
+    "tpa_face_coefficient_gradient": (C.c_int32, [P, f64p, f64p, f64p]),
     "tpa_apply": (C.c_int32, [P, f64p, f64p]),
     "tpa_vcycle": (C.c_int32, [P, f64p, f64p, C.c_int32]),
     "tpa_synchronize": (C.c_int32, [P]),

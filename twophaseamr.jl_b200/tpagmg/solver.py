@@ -156,6 +156,44 @@ class EllipticSolver:
         s.device_ms, s.restarts, s.kernel_launches = st.device_ms, st.restarts, st.kernel_launches
         return s
 
+    # -- adjoint --------------------------------------------------------------
+    def adjoint(self, p, pbar, *, rtol=1e-10, atol=0.0, max_cycles=100, precision=None):
+        """Reverse-mode derivative of `solve!` at the solution p for the
+        cotangent pbar = dJ/dp: returns (dJ/d strong rhs, dJ/d face
+        coefficient, stats of the adjoint solve)."""
+        p, pbar = _lib.f64(p), _lib.f64(pbar)
+        n, nf = self.operator.mesh.ncells, self.operator.mesh.nfaces
+        if p.shape != (n,) or pbar.shape != (n,):
+            raise ValueError("solution and cotangent must be cell fields of the solver's mesh")
+        rhs_bar = np.empty(n)
+        kappa_bar = np.empty(nf)
+        st = _lib.StatsC()
+        self.ctx.call("tpa_adjoint", _lib.ptr(p, C.c_double), _lib.ptr(pbar, C.c_double),
+                      _lib.ptr(rhs_bar, C.c_double), _lib.ptr(kappa_bar, C.c_double), float(rtol), float(atol),
+                      int(max_cycles), _PRECISION[precision or self.precision], C.byref(st))
+        return rhs_bar, kappa_bar, self._stats_from(st)
+
+    def adjoint_device(self, p_ptr, pbar_ptr, rhs_bar_ptr, kappa_bar_ptr, *, rtol=1e-10, atol=0.0, max_cycles=100,
+                       precision=None):
+        """`adjoint` on device arrays (raw CUDA pointers; either output may be 0)."""
+        st = _lib.StatsC()
+        self.ctx.call("tpa_adjoint_device", C.c_void_p(p_ptr), C.c_void_p(pbar_ptr),
+                      C.c_void_p(rhs_bar_ptr or None), C.c_void_p(kappa_bar_ptr or None), float(rtol), float(atol),
+                      int(max_cycles), _PRECISION[precision or self.precision], C.byref(st))
+        return self._stats_from(st)
+
+    def face_coefficient_gradient(self, p, lam):
+        """-lam' (dS/dkappa_f) p per interior face (the adjoint's face kernel)."""
+        p, lam = _lib.f64(p), _lib.f64(lam)
+        g = np.empty(self.operator.mesh.nfaces)
+        self.ctx.call("tpa_face_coefficient_gradient", _lib.ptr(p, C.c_double), _lib.ptr(lam, C.c_double),
+                      _lib.ptr(g, C.c_double))
+        return g
+
+    def set_stream(self, stream):
+        """Order device work after the given CUDA stream handle (int; 0 = own)."""
+        self.ctx.call("tpa_set_stream", C.c_void_p(int(stream) or None))
+
     def solve_device(self, rhs_ptr, x_ptr, *, rtol=1e-10, atol=0.0, max_cycles=100, compatibility="project",
                      precision=None):
         """`solve!` on device arrays (raw CUDA pointers, cell order)."""
@@ -169,6 +207,63 @@ def _compat(compatibility):
     if compatibility not in ("project", "error"):
         raise ValueError("compatibility must be :project or :error")
     return 0 if compatibility == "project" else 1
+
+
+class BatchResult(list):
+    """Per-problem `LinearSolverStats` of a batched solve, plus `device_ms`:
+    the device time from the batch's start to its last problem's end."""
+
+    device_ms = 0.0
+
+
+def solve_batched(solutions, solvers, rhs, *, rtol=1e-10, atol=0.0, max_cycles=100, compatibility="project",
+                  precision="mixed", workers=32):
+    """`solve!` for many independent problems at once (one `EllipticSolver`
+    per problem; solvers must be distinct).  `solutions[k]` (initial guess in,
+    solution out) and `rhs[k]` are float64 cell arrays of problem k: numpy
+    arrays, or raw CUDA pointers (ints) on the solvers' device.  Returns a
+    `BatchResult`; raises on the first failed problem after all have run."""
+    count = len(solvers)
+    if len(solutions) != count or len(rhs) != count:
+        raise ValueError("one solution and one right-hand side are required per solver")
+    if len({id(s) for s in solvers}) != count:
+        raise ValueError("every problem needs its own solver")
+    comp = _compat(compatibility)
+    device = count > 0 and isinstance(solutions[0], int)
+    if device:
+        if not all(isinstance(v, int) for v in list(solutions) + list(rhs)):
+            raise TypeError("device batches take raw pointers for every problem")
+        rp = (C.c_void_p * count)(*rhs)
+        xp = (C.c_void_p * count)(*solutions)
+        entry = "tpa_solve_batched_device"
+    else:
+        bs = [_lib.f64(b) for b in rhs]
+        for k, (x, s, b) in enumerate(zip(solutions, solvers, bs)):
+            if not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous):
+                raise TypeError("solutions must be contiguous float64 arrays")
+            n = s.operator.mesh.ncells
+            if x.shape != (n,) or b.shape != (n,):
+                raise ValueError(f"problem {k}: fields and multigrid solver must share a mesh")
+        rp = (_lib.f64p * count)(*[_lib.ptr(b, C.c_double) for b in bs])
+        xp = (_lib.f64p * count)(*[_lib.ptr(x, C.c_double) for x in solutions])
+        entry = "tpa_solve_batched"
+    ctxs = (C.c_void_p * count)(*[s.ctx.handle.value for s in solvers])
+    stats = (_lib.StatsC * count)()
+    status = np.zeros(count, dtype=np.int32)
+    span = C.c_double()
+    rc = getattr(_lib.lib(), entry)(ctxs, count, rp, xp, float(rtol), float(atol), int(max_cycles), comp,
+                                    _PRECISION[precision], int(workers), stats, _lib.ptr(status, C.c_int32),
+                                    C.byref(span))
+    if rc != _lib.TPA_OK:
+        bad = np.nonzero(status)[0]
+        if len(bad) == 0:
+            raise _lib.TpaError(int(rc), f"{entry}: invalid arguments")
+        k = int(bad[0])
+        msg = _lib.lib().tpa_last_error(solvers[k].ctx.handle).decode()
+        raise _lib.TpaError(int(rc), f"{entry}: problem {k}: {msg}")
+    out = BatchResult(s._stats_from(st) for s, st in zip(solvers, stats))
+    out.device_ms = span.value
+    return out
 
 
 def solve(solution, solver, rhs, *, rtol=1e-10, atol=0.0, max_cycles=100, compatibility="project", precision=None):

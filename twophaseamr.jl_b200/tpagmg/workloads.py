@@ -163,3 +163,39 @@ def droplet_rhs(mesh, L_psi, seed=SEEDS["droplet_amr"], noise=1.0):
     if noise:
         b = b + noise * rng(seed).standard_normal(mesh.ncells)
     return zero_mean(b, vol)
+
+
+# ---- batched uneven solves ------------------------------------------------------
+
+def batch_problems(count=256, seed=SEEDS["batch"]):
+    """Parameters of `count` independent two-phase problems on the unit square
+    with free-slip walls and base 2x2 blocks of 16x16 cells: tree depth
+    U{2..6}, circle radius U[0.05, 0.3], centre U[0.3, 0.7]^2, density ratio
+    from {10, 100, 1000} (heavy phase inside), RHS seed 404000 + k."""
+    g = rng(seed)
+    out = []
+    for k in range(count):
+        depth = int(g.integers(2, 7))
+        radius = float(g.uniform(0.05, 0.3))
+        center = (float(g.uniform(0.3, 0.7)), float(g.uniform(0.3, 0.7)))
+        ratio = float(g.choice([10.0, 100.0, 1000.0]))
+        out.append(dict(index=k, depth=depth, radius=radius, center=center, ratio=ratio, rhs_seed=seed * 1000 + k))
+    return out
+
+
+def batch_spec(problem, base=32, block=16):
+    """Mesh of one batched problem: refined to its depth in a band of 8 finest
+    cells around its circle."""
+    finest = 1.0 / (base << problem["depth"])
+    return dict(base_mesh=(base, base), block_size=(block, block), extent=(1.0, 1.0), periodic=(False, False),
+                max_level=problem["depth"],
+                refine=circle_band_refine(problem["center"], problem["radius"], 8 * finest))
+
+
+def batch_inputs(mesh, problem):
+    """Face coefficients kappa = 1/rho_f (rho = ratio inside, 1 outside) and the
+    zero-mean N(0, 1) strong right-hand side of one batched problem."""
+    from .operator import mixture_density
+    frac = circle_fractions(mesh, problem["center"], problem["radius"])
+    kappa = 1.0 / mixture_density(mesh, frac, (problem["ratio"], 1.0))
+    return kappa, gaussian_rhs(mesh, problem["rhs_seed"])
