@@ -168,6 +168,7 @@ private:
     double time_fused(int which, int level, int precision, int iters);
 
     bool fused_ok_ = false;
+    bool pdl_ = true;  // programmatic dependent launch between cycle kernels
     int tail_first_ = 0;
     std::vector<LevelView<double>> vd_;
     std::vector<LevelView<float>> vf_;

@@ -24,6 +24,16 @@ namespace tpa {
 constexpr int kTailCellsDefault = 2048;
 constexpr int kTailThreads = 1024;
 
+// First statement of every cycle kernel (programmatic dependent launch, sm_90
+// and later): allow the next kernel of the stream to be scheduled now, then wait
+// until the kernels this one depends on have completed and their writes are
+// visible.  Nothing is read or written before the wait.  For a launch without
+// the programmatic attribute both instructions return at once.
+__device__ __forceinline__ void pdl_entry() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // Pointers of one level in precision T, read by the fused kernels.
 template <typename T>
 struct LevelView {
@@ -188,6 +198,7 @@ __device__ __forceinline__ void sweep_cell(const LevelView<T>& L, const T* in, T
 // that produced b; mean = sum * cvol_inv.
 template <typename T, typename TB>
 __global__ void k_pre2(LevelView<T> L, const TB* __restrict__ b, const double* level_sum) {
+    pdl_entry();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
     if (i < L.n) pre2_cell<T, TB>(L, b, mean, i);
@@ -195,6 +206,7 @@ __global__ void k_pre2(LevelView<T> L, const TB* __restrict__ b, const double* l
 
 template <typename T>
 __global__ void k_residual(LevelView<T> L) {
+    pdl_entry();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < L.n) residual_cell(L, i);
 }
@@ -202,6 +214,7 @@ __global__ void k_residual(LevelView<T> L) {
 // b_c = P_tent'(r - wt A s); coarse RHS sum folded into `coarse_sum` when non-null.
 template <typename T>
 __global__ void k_restrict(LevelView<T> L, T* __restrict__ bc, double* partial, unsigned* counter, double* coarse_sum) {
+    pdl_entry();
     int J = blockIdx.x * blockDim.x + threadIdx.x;
     T v = T(0);
     if (J < L.nc) {
@@ -221,6 +234,7 @@ __global__ void k_restrict(LevelView<T> L, T* __restrict__ bc, double* partial, 
 
 template <typename T>
 __global__ void k_prolong(LevelView<T> L, const T* __restrict__ xc) {
+    pdl_entry();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < L.n) prolong_cell(L, xc, i);
 }
@@ -228,6 +242,7 @@ __global__ void k_prolong(LevelView<T> L, const T* __restrict__ xc) {
 // first post-sweep: y = sweep(x)
 template <typename T>
 __global__ void k_post1(LevelView<T> L) {
+    pdl_entry();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < L.n) sweep_cell(L, L.x, L.y, i);
 }
@@ -235,6 +250,7 @@ __global__ void k_post1(LevelView<T> L) {
 // second post-sweep x = sweep(y); with `mean_out`, also the volume-weighted mean
 template <typename T>
 __global__ void k_post2(LevelView<T> L, double* partial, unsigned* counter, double* mean_out) {
+    pdl_entry();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v = 0;
     if (i < L.n) {
@@ -272,6 +288,7 @@ template <typename T, typename TB>
 __global__ void __launch_bounds__(kTailThreads) k_tail(const LevelView<T>* __restrict__ levels, int first, int nl,
                                                        const TB* top_b, const double* __restrict__ G, int gn,
                                                        double* mean_out) {
+    pdl_entry();
     for (int l = first; l < nl; ++l) {
         LevelView<T> L = levels[l];
         const bool top = (l == 0);  // only the finest level reads the caller's RHS

@@ -35,9 +35,34 @@ constexpr int kMaxGrid = 1184;  // 8 CTAs on each of 148 SMs: bounds the partial
 inline int reduce_grid(int64_t n) { return int(std::min<int64_t>(blocks_for(n), kMaxGrid)); }
 #define TPA_GRID_STRIDE(i, n) for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += gridDim.x * blockDim.x)
 
+// Kernel launch on `s`, with programmatic dependent launch when `pdl`: the
+// next kernel of the cycle is scheduled while this one drains and waits in
+// pdl_entry() for its results, which hides the launch gap between the short,
+// dependent kernels of a V-cycle.
+struct Launch {
+    cudaStream_t s;
+    bool pdl;
+    template <typename... KArgs, typename... Args>
+    void operator()(void (*kernel)(KArgs...), int grid, int block, size_t smem, Args... args) const {
+        cudaLaunchConfig_t cfg;
+        std::memset(&cfg, 0, sizeof(cfg));
+        cfg.gridDim = dim3(unsigned(grid));
+        cfg.blockDim = dim3(unsigned(block));
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = pdl ? 1 : 0;
+        TPA_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
+    }
+};
+
 // r = b - A x, folds sum(r) into s->rsum
 __global__ void k_cg_residual(LevelView<double> A, const double* __restrict__ b, const double* __restrict__ x,
                               double* __restrict__ r, double* partial, unsigned* counter, CgState* s) {
+    pdl_entry();
     double v = 0;
     TPA_GRID_STRIDE(i, A.n) {
         double ri = b[i] - rowdot(A, x, i);
@@ -54,6 +79,7 @@ __global__ void k_cg_residual(LevelView<double> A, const double* __restrict__ b,
 }
 
 __global__ void k_sum_into(int n, const double* __restrict__ v, double* partial, unsigned* counter, double* out) {
+    pdl_entry();
     double acc = 0;
     TPA_GRID_STRIDE(i, n) acc += v[i];
     if (publish_partial(acc, partial, counter)) {
@@ -79,6 +105,7 @@ __device__ __forceinline__ void alpha_from(double pAp, CgState* s) {
 // Ap = A p and alpha = gamma / p'Ap with the zero-curvature guard
 __global__ void k_cg_ap(LevelView<double> A, const double* __restrict__ p, double* __restrict__ ap, double* partial,
                         unsigned* counter, CgState* s) {
+    pdl_entry();
     double v = 0;
     TPA_GRID_STRIDE(i, A.n) {
         double y = rowdot(A, p, i);
@@ -98,6 +125,7 @@ __global__ void k_cg_ap(LevelView<double> A, const double* __restrict__ p, doubl
 __global__ void k_cg_update(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
                             const double* __restrict__ ap, const double* __restrict__ vol, double* pmax, double* psum,
                             unsigned* counter, CgState* s) {
+    pdl_entry();
     __shared__ bool last;
     const bool skip = s->flags & 2;
     const double alpha = s->alpha;
@@ -163,6 +191,7 @@ __global__ void k_cg_update(int n, double* __restrict__ x, double* __restrict__ 
 template <int NXC>
 __global__ void s_cg_ap(SView<double> L, const double* __restrict__ p, double* __restrict__ ap, double* partial,
                         unsigned* counter, CgState* s) {
+    pdl_entry();
     s_apply_dot<double, NXC>(L, p, ap, partial, counter, [&](double pAp) { alpha_from(pAp, s); });
 }
 
@@ -170,6 +199,7 @@ __global__ void s_cg_ap(SView<double> L, const double* __restrict__ p, double* _
 template <int NXC>
 __global__ void s_cg_residual(SView<double> L, const double* __restrict__ b, const double* __restrict__ x,
                               double* __restrict__ r, double* partial, unsigned* counter, CgState* s) {
+    pdl_entry();
     double part = 0;
     for (int bk = blockIdx.x; bk < L.nblocks; bk += gridDim.x) {
         const int t = threadIdx.x;
@@ -199,6 +229,7 @@ template <typename T>
 __global__ void k_cg_z(int n, const T* __restrict__ xv, const double* mean, const double* __restrict__ r,
                        double* __restrict__ z, double* __restrict__ p, double* partial, unsigned* counter, CgState* s,
                        int init, cudaGraphConditionalHandle handle, int set_cond) {
+    pdl_entry();
     const double m = mean ? *mean : 0.0;
     double v = 0;
     TPA_GRID_STRIDE(i, n) {
@@ -244,12 +275,14 @@ __global__ void k_cg_z(int n, const T* __restrict__ xv, const double* mean, cons
 }
 
 __global__ void k_cg_p(int n, double* __restrict__ p, const double* __restrict__ z, const CgState* s) {
+    pdl_entry();
     if (s->flags & 6) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) p[i] = z[i] + s->beta * p[i];
 }
 
 __global__ void k_cg_set(CgState* s, double target, int itmax) {
+    pdl_entry();
     s->target = target;
     s->itmax = itmax;
     s->flags = 0;
@@ -258,6 +291,7 @@ __global__ void k_cg_set(CgState* s, double target, int itmax) {
 
 __global__ void k_z_out(int n, const float* __restrict__ xf, const double* __restrict__ xd, const double* mean,
                         double* __restrict__ z) {
+    pdl_entry();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double m = mean ? *mean : 0.0;
@@ -267,6 +301,7 @@ __global__ void k_z_out(int n, const float* __restrict__ xf, const double* __res
 }  // namespace
 
 void DeviceSolver::build_views() {
+    pdl_ = std::getenv("TPAGMG_NO_PDL") == nullptr;
     fused_ok_ = (pre_ == 2 && post_ == 2);
     for (auto& L : levels_)
         if (L.ncomp > 1) fused_ok_ = false;
@@ -338,6 +373,7 @@ void DeviceSolver::destroy_graphs() {
 // (device pointer); result in view 0's x, level-0 mean in *mean_out.
 template <typename T>
 void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* mean_out) {
+    const Launch go{stream_, pdl_};
     const int nl = int(levels_.size());
     const int t = tail_first_;
     const std::vector<LevelView<T>>* Vp;
@@ -361,26 +397,26 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
             const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
             with_nxc(S, [&](auto nxc) {
                 constexpr int N = decltype(nxc)::value;
-                if (l == 0) s_pre2<T, double, N><<<g, th, 0, stream_>>>(S, r, rsum);
-                else s_pre2<T, T, N><<<g, th, 0, stream_>>>(S, S.b, lsum_.p + l);
-                s_residual<T, N><<<g, th, 0, stream_>>>(S);
-                s_restrict<T, N><<<next_sum ? std::min(g, kMaxGrid) : g, th, th * sizeof(T), stream_>>>(
+                if (l == 0) go(s_pre2<T, double, N>, g, th, 0, S, r, rsum);
+                else go(s_pre2<T, T, N>, g, th, 0, S, S.b, lsum_.p + l);
+                go(s_residual<T, N>, g, th, 0, S);
+                go(s_restrict<T, N>, next_sum ? std::min(g, kMaxGrid) : g, th, th * sizeof(T), 
                     S, V[size_t(l + 1)].b, fpartial_.p, counters_.p + kRestrictSum,
                     next_sum ? lsum_.p + l + 1 : nullptr);
             });
             launches_ += 3;
             continue;
         }
-        if (l == 0) k_pre2<T, double><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, r, rsum);
-        else k_pre2<T, T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, L.b, lsum_.p + l);
+        if (l == 0) go(k_pre2<T, double>, blocks_for(L.n), kThreads, 0, L, r, rsum);
+        else go(k_pre2<T, T>, blocks_for(L.n), kThreads, 0, L, L.b, lsum_.p + l);
         const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
-        k_residual<T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L);
-        k_restrict<T><<<blocks_for(L.nc), kThreads, 0, stream_>>>(L, V[size_t(l + 1)].b, fpartial_.p,
+        go(k_residual<T>, blocks_for(L.n), kThreads, 0, L);
+        go(k_restrict<T>, blocks_for(L.nc), kThreads, 0, L, V[size_t(l + 1)].b, fpartial_.p,
                                                                   counters_.p + kRestrictSum,
                                                                   next_sum ? lsum_.p + l + 1 : nullptr);
         launches_ += 3;
     }
-    k_tail<T, double><<<1, kTailThreads, 0, stream_>>>(Vdev, t, nl, t == 0 ? r : nullptr, coarse_inv_.p, coarse_n_,
+    go(k_tail<T, double>, 1, kTailThreads, 0, Vdev, t, nl, t == 0 ? r : nullptr, coarse_inv_.p, coarse_n_,
                                                          t == 0 && V[0].singular ? mean_out : nullptr);
     ++launches_;
     for (int l = t - 1; l >= 0; --l) {
@@ -391,18 +427,18 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
             const bool want_mean = (l == 0) && L.singular;
             with_nxc(S, [&](auto nxc) {
                 constexpr int N = decltype(nxc)::value;
-                s_prolong<T, N><<<g, th, 0, stream_>>>(S, V[size_t(l + 1)].x);
-                s_post1<T, N><<<g, th, 0, stream_>>>(S);
-                s_post2<T, N><<<want_mean ? std::min(g, kMaxGrid) : g, th, 0, stream_>>>(
+                go(s_prolong<T, N>, g, th, 0, S, V[size_t(l + 1)].x);
+                go(s_post1<T, N>, g, th, 0, S);
+                go(s_post2<T, N>, want_mean ? std::min(g, kMaxGrid) : g, th, 0, 
                     S, fpartial_.p, counters_.p + kPostMean, want_mean ? mean_out : nullptr);
             });
             launches_ += 3;
             continue;
         }
-        k_prolong<T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, V[size_t(l + 1)].x);
-        k_post1<T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L);
+        go(k_prolong<T>, blocks_for(L.n), kThreads, 0, L, V[size_t(l + 1)].x);
+        go(k_post1<T>, blocks_for(L.n), kThreads, 0, L);
         const bool want_mean = (l == 0) && L.singular;
-        k_post2<T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, fpartial_.p, counters_.p + kPostMean,
+        go(k_post2<T>, blocks_for(L.n), kThreads, 0, L, fpartial_.p, counters_.p + kPostMean,
                                                               want_mean ? mean_out : nullptr);
         launches_ += 3;
     }
@@ -414,15 +450,16 @@ template void DeviceSolver::enqueue_vcycle<double>(const double*, const double*,
 template void DeviceSolver::enqueue_vcycle<float>(const double*, const double*, double*);
 
 void DeviceSolver::vcycle_fused(const double* r, double* z, int precision) {
+    const Launch go{stream_, pdl_};
     const int n = levels_[0].n;
     const int nl = int(levels_.size());
     double* rsum = lsum_.p;  // slot 0: level-0 RHS sum
     double* mean = lsum_.p + nl;
-    k_sum_into<<<reduce_grid(n), kThreads, 0, stream_>>>(n, r, fpartial_.p, counters_.p + kRsum, rsum);
+    go(k_sum_into, reduce_grid(n), kThreads, 0, n, r, fpartial_.p, counters_.p + kRsum, rsum);
     ++launches_;
     if (precision == 0) enqueue_vcycle<double>(r, rsum, mean);
     else enqueue_vcycle<float>(r, rsum, mean);
-    k_z_out<<<blocks_for(n), kThreads, 0, stream_>>>(n, precision ? vf_[0].x : nullptr,
+    go(k_z_out, blocks_for(n), kThreads, 0, n, precision ? vf_[0].x : nullptr,
                                                       precision ? nullptr : vd_[0].x, mean, z);
     ++launches_;
     TPA_CUDA(cudaGetLastError());
@@ -431,6 +468,7 @@ void DeviceSolver::vcycle_fused(const double* r, double* z, int precision) {
 // One CG iteration: Ap and alpha, the x / r update, the V-cycle, z and the
 // stopping rules (which set the loop condition when `set_cond`), p = z + beta p.
 void DeviceSolver::enqueue_cg_body(int precision, cudaGraphConditionalHandle handle, int set_cond) {
+    const Launch go{stream_, pdl_};
     const int n = levels_[0].n;
     const int nl = int(levels_.size());
     CgState* s = reinterpret_cast<CgState*>(cgs_.p);
@@ -439,23 +477,23 @@ void DeviceSolver::enqueue_cg_body(int precision, cudaGraphConditionalHandle han
     if (sdev_[0].on)
         with_nxc(sd_[0], [&](auto nxc) {
             constexpr int N = decltype(nxc)::value;
-            s_cg_ap<N><<<std::min(sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, stream_>>>(sd_[0], p_.p, ap_.p,
+            go(s_cg_ap<N>, std::min(sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, sd_[0], p_.p, ap_.p,
                                                                                        fpartial_.p, counters_.p + kCgAp, s);
         });
     else
-        k_cg_ap<<<reduce_grid(n), kThreads, 0, stream_>>>(A, p_.p, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
-    k_cg_update<<<reduce_grid(n), kThreads, 0, stream_>>>(n, xw_.p, r_.p, p_.p, ap_.p, A.vol, fpartial_.p,
+        go(k_cg_ap, reduce_grid(n), kThreads, 0, A, p_.p, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
+    go(k_cg_update, reduce_grid(n), kThreads, 0, n, xw_.p, r_.p, p_.p, ap_.p, A.vol, fpartial_.p,
                                                           fpartial2_.p, counters_.p + kCgUpdate, s);
     if (precision == 0) {
         enqueue_vcycle<double>(r_.p, &s->rsum, mean);
-        k_cg_z<double><<<reduce_grid(n), kThreads, 0, stream_>>>(n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+        go(k_cg_z<double>, reduce_grid(n), kThreads, 0, n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
                                                                 counters_.p + kCgZ, s, 0, handle, set_cond);
     } else {
         enqueue_vcycle<float>(r_.p, &s->rsum, mean);
-        k_cg_z<float><<<reduce_grid(n), kThreads, 0, stream_>>>(n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+        go(k_cg_z<float>, reduce_grid(n), kThreads, 0, n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
                                                                counters_.p + kCgZ, s, 0, handle, set_cond);
     }
-    k_cg_p<<<blocks_for(n), kThreads, 0, stream_>>>(n, p_.p, z_.p, s);
+    go(k_cg_p, blocks_for(n), kThreads, 0, n, p_.p, z_.p, s);
     TPA_CUDA(cudaGetLastError());
 }
 
@@ -503,29 +541,30 @@ cudaGraphExec_t DeviceSolver::cg_graph(int precision) {
 
 void DeviceSolver::cg_fused(int precision, double target, int itmax, int& niter, int& flags) {
     const int n = levels_[0].n;
+    const Launch go{stream_, pdl_};
     const int nl = int(levels_.size());
     CgState* s = reinterpret_cast<CgState*>(cgs_.p);
     double* mean = lsum_.p + nl;
     cudaGraphExec_t exec = cg_graph(precision);
-    k_cg_set<<<1, 1, 0, stream_>>>(s, target, itmax);
+    go(k_cg_set, 1, 1, 0, s, target, itmax);
     if (sdev_[0].on)
         with_nxc(sd_[0], [&](auto nxc) {
             constexpr int N = decltype(nxc)::value;
-            s_cg_residual<N><<<std::min(sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, stream_>>>(
+            go(s_cg_residual<N>, std::min(sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, 
                 sd_[0], b_.p, xw_.p, r_.p, fpartial_.p, counters_.p + kCgRes, s);
         });
     else
-        k_cg_residual<<<reduce_grid(n), kThreads, 0, stream_>>>(vd_[0], b_.p, xw_.p, r_.p, fpartial_.p,
+        go(k_cg_residual, reduce_grid(n), kThreads, 0, vd_[0], b_.p, xw_.p, r_.p, fpartial_.p,
                                                                 counters_.p + kCgRes, s);
     launches_ += 2;
     if (precision == 0) {
         enqueue_vcycle<double>(r_.p, &s->rsum, mean);
-        k_cg_z<double><<<reduce_grid(n), kThreads, 0, stream_>>>(n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+        go(k_cg_z<double>, reduce_grid(n), kThreads, 0, n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
                                                                 counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(),
                                                                 0);
     } else {
         enqueue_vcycle<float>(r_.p, &s->rsum, mean);
-        k_cg_z<float><<<reduce_grid(n), kThreads, 0, stream_>>>(n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+        go(k_cg_z<float>, reduce_grid(n), kThreads, 0, n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
                                                                counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(),
                                                                0);
     }

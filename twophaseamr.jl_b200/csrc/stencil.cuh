@@ -115,6 +115,7 @@ __device__ __forceinline__ int s_owner(const SView<T>& L, int q) {
 
 template <typename T, typename TB, int NXC>
 __global__ void s_pre2(SView<T> L, const TB* __restrict__ bin, const double* level_sum) {
+    pdl_entry();
     const int b = blockIdx.x;
     TPA_S_CELL(b);
     const double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
@@ -132,6 +133,7 @@ __global__ void s_pre2(SView<T> L, const TB* __restrict__ bin, const double* lev
 
 template <typename T, int NXC>
 __global__ void s_residual(SView<T> L) {
+    pdl_entry();
     const int b = blockIdx.x;
     TPA_S_CELL(b);
     const T* x = L.x;
@@ -145,6 +147,7 @@ __global__ void s_residual(SView<T> L) {
 // blocks so that the fold reads at most gridDim.x partials.
 template <typename T, int NXC>
 __global__ void s_restrict(SView<T> L, T* __restrict__ bc, double* partial, unsigned* counter, double* coarse_sum) {
+    pdl_entry();
     extern __shared__ unsigned char smem_raw[];
     T* tile = reinterpret_cast<T*>(smem_raw);
     const T* sv = L.s;
@@ -182,6 +185,7 @@ __global__ void s_restrict(SView<T> L, T* __restrict__ bc, double* partial, unsi
 // x += e - wt Dt^-1 A e with e = x_c[owner(.)], in place
 template <typename T, int NXC>
 __global__ void s_prolong(SView<T> L, const T* __restrict__ xc) {
+    pdl_entry();
     const int b = blockIdx.x;
     TPA_S_CELL(b);
     auto e = [&](int q) { return xc[s_owner<NXC>(L, q)]; };
@@ -191,6 +195,7 @@ __global__ void s_prolong(SView<T> L, const T* __restrict__ xc) {
 
 template <typename T, int NXC>
 __global__ void s_post1(SView<T> L) {
+    pdl_entry();
     const int b = blockIdx.x;
     TPA_S_CELL(b);
     const T* x = L.x;
@@ -199,6 +204,7 @@ __global__ void s_post1(SView<T> L) {
 
 template <typename T, int NXC>
 __global__ void s_post2(SView<T> L, double* partial, unsigned* counter, double* mean_out) {
+    pdl_entry();
     const T* y = L.y;
     double part = 0;
     for (int b = blockIdx.x; b < L.nblocks; b += gridDim.x) {
