@@ -126,7 +126,7 @@ def batch_main(args):
     from concurrent.futures import ThreadPoolExecutor
     import torch
     import torch.distributed as dist
-    from tpagmg import EllipticSolver, PoissonOperator, BlockTreeMesh, solve_batched
+    from tpagmg import BatchedSolver, EllipticSolver, PoissonOperator, BlockTreeMesh, solve_batched
     from tpagmg import workloads as W
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -156,13 +156,31 @@ def batch_main(args):
     xptr = [x_all.data_ptr() + 8 * int(o) for o in offs[:-1]]
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 
-    def step(precision):
+    def step_streams(precision):
         x_all.zero_()
         torch.cuda.synchronize()
         res = solve_batched(xptr, solvers, rptr, rtol=RTOL, precision=precision, workers=args.workers)
         assert all(st.converged for st in res)
         its = [st.cycles for st in res]
         return res.device_ms, its, sum(st.kernel_launches for st in res)
+
+    t0 = time.perf_counter()
+    merged = BatchedSolver(solvers) if args.batch_mode == "merged" else None
+    merge_s = time.perf_counter() - t0
+
+    def step_merged(precision):
+        x_all.zero_()
+        torch.cuda.synchronize()
+        st = merged.solve_device(rhs_all.data_ptr(), x_all.data_ptr(), rtol=RTOL, precision=precision)
+        assert all(s["converged"] for s in st)
+        return st[0]["device_ms"], [s["cycles"] for s in st], st[0]["kernel_launches"]
+
+    step = step_merged if merged else step_streams
+    streams_ms = None
+    if merged:
+        # the per-problem-stream path on the same problems, for comparison
+        step_streams("mixed")
+        streams_ms = step_streams("mixed")[0]
 
     for _ in range(args.warmup):
         step("mixed")
@@ -189,19 +207,27 @@ def batch_main(args):
     x64 = x_all.clone()
     step("mixed")
     errs = [float((x_all[a:b] - x64[a:b]).abs().max() / x64[a:b].abs().max()) for a, b in zip(offs[:-1], offs[1:])]
-    # end to end: host arrays through tpa_solve_batched, copies inside
+    # end to end: host arrays through the public batched entry point, copies inside
     xs = [np.zeros(n) for n in sizes]
     rh = [r for _, _, r in built]
+    xcat = np.zeros(int(offs[-1]))
+    rcat = np.concatenate(rh)
     e2e = []
     for k in range(args.steps + 1):
-        for x in xs:
-            x[:] = 0
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        res = solve_batched(xs, solvers, rh, rtol=RTOL, precision="mixed", workers=args.workers)
+        if merged:
+            xcat[:] = 0
+            res = merged.solve(xcat, rcat, rtol=RTOL, precision="mixed")
+            its = [s["cycles"] for s in res]
+        else:
+            for x in xs:
+                x[:] = 0
+            res = solve_batched(xs, solvers, rh, rtol=RTOL, precision="mixed", workers=args.workers)
+            its = [st.cycles for st in res]
         if k:
             e2e.append((time.perf_counter() - t1) * 1e3)
-    e2e_upd = float(np.dot(sizes, [st.cycles for st in res]))
+    e2e_upd = float(np.dot(sizes, its))
     t = torch.tensor([mixed_ms, fp64_ms, float(np.mean(e2e)), mixed_upd, fp64_upd, e2e_upd,
                       float(sum(sizes))], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -222,9 +248,13 @@ def batch_main(args):
         "warmup": args.warmup, "ms_per_step": mixed_ms, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic (seeded Philox)",
         "config": {"workload": f"batch_{args.batch} (base 2x2 roots of 16x16, depth U{{2..6}}, circle band)",
-                   "problems": args.batch, "fine_cells_total": cells, "workers": args.workers,
+                   "problems": args.batch, "fine_cells_total": cells, "batch_mode": args.batch_mode,
                    "parallelism": f"problems split over {world} ranks" if world > 1 else "1 GPU",
-                   "l2": "flushed between steps (256 MiB write)", "setup_s_rank0": setup_s},
+                   "l2": "flushed between steps (256 MiB write)", "setup_s_rank0": setup_s,
+                   "merge_s_rank0": merge_s,
+                   "batch_levels": merged.levels if merged else None,
+                   "tail_levels": merged.tail_levels if merged else None},
+        "per_problem_streams_ms_per_step": streams_ms,
         "time_to_tolerance_ms": {"mixed": mixed_ms, "fp64": fp64_ms, "speedup_mixed_over_fp64": fp64_ms / mixed_ms},
         "fp64_value": fp64_upd / (fp64_ms * 1e-3),
         "mixed_error_vs_fp64_max": max(errs),
@@ -252,7 +282,9 @@ def main():
     ap.add_argument("--levels", type=int, default=4)
     ap.add_argument("--workload", default="droplet_amr", choices=["droplet_amr", "uniform_2048", "batch"])
     ap.add_argument("--batch", type=int, default=256, help="problems of the batch workload")
-    ap.add_argument("--workers", type=int, default=32, help="host threads keeping batch problems in flight")
+    ap.add_argument("--workers", type=int, default=32, help="host threads of the per-problem-stream batch")
+    ap.add_argument("--batch-mode", default="merged", choices=["merged", "streams"],
+                    help="merged batch levels (one launch per phase) or one stream per problem")
     ap.add_argument("--size", type=int, default=2048, help="cells per side of the uniform workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true", help="only W warm-up and K mixed solves (for ncu)")

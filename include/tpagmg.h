@@ -151,6 +151,38 @@ tpa_status tpa_solve_batched_device(tpa_context* const* ctxs, int32_t count, con
                                     int32_t compatibility, int32_t precision, int32_t workers, tpa_stats* stats,
                                     tpa_status* statuses, double* device_ms);
 
+/* Merged batch: the hierarchies of `count` contexts (each after
+ * tpa_build_hierarchy, default cycle, one device) merged into one set of batch
+ * levels, so that one kernel launch advances a V-cycle phase of every problem
+ * (levels aligned at the coarse end; work lists of <= 256 rows that never
+ * straddle two problems; per-problem CG scalars and stopping rules; a problem
+ * that stops is frozen while the others continue).  Each problem's solve is
+ * `solve!` of its own context (elliptic_solver.jl:628-675), which the
+ * reference runs one problem at a time.  The batch copies what it needs: the
+ * contexts may be changed or destroyed afterwards (a new batch sees the
+ * change).  On failure *out still receives a handle holding the message. */
+typedef struct tpa_batch tpa_batch;
+tpa_status tpa_batch_create(tpa_batch** out, tpa_context* const* ctxs, int32_t count);
+void tpa_batch_destroy(tpa_batch* batch);
+const char* tpa_batch_last_error(const tpa_batch* batch);
+/* out = {problems, fine cells (all problems), batch levels, levels of the per-problem one-CTA tail} */
+tpa_status tpa_batch_sizes(const tpa_batch* batch, int64_t out[4]);
+/* offsets[k] = first fine cell of problem k in the concatenated arrays (count + 1 entries). */
+tpa_status tpa_batch_offsets(const tpa_batch* batch, int64_t* offsets);
+tpa_status tpa_batch_set_stream(tpa_batch* batch, void* stream);
+/* solve! of every problem: rhs and x are the problems' cell arrays concatenated
+ * in problem order (tpa_batch_offsets), host memory.  stats and statuses
+ * (NULL or one entry per problem).  A problem rejected before its solve (a
+ * nonzero mean with compatibility :error) gets a nonzero status; the others
+ * are still solved and the call returns that status. */
+tpa_status tpa_batch_solve(tpa_batch* batch, const double* rhs, double* x, double rtol, double atol,
+                           int32_t max_cycles, int32_t compatibility, int32_t precision, tpa_stats* stats,
+                           tpa_status* statuses);
+/* Same with device arrays on the batch's device. */
+tpa_status tpa_batch_solve_device(tpa_batch* batch, const double* rhs, double* x, double rtol, double atol,
+                                  int32_t max_cycles, int32_t compatibility, int32_t precision, tpa_stats* stats,
+                                  tpa_status* statuses);
+
 /* Reverse-mode derivative of tpa_solve (the rrule a Julia caller registers
  * with ChainRulesCore for solve!; the reference differentiates nothing, so
  * the forward map is that of solve!, elliptic_solver.jl:628-675, with

@@ -52,3 +52,17 @@ def test_batched_argument_checks_need_no_device():
         solve_batched([np.zeros(m.ncells), np.zeros(m.ncells)], [s, s], [rhs, rhs])
     with pytest.raises(ValueError):
         solve_batched([np.zeros(3)], [s], [rhs])
+
+
+def test_merged_batch_fails_loudly_without_a_device():
+    from tpagmg import BatchedSolver
+    from tpagmg._lib import TpaError
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    p = [q for q in W.batch_problems() if q["depth"] == 2][0]
+    m = BlockTreeMesh(**W.batch_spec(p))
+    kappa, rhs = W.batch_inputs(m, p)
+    s = EllipticSolver(PoissonOperator(m, kappa))
+    with pytest.raises(TpaError, match="CUDA device"):
+        BatchedSolver([s])

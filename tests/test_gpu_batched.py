@@ -74,3 +74,69 @@ def test_batched_rejects_shared_solver():
     _, m, _, rhs, s = probs[0]
     with pytest.raises(ValueError):
         solve_batched([np.zeros(m.ncells), np.zeros(m.ncells)], [s, s], [rhs, rhs])
+
+
+# ---- merged batch (one launch per V-cycle phase for every problem) ---------------
+
+from tpagmg import BatchedSolver  # noqa: E402
+
+
+def test_merged_batch_matches_single_solves():
+    """FP64: each merged-batch solution agrees with its own context's solve to
+    1e-10 relative (both to rtol 1e-12; the smoother weights are folded into
+    per-row arrays, so the arithmetic differs at rounding level), with the
+    same iteration counts within one; mixed precision to 1e-9."""
+    probs = make(small(5) + [p for p in W.batch_problems() if p["depth"] >= 5][:3], precision="fp64")
+    bs = BatchedSolver([s for *_, s in probs])
+    assert bs.count == len(probs) and bs.levels == max(len(s.level_sizes()) for *_, s in probs)
+    rhs = bs.concat([r for _, _, _, r, _ in probs])
+    for precision, tol in (("fp64", 1e-10), ("mixed", 1e-9)):
+        x = np.zeros(bs.ncells)
+        st = bs.solve(x, rhs, rtol=1e-12, precision=precision)
+        assert all(s["converged"] for s in st)
+        for (p, m, kappa, r, s), xk, sk in zip(probs, bs.split(x), st):
+            y = np.zeros(m.ncells)
+            s1 = solve(y, s, r, rtol=1e-12, precision=precision)
+            assert abs(s1.cycles - sk["cycles"]) <= 1
+            assert np.max(np.abs(xk - y)) <= tol * np.max(np.abs(y))
+
+
+def test_merged_batch_small_problems_match_oracle():
+    probs = make(small(3))
+    bs = BatchedSolver([s for *_, s in probs])
+    x = np.zeros(bs.ncells)
+    bs.solve(x, bs.concat([r for _, _, _, r, _ in probs]), rtol=1e-10)
+    for (p, m, kappa, rhs, s), xk in zip(probs, bs.split(x)):
+        oo = OOp(block_tree_mesh(**W.batch_spec(p)), kappa)
+        po, so = osolve(oo, TreeGeometricMultigrid(oo, OMG()), rhs, rtol=1e-12)
+        assert np.max(np.abs(xk - po)) <= 1e-9 * np.max(np.abs(po))
+
+
+def test_merged_batch_device_arrays_and_repeatability():
+    import torch
+    probs = make(small(4) + [p for p in W.batch_problems() if p["depth"] == 4][:2])
+    bs = BatchedSolver([s for *_, s in probs])
+    rhs = torch.from_numpy(bs.concat([r for _, _, _, r, _ in probs])).cuda()
+    x1 = torch.zeros(bs.ncells, dtype=torch.float64, device="cuda")
+    x2 = torch.zeros_like(x1)
+    torch.cuda.synchronize()
+    bs.solve_device(rhs.data_ptr(), x1.data_ptr(), rtol=1e-10)
+    bs.solve_device(rhs.data_ptr(), x2.data_ptr(), rtol=1e-10)
+    torch.cuda.synchronize()
+    assert torch.equal(x1, x2)
+    xh = np.zeros(bs.ncells)
+    bs.solve(xh, rhs.cpu().numpy(), rtol=1e-10)
+    assert np.array_equal(xh, x1.cpu().numpy())
+
+
+def test_merged_batch_compatibility_error_marks_one_problem():
+    probs = make(small(3))
+    bs = BatchedSolver([s for *_, s in probs])
+    rhs = [r.copy() for _, _, _, r, _ in probs]
+    rhs[1] = rhs[1] + 1.0  # nonzero volume mean
+    x = np.zeros(bs.ncells)
+    with pytest.raises(TpaError, match="problem 1"):
+        bs.solve(x, bs.concat(rhs), rtol=1e-10, compatibility="error")
+    parts = bs.split(x)
+    assert np.any(parts[0] != 0) and np.any(parts[2] != 0)
+    assert not np.any(parts[1] != 0)

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/tpagmg.h"
+#include "batch.hpp"
 #include "device.cuh"
 #include "host.hpp"
 
@@ -585,6 +586,165 @@ tpa_status tpa_device_info(tpa_context* ctx, int64_t out[4]) {
         out[1] = ctx->dev->exception_rows();
         out[2] = ctx->dev->tail_first();
         out[3] = ctx->dev->fused() ? 1 : 0;
+    });
+}
+
+}  // extern "C"
+
+struct tpa_batch {
+    int device = 0;
+    std::string error;
+    std::unique_ptr<tpa::BatchSolver> solver;
+    tpa::DevArray<double> d_rhs, d_x;
+};
+
+namespace {
+
+template <typename F>
+tpa_status bguard(tpa_batch* b, F&& f) {
+    if (!b) return TPA_ERR_INVALID_ARG;
+    try {
+        b->error.clear();
+        f();
+        return TPA_OK;
+    } catch (const tpa::Error& e) {
+        b->error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        b->error = "host allocation failed";
+        return TPA_ERR_INVALID_ARG;
+    } catch (const std::exception& e) {
+        b->error = e.what();
+        return TPA_ERR_INVALID_ARG;
+    }
+}
+
+// Solves every problem; returns the first rejected problem's error (code 0: none).
+tpa::Error batch_solve_body(tpa_batch* b, const double* rhs, double* x, double rtol, double atol, int32_t max_cycles,
+                            int32_t compatibility, int32_t precision, tpa_stats* stats, tpa_status* statuses) {
+    tpa::BatchSolver& s = *b->solver;
+    std::vector<tpa::SolveStats> st;
+    std::vector<int> status;
+    std::vector<std::string> msg;
+    s.reset_launches();
+    s.solve(rhs, x, rtol, atol, max_cycles, compatibility, precision, st, status, msg);
+    for (int k = 0; k < s.count(); ++k) {
+        if (stats) fill_stats(st[size_t(k)], precision, s.kernel_launches(), stats + k);
+        if (statuses) statuses[k] = status[size_t(k)];
+    }
+    for (int k = 0; k < s.count(); ++k)
+        if (status[size_t(k)]) return tpa::Error(status[size_t(k)], "problem " + std::to_string(k) + ": " + msg[size_t(k)]);
+    return tpa::Error(0, "");
+}
+
+}  // namespace
+
+extern "C" {
+
+tpa_status tpa_batch_create(tpa_batch** out, tpa_context* const* ctxs, int32_t count) {
+    if (!out || count <= 0 || !ctxs) return TPA_ERR_INVALID_ARG;
+    *out = nullptr;
+    tpa_batch* b = nullptr;
+    try {
+        b = new tpa_batch();
+    } catch (...) {
+        return TPA_ERR_INVALID_ARG;
+    }
+    tpa_status st = bguard(b, [&] {
+        std::vector<const tpa::Hierarchy*> hs;
+        for (int32_t k = 0; k < count; ++k) {
+            if (!ctxs[k]) throw tpa::Error(TPA_ERR_INVALID_ARG, "null context");
+            if (!ctxs[k]->have_hierarchy)
+                throw tpa::Error(TPA_ERR_STATE, "problem " + std::to_string(k) + " has no hierarchy");
+            if (ctxs[k]->device != ctxs[0]->device) throw tpa::Error(TPA_ERR_INVALID_ARG, "contexts on different devices");
+            hs.push_back(&ctxs[k]->hier);
+        }
+        int devices = 0;
+        if (cudaGetDeviceCount(&devices) != cudaSuccess || devices <= ctxs[0]->device)
+            throw tpa::Error(TPA_ERR_CUDA, "no usable CUDA device for the B200 solver");
+        b->device = ctxs[0]->device;
+        b->solver.reset(new tpa::BatchSolver(b->device, hs));
+    });
+    if (st != TPA_OK) {
+        // keep the handle so that the caller can read the message, then destroy it
+        *out = b;
+        return st;
+    }
+    *out = b;
+    return TPA_OK;
+}
+
+void tpa_batch_destroy(tpa_batch* b) {
+    if (!b) return;
+    try {
+        b->d_rhs.free();
+        b->d_x.free();
+        b->solver.reset();
+    } catch (...) {
+    }
+    delete b;
+}
+
+const char* tpa_batch_last_error(const tpa_batch* b) { return b ? b->error.c_str() : "null batch"; }
+
+tpa_status tpa_batch_sizes(const tpa_batch* cb, int64_t out[4]) {
+    auto* b = const_cast<tpa_batch*>(cb);
+    return bguard(b, [&] {
+        if (!b->solver) throw tpa::Error(TPA_ERR_STATE, "batch was not built");
+        out[0] = b->solver->count();
+        out[1] = b->solver->fine_cells();
+        out[2] = b->solver->levels();
+        out[3] = b->solver->tail_levels();
+    });
+}
+
+tpa_status tpa_batch_offsets(const tpa_batch* cb, int64_t* offsets) {
+    auto* b = const_cast<tpa_batch*>(cb);
+    return bguard(b, [&] {
+        if (!b->solver) throw tpa::Error(TPA_ERR_STATE, "batch was not built");
+        const auto& F = b->solver->offsets();
+        std::memcpy(offsets, F.data(), F.size() * sizeof(int64_t));
+    });
+}
+
+tpa_status tpa_batch_set_stream(tpa_batch* b, void* stream) {
+    return bguard(b, [&] {
+        if (!b->solver) throw tpa::Error(TPA_ERR_STATE, "batch was not built");
+        TPA_CUDA(cudaStreamSynchronize(b->solver->stream()));
+        b->solver->set_stream(static_cast<cudaStream_t>(stream));
+    });
+}
+
+tpa_status tpa_batch_solve_device(tpa_batch* b, const double* rhs, double* x, double rtol, double atol,
+                                  int32_t max_cycles, int32_t compatibility, int32_t precision, tpa_stats* stats,
+                                  tpa_status* statuses) {
+    return bguard(b, [&] {
+        if (!b->solver) throw tpa::Error(TPA_ERR_STATE, "batch was not built");
+        if (!rhs || !x) throw tpa::Error(TPA_ERR_INVALID_ARG, "null rhs or solution");
+        tpa::Error e = batch_solve_body(b, rhs, x, rtol, atol, max_cycles, compatibility, precision, stats, statuses);
+        if (e.code) throw e;
+    });
+}
+
+tpa_status tpa_batch_solve(tpa_batch* b, const double* rhs, double* x, double rtol, double atol, int32_t max_cycles,
+                           int32_t compatibility, int32_t precision, tpa_stats* stats, tpa_status* statuses) {
+    return bguard(b, [&] {
+        if (!b->solver) throw tpa::Error(TPA_ERR_STATE, "batch was not built");
+        if (!rhs || !x) throw tpa::Error(TPA_ERR_INVALID_ARG, "null rhs or solution");
+        const size_t n = size_t(b->solver->fine_cells());
+        for (size_t i = 0; i < n; ++i)
+            if (!std::isfinite(rhs[i])) throw tpa::Error(TPA_ERR_NONFINITE, "right-hand side must be finite");
+        if (b->d_rhs.n != n) b->d_rhs.alloc(n);
+        if (b->d_x.n != n) b->d_x.alloc(n);
+        cudaStream_t s = b->solver->stream();
+        TPA_CUDA(cudaSetDevice(b->device));
+        TPA_CUDA(cudaMemcpyAsync(b->d_rhs.p, rhs, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        TPA_CUDA(cudaMemcpyAsync(b->d_x.p, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        tpa::Error e = batch_solve_body(b, b->d_rhs.p, b->d_x.p, rtol, atol, max_cycles, compatibility, precision,
+                                        stats, statuses);
+        TPA_CUDA(cudaMemcpyAsync(x, b->d_x.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        TPA_CUDA(cudaStreamSynchronize(s));
+        if (e.code) throw e;
     });
 }
 

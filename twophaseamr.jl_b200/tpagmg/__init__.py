@@ -17,6 +17,8 @@ from .mesh import BlockTreeMesh
 from .options import LinearSolverOptions, MultigridOptions
 from .operator import PoissonOperator, mixture_density, surface_tension_jumps
 from .solver import EllipticSolver, LinearSolverStats, solve, solve_batched
+from .batch import BatchedSolver
 
 __all__ = ["BlockTreeMesh", "PoissonOperator", "MultigridOptions", "LinearSolverOptions", "EllipticSolver",
-           "LinearSolverStats", "solve", "solve_batched", "mixture_density", "surface_tension_jumps"]
+           "LinearSolverStats", "solve", "solve_batched", "BatchedSolver", "mixture_density",
+           "surface_tension_jumps"]

@@ -76,6 +76,16 @@ SIGNATURES = {
     "tpa_solve_batched_device": (C.c_int32, [C.POINTER(P), C.c_int32, C.POINTER(P), C.POINTER(P), C.c_double,
                                              C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                              C.POINTER(StatsC), i32p, f64p]),
+    "tpa_batch_create": (C.c_int32, [C.POINTER(P), C.POINTER(P), C.c_int32]),
+    "tpa_batch_destroy": (None, [P]),
+    "tpa_batch_last_error": (C.c_char_p, [P]),
+    "tpa_batch_sizes": (C.c_int32, [P, i64p]),
+    "tpa_batch_offsets": (C.c_int32, [P, i64p]),
+    "tpa_batch_set_stream": (C.c_int32, [P, P]),
+    "tpa_batch_solve": (C.c_int32, [P, f64p, f64p, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int32,
+                                    C.POINTER(StatsC), i32p]),
+    "tpa_batch_solve_device": (C.c_int32, [P, P, P, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int32,
+                                           C.POINTER(StatsC), i32p]),
     "tpa_adjoint": (C.c_int32, [P, f64p, f64p, f64p, f64p, C.c_double, C.c_double, C.c_int32, C.c_int32,
                                 C.POINTER(StatsC)]),
     "tpa_adjoint_device": (C.c_int32, [P, P, P, P, P, C.c_double, C.c_double, C.c_int32, C.c_int32,
