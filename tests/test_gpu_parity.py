@@ -216,3 +216,38 @@ def test_refresh_matches_rebuild():
     solve(a, s, rhs, rtol=1e-12)
     solve(b, fresh, rhs, rtol=1e-12)
     assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b))
+
+
+@pytest.mark.parametrize("spec", [W.taylor_green_spec(), dict(base_mesh=(64, 64), block_size=(16, 16),
+                                                              periodic=(False, False)),
+                                  dict(base_mesh=(256, 128), block_size=(16, 16), periodic=(True, False))],
+                         ids=["periodic_128", "walls_64", "channel_256x128"])
+def test_vectorized_levels_match_scalar_stencil(spec, monkeypatch):
+    """The vectorized constant-coefficient kernels (4-cell quads, walls and
+    periodic edges) give the V-cycle, CG operator and solution of the
+    one-thread-per-cell stencil kernels and of the oracle."""
+    m = BlockTreeMesh(**spec)
+    s = EllipticSolver(PoissonOperator(m), multigrid=MultigridOptions(coarse_size=64))
+    assert s.device_info()["structured_levels"] >= 1
+    monkeypatch.setenv("TPAGMG_NO_VEC", "1")
+    s2 = EllipticSolver(PoissonOperator(m), multigrid=MultigridOptions(coarse_size=64))
+    monkeypatch.delenv("TPAGMG_NO_VEC")
+    rng = np.random.default_rng(4)
+    vol = m.cell_volumes()
+    r = rng.standard_normal(m.ncells) * vol
+    r -= vol * np.sum(r) / np.sum(vol)
+    for precision, tol in (("fp64", 1e-12), ("mixed", 1e-5)):
+        z, z2 = s.vcycle(r, precision=precision), s2.vcycle(r, precision=precision)
+        assert np.max(np.abs(z - z2)) <= tol * np.max(np.abs(z2))
+    rhs = W.gaussian_rhs(m, 5)
+    x, x2 = np.zeros(m.ncells), np.zeros(m.ncells)
+    st, st2 = solve(x, s, rhs, rtol=1e-12), solve(x2, s2, rhs, rtol=1e-12)
+    assert st.converged and abs(st.cycles - st2.cycles) <= 1
+    assert np.max(np.abs(x - x2)) <= 1e-10 * np.max(np.abs(x2))
+    o = block_tree_mesh(**spec)
+    oo = OOp(o, np.ones(m.nfaces))
+    po, so = osolve(oo, TreeGeometricMultigrid(oo, OMG(coarse_size=64)), rhs, rtol=1e-12)
+    assert np.max(np.abs(x - po)) <= 1e-10 * np.max(np.abs(po))
+    xm = np.zeros(m.ncells)
+    assert solve(xm, s, rhs, rtol=1e-10, precision="mixed").converged
+    assert np.max(np.abs(xm - po)) <= 1e-9 * np.max(np.abs(po))

@@ -10,6 +10,7 @@
 #include "fused.cuh"
 #include "host.hpp"
 #include "stencil.cuh"
+#include "stencil4.cuh"
 #include "structure.hpp"
 
 namespace tpa {
@@ -183,6 +184,7 @@ private:
     // block-structured level data (stencil + exception rows)
     struct StructDev {
         bool on = false;
+        bool vec = false;  // constant-coefficient 16x16 level: vectorized quad kernels (stencil4.cuh)
         DevArray<int> nbr, ex, ex_ptr, ex_col, map;
         DevArray<double> cx_d, cy_d, exv_d;
         DevArray<float> cx_f, cy_f, exv_f;

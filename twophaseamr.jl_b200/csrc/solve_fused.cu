@@ -217,6 +217,45 @@ __global__ void s_cg_residual(SView<double> L, const double* __restrict__ b, con
     }
 }
 
+// constant-coefficient 16x16 finest level: Ap = A p and alpha (vectorized quads)
+__global__ void __launch_bounds__(256) v_cg_ap(SView<double> L, const double* __restrict__ p,
+                                               double* __restrict__ ap, double* partial, unsigned* counter,
+                                               CgState* s) {
+    pdl_entry();
+    v_apply_dot(L, p, ap, partial, counter, [&](double pAp) { alpha_from(pAp, s); });
+}
+
+// constant-coefficient 16x16 finest level: r = b - A x, folds sum(r) into s->rsum
+__global__ void __launch_bounds__(256) v_cg_residual(SView<double> L, const double* __restrict__ b,
+                                                     const double* __restrict__ x, double* __restrict__ r,
+                                                     double* partial, unsigned* counter, CgState* s) {
+    pdl_entry();
+    const int groups = (L.nblocks + 3) / 4;
+    double part = 0;
+    for (int grp = blockIdx.x; grp < groups; grp += gridDim.x) {
+        const QPos p = q_pos(grp);
+        const bool valid = p.b < L.nblocks;
+        const QNb<double> g =
+            q_gather<double>(L, p, valid, [&](int c) { return q_ldv(x + c); }, [](double v, int) { return v; });
+        if (!valid) continue;
+        const Quad<double> ax = q_apply(L, g);
+        const Quad<double> bb = q_ldv(b + p.c);
+        Quad<double> rr;
+        for (int m = 0; m < 4; ++m) {
+            rr.v[m] = bb.v[m] - ax.v[m];
+            part += rr.v[m];
+        }
+        q_st(r + p.c, rr);
+    }
+    if (publish_partial(part, partial, counter)) {
+        double tt = fold_partials(partial, gridDim.x);
+        if (threadIdx.x == 0) {
+            s->rsum = tt;
+            *counter = 0;
+        }
+    }
+}
+
 template <typename T, typename F>
 void with_nxc(const SView<T>& S, F f) {
     if (S.nx == 16 && S.ny == 16) f(std::integral_constant<int, 16>{});
@@ -391,6 +430,18 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
     else Sp = &sf_;
     for (int l = 0; l < t; ++l) {
         const LevelView<T>& L = V[size_t(l)];
+        if (sdev_[size_t(l)].vec) {
+            const SView<T>& S = (*Sp)[size_t(l)];
+            const int groups = (S.nblocks + 3) / 4;
+            const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
+            if (l == 0) go(v_pre2<T, double>, groups, 256, 0, S, r, rsum);
+            else go(v_pre2<T, T>, groups, 256, 0, S, S.b, lsum_.p + l);
+            go(v_residual<T>, groups, 256, 0, S);
+            go(v_restrict<T>, next_sum ? std::min(groups, kMaxGrid) : groups, 256, 0, S, V[size_t(l + 1)].b,
+               fpartial_.p, counters_.p + kRestrictSum, next_sum ? lsum_.p + l + 1 : nullptr);
+            launches_ += 3;
+            continue;
+        }
         if (sdev_[size_t(l)].on) {
             const SView<T>& S = (*Sp)[size_t(l)];
             const int g = S.nblocks, th = S.cpb;
@@ -421,6 +472,20 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
     ++launches_;
     for (int l = t - 1; l >= 0; --l) {
         const LevelView<T>& L = V[size_t(l)];
+        if (sdev_[size_t(l)].vec) {
+            const SView<T>& S = (*Sp)[size_t(l)];
+            const int groups = (S.nblocks + 3) / 4;
+            const bool want_mean = (l == 0) && L.singular;
+            go(v_prolong<T>, groups, 256, 0, S, V[size_t(l + 1)].x);
+            go(v_sweep<T, false>, groups, 256, 0, S, S.x, S.y, nullptr, nullptr, nullptr);
+            if (want_mean)
+                go(v_sweep<T, true>, std::min(groups, kMaxGrid), 256, 0, S, S.y, S.x, fpartial_.p,
+                   counters_.p + kPostMean, mean_out);
+            else
+                go(v_sweep<T, false>, groups, 256, 0, S, S.y, S.x, nullptr, nullptr, nullptr);
+            launches_ += 3;
+            continue;
+        }
         if (sdev_[size_t(l)].on) {
             const SView<T>& S = (*Sp)[size_t(l)];
             const int g = S.nblocks, th = S.cpb;
@@ -474,7 +539,10 @@ void DeviceSolver::enqueue_cg_body(int precision, cudaGraphConditionalHandle han
     CgState* s = reinterpret_cast<CgState*>(cgs_.p);
     double* mean = lsum_.p + nl;
     const LevelView<double>& A = vd_[0];
-    if (sdev_[0].on)
+    if (sdev_[0].vec)
+        go(v_cg_ap, std::min((sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0, sd_[0], p_.p, ap_.p, fpartial_.p,
+           counters_.p + kCgAp, s);
+    else if (sdev_[0].on)
         with_nxc(sd_[0], [&](auto nxc) {
             constexpr int N = decltype(nxc)::value;
             go(s_cg_ap<N>, std::min(sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, sd_[0], p_.p, ap_.p,
@@ -547,7 +615,10 @@ void DeviceSolver::cg_fused(int precision, double target, int itmax, int& niter,
     double* mean = lsum_.p + nl;
     cudaGraphExec_t exec = cg_graph(precision);
     go(k_cg_set, 1, 1, 0, s, target, itmax);
-    if (sdev_[0].on)
+    if (sdev_[0].vec)
+        go(v_cg_residual, std::min((sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0, sd_[0], b_.p, xw_.p, r_.p,
+           fpartial_.p, counters_.p + kCgRes, s);
+    else if (sdev_[0].on)
         with_nxc(sd_[0], [&](auto nxc) {
             constexpr int N = decltype(nxc)::value;
             go(s_cg_residual<N>, std::min(sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, 
@@ -623,6 +694,18 @@ double DeviceSolver::time_fused(int which, int level, int precision, int iters) 
         const int g = L.nblocks, th = L.cpb;
         T* bc = sizeof(T) == 8 ? (T*)vd_[size_t(level + 1)].b : (T*)vf_[size_t(level + 1)].b;
         const T* xc = sizeof(T) == 8 ? (const T*)vd_[size_t(level + 1)].x : (const T*)vf_[size_t(level + 1)].x;
+        if (sdev_[size_t(level)].vec) {
+            const int groups = (L.nblocks + 3) / 4;
+            switch (which) {
+                case 0: v_sweep<T, false><<<groups, 256, 0, stream_>>>(L, L.y, L.x, nullptr, nullptr, nullptr); break;
+                case 1: v_restrict<T><<<groups, 256, 0, stream_>>>(L, bc, fpartial_.p, counters_.p, nullptr); break;
+                case 2: v_prolong<T><<<groups, 256, 0, stream_>>>(L, xc); break;
+                case 4: v_pre2<T, T><<<groups, 256, 0, stream_>>>(L, L.b, nullptr); break;
+                case 5: v_residual<T><<<groups, 256, 0, stream_>>>(L); break;
+                default: throw Error(1, "unknown kernel");
+            }
+            return;
+        }
         with_nxc(L, [&](auto nxc) {
             constexpr int N = decltype(nxc)::value;
             switch (which) {
@@ -639,12 +722,16 @@ double DeviceSolver::time_fused(int which, int level, int precision, int iters) 
         if (which == 3) {
             if (precision != 0 || level != 0) throw Error(1, "the CG operator runs in FP64 on the finest level");
             CgState* s = reinterpret_cast<CgState*>(cgs_.p);
-            if (sdev_[0].on)
+            if (sdev_[0].vec)
+                v_cg_ap<<<std::min((sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0, stream_>>>(sd_[0], p_.p, ap_.p,
+                                                                                          fpartial_.p,
+                                                                                          counters_.p + kCgAp, s);
+            else if (sdev_[0].on)
                 with_nxc(sd_[0], [&](auto nxc) {
-            constexpr int N = decltype(nxc)::value;
-            s_cg_ap<N><<<std::min(sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, stream_>>>(sd_[0], p_.p, ap_.p,
-                                                                                       fpartial_.p, counters_.p + kCgAp, s);
-        });
+                    constexpr int N = decltype(nxc)::value;
+                    s_cg_ap<N><<<std::min(sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, stream_>>>(
+                        sd_[0], p_.p, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
+                });
             else
                 k_cg_ap<<<reduce_grid(vd_[0].n), kThreads, 0, stream_>>>(vd_[0], p_.p, ap_.p, fpartial_.p,
                                                                          counters_.p + kCgAp, s);
@@ -699,6 +786,7 @@ void DeviceSolver::upload_structured(const Hierarchy& h) {
         if (!all && !(st.const_coef && st.nex == 0)) continue;
         StructDev& D = sdev_[size_t(l)];
         D.on = true;
+        D.vec = st.const_coef && st.nex == 0 && st.nx == 16 && st.ny == 16 && !std::getenv("TPAGMG_NO_VEC");
         D.nex = st.nex;
         D.const_coef = st.const_coef;
         D.const_diag = st.const_diag;
