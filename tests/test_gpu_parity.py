@@ -218,10 +218,10 @@ def test_refresh_matches_rebuild():
     assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b))
 
 
-@pytest.mark.parametrize("spec", [W.taylor_green_spec(), dict(base_mesh=(64, 64), block_size=(16, 16),
+@pytest.mark.parametrize("spec", [W.taylor_green_spec(), dict(base_mesh=(128, 128), block_size=(16, 16),
                                                               periodic=(False, False)),
                                   dict(base_mesh=(256, 128), block_size=(16, 16), periodic=(True, False))],
-                         ids=["periodic_128", "walls_64", "channel_256x128"])
+                         ids=["periodic_128", "walls_128", "channel_256x128"])
 def test_vectorized_levels_match_scalar_stencil(spec, monkeypatch):
     """The vectorized constant-coefficient kernels (4-cell quads, walls and
     periodic edges) give the V-cycle, CG operator and solution of the

@@ -339,12 +339,12 @@ void BatchSolver::build(const std::vector<const Hierarchy*>& hs) {
     }
     L_ = Lmax;
     // tail: the last T batch levels, every problem's share of each at most
-    // kTailCellsDefault cells, and no problem's finest level among them
+    // kBatchTailCells cells, and no problem's finest level among them
     int T = std::min(kBatchTailLevels, Lmax);
     for (const Hierarchy* h : hs) {
         const int Lk = int(h->levels.size());
         int t = 0;
-        while (t < Lk - 1 && t < kBatchTailLevels && h->levels[size_t(Lk - 1 - t)].op.A.n <= kTailCellsDefault) ++t;
+        while (t < Lk - 1 && t < kBatchTailLevels && h->levels[size_t(Lk - 1 - t)].op.A.n <= kBatchTailCells) ++t;
         T = std::min(T, std::max(t, 1));
         if (Lk < 2) T = 1;
     }

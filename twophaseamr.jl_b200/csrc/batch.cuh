@@ -29,6 +29,7 @@ namespace tpa {
 constexpr int kItemRows = 256;
 constexpr int kNoExt = INT_MIN;
 constexpr int kBatchTailLevels = 4;
+constexpr int kBatchTailCells = 2048;  // per problem, for its one-CTA tail
 
 // rows [begin, end) of problem `prob`; delta != kNoExt on a problem's finest
 // level, where fine-space index = row + delta

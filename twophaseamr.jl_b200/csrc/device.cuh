@@ -171,6 +171,7 @@ private:
     bool fused_ok_ = false;
     bool pdl_ = true;  // programmatic dependent launch between cycle kernels
     int tail_first_ = 0;
+    int tail_ctas_ = 1;  // CTAs of the coarse-tail cluster
     std::vector<LevelView<double>> vd_;
     std::vector<LevelView<float>> vf_;
     DevArray<LevelView<double>> vd_dev_;

@@ -16,12 +16,18 @@
 // fixed-order fold: results do not depend on block scheduling).
 #pragma once
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 namespace tpa {
 
-// Levels at or below this many cells run inside one CTA (tunable: TPAGMG_TAIL_CELLS).
+// Levels at or below this many cells run in the coarse tail, one cluster of
+// kTailCtasDefault CTAs of kTailThreads threads (TPAGMG_TAIL_CELLS, TPAGMG_TAIL_CTAS).
+// Measured on the B200 (droplet AMR and uniform 2048^2 solves): the tail is bound
+// by the latency of its dependent loads, so more CTAs or a larger tail (4096 to
+// 32768 cells, 4 or 8 CTAs) were 2-15 % slower than 2048 cells in one CTA.
 constexpr int kTailCellsDefault = 2048;
+constexpr int kTailCtasDefault = 1;
 constexpr int kTailThreads = 1024;
 
 // First statement of every cycle kernel (programmatic dependent launch, sm_90
@@ -269,17 +275,27 @@ __global__ void k_post2(LevelView<T> L, double* partial, unsigned* counter, doub
 }
 
 // ---------------------------------------------------------------------------------
-// single-CTA tail: levels first..nl-1
+// coarse tail: levels first..nl-1 in one thread-block cluster (a launch without
+// clusters is the one-CTA case).  The CTAs stride the rows of each phase together
+// and meet at the hardware cluster barrier between phases (release/acquire at
+// cluster scope, which orders their global writes); sums go through distributed
+// shared memory in rank order, so every CTA folds the same total.
 
 template <typename T>
 __device__ double tail_sum(const T* v, const T* w, int n) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int nb = int(cl.num_blocks());
     double acc = 0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += w ? double(w[i]) * double(v[i]) : double(v[i]);
-    __syncthreads();
-    double s = block_sum_all(acc);
-    __shared__ double total;
-    if (threadIdx.x == 0) total = s;
-    __syncthreads();
+    for (int i = int(cl.block_rank()) * blockDim.x + threadIdx.x; i < n; i += nb * blockDim.x)
+        acc += w ? double(w[i]) * double(v[i]) : double(v[i]);
+    const double s = block_sum_all(acc);
+    __shared__ double part;
+    if (threadIdx.x == 0) part = s;
+    cl.sync();
+    double total = 0;
+    for (int r = 0; r < nb; ++r) total += *cl.map_shared_rank(&part, r);
+    cl.sync();  // every CTA has read `part` before the next sum overwrites it
     return total;
 }
 
@@ -288,7 +304,11 @@ template <typename T, typename TB>
 __global__ void __launch_bounds__(kTailThreads) k_tail(const LevelView<T>* __restrict__ levels, int first, int nl,
                                                        const TB* top_b, const double* __restrict__ G, int gn,
                                                        double* mean_out) {
+    namespace cg = cooperative_groups;
     pdl_entry();
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = int(cl.block_rank()), nb = int(cl.num_blocks());
+    const int gt = rank * blockDim.x + threadIdx.x, gs = nb * blockDim.x;
     for (int l = first; l < nl; ++l) {
         LevelView<T> L = levels[l];
         const bool top = (l == 0);  // only the finest level reads the caller's RHS
@@ -299,48 +319,49 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(const LevelView<T>* __res
         }
         if (l == nl - 1) {
             // projected RHS, then the dense (augmented) coarse solve in FP64
-            for (int i = threadIdx.x; i < L.n; i += blockDim.x)
+            for (int i = gt; i < L.n; i += gs)
                 L.bp[i] = top ? proj_b<T, TB>(L, top_b, mean, i) : proj_b<T, T>(L, L.b, mean, i);
-            __syncthreads();
+            cl.sync();
             // one warp per row, lanes striding the row: coalesced reads of G
-            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-            for (int i = warp; i < gn; i += nwarps) {
+            const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+            const int warp = rank * nwarps + (threadIdx.x >> 5);
+            for (int i = warp; i < gn; i += nb * nwarps) {
                 const double* row = G + size_t(i) * gn;
                 double acc = 0;
                 for (int k = lane; k < gn; k += 32) acc += row[k] * double(L.bp[k]);
                 for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
                 if (!lane) L.x[i] = T(acc);
             }
-            __syncthreads();
+            cl.sync();
             break;
         }
-        for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+        for (int i = gt; i < L.n; i += gs) {
             if (top) pre2_cell<T, TB>(L, top_b, mean, i);
             else pre2_cell<T, T>(L, L.b, mean, i);
         }
-        __syncthreads();
-        for (int i = threadIdx.x; i < L.n; i += blockDim.x) residual_cell(L, i);
-        __syncthreads();
+        cl.sync();
+        for (int i = gt; i < L.n; i += gs) residual_cell(L, i);
+        cl.sync();
         T* bc = levels[l + 1].b;
-        for (int J = threadIdx.x; J < L.nc; J += blockDim.x) bc[J] = restrict_cell(L, J);
-        __syncthreads();
+        for (int J = gt; J < L.nc; J += gs) bc[J] = restrict_cell(L, J);
+        cl.sync();
     }
     for (int l = nl - 2; l >= first; --l) {
         LevelView<T> L = levels[l];
         const T* xc = levels[l + 1].x;
-        for (int i = threadIdx.x; i < L.n; i += blockDim.x) prolong_cell(L, xc, i);
-        __syncthreads();
-        for (int i = threadIdx.x; i < L.n; i += blockDim.x) sweep_cell(L, L.x, L.y, i);
-        __syncthreads();
-        for (int i = threadIdx.x; i < L.n; i += blockDim.x) sweep_cell(L, L.y, L.x, i);
-        __syncthreads();
+        for (int i = gt; i < L.n; i += gs) prolong_cell(L, xc, i);
+        cl.sync();
+        for (int i = gt; i < L.n; i += gs) sweep_cell(L, L.x, L.y, i);
+        cl.sync();
+        for (int i = gt; i < L.n; i += gs) sweep_cell(L, L.y, L.x, i);
+        cl.sync();
     }
     if (mean_out && first == 0) {
         LevelView<T> L = levels[0];
         if (L.singular) {
             double s = tail_sum(L.x, L.vol, L.n);
-            if (threadIdx.x == 0) *mean_out = s * L.cvol_inv;
-        } else if (threadIdx.x == 0) {
+            if (gt == 0) *mean_out = s * L.cvol_inv;
+        } else if (gt == 0) {
             *mean_out = 0;
         }
     }

@@ -42,6 +42,7 @@ inline int reduce_grid(int64_t n) { return int(std::min<int64_t>(blocks_for(n), 
 struct Launch {
     cudaStream_t s;
     bool pdl;
+    int cluster = 1;  // CTAs per thread-block cluster (grid must be a multiple)
     template <typename... KArgs, typename... Args>
     void operator()(void (*kernel)(KArgs...), int grid, int block, size_t smem, Args... args) const {
         cudaLaunchConfig_t cfg;
@@ -50,11 +51,22 @@ struct Launch {
         cfg.blockDim = dim3(unsigned(block));
         cfg.dynamicSmemBytes = smem;
         cfg.stream = s;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cudaLaunchAttribute at[2];
+        unsigned na = 0;
+        if (pdl) {
+            at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            at[na].val.programmaticStreamSerializationAllowed = 1;
+            ++na;
+        }
+        if (cluster > 1) {
+            at[na].id = cudaLaunchAttributeClusterDimension;
+            at[na].val.clusterDim.x = unsigned(cluster);
+            at[na].val.clusterDim.y = 1;
+            at[na].val.clusterDim.z = 1;
+            ++na;
+        }
         cfg.attrs = at;
-        cfg.numAttrs = pdl ? 1 : 0;
+        cfg.numAttrs = na;
         TPA_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
     }
 };
@@ -349,6 +361,8 @@ void DeviceSolver::build_views() {
     vf_.assign(size_t(nl), LevelView<float>{});
     int tail_cells = kTailCellsDefault;
     if (const char* env = std::getenv("TPAGMG_TAIL_CELLS")) tail_cells = std::max(0, std::atoi(env));
+    tail_ctas_ = kTailCtasDefault;
+    if (const char* env = std::getenv("TPAGMG_TAIL_CTAS")) tail_ctas_ = std::min(8, std::max(1, std::atoi(env)));
     tail_first_ = nl - 1;  // the coarsest level always runs in the tail (dense solve)
     for (int l = nl - 1; l >= 0; --l)
         if (levels_[size_t(l)].n <= tail_cells) tail_first_ = l;
@@ -467,7 +481,8 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
                                                                   next_sum ? lsum_.p + l + 1 : nullptr);
         launches_ += 3;
     }
-    go(k_tail<T, double>, 1, kTailThreads, 0, Vdev, t, nl, t == 0 ? r : nullptr, coarse_inv_.p, coarse_n_,
+    const Launch gt{stream_, pdl_, tail_ctas_};
+    gt(k_tail<T, double>, tail_ctas_, kTailThreads, 0, Vdev, t, nl, t == 0 ? r : nullptr, coarse_inv_.p, coarse_n_,
                                                          t == 0 && V[0].singular ? mean_out : nullptr);
     ++launches_;
     for (int l = t - 1; l >= 0; --l) {
