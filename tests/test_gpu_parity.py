@@ -220,7 +220,8 @@ def test_refresh_matches_rebuild():
 
 @pytest.mark.parametrize("spec", [W.taylor_green_spec(), dict(base_mesh=(128, 128), block_size=(16, 16),
                                                               periodic=(False, False)),
-                                  dict(base_mesh=(256, 128), block_size=(16, 16), periodic=(True, False))],
+                                  dict(base_mesh=(256, 128), block_size=(16, 16), extent=(2.0, 1.0),
+                                       periodic=(True, False))],
                          ids=["periodic_128", "walls_128", "channel_256x128"])
 def test_vectorized_levels_match_scalar_stencil(spec, monkeypatch):
     """The vectorized constant-coefficient kernels (4-cell quads, walls and
@@ -251,3 +252,26 @@ def test_vectorized_levels_match_scalar_stencil(spec, monkeypatch):
     xm = np.zeros(m.ncells)
     assert solve(xm, s, rhs, rtol=1e-10, precision="mixed").converged
     assert np.max(np.abs(xm - po)) <= 1e-9 * np.max(np.abs(po))
+
+
+@pytest.mark.parametrize("name", ["droplet_l2", "taylor_green_128", "walls_affine"])
+def test_fused_solve_matches_plain_solve(name, monkeypatch):
+    """`solve!` with its set-up and checks fused into two passes gives the
+    statistics and solution of the kernel-by-kernel path."""
+    m, s, oo, mg = build(name)
+    rhs = W.gaussian_rhs(m, 13)
+    x0 = np.sin(np.arange(m.ncells) * 0.3)
+    monkeypatch.setenv("TPAGMG_PLAIN_SOLVE", "1")
+    xp = x0.copy()
+    sp = solve(xp, s, rhs, rtol=1e-11)
+    sp = dict(vars(sp))
+    monkeypatch.delenv("TPAGMG_PLAIN_SOLVE")
+    for precision in ("fp64", "mixed"):
+        xf = x0.copy()
+        sf = solve(xf, s, rhs, rtol=1e-11, precision=precision)
+        assert sf.converged and sp["converged"]
+        assert abs(sf.cycles - sp["cycles"]) <= (1 if precision == "fp64" else 2)
+        assert sf.initial_linf == pytest.approx(sp["initial_linf"], rel=1e-12)
+        assert sf.initial_l2 == pytest.approx(sp["initial_l2"], rel=1e-12)
+        assert sf.removed_rhs_mean == pytest.approx(sp["removed_rhs_mean"], rel=1e-12, abs=1e-300)
+        assert np.max(np.abs(xf - xp)) <= 1e-9 * np.max(np.abs(xp))

@@ -18,6 +18,7 @@
 // fixed order, so every result is bitwise repeatable.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "device.cuh"
@@ -456,6 +457,11 @@ void DeviceSolver::upload(const Hierarchy& h) {
             d.comp_volume = hl.op.comp.volume;
             d.slot.upload(hl.op.comp.slot.data(), hl.op.comp.slot.size(), stream_);
         }
+        if (l == 0) {
+            vol_total_ = 0;
+            for (double v : hl.op.volumes)
+                if (v > 0) vol_total_ += v;
+        }
         if (l + 1 < h.levels.size()) {
             d.nc = int(h.levels[l + 1].op.A.n);
             d.owner.upload(hl.owner.data(), hl.owner.size(), stream_);
@@ -713,6 +719,10 @@ void DeviceSolver::solve(const double* rhs, double* x_user, double rtol, double 
     if (max_cycles < 0) throw Error(1, "max_cycles must be nonnegative");
     if (compatibility != 0 && compatibility != 1) throw Error(1, "compatibility must be :project or :error");
     if (precision != 0 && precision != 1) throw Error(1, "precision must be 0 (FP64) or 1 (mixed)");
+    if (fused_ok_ && !std::getenv("TPAGMG_PLAIN_SOLVE")) {
+        solve_fast(rhs, x_user, rtol, atol, max_cycles, compatibility, precision, st);
+        return;
+    }
     const double eps = 2.220446049250313e-16;
     DevLevel& L = levels_[0];
     const int n = L.n;

@@ -168,6 +168,12 @@ private:
     void enqueue_cg_body(int precision, cudaGraphConditionalHandle handle, int set_cond);
     double time_fused(int which, int level, int precision, int iters);
 
+    // `solve!` with the set-up and checks fused into two passes (solve_fast.cu)
+    void solve_fast(const double* rhs, double* x, double rtol, double atol, int max_cycles, int compatibility,
+                    int precision, SolveStats& st);
+    DevArray<double> spartial_, spres_;
+    double vol_total_ = 0;  // finest-level volume of cells with V > 0
+
     bool fused_ok_ = false;
     bool pdl_ = true;  // programmatic dependent launch between cycle kernels
     int tail_first_ = 0;

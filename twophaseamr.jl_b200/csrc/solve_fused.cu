@@ -410,6 +410,8 @@ void DeviceSolver::build_views() {
     TPA_CUDA(cudaMemsetAsync(lsum_.p, 0, size_t(nl + 2) * sizeof(double), stream_));
     cgs_.alloc(sizeof(CgState));
     TPA_CUDA(cudaMemsetAsync(cgs_.p, 0, sizeof(CgState), stream_));
+    spartial_.alloc(size_t(4) * size_t(kMaxGrid));
+    spres_.alloc(8);
     TPA_CUDA(cudaStreamSynchronize(stream_));
     destroy_graphs();
 }
