@@ -287,6 +287,7 @@ def main():
                     help="merged batch levels (one launch per phase) or one stream per problem")
     ap.add_argument("--size", type=int, default=2048, help="cells per side of the uniform workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default device layout")
     ap.add_argument("--profile", action="store_true", help="only W warm-up and K mixed solves (for ncu)")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -324,6 +325,11 @@ def main():
     solver = EllipticSolver(PoissonOperator(mesh, kappa), device=local)
     stream = torch.cuda.current_stream()
     solver.ctx.call("tpa_set_stream", C.c_void_p(stream.cuda_stream))
+    layout, tune_s = solver.tuning(), 0.0
+    if not (args.no_autotune or args.profile):
+        t0 = time.perf_counter()
+        layout, _ = solver.autotune(precision="mixed", vcycles=20)
+        tune_s = time.perf_counter() - t0
     if args.workload == "droplet_amr":
         rhs_h = W.droplet_rhs(mesh, solver.apply(psi))
     else:
@@ -436,7 +442,8 @@ def main():
         "dtype": "f32/f64", "data": "synthetic (seeded Philox)",
         "config": {"workload": f"droplet_amr levels={args.levels} (unit square, 4x4 roots of 16x16, circle band)",
                    "fine_cells": n, "levels": solver.level_sizes(), "parallelism": "replicas" if world > 1 else "1 GPU",
-                   "l2": "flushed between steps (256 MiB write)", "device_layout": solver.device_info()},
+                   "l2": "flushed between steps (256 MiB write)", "device_layout": solver.device_info(),
+                   "autotuned_layout": layout, "autotune_s": tune_s},
         "time_to_tolerance_ms": {"mixed": mixed_ms, "fp64": fp64_ms, "speedup_mixed_over_fp64": fp64_ms / mixed_ms},
         "cg_iterations": {"mixed": mixed_it, "fp64": fp64_it},
         "fp64_value": world * n * fp64_it / (fp64_ms * 1e-3),

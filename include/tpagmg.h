@@ -183,6 +183,31 @@ tpa_status tpa_batch_solve_device(tpa_batch* batch, const double* rhs, double* x
                                   int32_t max_cycles, int32_t compatibility, int32_t precision, tpa_stats* stats,
                                   tpa_status* statuses);
 
+/* Device layout of the V-cycle (no reference counterpart: the reference's
+ * cycle runs on the host).  Negative fields mean "default".  tail_cells: levels
+ * with at most this many cells run in the coarse tail; tail_ctas: CTAs of the
+ * tail's thread-block cluster (1-8); structured: 0 CSR kernels everywhere, 1
+ * stencil kernels on constant-coefficient levels without coarse-fine rows,
+ * 2 stencil kernels wherever the transfer has a block map; vectorized: 4-cell
+ * kernels on constant-coefficient 16x16 levels; pdl: programmatic dependent
+ * launch between cycle kernels.  Every layout gives the same V-cycle to
+ * rounding. */
+typedef struct {
+    int32_t tail_cells, tail_ctas, structured, vectorized, pdl;
+    double ms_per_vcycle; /* measured time (tpa_autotune), else 0 */
+} tpa_tune_config;
+/* Autotuner: times `vcycles` V-cycles (precision 0 FP64, 1 mixed) of every
+ * candidate layout on the uploaded hierarchy (tail size x tail CTAs x stencil
+ * policy, then the best without vectorized kernels and without PDL), keeps the
+ * fastest and returns it in *best; tried (capacity entries, may be NULL)
+ * receives every measurement and *ntried their count.  The choice persists
+ * across tpa_refresh; a new hierarchy starts from the defaults. */
+tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tpa_tune_config* best,
+                        tpa_tune_config* tried, int32_t capacity, int32_t* ntried);
+tpa_status tpa_set_tuning(tpa_context* ctx, const tpa_tune_config* config);
+/* the layout in effect (defaults resolved; ms_per_vcycle = 0) */
+tpa_status tpa_get_tuning(tpa_context* ctx, tpa_tune_config* config);
+
 /* Reverse-mode derivative of tpa_solve (the rrule a Julia caller registers
  * with ChainRulesCore for solve!; the reference differentiates nothing, so
  * the forward map is that of solve!, elliptic_solver.jl:628-675, with

@@ -373,6 +373,7 @@ tpa_status tpa_build_hierarchy(tpa_context* ctx, const tpa_multigrid_options* op
         ctx->have_hierarchy = true;
         ctx->have_operator = true;
         ctx->uploaded = false;
+        if (ctx->dev) ctx->dev->reset_tuning();  // a new hierarchy starts from the default layout
     });
 }
 
@@ -749,6 +750,100 @@ tpa_status tpa_batch_solve(tpa_batch* b, const double* rhs, double* x, double rt
         if (e.code) throw e;
     });
 }
+
+}  // extern "C"
+
+namespace {
+tpa::TuneConfig from_c(const tpa_tune_config& c) {
+    tpa::TuneConfig t;
+    t.tail_cells = c.tail_cells;
+    t.tail_ctas = c.tail_ctas;
+    t.structured = c.structured;
+    t.vectorized = c.vectorized;
+    t.pdl = c.pdl;
+    return t;
+}
+tpa_tune_config to_c(const tpa::TuneConfig& t, double ms) {
+    tpa_tune_config c;
+    c.tail_cells = t.tail_cells;
+    c.tail_ctas = t.tail_ctas;
+    c.structured = t.structured;
+    c.vectorized = t.vectorized;
+    c.pdl = t.pdl;
+    c.ms_per_vcycle = ms;
+    return c;
+}
+}  // namespace
+
+extern "C" {
+
+tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tpa_tune_config* best,
+                        tpa_tune_config* tried, int32_t capacity, int32_t* ntried) {
+    return guard(ctx, [&] {
+        if (precision != 0 && precision != 1) throw tpa::Error(TPA_ERR_INVALID_ARG, "bad precision");
+        if (vcycles <= 0) throw tpa::Error(TPA_ERR_INVALID_ARG, "vcycles must be positive");
+        ensure_device(ctx);
+        tpa::DeviceSolver& d = *ctx->dev;
+        std::vector<tpa::TuneConfig> cand;
+        for (int cells : {1024, 2048, 4096, 8192})
+            for (int ctas : {1, 4})
+                for (int st : {1, 2}) {
+                    tpa::TuneConfig c;
+                    c.tail_cells = cells;
+                    c.tail_ctas = ctas;
+                    c.structured = st;
+                    c.vectorized = 1;
+                    c.pdl = 1;
+                    cand.push_back(c);
+                }
+        std::vector<std::pair<tpa::TuneConfig, double>> res;
+        auto run = [&](const tpa::TuneConfig& c) {
+            d.reconfigure(ctx->hier, c);
+            res.emplace_back(d.effective_tuning(), d.time_vcycles(precision, vcycles));
+        };
+        for (const auto& c : cand) run(c);
+        auto best_of = [&] {
+            size_t b = 0;
+            for (size_t k = 1; k < res.size(); ++k)
+                if (res[k].second < res[b].second) b = k;
+            return b;
+        };
+        // then the best one without the vectorized kernels and without PDL
+        tpa::TuneConfig b0 = res[best_of()].first;
+        tpa::TuneConfig nv = b0, np = b0;
+        nv.vectorized = 0;
+        np.pdl = 0;
+        run(nv);
+        run(np);
+        const size_t b = best_of();
+        d.reconfigure(ctx->hier, res[b].first);
+        if (best) *best = to_c(res[b].first, res[b].second);
+        if (ntried) *ntried = int32_t(res.size());
+        for (int32_t k = 0; tried && k < capacity && size_t(k) < res.size(); ++k)
+            tried[k] = to_c(res[size_t(k)].first, res[size_t(k)].second);
+    });
+}
+
+tpa_status tpa_set_tuning(tpa_context* ctx, const tpa_tune_config* cfg) {
+    return guard(ctx, [&] {
+        if (!cfg) throw tpa::Error(TPA_ERR_INVALID_ARG, "null configuration");
+        if (cfg->tail_ctas > 8 || cfg->structured > 2) throw tpa::Error(TPA_ERR_INVALID_ARG, "bad configuration");
+        ensure_device(ctx);
+        ctx->dev->reconfigure(ctx->hier, from_c(*cfg));
+    });
+}
+
+tpa_status tpa_get_tuning(tpa_context* ctx, tpa_tune_config* cfg) {
+    return guard(ctx, [&] {
+        if (!cfg) throw tpa::Error(TPA_ERR_INVALID_ARG, "null configuration");
+        ensure_device(ctx);
+        *cfg = to_c(ctx->dev->effective_tuning(), 0.0);
+    });
+}
+
+}  // extern "C"
+
+extern "C" {
 
 tpa_status tpa_synchronize(tpa_context* ctx) {
     return guard(ctx, [&] {

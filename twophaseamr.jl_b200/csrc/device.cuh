@@ -92,6 +92,14 @@ struct CgScalars {
     int iter;
 };
 
+// Device layout choices (negative: the default, or the TPAGMG_* environment
+// override).  structured: 0 CSR everywhere, 1 stencil path on constant-
+// coefficient levels without exception rows, 2 stencil path wherever the block
+// map allows it.
+struct TuneConfig {
+    int tail_cells = -1, tail_ctas = -1, structured = -1, vectorized = -1, pdl = -1;
+};
+
 struct SolveStats {
     int cycles = 0, converged = 0;
     double initial_l2 = 0, initial_linf = 0, final_l2 = 0, final_linf = 0, target_linf = 0;
@@ -167,6 +175,21 @@ private:
     cudaGraphExec_t cg_graph(int precision);
     void enqueue_cg_body(int precision, cudaGraphConditionalHandle handle, int set_cond);
     double time_fused(int which, int level, int precision, int iters);
+
+public:
+    // Layout (autotune.cu): apply a configuration to the uploaded hierarchy
+    // (rebuilds the level views and the stencil copies, not the CSR data).
+    void reconfigure(const Hierarchy& h, const TuneConfig& c);
+    const TuneConfig& tuning() const { return tune_; }
+    void reset_tuning() { tune_ = TuneConfig(); }
+    // the configuration actually in effect (defaults and overrides resolved)
+    TuneConfig effective_tuning() const;
+    // average device time (ms) of `count` V-cycles of a fixed residual
+    double time_vcycles(int precision, int count);
+
+private:
+    TuneConfig tune_;
+    int structured_mode_ = 1;
 
     // `solve!` with the set-up and checks fused into two passes (solve_fast.cu)
     void solve_fast(const double* rhs, double* x, double rtol, double atol, int max_cycles, int compatibility,

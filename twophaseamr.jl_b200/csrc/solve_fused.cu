@@ -351,18 +351,37 @@ __global__ void k_z_out(int n, const float* __restrict__ xf, const double* __res
 
 }  // namespace
 
+TuneConfig DeviceSolver::effective_tuning() const {
+    TuneConfig c;
+    c.pdl = tune_.pdl >= 0 ? tune_.pdl : (std::getenv("TPAGMG_NO_PDL") ? 0 : 1);
+    c.tail_cells = kTailCellsDefault;
+    if (const char* env = std::getenv("TPAGMG_TAIL_CELLS")) c.tail_cells = std::max(0, std::atoi(env));
+    if (tune_.tail_cells >= 0) c.tail_cells = tune_.tail_cells;
+    c.tail_ctas = kTailCtasDefault;
+    if (const char* env = std::getenv("TPAGMG_TAIL_CTAS")) c.tail_ctas = std::atoi(env);
+    if (tune_.tail_ctas >= 0) c.tail_ctas = tune_.tail_ctas;
+    c.tail_ctas = std::min(8, std::max(1, c.tail_ctas));
+    c.structured = 1;
+    if (const char* p = std::getenv("TPAGMG_STRUCTURED"))
+        if (std::string(p) == "all") c.structured = 2;
+    if (std::getenv("TPAGMG_NO_STRUCTURED")) c.structured = 0;
+    if (tune_.structured >= 0) c.structured = std::min(2, tune_.structured);
+    c.vectorized = std::getenv("TPAGMG_NO_VEC") ? 0 : 1;
+    if (tune_.vectorized >= 0) c.vectorized = tune_.vectorized ? 1 : 0;
+    return c;
+}
+
 void DeviceSolver::build_views() {
-    pdl_ = std::getenv("TPAGMG_NO_PDL") == nullptr;
+    const TuneConfig cfg = effective_tuning();
+    pdl_ = cfg.pdl != 0;
     fused_ok_ = (pre_ == 2 && post_ == 2);
     for (auto& L : levels_)
         if (L.ncomp > 1) fused_ok_ = false;
     const int nl = int(levels_.size());
     vd_.assign(size_t(nl), LevelView<double>{});
     vf_.assign(size_t(nl), LevelView<float>{});
-    int tail_cells = kTailCellsDefault;
-    if (const char* env = std::getenv("TPAGMG_TAIL_CELLS")) tail_cells = std::max(0, std::atoi(env));
-    tail_ctas_ = kTailCtasDefault;
-    if (const char* env = std::getenv("TPAGMG_TAIL_CTAS")) tail_ctas_ = std::min(8, std::max(1, std::atoi(env)));
+    const int tail_cells = cfg.tail_cells;
+    tail_ctas_ = cfg.tail_ctas;
     tail_first_ = nl - 1;  // the coarsest level always runs in the tail (dense solve)
     for (int l = nl - 1; l >= 0; --l)
         if (levels_[size_t(l)].n <= tail_cells) tail_first_ = l;
@@ -787,7 +806,8 @@ void DeviceSolver::upload_structured(const Hierarchy& h) {
     sdev_.resize(size_t(nl));
     sd_.assign(size_t(nl), SView<double>{});
     sf_.assign(size_t(nl), SView<float>{});
-    const bool disabled = std::getenv("TPAGMG_NO_STRUCTURED") != nullptr;
+    const TuneConfig cfg = effective_tuning();
+    const bool disabled = cfg.structured == 0;
     for (int l = 0; l < nl; ++l) {
         const HostLevel& hl = h.levels[size_t(l)];
         const int cpb = hl.op.mesh.bs[0] * hl.op.mesh.bs[1];
@@ -796,14 +816,13 @@ void DeviceSolver::upload_structured(const Hierarchy& h) {
         if (!st.has_map || !st.tinv_same) continue;
         // Variable-coefficient levels with coarse-fine exception rows are small and
         // latency-bound; the CSR kernels (one index chain per row, no divergence
-        // between stencil and exception rows) are faster there.  Force the stencil
-        // path on every level with TPAGMG_STRUCTURED=all.
-        const char* policy = std::getenv("TPAGMG_STRUCTURED");
-        const bool all = policy && std::string(policy) == "all";
-        if (!all && !(st.const_coef && st.nex == 0)) continue;
+        // between stencil and exception rows) are faster there.  Structured mode 2
+        // (TPAGMG_STRUCTURED=all, or the autotuner) uses the stencil path on every
+        // level that has a block map.
+        if (cfg.structured < 2 && !(st.const_coef && st.nex == 0)) continue;
         StructDev& D = sdev_[size_t(l)];
         D.on = true;
-        D.vec = st.const_coef && st.nex == 0 && st.nx == 16 && st.ny == 16 && !std::getenv("TPAGMG_NO_VEC");
+        D.vec = st.const_coef && st.nex == 0 && st.nx == 16 && st.ny == 16 && cfg.vectorized;
         D.nex = st.nex;
         D.const_coef = st.const_coef;
         D.const_diag = st.const_diag;

@@ -43,6 +43,11 @@ class StatsC(C.Structure):
                 ("device_ms", C.c_double), ("kernel_launches", C.c_int32), ("precision", C.c_int32)]
 
 
+class TuneC(C.Structure):
+    _fields_ = [("tail_cells", C.c_int32), ("tail_ctas", C.c_int32), ("structured", C.c_int32),
+                ("vectorized", C.c_int32), ("pdl", C.c_int32), ("ms_per_vcycle", C.c_double)]
+
+
 P = C.c_void_p
 i32p = C.POINTER(C.c_int32)
 i64p = C.POINTER(C.c_int64)
@@ -76,6 +81,9 @@ SIGNATURES = {
     "tpa_solve_batched_device": (C.c_int32, [C.POINTER(P), C.c_int32, C.POINTER(P), C.POINTER(P), C.c_double,
                                              C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                              C.POINTER(StatsC), i32p, f64p]),
+    "tpa_autotune": (C.c_int32, [P, C.c_int32, C.c_int32, C.POINTER(TuneC), C.POINTER(TuneC), C.c_int32, i32p]),
+    "tpa_set_tuning": (C.c_int32, [P, C.POINTER(TuneC)]),
+    "tpa_get_tuning": (C.c_int32, [P, C.POINTER(TuneC)]),
     "tpa_batch_create": (C.c_int32, [C.POINTER(P), C.POINTER(P), C.c_int32]),
     "tpa_batch_destroy": (None, [P]),
     "tpa_batch_last_error": (C.c_char_p, [P]),

@@ -120,6 +120,37 @@ class EllipticSolver:
         return {"structured_levels": int(out[0]), "exception_rows": int(out[1]),
                 "tail_first_level": int(out[2]), "fused_cycle": bool(out[3])}
 
+    # -- device layout ---------------------------------------------------------
+    @staticmethod
+    def _tune_dict(t):
+        return {"tail_cells": t.tail_cells, "tail_ctas": t.tail_ctas, "structured": t.structured,
+                "vectorized": t.vectorized, "pdl": t.pdl, "ms_per_vcycle": t.ms_per_vcycle}
+
+    def autotune(self, precision=None, vcycles=20):
+        """Time the candidate device layouts of the V-cycle and keep the
+        fastest; returns (best, every measurement) as dicts."""
+        best = _lib.TuneC()
+        tried = (_lib.TuneC * 64)()
+        n = C.c_int32()
+        self.ctx.call("tpa_autotune", _PRECISION[precision or self.precision], int(vcycles), C.byref(best), tried,
+                      64, C.byref(n))
+        return self._tune_dict(best), [self._tune_dict(tried[k]) for k in range(n.value)]
+
+    def tuning(self):
+        t = _lib.TuneC()
+        self.ctx.call("tpa_get_tuning", C.byref(t))
+        return self._tune_dict(t)
+
+    def set_tuning(self, **fields):
+        """Apply a layout (tail_cells, tail_ctas, structured, vectorized, pdl;
+        omitted fields: default)."""
+        unknown = set(fields) - {"tail_cells", "tail_ctas", "structured", "vectorized", "pdl"}
+        if unknown:
+            raise ValueError(f"unknown layout fields: {sorted(unknown)}")
+        t = _lib.TuneC(*(int(fields.get(k, -1)) for k in ("tail_cells", "tail_ctas", "structured",
+                                                           "vectorized", "pdl")), 0.0)
+        self.ctx.call("tpa_set_tuning", C.byref(t))
+
     def residual_norms_device(self, r_ptr):
         """`_integrated_residual_norms` of an integrated residual held on the
         device (raw CUDA pointer, cell order): (L2, strong L-infinity)."""
