@@ -761,6 +761,7 @@ tpa::TuneConfig from_c(const tpa_tune_config& c) {
     t.structured = c.structured;
     t.vectorized = c.vectorized;
     t.pdl = c.pdl;
+    t.fuse_restrict = c.fuse_restrict;
     return t;
 }
 tpa_tune_config to_c(const tpa::TuneConfig& t, double ms) {
@@ -770,6 +771,7 @@ tpa_tune_config to_c(const tpa::TuneConfig& t, double ms) {
     c.structured = t.structured;
     c.vectorized = t.vectorized;
     c.pdl = t.pdl;
+    c.fuse_restrict = t.fuse_restrict;
     c.ms_per_vcycle = ms;
     return c;
 }
@@ -794,6 +796,7 @@ tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tp
                     c.structured = st;
                     c.vectorized = 1;
                     c.pdl = 1;
+                    c.fuse_restrict = 0;
                     cand.push_back(c);
                 }
         std::vector<std::pair<tpa::TuneConfig, double>> res;
@@ -813,8 +816,11 @@ tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tp
         tpa::TuneConfig nv = b0, np = b0;
         nv.vectorized = 0;
         np.pdl = 0;
+        tpa::TuneConfig fr = b0;
+        fr.fuse_restrict = 1;
         run(nv);
         run(np);
+        run(fr);
         const size_t b = best_of();
         d.reconfigure(ctx->hier, res[b].first);
         if (best) *best = to_c(res[b].first, res[b].second);

@@ -98,6 +98,7 @@ struct CgScalars {
 // map allows it.
 struct TuneConfig {
     int tail_cells = -1, tail_ctas = -1, structured = -1, vectorized = -1, pdl = -1;
+    int fuse_restrict = -1;  // CSR levels: residual recomputed inside the restriction
 };
 
 struct SolveStats {
@@ -199,6 +200,7 @@ private:
 
     bool fused_ok_ = false;
     bool pdl_ = true;  // programmatic dependent launch between cycle kernels
+    bool fuse_rr_ = false;  // residual + restriction in one launch on CSR levels
     int tail_first_ = 0;
     int tail_ctas_ = 1;  // CTAs of the coarse-tail cluster
     std::vector<LevelView<double>> vd_;

@@ -174,13 +174,20 @@ __device__ __forceinline__ void residual_cell(const LevelView<T>& L, int i) {
     L.s[i] = L.tinv[i] * ri;
 }
 
+// Restriction with four lanes per coarse cell (lane q takes children q, q + 4,
+// ...; a coarse cell has one or four children): call from thread g = 4 J + q
+// of a whole warp; returns the coarse value in every lane of the group, summed
+// in the fixed order (c0 + c1) + (c2 + c3).
 template <typename T>
-__device__ __forceinline__ T restrict_cell(const LevelView<T>& L, int J) {
+__device__ __forceinline__ T restrict_quad(const LevelView<T>& L, int J, int q) {
     T acc = T(0);
-    for (int k = L.cptr[J]; k < L.cptr[J + 1]; ++k) {
-        int i = L.child[k];
-        acc += L.r[i] - L.tw * rowdot(L, L.s, i);
-    }
+    if (J < L.nc)
+        for (int k = L.cptr[J] + q; k < L.cptr[J + 1]; k += 4) {
+            const int i = L.child[k];
+            acc += L.r[i] - L.tw * rowdot(L, L.s, i);
+        }
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
     return acc;
 }
 
@@ -217,18 +224,67 @@ __global__ void k_residual(LevelView<T> L) {
     if (i < L.n) residual_cell(L, i);
 }
 
-// b_c = P_tent'(r - wt A s); coarse RHS sum folded into `coarse_sum` when non-null.
+// b_c = P_tent'(r - wt A s), four threads per coarse cell (grid over 4 nc);
+// coarse RHS sum folded into `coarse_sum` when non-null.
 template <typename T>
 __global__ void k_restrict(LevelView<T> L, T* __restrict__ bc, double* partial, unsigned* counter, double* coarse_sum) {
     pdl_entry();
-    int J = blockIdx.x * blockDim.x + threadIdx.x;
-    T v = T(0);
-    if (J < L.nc) {
-        v = restrict_cell(L, J);
-        bc[J] = v;
+    // grid-stride over whole warps (the shuffles need every lane of a warp)
+    const int quads = (4 * L.nc + 31) & ~31;
+    double part = 0;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < quads; g += gridDim.x * blockDim.x) {
+        const int J = g >> 2;
+        const T v = restrict_quad(L, J, g & 3);
+        if ((g & 3) == 0 && J < L.nc) {
+            bc[J] = v;
+            part += double(v);
+        }
     }
     if (coarse_sum) {
-        if (publish_partial(double(v), partial, counter)) {
+        if (publish_partial(part, partial, counter)) {
+            double s = fold_partials(partial, gridDim.x);
+            if (threadIdx.x == 0) {
+                *coarse_sum = s;
+                *counter = 0;
+            }
+        }
+    }
+}
+
+// Residual and restriction in one launch: b_c = P_tent'(r - wt A Dt^-1 r) with
+// r = bp - A x recomputed at every neighbour of a child (four lanes per coarse
+// cell, as k_restrict).  Saves the residual phase and the r / s round trip at
+// the price of about nnz_row^2 products per fine cell.
+template <typename T>
+__global__ void k_resrest(LevelView<T> L, T* __restrict__ bc, double* partial, unsigned* counter,
+                          double* coarse_sum) {
+    pdl_entry();
+    const int quads = (4 * L.nc + 31) & ~31;
+    double part = 0;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < quads; g += gridDim.x * blockDim.x) {
+        const int J = g >> 2, q = g & 3;
+        T acc = T(0);
+        if (J < L.nc)
+            for (int c = L.cptr[J] + q; c < L.cptr[J + 1]; c += 4) {
+                const int i = L.child[c];
+                const T ri = L.bp[i] - rowdot(L, L.x, i);
+                T as = T(0);
+                for (int k = L.rp[i]; k < L.rp[i + 1]; ++k) {
+                    const int j = L.ci[k];
+                    const T rj = j == i ? ri : L.bp[j] - rowdot(L, L.x, j);
+                    as += L.val[k] * (L.tinv[j] * rj);
+                }
+                acc += ri - L.tw * as;
+            }
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+        if (q == 0 && J < L.nc) {
+            bc[J] = acc;
+            part += double(acc);
+        }
+    }
+    if (coarse_sum) {
+        if (publish_partial(part, partial, counter)) {
             double s = fold_partials(partial, gridDim.x);
             if (threadIdx.x == 0) {
                 *coarse_sum = s;
@@ -343,7 +399,13 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(const LevelView<T>* __res
         for (int i = gt; i < L.n; i += gs) residual_cell(L, i);
         cl.sync();
         T* bc = levels[l + 1].b;
-        for (int J = gt; J < L.nc; J += gs) bc[J] = restrict_cell(L, J);
+        // four lanes per coarse cell; the bound is rounded up to whole warps so
+        // that every lane of a warp takes part in the shuffles
+        const int quads = (4 * L.nc + 31) & ~31;
+        for (int g = gt; g < quads; g += gs) {
+            const T v = restrict_quad(L, g >> 2, g & 3);
+            if ((g & 3) == 0 && (g >> 2) < L.nc) bc[g >> 2] = v;
+        }
         cl.sync();
     }
     for (int l = nl - 2; l >= first; --l) {

@@ -368,12 +368,15 @@ TuneConfig DeviceSolver::effective_tuning() const {
     if (tune_.structured >= 0) c.structured = std::min(2, tune_.structured);
     c.vectorized = std::getenv("TPAGMG_NO_VEC") ? 0 : 1;
     if (tune_.vectorized >= 0) c.vectorized = tune_.vectorized ? 1 : 0;
+    c.fuse_restrict = std::getenv("TPAGMG_FUSE_RESTRICT") ? 1 : 0;
+    if (tune_.fuse_restrict >= 0) c.fuse_restrict = tune_.fuse_restrict ? 1 : 0;
     return c;
 }
 
 void DeviceSolver::build_views() {
     const TuneConfig cfg = effective_tuning();
     pdl_ = cfg.pdl != 0;
+    fuse_rr_ = cfg.fuse_restrict != 0;
     fused_ok_ = (pre_ == 2 && post_ == 2);
     for (auto& L : levels_)
         if (L.ncomp > 1) fused_ok_ = false;
@@ -420,7 +423,7 @@ void DeviceSolver::build_views() {
     }
     vd_dev_.upload(vd_.data(), vd_.size(), stream_);
     vf_dev_.upload(vf_.data(), vf_.size(), stream_);
-    fpartial_.alloc(size_t(maxgrid));
+    fpartial_.alloc(size_t(std::max<int64_t>(maxgrid, kMaxGrid)));
     fpartial2_.alloc(size_t(maxgrid));
     lsum_.alloc(size_t(nl + 2));
     xw_.alloc(size_t(levels_[0].n));
@@ -496,10 +499,16 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
         if (l == 0) go(k_pre2<T, double>, blocks_for(L.n), kThreads, 0, L, r, rsum);
         else go(k_pre2<T, T>, blocks_for(L.n), kThreads, 0, L, L.b, lsum_.p + l);
         const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
+        const int rgrid = next_sum ? reduce_grid(4 * int64_t(L.nc)) : blocks_for(4 * int64_t(L.nc));
+        if (fuse_rr_) {
+            go(k_resrest<T>, rgrid, kThreads, 0, L, V[size_t(l + 1)].b, fpartial_.p, counters_.p + kRestrictSum,
+               next_sum ? lsum_.p + l + 1 : nullptr);
+            launches_ += 2;
+            continue;
+        }
         go(k_residual<T>, blocks_for(L.n), kThreads, 0, L);
-        go(k_restrict<T>, blocks_for(L.nc), kThreads, 0, L, V[size_t(l + 1)].b, fpartial_.p,
-                                                                  counters_.p + kRestrictSum,
-                                                                  next_sum ? lsum_.p + l + 1 : nullptr);
+        go(k_restrict<T>, rgrid, kThreads, 0, L, V[size_t(l + 1)].b, fpartial_.p, counters_.p + kRestrictSum,
+           next_sum ? lsum_.p + l + 1 : nullptr);
         launches_ += 3;
     }
     const Launch gt{stream_, pdl_, tail_ctas_};
@@ -715,8 +724,9 @@ double DeviceSolver::time_fused(int which, int level, int precision, int iters) 
         switch (which) {
             case 0: k_post2<T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, fpartial_.p, counters_.p, nullptr); break;
             case 1:
-                k_restrict<T><<<blocks_for(L.nc), kThreads, 0, stream_>>>(L, V[size_t(level + 1)].b, fpartial_.p,
-                                                                          counters_.p, nullptr);
+                k_restrict<T><<<blocks_for(4 * int64_t(L.nc)), kThreads, 0, stream_>>>(L, V[size_t(level + 1)].b,
+                                                                                        fpartial_.p, counters_.p,
+                                                                                        nullptr);
                 break;
             case 2: k_prolong<T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, V[size_t(level + 1)].x); break;
             case 4: k_pre2<T, T><<<blocks_for(L.n), kThreads, 0, stream_>>>(L, L.b, nullptr); break;

@@ -124,7 +124,8 @@ class EllipticSolver:
     @staticmethod
     def _tune_dict(t):
         return {"tail_cells": t.tail_cells, "tail_ctas": t.tail_ctas, "structured": t.structured,
-                "vectorized": t.vectorized, "pdl": t.pdl, "ms_per_vcycle": t.ms_per_vcycle}
+                "vectorized": t.vectorized, "pdl": t.pdl, "fuse_restrict": t.fuse_restrict,
+                "ms_per_vcycle": t.ms_per_vcycle}
 
     def autotune(self, precision=None, vcycles=20):
         """Time the candidate device layouts of the V-cycle and keep the
@@ -142,13 +143,13 @@ class EllipticSolver:
         return self._tune_dict(t)
 
     def set_tuning(self, **fields):
-        """Apply a layout (tail_cells, tail_ctas, structured, vectorized, pdl;
-        omitted fields: default)."""
-        unknown = set(fields) - {"tail_cells", "tail_ctas", "structured", "vectorized", "pdl"}
+        """Apply a layout (tail_cells, tail_ctas, structured, vectorized, pdl,
+        fuse_restrict; omitted fields: default)."""
+        keys = ("tail_cells", "tail_ctas", "structured", "vectorized", "pdl", "fuse_restrict")
+        unknown = set(fields) - set(keys)
         if unknown:
             raise ValueError(f"unknown layout fields: {sorted(unknown)}")
-        t = _lib.TuneC(*(int(fields.get(k, -1)) for k in ("tail_cells", "tail_ctas", "structured",
-                                                           "vectorized", "pdl")), 0.0)
+        t = _lib.TuneC(*(int(fields.get(k, -1)) for k in keys), 0.0)
         self.ctx.call("tpa_set_tuning", C.byref(t))
 
     def residual_norms_device(self, r_ptr):
