@@ -191,16 +191,19 @@ tpa_status tpa_batch_solve_device(tpa_batch* batch, const double* rhs, double* x
  * 2 stencil kernels wherever the transfer has a block map; vectorized: 4-cell
  * kernels on constant-coefficient 16x16 levels; pdl: programmatic dependent
  * launch between cycle kernels; fuse_restrict: on CSR levels, the residual is
- * recomputed inside the restriction (one launch instead of two).  Every layout
- * gives the same V-cycle to rounding. */
+ * recomputed inside the restriction (one launch instead of two); persistent:
+ * when every multi-CTA level is a CSR level, the whole V-cycle runs as one
+ * cooperative launch with grid barriers (bounded waits; a barrier that gives up
+ * makes the solve return TPA_ERR_TIMEOUT).  Every layout gives the same V-cycle
+ * to rounding. */
 typedef struct {
-    int32_t tail_cells, tail_ctas, structured, vectorized, pdl, fuse_restrict;
+    int32_t tail_cells, tail_ctas, structured, vectorized, pdl, fuse_restrict, persistent;
     double ms_per_vcycle; /* measured time (tpa_autotune), else 0 */
 } tpa_tune_config;
 /* Autotuner: times `vcycles` V-cycles (precision 0 FP64, 1 mixed) of every
  * candidate layout on the uploaded hierarchy (tail size x tail CTAs x stencil
- * policy, then the best without vectorized kernels, without PDL and with the
- * fused restriction), keeps the
+ * policy, then the best without vectorized kernels, without PDL, with the
+ * fused restriction and as one cooperative launch), keeps the
  * fastest and returns it in *best; tried (capacity entries, may be NULL)
  * receives every measurement and *ntried their count.  The choice persists
  * across tpa_refresh; a new hierarchy starts from the defaults. */

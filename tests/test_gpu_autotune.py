@@ -25,6 +25,7 @@ def droplet():
 
 @pytest.mark.parametrize("layout", [dict(tail_cells=512), dict(tail_cells=8192, tail_ctas=4),
                                     dict(structured=0), dict(structured=2), dict(pdl=0), dict(fuse_restrict=1),
+                                    dict(persistent=1), dict(persistent=1, tail_cells=4096),
                                     dict(tail_cells=1024, tail_ctas=8, structured=2, pdl=0)])
 def test_every_layout_gives_the_same_vcycle(layout):
     spec, m, kappa = droplet()
@@ -49,7 +50,7 @@ def test_autotune_keeps_the_fastest_layout_and_solves_match_the_oracle():
     assert len(tried) >= 16 and all(t["ms_per_vcycle"] > 0 for t in tried)
     assert best["ms_per_vcycle"] == min(t["ms_per_vcycle"] for t in tried)
     now = s.tuning()
-    for k in ("tail_cells", "tail_ctas", "structured", "vectorized", "pdl", "fuse_restrict"):
+    for k in ("tail_cells", "tail_ctas", "structured", "vectorized", "pdl", "fuse_restrict", "persistent"):
         assert now[k] == best[k]
     rhs = W.gaussian_rhs(m, 8)
     oo = OOp(block_tree_mesh(**spec), kappa)

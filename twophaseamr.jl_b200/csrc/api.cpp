@@ -488,6 +488,7 @@ tpa_status tpa_vcycle(tpa_context* ctx, const double* r, double* z, int32_t prec
         ctx->dev->vcycle(ctx->d_x.p, ctx->d_y.p, precision);
         TPA_CUDA(cudaMemcpyAsync(z, ctx->d_y.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
         TPA_CUDA(cudaStreamSynchronize(s));
+        ctx->dev->check_barrier();
     });
 }
 
@@ -762,6 +763,7 @@ tpa::TuneConfig from_c(const tpa_tune_config& c) {
     t.vectorized = c.vectorized;
     t.pdl = c.pdl;
     t.fuse_restrict = c.fuse_restrict;
+    t.persistent = c.persistent;
     return t;
 }
 tpa_tune_config to_c(const tpa::TuneConfig& t, double ms) {
@@ -772,6 +774,7 @@ tpa_tune_config to_c(const tpa::TuneConfig& t, double ms) {
     c.vectorized = t.vectorized;
     c.pdl = t.pdl;
     c.fuse_restrict = t.fuse_restrict;
+    c.persistent = t.persistent;
     c.ms_per_vcycle = ms;
     return c;
 }
@@ -797,6 +800,7 @@ tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tp
                     c.vectorized = 1;
                     c.pdl = 1;
                     c.fuse_restrict = 0;
+                    c.persistent = 0;
                     cand.push_back(c);
                 }
         std::vector<std::pair<tpa::TuneConfig, double>> res;
@@ -816,11 +820,14 @@ tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tp
         tpa::TuneConfig nv = b0, np = b0;
         nv.vectorized = 0;
         np.pdl = 0;
-        tpa::TuneConfig fr = b0;
+        tpa::TuneConfig fr = b0, pe = b0;
         fr.fuse_restrict = 1;
+        pe.persistent = 1;
+        pe.tail_ctas = 1;
         run(nv);
         run(np);
         run(fr);
+        run(pe);
         const size_t b = best_of();
         d.reconfigure(ctx->hier, res[b].first);
         if (best) *best = to_c(res[b].first, res[b].second);

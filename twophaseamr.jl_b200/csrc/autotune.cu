@@ -43,6 +43,7 @@ double DeviceSolver::time_vcycles(int precision, int count) {
     TPA_CUDA(cudaEventRecord(e1, stream_));
     TPA_CUDA(cudaEventSynchronize(e1));
     TPA_CUDA(cudaGetLastError());
+    check_barrier();
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);

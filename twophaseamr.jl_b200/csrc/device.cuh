@@ -99,6 +99,7 @@ struct CgScalars {
 struct TuneConfig {
     int tail_cells = -1, tail_ctas = -1, structured = -1, vectorized = -1, pdl = -1;
     int fuse_restrict = -1;  // CSR levels: residual recomputed inside the restriction
+    int persistent = -1;     // all-CSR hierarchies: the V-cycle as one cooperative launch
 };
 
 struct SolveStats {
@@ -201,6 +202,15 @@ private:
     bool fused_ok_ = false;
     bool pdl_ = true;  // programmatic dependent launch between cycle kernels
     bool fuse_rr_ = false;  // residual + restriction in one launch on CSR levels
+    int coop_grid_ = 0;     // > 0: the V-cycle runs as one cooperative launch of this many CTAs
+    DevArray<unsigned> bar_;  // grid barrier: arrivals, generation
+    DevArray<int> err_;       // set when a grid barrier gave up waiting
+
+public:
+    // throws (status 3) if a grid barrier of the cooperative V-cycle gave up
+    void check_barrier();
+
+private:
     int tail_first_ = 0;
     int tail_ctas_ = 1;  // CTAs of the coarse-tail cluster
     std::vector<LevelView<double>> vd_;

@@ -355,13 +355,24 @@ __device__ double tail_sum(const T* v, const T* w, int n) {
     return total;
 }
 
+template <typename T, typename TB>
+__device__ void tail_run(const LevelView<T>* __restrict__ levels, int first, int nl, const TB* top_b,
+                         const double* __restrict__ G, int gn, double* mean_out);
+
 // `top_b`: RHS of level 0 (type TB), used only when first == 0
 template <typename T, typename TB>
 __global__ void __launch_bounds__(kTailThreads) k_tail(const LevelView<T>* __restrict__ levels, int first, int nl,
                                                        const TB* top_b, const double* __restrict__ G, int gn,
                                                        double* mean_out) {
-    namespace cg = cooperative_groups;
     pdl_entry();
+    tail_run<T, TB>(levels, first, nl, top_b, G, gn, mean_out);
+}
+
+// The tail's levels in the calling cluster (one CTA when launched without clusters).
+template <typename T, typename TB>
+__device__ void tail_run(const LevelView<T>* __restrict__ levels, int first, int nl, const TB* top_b,
+                         const double* __restrict__ G, int gn, double* mean_out) {
+    namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
     const int rank = int(cl.block_rank()), nb = int(cl.num_blocks());
     const int gt = rank * blockDim.x + threadIdx.x, gs = nb * blockDim.x;

@@ -214,6 +214,7 @@ void DeviceSolver::solve_fast(const double* rhs, double* x_user, double rtol, do
             if (!std::isfinite(fin.linf) || niter == 0) break;
         }
     }
+    check_barrier();
     const double tfinal = guarded(fin.linf, fin.floor);
     TPA_CUDA(cudaMemcpyAsync(x_user, xw_.p, sizeof(double) * size_t(n), cudaMemcpyDeviceToDevice, stream_));
     TPA_CUDA(cudaEventRecord(e1, stream_));

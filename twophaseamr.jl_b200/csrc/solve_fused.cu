@@ -14,6 +14,7 @@
 #include <type_traits>
 
 #include "device.cuh"
+#include "persistent.cuh"
 
 namespace tpa {
 namespace {
@@ -42,7 +43,8 @@ inline int reduce_grid(int64_t n) { return int(std::min<int64_t>(blocks_for(n), 
 struct Launch {
     cudaStream_t s;
     bool pdl;
-    int cluster = 1;  // CTAs per thread-block cluster (grid must be a multiple)
+    int cluster = 1;     // CTAs per thread-block cluster (grid must be a multiple)
+    bool coop = false;   // cooperative launch (every CTA resident at once)
     template <typename... KArgs, typename... Args>
     void operator()(void (*kernel)(KArgs...), int grid, int block, size_t smem, Args... args) const {
         cudaLaunchConfig_t cfg;
@@ -51,8 +53,13 @@ struct Launch {
         cfg.blockDim = dim3(unsigned(block));
         cfg.dynamicSmemBytes = smem;
         cfg.stream = s;
-        cudaLaunchAttribute at[2];
+        cudaLaunchAttribute at[3];
         unsigned na = 0;
+        if (coop) {
+            at[na].id = cudaLaunchAttributeCooperative;
+            at[na].val.cooperative = 1;
+            ++na;
+        }
         if (pdl) {
             at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
             at[na].val.programmaticStreamSerializationAllowed = 1;
@@ -370,7 +377,21 @@ TuneConfig DeviceSolver::effective_tuning() const {
     if (tune_.vectorized >= 0) c.vectorized = tune_.vectorized ? 1 : 0;
     c.fuse_restrict = std::getenv("TPAGMG_FUSE_RESTRICT") ? 1 : 0;
     if (tune_.fuse_restrict >= 0) c.fuse_restrict = tune_.fuse_restrict ? 1 : 0;
+    c.persistent = std::getenv("TPAGMG_PERSISTENT") ? 1 : 0;
+    if (tune_.persistent >= 0) c.persistent = tune_.persistent ? 1 : 0;
     return c;
+}
+
+void DeviceSolver::check_barrier() {
+    if (!err_.p) return;
+    int e = 0;
+    TPA_CUDA(cudaMemcpyAsync(&e, err_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    TPA_CUDA(cudaStreamSynchronize(stream_));
+    if (e) {
+        TPA_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), stream_));
+        TPA_CUDA(cudaMemsetAsync(bar_.p, 0, 2 * sizeof(unsigned), stream_));
+        throw Error(3, "a grid barrier of the cooperative V-cycle gave up waiting; the solve result is invalid");
+    }
 }
 
 void DeviceSolver::build_views() {
@@ -434,6 +455,10 @@ void DeviceSolver::build_views() {
     TPA_CUDA(cudaMemsetAsync(cgs_.p, 0, sizeof(CgState), stream_));
     spartial_.alloc(size_t(4) * size_t(kMaxGrid));
     spres_.alloc(8);
+    bar_.alloc(2);
+    err_.alloc(1);
+    TPA_CUDA(cudaMemsetAsync(bar_.p, 0, 2 * sizeof(unsigned), stream_));
+    TPA_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(int), stream_));
     TPA_CUDA(cudaStreamSynchronize(stream_));
     destroy_graphs();
 }
@@ -463,6 +488,15 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
         Vdev = vf_dev_.p;
     }
     const std::vector<LevelView<T>>& V = *Vp;
+    if (coop_grid_ > 0) {
+        // the whole cycle in one cooperative launch (persistent.cuh)
+        const Launch gc{stream_, false, 1, true};
+        gc(k_vcycle_grid<T>, coop_grid_, kTailThreads, 0, Vdev, t, nl, r, rsum, mean_out, coarse_inv_.p, coarse_n_,
+           fpartial_.p, bar_.p, lsum_.p, err_.p);
+        ++launches_;
+        if (!V[0].singular) TPA_CUDA(cudaMemsetAsync(mean_out, 0, sizeof(double), stream_));
+        return;
+    }
     const std::vector<SView<T>>* Sp;
     if constexpr (std::is_same<T, double>::value) Sp = &sd_;
     else Sp = &sf_;
@@ -891,6 +925,17 @@ void DeviceSolver::upload_structured(const Hierarchy& h) {
         };
         fill(sd_[size_t(l)], L.d, D.cx_d.p, D.cy_d.p, D.exv_d.p, [](double v) { return v; });
         fill(sf_[size_t(l)], L.f, D.cx_f.p, D.cy_f.p, D.exv_f.p, [](double v) { return float(v); });
+    }
+    // the cooperative V-cycle covers CSR levels only, one CTA of kTailThreads per SM
+    coop_grid_ = 0;
+    if (cfg.persistent && fused_ok_ && tail_ctas_ == 1) {
+        bool csr = true;
+        for (int l = 0; l < tail_first_; ++l) csr = csr && !sdev_[size_t(l)].on;
+        int sms = 0, occ_f = 0, occ_d = 0;
+        TPA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
+        TPA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_vcycle_grid<float>, kTailThreads, 0));
+        TPA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k_vcycle_grid<double>, kTailThreads, 0));
+        if (csr && occ_f >= 1 && occ_d >= 1) coop_grid_ = sms;
     }
     TPA_CUDA(cudaStreamSynchronize(stream_));
     destroy_graphs();

@@ -46,6 +46,7 @@ class StatsC(C.Structure):
 class TuneC(C.Structure):
     _fields_ = [("tail_cells", C.c_int32), ("tail_ctas", C.c_int32), ("structured", C.c_int32),
                 ("vectorized", C.c_int32), ("pdl", C.c_int32), ("fuse_restrict", C.c_int32),
+                ("persistent", C.c_int32),
                 ("ms_per_vcycle", C.c_double)]
 
 

@@ -124,7 +124,7 @@ class EllipticSolver:
     @staticmethod
     def _tune_dict(t):
         return {"tail_cells": t.tail_cells, "tail_ctas": t.tail_ctas, "structured": t.structured,
-                "vectorized": t.vectorized, "pdl": t.pdl, "fuse_restrict": t.fuse_restrict,
+                "vectorized": t.vectorized, "pdl": t.pdl, "fuse_restrict": t.fuse_restrict, "persistent": t.persistent,
                 "ms_per_vcycle": t.ms_per_vcycle}
 
     def autotune(self, precision=None, vcycles=20):
@@ -144,8 +144,8 @@ class EllipticSolver:
 
     def set_tuning(self, **fields):
         """Apply a layout (tail_cells, tail_ctas, structured, vectorized, pdl,
-        fuse_restrict; omitted fields: default)."""
-        keys = ("tail_cells", "tail_ctas", "structured", "vectorized", "pdl", "fuse_restrict")
+        fuse_restrict, persistent; omitted fields: default)."""
+        keys = ("tail_cells", "tail_ctas", "structured", "vectorized", "pdl", "fuse_restrict", "persistent")
         unknown = set(fields) - set(keys)
         if unknown:
             raise ValueError(f"unknown layout fields: {sorted(unknown)}")
