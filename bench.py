@@ -427,20 +427,33 @@ def main():
     achieved = alg32 / (sweep.value * 1e-3) / 1e9
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "droplet_amr":
         from oracle import cgmg
         res = cgmg.bench_droplet(steps=1, warmup=0, levels=args.levels, threads=os.cpu_count())
         cpu = {"value": res["cell_updates_per_s"], "unit": "cell-updates/s", "cores": res["threads"],
                "kind": "port", "sample": "1 full solve of the same droplet workload (setup excluded)"}
+    # DRAM bytes per launch of the roofline kernel from a committed ncu capture
+    traffic = None
+    tp = ROOT / "profiles" / "roofline_traffic.json"
+    if tp.exists():
+        rec = json.loads(tp.read_text()).get(args.workload)
+        if rec:
+            traffic = rec["dram_bytes_per_launch"]
 
     cells_updates = n * mixed_it
     value = world * cells_updates / (mixed_ms * 1e-3)
+    if args.workload == "droplet_amr":
+        metric = "cell-updates/s to rel. residual 1e-10 (droplet AMR pressure solve, mixed FP32/FP64 GMG)"
+        wname = f"droplet_amr levels={args.levels} (unit square, 4x4 roots of 16x16, circle band)"
+    else:
+        metric = f"cell-updates/s to rel. residual 1e-10 ({args.size}^2 uniform periodic solve, mixed FP32/FP64 GMG)"
+        wname = f"uniform_{args.size} (periodic unit square, {args.size // 16}x{args.size // 16} roots of 16x16)"
     line = {
-        "metric": "cell-updates/s to rel. residual 1e-10 (droplet AMR pressure solve, mixed FP32/FP64 GMG)",
+        "metric": metric,
         "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": mixed_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32/f64", "data": "synthetic (seeded Philox)",
-        "config": {"workload": f"droplet_amr levels={args.levels} (unit square, 4x4 roots of 16x16, circle band)",
+        "config": {"workload": wname,
                    "fine_cells": n, "levels": solver.level_sizes(), "parallelism": "replicas" if world > 1 else "1 GPU",
                    "l2": "flushed between steps (256 MiB write)", "device_layout": solver.device_info(),
                    "autotuned_layout": layout, "autotune_s": tune_s},
@@ -452,7 +465,7 @@ def main():
                 "ms_per_step": e2e_ms_mean, "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 8 * n},
         "gpu_launches": mixed_launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "damped-Jacobi sweep, finest level, FP32",
+                     "traffic": traffic, "kernel": "damped-Jacobi sweep, finest level, FP32",
                      "kernel_ms": sweep.value, "kernel_ms_fp64": sweep64.value,
                      "algorithmic_bytes": alg32, "peak_kind": peak_kind},
         "clocks": clk.summary(),

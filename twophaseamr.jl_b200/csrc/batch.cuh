@@ -178,7 +178,24 @@ __global__ void bk_residual(BLevel<T> L, const int* __restrict__ active) {
     L.s[i] = L.td[i] * ri;
 }
 
-// b_c = P_tent'(r - A s) over the coarse rows of C; per-problem coarse RHS sums
+// Restriction sum of coarse row J by four lanes (lane q takes children q, q + 4,
+// ...), combined in the fixed order (c0 + c1) + (c2 + c3); whole warps call it.
+template <typename T>
+__device__ __forceinline__ T brestrict_quad(const BLevel<T>& F, int J, bool valid, int q) {
+    T v = T(0);
+    if (valid)
+        for (int k = F.cptr[J] + q; k < F.cptr[J + 1]; k += 4) {
+            const int i = F.child[k];
+            v += F.r[i] - brow(F, F.s, i);
+        }
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    return v;
+}
+
+// b_c = P_tent'(r - A s) over the coarse rows of C, one thread per coarse row
+// (the merged levels are large: measured faster than four lanes per row);
+// per-problem coarse RHS sums
 template <typename T>
 __global__ void bk_restrict(BLevel<T> F, BLevel<T> C, double* partial, unsigned* counters,
                             const int* __restrict__ active) {
@@ -307,13 +324,15 @@ __global__ void __launch_bounds__(kTailThreads) bk_tail(const BLevel<T>* __restr
         }
         __syncthreads();
         const BLevel<T> C = levels[first + t + 1];
-        for (int J = tl.begin[t + 1] + int(threadIdx.x); J < tl.end[t + 1]; J += blockDim.x) {
-            T v = T(0);
-            for (int c = L.cptr[J]; c < L.cptr[J + 1]; ++c) {
-                const int i = L.child[c];
-                v += L.r[i] - brow(L, L.s, i);
+        {
+            // four lanes per coarse row, over whole warps
+            const int cb = tl.begin[t + 1], nc = tl.end[t + 1] - cb;
+            const int quads = (4 * nc + 31) & ~31;
+            for (int g = int(threadIdx.x); g < quads; g += blockDim.x) {
+                const int J = cb + (g >> 2);
+                const T v = brestrict_quad(L, J, (g >> 2) < nc, g & 3);
+                if ((g & 3) == 0 && (g >> 2) < nc) C.b[J] = v;
             }
-            C.b[J] = v;
         }
         __syncthreads();
     }
