@@ -47,6 +47,25 @@ def workload(levels=4):
     return W.droplet_spec(levels=levels)
 
 
+def rank_share(items, rank, world):
+    """The independent problems one rank solves (round robin; no data exchange)."""
+    return list(items)[rank::world]
+
+
+def combine_over_ranks(max_vals, sum_vals, world, device="cpu"):
+    """Max over ranks of the timings and sum of the work counts (the only
+    collectives of the multi-rank bench: every rank calls it once, in the same
+    order)."""
+    import torch
+    import torch.distributed as dist
+    mx = torch.tensor([float(v) for v in max_vals], dtype=torch.float64, device=device)
+    sm = torch.tensor([float(v) for v in sum_vals], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return [float(v) for v in mx.cpu()], [float(v) for v in sm.cpu()]
+
+
 def reference_arm(args):
     """CPU restatement of the reference solve, on this host's cores."""
     rank = int(os.environ.get("RANK", "0"))
@@ -136,7 +155,7 @@ def batch_main(args):
     if world > 1:
         dist.init_process_group("nccl", device_id=torch.device("cuda", local),
                                 timeout=__import__("datetime").timedelta(seconds=300))
-    problems = W.batch_problems(args.batch)[rank::world]
+    problems = rank_share(W.batch_problems(args.batch), rank, world)
     t0 = time.perf_counter()
 
     def make(p):
@@ -228,15 +247,8 @@ def batch_main(args):
         if k:
             e2e.append((time.perf_counter() - t1) * 1e3)
     e2e_upd = float(np.dot(sizes, its))
-    t = torch.tensor([mixed_ms, fp64_ms, float(np.mean(e2e)), mixed_upd, fp64_upd, e2e_upd,
-                      float(sum(sizes))], dtype=torch.float64, device="cuda")
-    if world > 1:
-        mx = t[:3].clone()
-        sm = t[3:].clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        t = torch.cat([mx, sm])
-    mixed_ms, fp64_ms, e2e_ms, mixed_upd, fp64_upd, e2e_upd, cells = (float(v) for v in t.cpu())
+    (mixed_ms, fp64_ms, e2e_ms), (mixed_upd, fp64_upd, e2e_upd, cells) = combine_over_ranks(
+        [mixed_ms, fp64_ms, float(np.mean(e2e))], [mixed_upd, fp64_upd, e2e_upd, float(sum(sizes))], world, "cuda")
     peak, peak_kind = measured_peaks()
     # algorithmic bytes per fine cell and CG iteration (FP32 V-cycle with variable
     # coefficients, hierarchy factor 4/3, plus the FP64 CG vectors)
@@ -389,11 +401,8 @@ def main():
     x_ref = x_d.clone()
     mixed_err = float((x_mixed - x_ref).abs().max() / x_ref.abs().max())
 
-    # max over ranks
-    t = torch.tensor([mixed_ms, fp64_ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    mixed_ms, fp64_ms = (float(v) for v in t.cpu())
+    # max over ranks (each rank solves its own replica: no work to sum)
+    (mixed_ms, fp64_ms), _ = combine_over_ranks([mixed_ms, fp64_ms], [], world, "cuda")
 
     # end to end through the public C-ABI with pinned host buffers
     rhs_pin = torch.from_numpy(rhs_h).pin_memory()
