@@ -116,8 +116,17 @@ tpa_status tpa_level_info(const tpa_context* ctx, int32_t level, double* smoothe
 tpa_status tpa_level_face_coefficients(const tpa_context* ctx, int32_t level, double* kappa);
 
 /* `_refresh_geometric_multigrid!` (geometric_preconditioner.jl:483-594): new
- * fine face coefficients on the fixed topology; refreshes every level. */
+ * fine face coefficients on the fixed topology; refreshes every level.  Once
+ * the hierarchy is on the device, a refresh that keeps the set of zero
+ * coefficients runs on the GPU (operator values, both Jacobi weights and the
+ * coarse inverse; CSR levels and a coarsest matrix of at most 2048 unknowns);
+ * otherwise, or with TPAGMG_HOST_REFRESH set, the host rebuilds the levels and
+ * uploads them.  Host-side level queries recompute the host copy on demand. */
 tpa_status tpa_refresh(tpa_context* ctx, const double* face_coefficient);
+/* How the last tpa_refresh ran: path 1 = on the host, 2 = on the device,
+ * 0 = none yet; ms = its host wall time.  Replaces nothing in the reference
+ * (measurement support). */
+tpa_status tpa_last_refresh(const tpa_context* ctx, int32_t* path, double* ms);
 
 /* solve!(solution, solver, rhs; rtol, atol, max_cycles, compatibility)
  * (src/solvers/multigrid/elliptic_solver.jl:628-675).  rhs is the strong-form

@@ -1,7 +1,9 @@
 // C-ABI of the B200 pressure solver (declared in include/tpagmg.h).
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -23,6 +25,11 @@ struct tpa_context {
     std::unique_ptr<tpa::DeviceSolver> dev;
     tpa::DevArray<double> d_rhs, d_x, d_y, d_aux, d_face;
     void* user_stream = nullptr;
+    // after a device refresh the host copy of the hierarchy beyond the finest
+    // face coefficients is out of date; host readers recompute it first
+    bool host_stale = false;
+    int refresh_path = 0;  // 1 host, 2 device (tpa_last_refresh)
+    double refresh_ms = 0;
 };
 
 namespace tpa {
@@ -56,9 +63,16 @@ const tpa::LevelOperator& fine_op(const tpa_context* ctx) {
     return ctx->op;
 }
 
+void ensure_host_fresh(tpa_context* ctx) {
+    if (!ctx->host_stale) return;
+    tpa::refresh_hierarchy(ctx->hier, ctx->hier.levels[0].op.kappa);
+    ctx->host_stale = false;
+}
+
 void ensure_device(tpa_context* ctx) {
     if (!ctx->have_hierarchy) throw tpa::Error(TPA_ERR_STATE, "no hierarchy: call tpa_build_hierarchy first");
     if (ctx->uploaded) return;
+    ensure_host_fresh(ctx);
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
     if (e != cudaSuccess || count <= ctx->device)
@@ -366,6 +380,7 @@ tpa_status tpa_build_hierarchy(tpa_context* ctx, const tpa_multigrid_options* op
         if (o.pre_sweeps != o.post_sweeps)
             throw tpa::Error(TPA_ERR_INVALID_ARG,
                              "CG requires equal pre_sweeps and post_sweeps for a geometric multigrid preconditioner");
+        if (ctx->have_hierarchy) ensure_host_fresh(ctx);
         tpa::LevelOperator fine = ctx->have_hierarchy ? ctx->hier.levels[0].op : std::move(ctx->op);
         ctx->have_hierarchy = false;
         ctx->hier = tpa::build_hierarchy(std::move(fine), o);
@@ -405,6 +420,7 @@ tpa_status tpa_level_owners(const tpa_context* cctx, int32_t level, int32_t* own
 tpa_status tpa_level_info(const tpa_context* cctx, int32_t level, double* sw, double* tw, int32_t* comps) {
     auto* ctx = const_cast<tpa_context*>(cctx);
     return guard(ctx, [&] {
+        ensure_host_fresh(ctx);
         const tpa::HostLevel& l = level_of(ctx, level);
         if (sw) *sw = l.weight;
         if (tw) *tw = l.transfer_weight;
@@ -415,23 +431,58 @@ tpa_status tpa_level_info(const tpa_context* cctx, int32_t level, double* sw, do
 tpa_status tpa_level_face_coefficients(const tpa_context* cctx, int32_t level, double* kappa) {
     auto* ctx = const_cast<tpa_context*>(cctx);
     return guard(ctx, [&] {
+        ensure_host_fresh(ctx);
         const tpa::HostLevel& l = level_of(ctx, level);
         std::memcpy(kappa, l.op.kappa.data(), l.op.kappa.size() * sizeof(double));
     });
 }
 
+tpa_status tpa_last_refresh(const tpa_context* cctx, int32_t* path, double* ms) {
+    auto* ctx = const_cast<tpa_context*>(cctx);
+    return guard(ctx, [&] {
+        if (path) *path = ctx->refresh_path;
+        if (ms) *ms = ctx->refresh_ms;
+    });
+}
+
 tpa_status tpa_refresh(tpa_context* ctx, const double* face_coefficient) {
+    const auto t0 = std::chrono::steady_clock::now();
+    auto stamp = [&](int path) {
+        ctx->refresh_path = path;
+        ctx->refresh_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    };
     return guard(ctx, [&] {
         if (!ctx->have_hierarchy) throw tpa::Error(TPA_ERR_STATE, "no hierarchy");
         size_t nf = ctx->hier.levels[0].op.kappa.size();
         for (size_t f = 0; f < nf; ++f)
             if (!std::isfinite(face_coefficient[f]) || face_coefficient[f] < 0)
                 throw tpa::Error(TPA_ERR_INVALID_ARG, "face coefficients must be finite and nonnegative");
+        // the device path keeps the sparsity and the components, so the set of
+        // zero coefficients must not change
+        const std::vector<double>& old = ctx->hier.levels[0].op.kappa;
+        bool same_zeros = old.size() == nf;
+        for (size_t f = 0; same_zeros && f < nf; ++f) same_zeros = (face_coefficient[f] == 0) == (old[f] == 0);
+        if (ctx->uploaded && same_zeros && !std::getenv("TPAGMG_HOST_REFRESH") &&
+            ctx->dev->refresh_applicable(ctx->hier)) {
+            try {
+                ctx->dev->refresh_on_device(ctx->hier, face_coefficient);
+                ctx->hier.levels[0].op.kappa.assign(face_coefficient, face_coefficient + nf);
+                ctx->host_stale = true;
+                stamp(2);
+                return;
+            } catch (const tpa::Error&) {
+                // the host path below reports the same condition; the device copy
+                // is re-uploaded from the host hierarchy
+                ctx->uploaded = false;
+            }
+        }
         tpa::refresh_hierarchy(ctx->hier, std::vector<double>(face_coefficient, face_coefficient + nf));
+        ctx->host_stale = false;
         if (ctx->uploaded) {
             ctx->dev->upload(ctx->hier);
             ctx->dev->invalidate_faces();
         }
+        stamp(1);
     });
 }
 
@@ -661,6 +712,7 @@ tpa_status tpa_batch_create(tpa_batch** out, tpa_context* const* ctxs, int32_t c
             if (!ctxs[k]->have_hierarchy)
                 throw tpa::Error(TPA_ERR_STATE, "problem " + std::to_string(k) + " has no hierarchy");
             if (ctxs[k]->device != ctxs[0]->device) throw tpa::Error(TPA_ERR_INVALID_ARG, "contexts on different devices");
+            ensure_host_fresh(ctxs[k]);
             hs.push_back(&ctxs[k]->hier);
         }
         int devices = 0;
@@ -788,6 +840,7 @@ tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tp
         if (precision != 0 && precision != 1) throw tpa::Error(TPA_ERR_INVALID_ARG, "bad precision");
         if (vcycles <= 0) throw tpa::Error(TPA_ERR_INVALID_ARG, "vcycles must be positive");
         ensure_device(ctx);
+        ensure_host_fresh(ctx);  // stencil copies come from the host levels
         tpa::DeviceSolver& d = *ctx->dev;
         std::vector<tpa::TuneConfig> cand;
         for (int cells : {1024, 2048, 4096, 8192})
@@ -842,6 +895,7 @@ tpa_status tpa_set_tuning(tpa_context* ctx, const tpa_tune_config* cfg) {
         if (!cfg) throw tpa::Error(TPA_ERR_INVALID_ARG, "null configuration");
         if (cfg->tail_ctas > 8 || cfg->structured > 2) throw tpa::Error(TPA_ERR_INVALID_ARG, "bad configuration");
         ensure_device(ctx);
+        ensure_host_fresh(ctx);  // stencil copies come from the host levels
         ctx->dev->reconfigure(ctx->hier, from_c(*cfg));
     });
 }

@@ -426,6 +426,8 @@ template <> DevLevelT<float>& DeviceSolver::lv<float>(int l) { return levels_[si
 void DeviceSolver::upload(const Hierarchy& h) {
     TPA_CUDA(cudaSetDevice(device_));
     TPA_CUDA(cudaStreamSynchronize(stream_));
+    rl_ready_ = false;  // the refresh term lists belong to the previous topology
+    rl_.clear();
     levels_.clear();
     levels_.resize(h.levels.size());
     pre_ = h.opts.pre_sweeps;

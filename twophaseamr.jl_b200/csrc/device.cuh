@@ -243,6 +243,35 @@ public:
     int structured_levels() const;
     int64_t exception_rows() const;
 
+    // ---- coefficient refresh on the device (csrc/refresh.cu) ----
+    // Largest augmented coarsest matrix the device refresh factors (larger: host path).
+    static constexpr int kRefreshMaxCoarse = 2048;
+    // The device path applies when no level keeps stencil coefficients of its
+    // own and the coarsest matrix is small enough.
+    bool refresh_applicable(const Hierarchy& h) const;
+    // New finest-level face coefficients (host array, the uploaded topology):
+    // every level operator, D^-1, Dt^-1, both weights and the coarse inverse are
+    // recomputed on the GPU.  `h` supplies the topology the first time.
+    void refresh_on_device(const Hierarchy& h, const double* kappa_host);
+    // smoother and transfer weight per level, as uploaded or refreshed
+    std::vector<double> level_weights();
+
+private:
+    struct RefreshLevel {
+        int nf = 0, nnz = 0;
+        DevArray<int> tptr, tf, tg, rptr, ridx;
+        DevArray<double> tc, rw, kappa, sk;
+    };
+    void prepare_refresh(const Hierarchy& h);
+    std::vector<RefreshLevel> rl_;
+    bool rl_ready_ = false;
+    int coarse_N_ = 0, coarse_ncomp_ = 0;
+    bool lu_cluster_ = false;  // coarse LU on a cluster with the rows in shared memory
+    DevArray<double> coarse_M_, rwtw_, rpart_;
+    DevArray<int> coarse_piv_, rerr_;
+    DevArray<unsigned> rcnt_;
+
+public:
     // ---- adjoint (csrc/adjoint.cu) ----
     // Finest-level faces, the inverse face metric K as CSR rows (diagonal
     // first) and sqrt(kappa); uploaded on first use and after every refresh.

@@ -73,6 +73,7 @@ SIGNATURES = {
     "tpa_level_info": (C.c_int32, [P, C.c_int32, f64p, f64p, i32p]),
     "tpa_level_face_coefficients": (C.c_int32, [P, C.c_int32, f64p]),
     "tpa_refresh": (C.c_int32, [P, f64p]),
+    "tpa_last_refresh": (C.c_int32, [P, i32p, f64p]),
     "tpa_solve": (C.c_int32, [P, f64p, f64p, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int32,
                               C.POINTER(StatsC)]),
     "tpa_solve_device": (C.c_int32, [P, P, P, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int32,

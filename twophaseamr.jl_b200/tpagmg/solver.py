@@ -166,6 +166,13 @@ class EllipticSolver:
         self.ctx.call("tpa_refresh", _lib.ptr(self._kappa, C.c_double))
         self.operator.face_coefficient = self._kappa.copy()
 
+    def last_refresh(self):
+        """How the last `refresh` ran: ("host" | "device" | None, wall ms)."""
+        path = C.c_int32()
+        ms = C.c_double()
+        self.ctx.call("tpa_last_refresh", C.byref(path), C.byref(ms))
+        return {0: None, 1: "host", 2: "device"}[path.value], ms.value
+
     def apply(self, x):
         x = _lib.f64(x)
         y = np.empty_like(x)
