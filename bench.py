@@ -435,6 +435,30 @@ def main():
     peak, peak_kind = measured_peaks()
     achieved = alg32 / (sweep.value * 1e-3) / 1e9
 
+    # the per-step coefficient refresh (`_refresh_geometric_multigrid!`), after
+    # the timed solves: device path, then the host path, median wall ms
+    refresh = None
+    if args.workload == "droplet_amr":
+        def refresh_ms(reps, host):
+            if host:
+                os.environ["TPAGMG_HOST_REFRESH"] = "1"
+            out, path = [], None
+            try:
+                for k in range(reps):
+                    solver.refresh(kappa * (1.0 + 0.01 * (k % 3)))
+                    path, ms = solver.last_refresh()
+                    out.append(ms)
+            finally:
+                os.environ.pop("TPAGMG_HOST_REFRESH", None)
+            return path, float(np.median(out))
+        solver.refresh(kappa)  # the first device refresh lists the entry terms (set-up)
+        dpath, dms = refresh_ms(10, False)
+        hpath, hms = refresh_ms(3, True)
+        solver.refresh(kappa)
+        refresh = {"device_ms": dms, "device_path": dpath, "host_ms": hms, "host_path": hpath,
+                   "what": "tpa_refresh wall time: new face coefficients -> every level operator, "
+                           "Jacobi and transfer weights, coarse inverse"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "droplet_amr":
         from oracle import cgmg
@@ -479,6 +503,7 @@ def main():
                      "algorithmic_bytes": alg32, "peak_kind": peak_kind},
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
+        "refresh": refresh,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

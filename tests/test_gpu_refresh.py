@@ -135,8 +135,43 @@ def test_refresh_with_new_zero_faces_takes_the_host_path():
     assert np.max(np.abs(a - b)) <= 1e-10 * np.max(np.abs(b))
 
 
+@pytest.mark.parametrize("case", ["pruned_b8", "droplet_l2"])
+def test_device_refresh_of_stencil_levels(case, monkeypatch):
+    """Variable-coefficient block-structured levels (stencil couplings plus
+    exception rows): the device refresh gathers their copies from the refreshed
+    operator; the cycle matches the host refresh and solves match the oracle."""
+    spec, coarse = CASES[case]
+    m = BlockTreeMesh(**spec)
+    k1, k2 = coefficients(m, 31), coefficients(m, 32)
+
+    def stencil_solver():
+        s = EllipticSolver(PoissonOperator(m, k1), multigrid=MultigridOptions(coarse_size=coarse))
+        s.set_tuning(structured=2, tail_cells=64)
+        return s
+
+    dev, host = stencil_solver(), stencil_solver()
+    assert dev.device_info()["structured_levels"] >= 1
+    dev.refresh(k2)
+    assert dev.last_refresh()[0] == "device"
+    monkeypatch.setenv("TPAGMG_HOST_REFRESH", "1")
+    host.refresh(k2)
+    monkeypatch.delenv("TPAGMG_HOST_REFRESH")
+    assert dev.device_info()["structured_levels"] == host.device_info()["structured_levels"] >= 1
+    r = zero_mean_residual(m, 33)
+    for precision, tol in (("fp64", 1e-12), ("mixed", 1e-6)):
+        za, zb = dev.vcycle(r, precision), host.vcycle(r, precision)
+        assert np.max(np.abs(za - zb)) <= tol * np.max(np.abs(zb)), precision
+    rhs = W.gaussian_rhs(m, 34)
+    oo = OOp(block_tree_mesh(**spec), k2)
+    ref, _ = osolve(oo, TreeGeometricMultigrid(oo, OMG(coarse_size=coarse)), rhs, rtol=1e-12)
+    x = np.zeros(m.ncells)
+    assert solve(x, dev, rhs, rtol=1e-12).converged
+    assert np.max(np.abs(x - ref)) <= 1e-10 * np.max(np.abs(ref))
+
+
 def test_refresh_of_structured_levels_takes_the_host_path():
-    """Stencil copies hold coefficients of their own: refreshed on the host."""
+    """Levels kept as one constant coupling change layout when the
+    coefficients vary: refreshed on the host."""
     m = BlockTreeMesh(**W.taylor_green_spec())
     s = EllipticSolver(PoissonOperator(m), multigrid=MultigridOptions(coarse_size=64))
     assert s.device_info()["structured_levels"] >= 1

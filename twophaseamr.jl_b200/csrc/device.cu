@@ -417,6 +417,7 @@ DeviceSolver::~DeviceSolver() {
     levels_.clear();
     if (host_sc_) cudaFreeHost(host_sc_);
     if (host_d_) cudaFreeHost(host_d_);
+    if (rstage_) cudaFreeHost(rstage_);
     if (own_stream_) cudaStreamDestroy(own_stream_);
 }
 

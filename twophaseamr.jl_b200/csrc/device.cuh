@@ -261,12 +261,18 @@ private:
         int nf = 0, nnz = 0;
         DevArray<int> tptr, tf, tg, rptr, ridx;
         DevArray<double> tc, rw, kappa, sk;
+        // block-structured level: CSR positions of the east / north couplings
+        // per cell (-1: none) and of the exception rows' entries
+        bool structured = false;
+        int nex_entries = 0;
+        DevArray<int> sx, sy, sex;
     };
     void prepare_refresh(const Hierarchy& h);
     std::vector<RefreshLevel> rl_;
     bool rl_ready_ = false;
     int coarse_N_ = 0, coarse_ncomp_ = 0;
     bool lu_cluster_ = false;  // coarse LU on a cluster with the rows in shared memory
+    double* rstage_ = nullptr; // pinned staging of the finest-level coefficients
     DevArray<double> coarse_M_, rwtw_, rpart_;
     DevArray<int> coarse_piv_, rerr_;
     DevArray<unsigned> rcnt_;

@@ -19,8 +19,10 @@
 #include <cstring>
 
 #include <cooperative_groups.h>
+#include <cuda_pipeline.h>
 
 #include "device.cuh"
+#include "structure.hpp"
 
 namespace tpa {
 namespace {
@@ -135,6 +137,30 @@ __global__ void kr_weights(int n, const int* __restrict__ rp, const int* __restr
     }
 }
 
+// stencil copies of a block-structured level: east / north couplings -a_ij
+// gathered from the refreshed operator (0 where the entry is absent)
+__global__ void kr_gather_stencil(int n, const int* __restrict__ px, const int* __restrict__ py,
+                                  const double* __restrict__ val, double* __restrict__ cx_d, float* __restrict__ cx_f,
+                                  double* __restrict__ cy_d, float* __restrict__ cy_f) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double cx = px[i] >= 0 ? -val[px[i]] : 0.0, cy = py[i] >= 0 ? -val[py[i]] : 0.0;
+        cx_d[i] = cx;
+        cx_f[i] = float(cx);
+        cy_d[i] = cy;
+        cy_f[i] = float(cy);
+    }
+}
+
+// the exception rows' values (their CSR entries in row order)
+__global__ void kr_gather(int m, const int* __restrict__ pos, const double* __restrict__ val,
+                          double* __restrict__ out_d, float* __restrict__ out_f) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        const double v = val[pos[k]];
+        out_d[k] = v;
+        out_f[k] = float(v);
+    }
+}
+
 // the augmented coarsest matrix [A v; v' 0] (M zeroed before)
 __global__ void kr_coarse_fill(int n, int N, const int* __restrict__ rp, const int* __restrict__ ci,
                                const double* __restrict__ val, const int* __restrict__ slot,
@@ -166,26 +192,31 @@ __device__ __forceinline__ void lu_sync() {
     else __syncthreads();
 }
 
+constexpr int kLuMaxCluster = 8;
+
 // LU with partial pivoting of the augmented coarsest matrix M (N x N,
 // row-major, overwritten by the factors; piv[k] = row exchanged with row k).
-// Cl: the rows are spread cyclically over the CTAs of a thread-block cluster
-// (row r on CTA r % C at local row r / C) and held in shared memory, each CTA
-// reading the pivot row and the candidates of the others through distributed
-// shared memory; otherwise one CTA works on M in global memory.  Each step
-// follows the host factorisation operation for operation: the pivot is the
-// first row of largest |M[r][k]| (r >= k), rows k and p are exchanged whole,
-// l = M[r][k] * (1 / M[k][k]) overwrites M[r][k] and M[r][c] -= l M[k][c]
-// (c > k, l != 0).  The search for the next pivot is fused into the update.
-// err = 2 on a zero pivot.
+// Cl: the rows are spread cyclically over the C CTAs of a thread-block cluster
+// (row r on CTA r % C at local row r / C) and held in shared memory; otherwise
+// one CTA works on M in global memory (C = 1).  Each step follows the host
+// factorisation operation for operation: the pivot is the first row of largest
+// |M[r][k]| (r >= k), rows k and p are exchanged whole, l = M[r][k] *
+// (1 / M[k][k]) overwrites M[r][k] and M[r][c] -= l M[k][c] (c > k, l != 0).
+//
+// One cluster barrier per step: after its update every CTA pushes its best
+// candidate for the next pivot -- value, row and the whole row -- into the
+// shared memory of every CTA, and the owner of row k + 1 pushes that row too,
+// so the next step picks the pivot and exchanges rows from local copies.  The
+// push buffers alternate between two sets (a step reads one while the pushes
+// for the next fill the other).  err = 2 on a zero pivot.
 template <bool Cl>
 __global__ void __launch_bounds__(1024) kr_lu(int N, double* __restrict__ M, int* __restrict__ piv, int* err) {
     namespace cg = cooperative_groups;
     extern __shared__ double lu_sm[];
     __shared__ double wv[32];
     __shared__ int wi[32];
-    __shared__ double cand_v;
-    __shared__ int cand_i;
-    __shared__ int pivot;
+    __shared__ double cval[2][kLuMaxCluster];
+    __shared__ int cidx[2][kLuMaxCluster];
     int C = 1, rank = 0;
     if constexpr (Cl) {
         C = int(cg::this_cluster().num_blocks());
@@ -193,19 +224,21 @@ __global__ void __launch_bounds__(1024) kr_lu(int N, double* __restrict__ M, int
     }
     const int R = (N + C - 1) / C;
     double* rows = Cl ? lu_sm : M;
-    double* prow = Cl ? lu_sm + size_t(R) * N : lu_sm;
-    double* trow = prow + N;
+    double* cbuf = Cl ? lu_sm + size_t(R) * N : lu_sm;  // [2][C][N] candidate rows by source
+    double* kbuf = cbuf + size_t(2) * C * N;             // [2][N] row k before the exchange
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = int(blockDim.x >> 5);
+    // the same shared-memory word in CTA q of the cluster (this CTA's own for C = 1)
+    auto peer = [&](auto* ptr, int q) {
+        if constexpr (Cl) return cg::this_cluster().map_shared_rank(ptr, q);
+        else return ptr;
+    };
+    const size_t cb_off = size_t(cbuf - lu_sm), kb_off = size_t(kbuf - lu_sm);
     auto first_local = [&](int j) {  // smallest local row whose global row is >= j
         const int t = j - rank;
         return t <= 0 ? 0 : (t + C - 1) / C;
     };
-    auto row_of = [&](int owner, int r) -> double* {
-        double* base = rows;
-        if constexpr (Cl) base = cg::this_cluster().map_shared_rank(rows, owner);
-        return base + size_t(r / C) * N;
-    };
-    auto publish = [&](double bv, int bi) {  // this CTA's candidate into cand_v / cand_i
+    // CTA-wide best (value, row); every thread returns the same pair
+    auto reduce = [&](double bv, int bi, double& v, int& i) {
         for (int o = 16; o; o >>= 1) better(bv, bi, __shfl_down_sync(0xffffffffu, bv, o),
                                             __shfl_down_sync(0xffffffffu, bi, o));
         if (!lane) {
@@ -213,12 +246,31 @@ __global__ void __launch_bounds__(1024) kr_lu(int N, double* __restrict__ M, int
             wi[wid] = bi;
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            double v = wv[0];
-            int i = wi[0];
-            for (int w = 1; w < nw; ++w) better(v, i, wv[w], wi[w]);
-            cand_v = v;
-            cand_i = i;
+        v = lane < nw ? wv[lane] : -1.0;
+        i = lane < nw ? wi[lane] : N;
+        for (int o = 16; o; o >>= 1) better(v, i, __shfl_xor_sync(0xffffffffu, v, o), __shfl_xor_sync(0xffffffffu, i, o));
+    };
+    // the candidate (v, i) and row i, and row j if this CTA owns it, into set b everywhere
+    auto push = [&](int b, double v, int i, int j) {
+        if (threadIdx.x < C) {
+            *peer(&cval[b][rank], int(threadIdx.x)) = v;
+            *peer(&cidx[b][rank], int(threadIdx.x)) = i;
+        }
+        if (i < N) {
+            const double* src = rows + size_t(i / C) * N;
+            const size_t off = cb_off + (size_t(b) * C + rank) * N;
+            for (int c = threadIdx.x; c < N; c += blockDim.x) {
+                const double x = src[c];
+                for (int q = 0; q < C; ++q) *peer(lu_sm + off + c, q) = x;
+            }
+        }
+        if (j < N && j % C == rank) {
+            const double* src = rows + size_t(j / C) * N;
+            const size_t off = kb_off + size_t(b) * N;
+            for (int c = threadIdx.x; c < N; c += blockDim.x) {
+                const double x = src[c];
+                for (int q = 0; q < C; ++q) *peer(lu_sm + off + c, q) = x;
+            }
         }
     };
     if constexpr (Cl) {
@@ -228,51 +280,34 @@ __global__ void __launch_bounds__(1024) kr_lu(int N, double* __restrict__ M, int
         __syncthreads();
     }
     {
-        double bv = -1.0;
-        int bi = N;
+        double bv = -1.0, v;
+        int bi = N, i;
         for (int lr = first_local(0) + int(threadIdx.x); lr < R && lr * C + rank < N; lr += blockDim.x)
             better(bv, bi, fabs(rows[size_t(lr) * N]), lr * C + rank);
-        publish(bv, bi);
+        reduce(bv, bi, v, i);
+        push(0, v, i, 0);
     }
     lu_sync<Cl>();
     for (int k = 0; k < N; ++k) {
-        if (wid == 0) {
-            double v = -1.0;
-            int i = N;
-            if (lane < C) {
-                if constexpr (Cl) {
-                    v = *cg::this_cluster().map_shared_rank(&cand_v, lane);
-                    i = *cg::this_cluster().map_shared_rank(&cand_i, lane);
-                } else {
-                    v = cand_v;
-                    i = cand_i;
-                }
-            }
-            for (int o = 16; o; o >>= 1) better(v, i, __shfl_down_sync(0xffffffffu, v, o),
-                                                __shfl_down_sync(0xffffffffu, i, o));
-            if (lane == 0) {
-                pivot = (v > 0.0 && i < N) ? i : -1;
-                if (rank == 0) piv[k] = i < N ? i : k;
-            }
-        }
-        __syncthreads();
-        const int p = pivot;
-        if (p < 0) {
+        const int b = k & 1;
+        // lane q of every group of eight holds the candidate pushed by CTA q
+        const int q8 = lane & (kLuMaxCluster - 1);
+        double v = q8 < C ? cval[b][q8] : -1.0;
+        int p = q8 < C ? cidx[b][q8] : N;
+        for (int o = 4; o; o >>= 1) better(v, p, __shfl_xor_sync(0xffffffffu, v, o), __shfl_xor_sync(0xffffffffu, p, o));
+        const int src = p % C;  // the owner of row p pushed it
+        if (!(v > 0.0) || p >= N) {  // every CTA takes the same decision
             if (rank == 0 && threadIdx.x == 0) atomicExch(err, 2);
-            break;  // every CTA takes the same decision
+            break;
         }
-        const double* src_p = row_of(p % C, p);
-        for (int c = threadIdx.x; c < N; c += blockDim.x) prow[c] = src_p[c];
-        if (p != k && rank == p % C) {
-            const double* src_k = row_of(k % C, k);
-            for (int c = threadIdx.x; c < N; c += blockDim.x) trow[c] = src_k[c];
-        }
-        lu_sync<Cl>();  // rows k and p are read everywhere before they change
+        if (rank == 0 && threadIdx.x == 0) piv[k] = p;
+        const double* prow = cbuf + (size_t(b) * C + src) * N;
+        const double* krow = kbuf + size_t(b) * N;
         if (p != k) {
             if (rank == k % C)
                 for (int c = threadIdx.x; c < N; c += blockDim.x) rows[size_t(k / C) * N + c] = prow[c];
             if (rank == p % C)
-                for (int c = threadIdx.x; c < N; c += blockDim.x) rows[size_t(p / C) * N + c] = trow[c];
+                for (int c = threadIdx.x; c < N; c += blockDim.x) rows[size_t(p / C) * N + c] = krow[c];
         }
         __syncthreads();
         const double inv = 1.0 / prow[k];
@@ -289,10 +324,13 @@ __global__ void __launch_bounds__(1024) kr_lu(int N, double* __restrict__ M, int
                 if (k + 1 < N) better(bv, bi, fabs(row[k + 1]), lr * C + rank);
             }
         }
-        publish(bv, bi);
-        lu_sync<Cl>();  // updates and candidates complete before the next step
+        double nv;
+        int ni;
+        reduce(bv, bi, nv, ni);  // its barrier also orders the updates before the pushes
+        if (k + 1 < N) push(b ^ 1, nv, ni, k + 1);
+        lu_sync<Cl>();
     }
-    lu_sync<Cl>();  // no CTA leaves while another may still read its rows
+    lu_sync<Cl>();  // no CTA leaves while another may still write into its buffers
     if constexpr (Cl) {
         for (int lr = 0; lr < R && lr * C + rank < N; ++lr)
             for (int c = threadIdx.x; c < N; c += blockDim.x)
@@ -300,49 +338,105 @@ __global__ void __launch_bounds__(1024) kr_lu(int N, double* __restrict__ M, int
     }
 }
 
+// Shared memory (bytes) of kr_lu: rows (cluster form only), two sets of C
+// candidate rows and two copies of row k.
+size_t lu_smem(int N, int C, bool cluster) {
+    const size_t R = size_t((N + C - 1) / C);
+    return ((cluster ? R * size_t(N) : 0) + 2 * size_t(C) * N + 2 * size_t(N)) * sizeof(double);
+}
+
+constexpr int kInvWarps = 8;  // columns of the inverse per CTA
+constexpr int kInvStages = 4; // factor rows in flight
+
 // The first n columns of M^-1 from the factors, one warp per column: e = P
 // e_col (a unit vector: only its position moves), forward substitution with
 // the unit lower factor (rows above the 1 stay zero), back substitution with
-// the upper factor; G[r][col] = e[r] for r < n.  Dot products run across the
-// lanes with a fixed shuffle tree (deterministic).
-__global__ void __launch_bounds__(128) kr_coarse_inv(int N, int n, const double* __restrict__ M,
-                                                     const int* __restrict__ piv, double* __restrict__ G,
-                                                     const int* __restrict__ err) {
+// the upper factor; G[r][col] = e[r] for r < n.  The CTA streams the factor
+// rows through a ring of shared-memory stages (asynchronous copies kInvStages
+// - 1 rows ahead), every warp taking its dot product from the staged row; dot
+// products run across the lanes with a fixed shuffle tree (deterministic).
+__global__ void __launch_bounds__(32 * kInvWarps) kr_coarse_inv(int N, int n, const double* __restrict__ M,
+                                                               const int* __restrict__ piv,
+                                                               double* __restrict__ G,
+                                                               const int* __restrict__ err) {
     extern __shared__ double inv_sm[];
+    __shared__ int first;
+    if (*err) return;  // uniform over the grid
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int col = int(blockIdx.x) * int(blockDim.x >> 5) + wid;
-    if (col >= n || *err) return;  // whole warps; no block-wide barrier follows
+    const int col = int(blockIdx.x) * kInvWarps + wid;
     double* e = inv_sm + size_t(wid) * N;
-    int pos = col;
-    for (int k = 0; k < N; ++k) {
-        const int p = piv[k];
-        if (pos == k) pos = p;
-        else if (pos == p) pos = k;
+    double* ring = inv_sm + size_t(kInvWarps) * N;
+    if (threadIdx.x == 0) first = N;
+    __syncthreads();
+    int pos = N;  // warps past the last column idle through the barriers
+    if (col < n) {
+        pos = col;
+        for (int k = 0; k < N; ++k) {
+            const int p = piv[k];
+            if (pos == k) pos = p;
+            else if (pos == p) pos = k;
+        }
+        for (int r = lane; r < N; r += 32) e[r] = r == pos ? 1.0 : 0.0;
+        if (lane == 0) atomicMin(&first, pos);
     }
-    for (int r = lane; r < N; r += 32) e[r] = r == pos ? 1.0 : 0.0;
-    __syncwarp();
-    for (int r = pos + 1; r < N; ++r) {
-        const double* Mr = M + size_t(r) * N;
-        double s = 0.0;
-        for (int k = pos + lane; k < r; k += 32) s += Mr[k] * e[k];
-        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) e[r] -= s;
-        __syncwarp();
+    __syncthreads();
+    const int r0 = first + 1;  // rows above stay zero in every column of this CTA
+    // forward: row r of the lower factor, columns [first, r)
+    auto load_fwd = [&](int r) {
+        if (r < N) {
+            double* dst = ring + size_t(r % kInvStages) * N;
+            const double* srow = M + size_t(r) * N;
+            for (int c = first + int(threadIdx.x); c < r; c += blockDim.x) __pipeline_memcpy_async(dst + c, srow + c, 8);
+        }
+        __pipeline_commit();
+    };
+    for (int j = 0; j < kInvStages - 1; ++j) load_fwd(r0 + j);
+    for (int r = r0; r < N; ++r) {
+        __pipeline_wait_prior(kInvStages - 2);
+        __syncthreads();  // row r is staged; the stage refilled next was read by everyone
+        load_fwd(r + kInvStages - 1);
+        if (r > pos) {
+            const double* mr = ring + size_t(r % kInvStages) * N;
+            double s = 0.0;
+            for (int k = pos + lane; k < r; k += 32) s += mr[k] * e[k];
+            for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) e[r] -= s;
+            __syncwarp();
+        }
     }
+    __pipeline_wait_prior(0);
+    __syncthreads();
+    // backward: row r of the upper factor, columns [r, N)
+    auto load_bwd = [&](int r) {
+        if (r >= 0) {
+            double* dst = ring + size_t(r % kInvStages) * N;
+            const double* srow = M + size_t(r) * N;
+            for (int c = r + int(threadIdx.x); c < N; c += blockDim.x) __pipeline_memcpy_async(dst + c, srow + c, 8);
+        }
+        __pipeline_commit();
+    };
+    for (int j = 0; j < kInvStages - 1; ++j) load_bwd(N - 1 - j);
     for (int r = N - 1; r >= 0; --r) {
-        const double* Mr = M + size_t(r) * N;
-        double s = 0.0;
-        for (int k = r + 1 + lane; k < N; k += 32) s += Mr[k] * e[k];
-        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) e[r] = (e[r] - s) / Mr[r];
-        __syncwarp();
+        __pipeline_wait_prior(kInvStages - 2);
+        __syncthreads();
+        load_bwd(r - (kInvStages - 1));
+        if (col < n) {
+            const double* mr = ring + size_t(r % kInvStages) * N;
+            double s = 0.0;
+            for (int k = r + 1 + lane; k < N; k += 32) s += mr[k] * e[k];
+            for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) e[r] = (e[r] - s) / mr[r];
+            __syncwarp();
+        }
     }
-    for (int r = lane; r < n; r += 32) G[size_t(r) * n + col] = e[r];
+    if (col < n)
+        for (int r = lane; r < n; r += 32) G[size_t(r) * n + col] = e[r];
 }
 
-constexpr int kLuCluster = 8;      // CTAs sharing the rows of the coarsest matrix
+size_t inv_smem(int N) { return size_t(kInvWarps + kInvStages) * size_t(N) * sizeof(double); }
+
+constexpr int kLuCluster = 8;  // CTAs sharing the rows of the coarsest matrix
 constexpr int kLuClusterThreads = 512;
-constexpr int kInvWarps = 4;       // columns of the inverse per CTA
 
 }  // namespace
 
@@ -421,6 +515,40 @@ void DeviceSolver::prepare_refresh(const Hierarchy& h) {
         R.kappa.alloc(size_t(std::max<int64_t>(nf, 1)));
         R.sk.alloc(size_t(std::max<int64_t>(nf, 1)));
         const HostLevel& hl = h.levels[size_t(l)];
+        if (size_t(l) < sdev_.size() && sdev_[size_t(l)].on) {
+            // the same block structure as the stencil copies (upload_structured)
+            const StructLevel st = build_struct(hl, &h.levels[size_t(l + 1)].op.mesh);
+            const int nx = st.nx, ny = st.ny, cpb = nx * ny;
+            auto neighbour = [&](int64_t c, int d) -> int64_t {  // 0 W, 1 E, 2 S, 3 N
+                const int64_t b = c / cpb, r = c % cpb;
+                int i = int(r % nx) + (d == 0 ? -1 : d == 1 ? 1 : 0), j = int(r / nx) + (d == 2 ? -1 : d == 3 ? 1 : 0);
+                if (i >= 0 && i < nx && j >= 0 && j < ny) return b * cpb + j * nx + i;
+                const int32_t q = st.nbr[size_t(4 * b + d)];
+                if (q < 0) return -1;
+                return int64_t(q) * cpb + ((j + ny) % ny) * nx + (i + nx) % nx;
+            };
+            auto at = [&](int64_t r, int64_t c) -> int {
+                if (c < 0) return -1;
+                auto b = A.col.begin() + A.ptr[size_t(r)], e = A.col.begin() + A.ptr[size_t(r + 1)];
+                auto it = std::lower_bound(b, e, int32_t(c));
+                return (it == e || *it != c) ? -1 : int(it - A.col.begin());
+            };
+            std::vector<int> px(size_t(A.n)), py(size_t(A.n)), sex;
+            for (int64_t c = 0; c < A.n; ++c) {
+                px[size_t(c)] = at(c, neighbour(c, 1));
+                py[size_t(c)] = at(c, neighbour(c, 3));
+                if (st.ex[size_t(c)] >= 0)
+                    for (int64_t k = A.ptr[size_t(c)]; k < A.ptr[size_t(c + 1)]; ++k) sex.push_back(int(k));
+            }
+            if (int64_t(sex.size()) != int64_t(st.ex_val.size()))
+                throw Error(7, "exception rows of the device refresh disagree with the stencil copies");
+            R.structured = true;
+            R.nex_entries = int(sex.size());
+            R.sx.upload(px.data(), px.size(), stream_);
+            R.sy.upload(py.data(), py.size(), stream_);
+            R.sex.upload(sex.data(), sex.size(), stream_);
+            TPA_CUDA(cudaStreamSynchronize(stream_));
+        }
         if (l + 1 < nl) {
             std::vector<int> rptr(hl.rptr.begin(), hl.rptr.end());
             R.rptr.upload(rptr.data(), rptr.size(), stream_);
@@ -437,10 +565,11 @@ void DeviceSolver::prepare_refresh(const Hierarchy& h) {
     {
         // the cluster LU when a cluster's shared memory holds the matrix
         const int N = coarse_N_;
-        const size_t cl_bytes = (size_t((N + kLuCluster - 1) / kLuCluster) * N + 2 * size_t(N)) * sizeof(double);
         int optin = 0;
         TPA_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
-        lu_cluster_ = cl_bytes + 1024 <= size_t(optin) && !std::getenv("TPAGMG_LU_ONE_CTA");
+        const size_t room = size_t(optin) - 1024;  // static shared memory of the kernels
+        const size_t cl_bytes = lu_smem(N, kLuCluster, true);
+        lu_cluster_ = cl_bytes <= room && !std::getenv("TPAGMG_LU_ONE_CTA");
         if (lu_cluster_) {
             TPA_CUDA(cudaFuncSetAttribute(kr_lu<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(cl_bytes)));
             cudaLaunchConfig_t cfg;
@@ -461,10 +590,15 @@ void DeviceSolver::prepare_refresh(const Hierarchy& h) {
                 lu_cluster_ = false;
             }
         }
-        const size_t inv_bytes = size_t(kInvWarps) * size_t(N) * sizeof(double);
+        const size_t one_bytes = lu_smem(N, 1, false), inv_bytes = inv_smem(N);
+        if (one_bytes > room || inv_bytes > room) throw Error(5, "coarsest matrix too large for the device refresh");
+        TPA_CUDA(cudaFuncSetAttribute(kr_lu<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(one_bytes)));
         TPA_CUDA(cudaFuncSetAttribute(kr_coarse_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, int(inv_bytes)));
     }
     coarse_piv_.alloc(size_t(coarse_N_));
+    if (rstage_) cudaFreeHost(rstage_);
+    rstage_ = nullptr;
+    TPA_CUDA(cudaMallocHost(&rstage_, sizeof(double) * std::max<size_t>(1, size_t(rl_[0].nf))));
     rwtw_.alloc(size_t(2 * nl));
     rpart_.alloc(size_t(2 * 1184));
     rcnt_.alloc(1);
@@ -476,7 +610,10 @@ void DeviceSolver::prepare_refresh(const Hierarchy& h) {
 }
 
 bool DeviceSolver::refresh_applicable(const Hierarchy& h) const {
-    if (structured_levels() > 0) return false;  // stencil copies hold coefficients of their own
+    // stencil copies are gathered from the refreshed operator; a level kept as
+    // one constant coupling or diagonal would change layout, so it needs the host
+    for (const StructDev& D : sdev_)
+        if (D.on && (D.const_coef || D.const_diag)) return false;
     const HostLevel& c = h.levels.back();
     const int64_t N = c.op.A.n + (c.op.singular ? int64_t(c.op.comp.volume.size()) : 0);
     return N <= kRefreshMaxCoarse;
@@ -488,14 +625,22 @@ void DeviceSolver::refresh_on_device(const Hierarchy& h, const double* kappa_hos
     const int nl = int(levels_.size());
     cudaStream_t s = stream_;
     TPA_CUDA(cudaMemsetAsync(rerr_.p, 0, sizeof(int), s));
-    TPA_CUDA(cudaMemcpyAsync(rl_[0].kappa.p, kappa_host, sizeof(double) * size_t(rl_[0].nf), cudaMemcpyHostToDevice,
-                             s));
+    std::memcpy(rstage_, kappa_host, sizeof(double) * size_t(rl_[0].nf));  // no copy is in flight here
+    TPA_CUDA(cudaMemcpyAsync(rl_[0].kappa.p, rstage_, sizeof(double) * size_t(rl_[0].nf), cudaMemcpyHostToDevice, s));
     for (int l = 0; l < nl; ++l) {
         RefreshLevel& R = rl_[size_t(l)];
         DevLevel& L = levels_[size_t(l)];
         if (R.nf > 0) kr_sqrt<<<rgrid(R.nf), kRThreads, 0, s>>>(R.nf, R.kappa.p, R.sk.p);
         kr_assemble<<<rgrid(R.nnz), kRThreads, 0, s>>>(R.nnz, R.tptr.p, R.tf.p, R.tg.p, R.tc.p, R.kappa.p, R.sk.p,
                                                       L.d.val.p, L.f.val.p);
+        if (R.structured) {
+            StructDev& D = sdev_[size_t(l)];
+            kr_gather_stencil<<<rgrid(L.n), kRThreads, 0, s>>>(L.n, R.sx.p, R.sy.p, L.d.val.p, D.cx_d.p, D.cx_f.p,
+                                                               D.cy_d.p, D.cy_f.p);
+            if (R.nex_entries)
+                kr_gather<<<rgrid(R.nex_entries), kRThreads, 0, s>>>(R.nex_entries, R.sex.p, L.d.val.p, D.exv_d.p,
+                                                                     D.exv_f.p);
+        }
         if (l + 1 < nl && rl_[size_t(l + 1)].nf > 0)
             kr_restrict<<<rgrid(rl_[size_t(l + 1)].nf), kRThreads, 0, s>>>(rl_[size_t(l + 1)].nf, R.rptr.p, R.ridx.p,
                                                                            R.rw.p, R.kappa.p,
@@ -511,13 +656,12 @@ void DeviceSolver::refresh_on_device(const Hierarchy& h, const double* kappa_hos
                                                    coarse_ncomp_ > 0 ? C.slot.p : nullptr, C.d.vol.p, coarse_ncomp_,
                                                    coarse_M_.p);
     const int N = coarse_N_;
-    const size_t cl_bytes = (size_t((N + kLuCluster - 1) / kLuCluster) * N + 2 * size_t(N)) * sizeof(double);
     if (lu_cluster_) {
         cudaLaunchConfig_t cfg;
         std::memset(&cfg, 0, sizeof(cfg));
         cfg.gridDim = dim3(kLuCluster);
         cfg.blockDim = dim3(kLuClusterThreads);
-        cfg.dynamicSmemBytes = cl_bytes;
+        cfg.dynamicSmemBytes = lu_smem(N, kLuCluster, true);
         cfg.stream = s;
         cudaLaunchAttribute at[1];
         at[0].id = cudaLaunchAttributeClusterDimension;
@@ -528,11 +672,10 @@ void DeviceSolver::refresh_on_device(const Hierarchy& h, const double* kappa_hos
         cfg.numAttrs = 1;
         TPA_CUDA(cudaLaunchKernelEx(&cfg, kr_lu<true>, N, coarse_M_.p, coarse_piv_.p, rerr_.p));
     } else {
-        kr_lu<false><<<1, 1024, 2 * size_t(N) * sizeof(double), s>>>(N, coarse_M_.p, coarse_piv_.p, rerr_.p);
+        kr_lu<false><<<1, 1024, lu_smem(N, 1, false), s>>>(N, coarse_M_.p, coarse_piv_.p, rerr_.p);
     }
-    const size_t inv_bytes = size_t(kInvWarps) * size_t(N) * sizeof(double);
-    kr_coarse_inv<<<(C.n + kInvWarps - 1) / kInvWarps, 32 * kInvWarps, inv_bytes, s>>>(N, C.n, coarse_M_.p,
-                                                                                     coarse_piv_.p, coarse_inv_.p, rerr_.p);
+    kr_coarse_inv<<<(C.n + kInvWarps - 1) / kInvWarps, 32 * kInvWarps, inv_smem(N), s>>>(
+        N, C.n, coarse_M_.p, coarse_piv_.p, coarse_inv_.p, rerr_.p);
     TPA_CUDA(cudaGetLastError());
     std::vector<double> wtw(size_t(2 * nl));
     int err = 0;
@@ -553,6 +696,12 @@ void DeviceSolver::refresh_on_device(const Hierarchy& h, const double* kappa_hos
         vf_[size_t(l)].w = L.f.w;
         vd_[size_t(l)].tw = L.d.tw;
         vf_[size_t(l)].tw = L.f.tw;
+        if (size_t(l) < sd_.size()) {
+            sd_[size_t(l)].w = L.d.w;
+            sf_[size_t(l)].w = L.f.w;
+            sd_[size_t(l)].tw = L.d.tw;
+            sf_[size_t(l)].tw = L.f.tw;
+        }
     }
     // the level views (and the captured graphs, which hold them by value) change
     vd_dev_.upload(vd_.data(), vd_.size(), s);

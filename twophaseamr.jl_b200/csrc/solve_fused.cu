@@ -846,6 +846,7 @@ namespace tpa {
 // the transfer's inverse diagonal equal to the smoother's.
 void DeviceSolver::upload_structured(const Hierarchy& h) {
     const int nl = int(levels_.size());
+    rl_ready_ = false;  // the device refresh gathers into the stencil copies made here
     sdev_.clear();
     sdev_.resize(size_t(nl));
     sd_.assign(size_t(nl), SView<double>{});
