@@ -123,6 +123,10 @@ tpa_status tpa_level_face_coefficients(const tpa_context* ctx, int32_t level, do
  * otherwise, or with TPAGMG_HOST_REFRESH set, the host rebuilds the levels and
  * uploads them.  Host-side level queries recompute the host copy on demand. */
 tpa_status tpa_refresh(tpa_context* ctx, const double* face_coefficient);
+/* tpa_refresh from a device array (e.g. the output of
+ * tpa_face_coefficients_device): on the GPU when the set of zero coefficients
+ * is unchanged (checked on the device), otherwise the host rebuilds. */
+tpa_status tpa_refresh_device(tpa_context* ctx, const double* face_coefficient);
 /* How the last tpa_refresh ran: path 1 = on the host, 2 = on the device,
  * 0 = none yet; ms = its host wall time.  Replaces nothing in the reference
  * (measurement support). */
@@ -292,6 +296,64 @@ tpa_status tpa_set_stream(tpa_context* ctx, void* stream);
  * support for the roofline; it overwrites the level's work vectors. */
 tpa_status tpa_time_kernel(tpa_context* ctx, int32_t which, int32_t level, int32_t precision, int32_t iters,
                            double* ms);
+
+/* ---- the projection step around the solve (device arrays unless noted) ----
+ * Face arrays follow the mesh's face order (tpa_mesh_faces), boundary arrays
+ * its boundary-face order (tpa_mesh_boundary_faces), cell arrays cell order.
+ * All run on the context's stream and return after it has finished. */
+
+/* `_refresh_conditional_fraction!` without embedded geometry
+ * (src/interface/interface_field.jl:248-291): the physical fraction clamped to
+ * [0, 1] (physical may be NULL) and the conditional fraction with the floor
+ * (<= floor -> 0, >= 1 - floor -> 1; the reference's default floor is
+ * sqrt(eps)).  TPA_ERR_INVALID_ARG if a value is not finite or lies more than
+ * 128 eps outside [0, 1]. */
+tpa_status tpa_conditional_fraction_device(tpa_context* ctx, const double* fraction, double fraction_floor,
+                                           double* physical, double* conditional);
+/* Face coefficients 1/rho_f of `PoissonOperator(field; density)`
+ * (src/two_phase/forces.jl:23-36, 69-84, 113-140): rho_f = rho_l c + rho_g (1 - c),
+ * c the spacing-weighted mean of the two conditional fractions. */
+tpa_status tpa_face_coefficients_device(tpa_context* ctx, const double* conditional, double rho_liquid,
+                                        double rho_gas, double* face_coefficient);
+/* `surface_tension!` with a constant curvature (forces.jl:179-209, 312-378):
+ * jumps sigma * curvature * [c+ > 1/2] - [c- > 1/2] (formulation 0, CGFM) or
+ * c+ - c- (1, CSF) times |f|, then sqrt(k) K sqrt(k) of them; boundary
+ * values 0 (accel_boundary may be NULL).  Uses the current face coefficients. */
+tpa_status tpa_surface_tension_device(tpa_context* ctx, const double* conditional, double sigma, double curvature,
+                                      int32_t formulation, double* accel_interior, double* accel_boundary);
+/* `weighted_gradient!` (src/operators/elliptic.jl:1255-1297):
+ * sqrt(k) K sqrt(k) |f| (p+ - p-) on interior faces; boundary faces carry the
+ * zero gradient of a wall (grad_boundary may be NULL). */
+tpa_status tpa_weighted_gradient_device(tpa_context* ctx, const double* pressure, double* grad_interior,
+                                        double* grad_boundary);
+/* `divergence!` (src/operators/advection/cell_advection.jl:205-220). */
+tpa_status tpa_divergence_device(tpa_context* ctx, const double* u_interior, const double* u_boundary,
+                                 double* divergence);
+
+/* Options of `project!` (src/navier_stokes/projection.jl:183-260). */
+typedef struct {
+    double dt;                          /* > 0 */
+    double tolerance;                   /* in (0, 1); the reference's default is sqrt(eps) */
+    double reference_dt;                /* >= dt, or 0 for dt (`_reference_dt`) */
+    const double* inherited_divergence; /* NULL, or the `_inherited_divergence` cell array */
+    int32_t max_cycles;                 /* default 100 */
+    int32_t compatibility;              /* 0 :project, 1 :error */
+    int32_t precision;                  /* 0 FP64 V-cycle, 1 FP32 V-cycle */
+    int32_t prepared;                   /* 0: `project!` (walls made impermeable first),
+                                           1: `_project_prepared!` (boundary velocity as given) */
+} tpa_projection_options;
+
+/* `project!` / `_project_prepared!` (projection.jl:221-260): divergence of u,
+ * the RHS -div/dt (+ inherited term), the increment solve with rtol 0 and
+ * atol tolerance/dt^2, u -= dt G_k phi, p += phi (split domains re-gauged per
+ * component).  stats: the solve's, with residual_scale 1/dt^2 and compatible =
+ * dt^2 |removed mean| <= tolerance (`_projection_compatibility!`).
+ * tpa_project takes host arrays (copied in and out); tpa_project_device takes
+ * device arrays (and a device inherited_divergence). */
+tpa_status tpa_project(tpa_context* ctx, double* u_interior, double* u_boundary, double* pressure,
+                       const tpa_projection_options* options, tpa_stats* stats);
+tpa_status tpa_project_device(tpa_context* ctx, double* u_interior, double* u_boundary, double* pressure,
+                              const tpa_projection_options* options, tpa_stats* stats);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,219 @@
+"""The projection step around the solve on the B200 against the oracle
+(oracle/projection.py) and the reference's balanced-force known answer
+(test/two_phase/forces.jl:110-158 of ronaldremmerswaal/TwoPhaseAMR.jl).
+
+Bars: elementwise kernels (conditional fraction, face coefficients, the
+divergence with its per-cell face-order sums, the surface-tension jumps) are
+bit-exact; products with the AMR face metric K agree to 1e-14 relative (row
+sums in another order; bit-exact where K is diagonal); a projection (which
+contains a solve to `tolerance`) agrees with the oracle's to 1e-9 relative in
+velocity and pressure; a balanced force projects to |u| < 1e-9.
+"""
+import numpy as np
+import pytest
+
+from oracle import projection as OP
+from oracle.mesh import block_tree_mesh
+from oracle.multigrid import MultigridOptions as OMG, TreeGeometricMultigrid
+from oracle.operator import PoissonOperator as OOp
+
+pytestmark = pytest.mark.gpu
+
+import torch  # noqa: E402
+
+from tpagmg import BlockTreeMesh, EllipticSolver, MultigridOptions, PoissonOperator  # noqa: E402
+from tpagmg import projection as P  # noqa: E402
+from tpagmg import workloads as W  # noqa: E402
+from tpagmg._lib import TpaError  # noqa: E402
+
+CENTER, RADIUS = (0.5, 0.5), 0.2
+
+
+def spec_of(kind):
+    if kind == "uniform":
+        return dict(block_size=(8, 8), max_level=2)
+    if kind == "two_level":
+        return dict(block_size=(8, 8), max_level=2,
+                    refine=lambda k, o, e: k[0] == 0 or (k[0] == 1 and k[1] == 0 and k[2] == 0))
+    if kind == "walls":
+        return dict(base_mesh=(32, 32), block_size=(8, 8), periodic=(False, False), max_level=1,
+                    refine=lambda k, o, e: k[0] == 0 and o[0] < 0.5)
+    if kind == "band":
+        def cut(k, o, e):
+            cx, cy = o[0] + e[0] / 2 - CENTER[0], o[1] + e[1] / 2 - CENTER[1]
+            near = np.hypot(max(abs(cx) - e[0] / 2, 0.0), max(abs(cy) - e[1] / 2, 0.0))
+            far = np.hypot(abs(cx) + e[0] / 2, abs(cy) + e[1] / 2)
+            return near <= RADIUS <= far
+        return dict(block_size=(8, 8), max_level=2, refine=cut)
+    raise KeyError(kind)
+
+
+def setup(kind, ratio=1000.0):
+    spec = spec_of(kind)
+    m = BlockTreeMesh(**spec)
+    om = block_tree_mesh(**spec)
+    raw = W.circle_fractions(m, CENTER, RADIUS)
+    return spec, m, om, raw
+
+
+def bits(a):
+    return np.asarray(a, dtype=np.float64).view(np.uint64)
+
+
+@pytest.mark.parametrize("kind", ["uniform", "two_level", "walls", "band"])
+def test_elementwise_kernels_bit_exact(kind):
+    spec, m, om, raw = setup(kind)
+    _, ocond = OP.conditional_fraction(raw)
+    kappa = OP.face_coefficients(om, ocond, (1000.0, 1.0))
+    s = EllipticSolver(PoissonOperator(m, kappa))
+    phys, cond = P.conditional_fraction(raw, s)
+    ophys, ocond = OP.conditional_fraction(raw)
+    assert np.array_equal(bits(phys), bits(ophys)) and np.array_equal(bits(cond), bits(ocond))
+    k = P.face_coefficients(cond, s, (1000.0, 1.0))
+    assert np.array_equal(bits(k), bits(kappa))
+    rng = np.random.default_rng(3)
+    u = P.FaceVelocity(m, rng.standard_normal(m.nfaces), rng.standard_normal(m.nboundary_faces))
+    d = P.divergence(u, s)
+    assert np.array_equal(bits(d), bits(OP.divergence(om, u.interior, u.boundary)))
+
+
+@pytest.mark.parametrize("kind", ["uniform", "two_level", "walls", "band"])
+@pytest.mark.parametrize("formulation", ["csf", "cgfm"])
+def test_force_and_weighted_gradient_match_oracle(kind, formulation):
+    spec, m, om, raw = setup(kind)
+    _, cond = OP.conditional_fraction(raw)
+    kappa = OP.face_coefficients(om, cond, (1000.0, 1.0))
+    s = EllipticSolver(PoissonOperator(m, kappa))
+    oop = OOp(om, kappa)
+    a = P.surface_tension(cond, s, sigma=1.0, curvature=5.0, formulation=formulation)
+    oa, _ = OP.weighted_jump_force(oop, OP.surface_tension_jumps(om, cond, 1.0, 5.0, formulation))
+    scale = np.max(np.abs(oa)) + 1e-300
+    assert np.max(np.abs(a.interior - oa)) <= 1e-14 * scale
+    assert not np.any(a.boundary)
+    p = np.random.default_rng(4).standard_normal(m.ncells)
+    g = P.weighted_gradient(p, s)
+    og, ogb = OP.weighted_gradient(oop, p)
+    assert np.max(np.abs(g.interior - og)) <= 1e-14 * np.max(np.abs(og))
+    assert np.array_equal(bits(g.boundary), bits(ogb))
+    if kind == "uniform":  # diagonal K: every product is a single rounding
+        assert np.array_equal(bits(g.interior), bits(og))
+
+
+@pytest.mark.parametrize("kind", ["two_level", "walls", "band"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_project_matches_oracle(kind, precision):
+    spec, m, om, raw = setup(kind)
+    rng = np.random.default_rng(5)
+    kappa = np.exp(rng.uniform(-2, 2, m.nfaces))
+    s = EllipticSolver(PoissonOperator(m, kappa), preconditioner_options={"precision": precision})
+    oop = OOp(om, kappa)
+    u0 = rng.standard_normal(m.nfaces)
+    ub0 = rng.standard_normal(m.nboundary_faces)
+    p0 = rng.standard_normal(m.ncells)
+    inh = rng.standard_normal(m.ncells)
+    for kw in (dict(), dict(inherited_divergence=inh, reference_dt=0.08), dict(prepared=True)):
+        u = P.FaceVelocity(m, u0, ub0)
+        p = p0.copy()
+        st = P.project(u, p, s, 0.05, tolerance=1e-10, **kw)
+        ou, oub, opr, phi, ost = OP.project(oop, TreeGeometricMultigrid(oop, OMG()), u0, ub0, p0, 0.05,
+                                            tolerance=1e-10, inherited=kw.get("inherited_divergence"),
+                                            reference_dt=kw.get("reference_dt"), prepared=kw.get("prepared", False))
+        assert st.converged and ost.converged
+        assert st.residual_scale == 1 / 0.05 ** 2 and st.compatible == ost.compatible
+        assert np.max(np.abs(u.interior - ou)) <= 1e-9 * np.max(np.abs(ou))
+        assert np.max(np.abs(u.boundary - oub), initial=0.0) <= 1e-9 * max(np.max(np.abs(oub), initial=0.0), 1.0)
+        assert np.max(np.abs(p - opr)) <= 1e-9 * np.max(np.abs(opr))
+        if not kw.get("prepared") and m.nboundary_faces:
+            # `project!` makes the walls impermeable first
+            assert not np.any(u.boundary)
+        # the projected velocity is divergence-free to the solve tolerance, up
+        # to the volume mean of the incoming divergence (a net boundary inflow
+        # no pressure removes) and the retained part dt w (inh - its mean) of
+        # an inherited divergence
+        vol = m.cell_volumes()
+        d0 = P.divergence(P.FaceVelocity(m, u0, ub0 if kw.get("prepared") else None), s)
+        target = np.full(m.ncells, np.sum(vol * d0) / np.sum(vol))
+        if "inherited_divergence" in kw:
+            w = (0.08 - 0.05) / (0.05 * 0.08)
+            target += 0.05 * w * (inh - np.sum(vol * inh) / np.sum(vol))
+        assert np.max(np.abs(P.divergence(u, s) - target)) * 0.05 <= 1e-8
+
+
+@pytest.mark.parametrize("kind", ["uniform", "two_level", "band"])
+@pytest.mark.parametrize("ratio", [1.0, 1000.0])
+@pytest.mark.parametrize("formulation", ["csf", "cgfm"])
+def test_balanced_force_device_pipeline(kind, ratio, formulation):
+    """test/two_phase/forces.jl:110-158 on the GPU, every field resident:
+    fractions -> kappa -> refresh -> force -> u = dt a -> project! -> |u| < 1e-9."""
+    spec, m, om, raw = setup(kind)
+    s = EllipticSolver(PoissonOperator(m, np.ones(m.nfaces)))
+    step = P.TwoPhaseStep(s, (ratio, 1.0), sigma=1.0, curvature=5.0, formulation=formulation)
+    frac = torch.from_numpy(raw).cuda()
+    step.update_interface(frac)
+    _, cond = OP.conditional_fraction(raw)
+    okappa = OP.face_coefficients(om, cond, (ratio, 1.0))
+    assert np.array_equal(bits(step.kappa.cpu().numpy()), bits(okappa))
+    u = step.force() * 0.01
+    ub = torch.zeros(max(m.nboundary_faces, 1), dtype=torch.float64, device="cuda")
+    p = torch.zeros(m.ncells, dtype=torch.float64, device="cuda")
+    st = step.project(u, ub, p, 0.01, tolerance=1e-11)
+    assert st.converged and st.compatible
+    assert float(u.abs().max()) < 1e-9
+    # the pressure is the CGFM / CSF potential up to a constant
+    pot = 5.0 * (cond if formulation == "csf" else (cond > 0.5).astype(float))
+    pc = p.cpu().numpy()
+    vol = m.cell_volumes()
+    diff = (pc - np.sum(vol * pc) / np.sum(vol)) - (pot - np.sum(vol * pot) / np.sum(vol))
+    assert np.max(np.abs(diff)) < 1e-4
+
+
+def test_host_and_device_projection_agree_bitwise():
+    spec, m, om, raw = setup("walls")
+    rng = np.random.default_rng(9)
+    kappa = np.exp(rng.uniform(-1, 1, m.nfaces))
+    s = EllipticSolver(PoissonOperator(m, kappa))
+    u0, ub0, p0 = rng.standard_normal(m.nfaces), rng.standard_normal(m.nboundary_faces), rng.standard_normal(m.ncells)
+    u = P.FaceVelocity(m, u0, ub0)
+    p = p0.copy()
+    P.project(u, p, s, 0.02, tolerance=1e-10, prepared=True)
+    ud, ubd, pd = (torch.from_numpy(a.copy()).cuda() for a in (u0, ub0, p0))
+    P.project_device(ud, ubd, pd, s, 0.02, tolerance=1e-10, prepared=True)
+    assert np.array_equal(bits(ud.cpu().numpy()), bits(u.interior))
+    assert np.array_equal(bits(ubd.cpu().numpy()), bits(u.boundary))
+    assert np.array_equal(bits(pd.cpu().numpy()), bits(p))
+
+
+def test_device_refresh_with_new_zero_faces_falls_back_to_the_host():
+    spec, m, om, raw = setup("two_level")
+    s = EllipticSolver(PoissonOperator(m, np.ones(m.nfaces)))
+    s.set_tuning(structured=0)  # CSR levels: the device refresh applies
+    k = torch.ones(m.nfaces, dtype=torch.float64, device="cuda") * 2.0
+    P.refresh_device(s, k)
+    assert s.last_refresh()[0] == "device"
+    k[::5] = 0.0
+    P.refresh_device(s, k)
+    assert s.last_refresh()[0] == "host"
+    P.refresh_device(s, k * 3.0)
+    assert s.last_refresh()[0] == "device"
+    with pytest.raises(TpaError) as e:
+        P.refresh_device(s, k * float("nan"))
+    assert e.value.code == 1
+
+
+def test_argument_errors():
+    spec, m, om, raw = setup("uniform")
+    s = EllipticSolver(PoissonOperator(m, np.ones(m.nfaces)))
+    bad = raw.copy()
+    bad[3] = 1.5
+    with pytest.raises(TpaError) as e:
+        P.conditional_fraction(bad, s)
+    assert e.value.code == 1
+    u = P.FaceVelocity(m)
+    p = np.zeros(m.ncells)
+    for kw in (dict(dt=0.0), dict(dt=0.1, tolerance=1.0), dict(dt=0.1, reference_dt=0.05)):
+        dt = kw.pop("dt")
+        with pytest.raises(TpaError) as e:
+            P.project(u, p, s, dt, **kw)
+        assert e.value.code == 1
+    with pytest.raises(TpaError):
+        P.face_coefficients(raw, s, (0.0, 1.0))

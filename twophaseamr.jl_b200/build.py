@@ -17,7 +17,7 @@ BUILD = HERE / "_build"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_SRC = ["mesh.cpp", "metric.cpp", "hierarchy.cpp", "structure.cpp"]
-DEVICE_SRC = ["device.cu", "solve_fused.cu", "solve_fast.cu", "noalloc.cu", "adjoint.cu", "batch.cu", "autotune.cu", "refresh.cu", "api.cpp"]
+DEVICE_SRC = ["device.cu", "solve_fused.cu", "solve_fast.cu", "noalloc.cu", "adjoint.cu", "batch.cu", "autotune.cu", "refresh.cu", "projection.cu", "api.cpp"]
 
 
 def _stale(target, deps):

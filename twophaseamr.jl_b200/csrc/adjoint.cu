@@ -95,11 +95,11 @@ void DeviceSolver::upload_faces(const Mesh& mesh, const Metric& metric, const st
             throw Error(1, "face coefficients must be finite and nonnegative");
         sk[size_t(f)] = std::sqrt(kappa[size_t(f)]);
     }
-    // a row with off-diagonal couplings needs kappa_f > 0 (the derivative of
-    // sqrt(kappa_f) is unbounded at 0)
+    // a row with off-diagonal couplings needs kappa_f > 0 for the gradient (the
+    // derivative of sqrt(kappa_f) is unbounded at 0)
+    hang_zero_ = false;
     for (int64_t f = 0; f < nf; ++f)
-        if (ptr[size_t(f) + 1] - ptr[size_t(f)] > 1 && sk[size_t(f)] == 0)
-            throw Error(1, "the face-coefficient gradient needs kappa > 0 on faces of hanging-vertex patches");
+        if (ptr[size_t(f) + 1] - ptr[size_t(f)] > 1 && sk[size_t(f)] == 0) hang_zero_ = true;
     std::vector<int> fm(mesh.fm.begin(), mesh.fm.end()), fp(mesh.fp.begin(), mesh.fp.end());
     f_minus_.upload(fm.data(), fm.size(), stream_);
     f_plus_.upload(fp.data(), fp.size(), stream_);
@@ -110,10 +110,13 @@ void DeviceSolver::upload_faces(const Mesh& mesh, const Metric& metric, const st
     f_sqrtk_.upload(sk.data(), sk.size(), stream_);
     TPA_CUDA(cudaStreamSynchronize(stream_));
     nfaces_ = nf;
+    nbfaces_ = -1;  // the projection topology follows the faces
 }
 
 void DeviceSolver::face_gradient(const double* p, const double* lam, double* g) {
     if (nfaces_ < 0) throw Error(7, "face data not uploaded");
+    if (hang_zero_)
+        throw Error(1, "the face-coefficient gradient needs kappa > 0 on faces of hanging-vertex patches");
     TPA_CUDA(cudaSetDevice(device_));
     if (nfaces_ == 0) return;
     k_face_gradient<<<grid_cap(nfaces_), kThreads, 0, stream_>>>(int(nfaces_), f_minus_.p, f_plus_.p, f_area_.p,

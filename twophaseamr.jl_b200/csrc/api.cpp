@@ -96,6 +96,11 @@ void ensure_faces(tpa_context* ctx) {
     }
 }
 
+void ensure_projection(tpa_context* ctx) {
+    ensure_faces(ctx);
+    if (!ctx->dev->projection_ready()) ctx->dev->upload_projection(ctx->hier.levels[0].op.mesh);
+}
+
 void fill_stats(const tpa::SolveStats& s, int precision, int launches, tpa_stats* out) {
     if (!out) return;
     std::memset(out, 0, sizeof(*out));
@@ -486,6 +491,41 @@ tpa_status tpa_refresh(tpa_context* ctx, const double* face_coefficient) {
     });
 }
 
+tpa_status tpa_refresh_device(tpa_context* ctx, const double* face_coefficient) {
+    const auto t0 = std::chrono::steady_clock::now();
+    auto stamp = [&](int path) {
+        ctx->refresh_path = path;
+        ctx->refresh_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    };
+    return guard(ctx, [&] {
+        if (!face_coefficient) throw tpa::Error(TPA_ERR_INVALID_ARG, "null face coefficients");
+        ensure_device(ctx);
+        std::vector<double>& kappa = ctx->hier.levels[0].op.kappa;
+        const size_t nf = kappa.size();
+        cudaStream_t s = ctx->dev->stream();
+        if (!std::getenv("TPAGMG_HOST_REFRESH") && ctx->dev->refresh_applicable(ctx->hier) &&
+            ctx->dev->refresh_from_device(ctx->hier, face_coefficient) == 0) {
+            // the host keeps the finest coefficients (the rest is recomputed on demand)
+            TPA_CUDA(cudaMemcpyAsync(kappa.data(), face_coefficient, nf * sizeof(double), cudaMemcpyDeviceToHost, s));
+            TPA_CUDA(cudaStreamSynchronize(s));
+            ctx->host_stale = true;
+            stamp(2);
+            return;
+        }
+        std::vector<double> k(nf);
+        TPA_CUDA(cudaMemcpyAsync(k.data(), face_coefficient, nf * sizeof(double), cudaMemcpyDeviceToHost, s));
+        TPA_CUDA(cudaStreamSynchronize(s));
+        for (size_t f = 0; f < nf; ++f)
+            if (!std::isfinite(k[f]) || k[f] < 0)
+                throw tpa::Error(TPA_ERR_INVALID_ARG, "face coefficients must be finite and nonnegative");
+        tpa::refresh_hierarchy(ctx->hier, k);
+        ctx->host_stale = false;
+        ctx->dev->upload(ctx->hier);
+        ctx->dev->invalidate_faces();
+        stamp(1);
+    });
+}
+
 tpa_status tpa_solve_device(tpa_context* ctx, const double* rhs, double* x, double rtol, double atol,
                             int32_t max_cycles, int32_t compatibility, int32_t precision, tpa_stats* stats) {
     return guard(ctx, [&] { solve_device_body(ctx, rhs, x, rtol, atol, max_cycles, compatibility, precision, stats); });
@@ -631,6 +671,126 @@ tpa_status tpa_residual_norms(tpa_context* ctx, const double* r, double out[2]) 
         if (!r || !out) throw tpa::Error(TPA_ERR_INVALID_ARG, "null residual or output");
         ensure_device(ctx);
         ctx->dev->residual_norms(r, out);
+    });
+}
+
+tpa_status tpa_conditional_fraction_device(tpa_context* ctx, const double* fraction, double fraction_floor,
+                                           double* physical, double* conditional) {
+    return guard(ctx, [&] {
+        if (!fraction || !conditional) throw tpa::Error(TPA_ERR_INVALID_ARG, "null argument");
+        ensure_projection(ctx);
+        ctx->dev->conditional_fraction(fraction, fraction_floor, physical, conditional);
+    });
+}
+
+tpa_status tpa_face_coefficients_device(tpa_context* ctx, const double* conditional, double rho_liquid,
+                                        double rho_gas, double* face_coefficient) {
+    return guard(ctx, [&] {
+        if (!conditional || !face_coefficient) throw tpa::Error(TPA_ERR_INVALID_ARG, "null argument");
+        ensure_projection(ctx);
+        ctx->dev->face_coefficients(conditional, rho_liquid, rho_gas, face_coefficient);
+        TPA_CUDA(cudaStreamSynchronize(ctx->dev->stream()));
+    });
+}
+
+tpa_status tpa_surface_tension_device(tpa_context* ctx, const double* conditional, double sigma, double curvature,
+                                      int32_t formulation, double* accel_interior, double* accel_boundary) {
+    return guard(ctx, [&] {
+        if (!conditional || !accel_interior) throw tpa::Error(TPA_ERR_INVALID_ARG, "null argument");
+        if (formulation != 0 && formulation != 1) throw tpa::Error(TPA_ERR_INVALID_ARG, "formulation must be CSF() or CGFM()");
+        ensure_projection(ctx);
+        ctx->dev->surface_tension(conditional, sigma, curvature, formulation, accel_interior, accel_boundary);
+        TPA_CUDA(cudaStreamSynchronize(ctx->dev->stream()));
+    });
+}
+
+tpa_status tpa_weighted_gradient_device(tpa_context* ctx, const double* pressure, double* grad_interior,
+                                        double* grad_boundary) {
+    return guard(ctx, [&] {
+        if (!pressure || !grad_interior) throw tpa::Error(TPA_ERR_INVALID_ARG, "null argument");
+        ensure_projection(ctx);
+        ctx->dev->weighted_gradient(pressure, grad_interior, grad_boundary);
+        TPA_CUDA(cudaStreamSynchronize(ctx->dev->stream()));
+    });
+}
+
+tpa_status tpa_divergence_device(tpa_context* ctx, const double* u_interior, const double* u_boundary,
+                                 double* divergence) {
+    return guard(ctx, [&] {
+        if (!u_interior || !divergence) throw tpa::Error(TPA_ERR_INVALID_ARG, "null argument");
+        ensure_projection(ctx);
+        if (ctx->dev->nboundary_faces() > 0 && !u_boundary)
+            throw tpa::Error(TPA_ERR_INVALID_ARG, "the mesh has boundary faces: u_boundary is required");
+        ctx->dev->divergence(u_interior, u_boundary, divergence);
+        TPA_CUDA(cudaStreamSynchronize(ctx->dev->stream()));
+    });
+}
+
+namespace {
+
+void project_body(tpa_context* ctx, double* u_int, double* u_bnd, double* p, const tpa_projection_options* o,
+                  const double* inherited, tpa_stats* stats) {
+    if (!o) throw tpa::Error(TPA_ERR_INVALID_ARG, "null options");
+    if (o->compatibility != 0 && o->compatibility != 1)
+        throw tpa::Error(TPA_ERR_INVALID_ARG, "compatibility must be :project or :error");
+    if (o->precision != 0 && o->precision != 1) throw tpa::Error(TPA_ERR_INVALID_ARG, "bad precision");
+    if (o->max_cycles < 0) throw tpa::Error(TPA_ERR_INVALID_ARG, "max_cycles must be nonnegative");
+    const double reference_dt = o->reference_dt > 0 ? o->reference_dt : o->dt;
+    tpa::SolveStats st;
+    ctx->dev->reset_launches();
+    ctx->dev->project(u_int, u_bnd, p, o->dt, o->tolerance, o->max_cycles, o->compatibility, inherited,
+                      reference_dt, o->precision, o->prepared != 0, st);
+    TPA_CUDA(cudaStreamSynchronize(ctx->dev->stream()));
+    fill_stats(st, o->precision, ctx->dev->kernel_launches(), stats);
+    if (stats) {
+        // `_projection_compatibility!`: dt^2 times the removed component mean
+        const double m = std::fabs(st.removed_rhs_mean);
+        const double scaled = (m == 0) ? 0.0 : o->dt * o->dt * m;
+        stats->compatible = std::isfinite(m) && scaled <= o->tolerance;
+        stats->residual_scale = 1.0 / (o->dt * o->dt);
+    }
+}
+
+}  // namespace
+
+tpa_status tpa_project_device(tpa_context* ctx, double* u_interior, double* u_boundary, double* pressure,
+                              const tpa_projection_options* options, tpa_stats* stats) {
+    return guard(ctx, [&] {
+        if (!u_interior || !pressure) throw tpa::Error(TPA_ERR_INVALID_ARG, "null argument");
+        ensure_projection(ctx);
+        if (ctx->dev->nboundary_faces() > 0 && !u_boundary)
+            throw tpa::Error(TPA_ERR_INVALID_ARG, "the mesh has boundary faces: u_boundary is required");
+        project_body(ctx, u_interior, u_boundary, pressure, options, options ? options->inherited_divergence : nullptr,
+                     stats);
+    });
+}
+
+tpa_status tpa_project(tpa_context* ctx, double* u_interior, double* u_boundary, double* pressure,
+                       const tpa_projection_options* options, tpa_stats* stats) {
+    return guard(ctx, [&] {
+        if (!u_interior || !pressure) throw tpa::Error(TPA_ERR_INVALID_ARG, "null argument");
+        ensure_projection(ctx);
+        const size_t n = size_t(ctx->dev->ncells()), nf = size_t(ctx->dev->nfaces()),
+                     nb = size_t(ctx->dev->nboundary_faces());
+        if (nb > 0 && !u_boundary) throw tpa::Error(TPA_ERR_INVALID_ARG, "the mesh has boundary faces: u_boundary is required");
+        // one device buffer: u interior, u boundary, pressure, inherited divergence
+        const bool inh = options && options->inherited_divergence;
+        const size_t total = nf + nb + n + (inh ? n : 0);
+        if (ctx->d_aux.n < total) ctx->d_aux.alloc(total);
+        double* du = ctx->d_aux.p;
+        double* db = du + nf;
+        double* dp = db + nb;
+        double* di = inh ? dp + n : nullptr;
+        cudaStream_t s = ctx->dev->stream();
+        TPA_CUDA(cudaMemcpyAsync(du, u_interior, nf * sizeof(double), cudaMemcpyHostToDevice, s));
+        if (nb) TPA_CUDA(cudaMemcpyAsync(db, u_boundary, nb * sizeof(double), cudaMemcpyHostToDevice, s));
+        TPA_CUDA(cudaMemcpyAsync(dp, pressure, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        if (inh) TPA_CUDA(cudaMemcpyAsync(di, options->inherited_divergence, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        project_body(ctx, du, db, dp, options, di, stats);
+        TPA_CUDA(cudaMemcpyAsync(u_interior, du, nf * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (nb) TPA_CUDA(cudaMemcpyAsync(u_boundary, db, nb * sizeof(double), cudaMemcpyDeviceToHost, s));
+        TPA_CUDA(cudaMemcpyAsync(pressure, dp, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        TPA_CUDA(cudaStreamSynchronize(s));
     });
 }
 

@@ -253,6 +253,10 @@ public:
     // every level operator, D^-1, Dt^-1, both weights and the coarse inverse are
     // recomputed on the GPU.  `h` supplies the topology the first time.
     void refresh_on_device(const Hierarchy& h, const double* kappa_host);
+    // The same from a device array: 0 when refreshed, 1 when the set of zero
+    // coefficients differs from the current one (nothing changed; the host
+    // path must rebuild); throws on a non-finite or negative coefficient.
+    int refresh_from_device(const Hierarchy& h, const double* kappa_dev);
     // smoother and transfer weight per level, as uploaded or refreshed
     std::vector<double> level_weights();
 
@@ -268,6 +272,7 @@ private:
         DevArray<int> sx, sy, sex;
     };
     void prepare_refresh(const Hierarchy& h);
+    void refresh_levels();  // from the finest coefficients in rl_[0].kappa
     std::vector<RefreshLevel> rl_;
     bool rl_ready_ = false;
     int coarse_N_ = 0, coarse_ncomp_ = 0;
@@ -283,7 +288,10 @@ public:
     // first) and sqrt(kappa); uploaded on first use and after every refresh.
     void upload_faces(const Mesh& mesh, const Metric& metric, const std::vector<double>& kappa);
     bool faces_ready() const { return nfaces_ >= 0; }
-    void invalidate_faces() { nfaces_ = -1; }
+    void invalidate_faces() {
+        nfaces_ = -1;
+        nbfaces_ = -1;
+    }
     int64_t nfaces() const { return nfaces_; }
     // g_f = -lam' (dS/dkappa_f) p for cell vectors p, lam (device pointers).
     void face_gradient(const double* p, const double* lam, double* g);
@@ -292,8 +300,39 @@ public:
 
 private:
     int64_t nfaces_ = -1;
+    bool hang_zero_ = false;  // a face of a hanging-vertex patch has kappa = 0
     DevArray<int> f_minus_, f_plus_, k_ptr_, k_col_;
     DevArray<double> f_area_, k_val_, f_sqrtk_;
+
+public:
+    // ---- the projection step around the solve (csrc/projection.cu) ----
+    // Boundary faces, each cell's incident faces in face order and the face
+    // spacings (after upload_faces).
+    void upload_projection(const Mesh& mesh);
+    bool projection_ready() const { return nbfaces_ >= 0 && nfaces_ >= 0; }
+    int64_t nboundary_faces() const { return nbfaces_; }
+    // `_refresh_conditional_fraction!` (no embedded geometry); physical may be null
+    void conditional_fraction(const double* raw, double floor, double* physical, double* conditional);
+    // kappa_f = 1 / rho_f of `PoissonOperator(field; density)`
+    void face_coefficients(const double* conditional, double rho_l, double rho_g, double* kappa);
+    // `surface_tension!` with a constant curvature (csf = 0: CGFM)
+    void surface_tension(const double* conditional, double sigma, double curvature, int csf, double* a_int,
+                         double* a_bnd);
+    // `weighted_gradient!` into g (may be null) and / or u -= dt g
+    void weighted_gradient(const double* p, double* g_int, double* g_bnd, double* u_int = nullptr,
+                           double* u_bnd = nullptr, double dt = 0.0);
+    // `divergence!`; rhs: the projection right-hand side -div / dt + weight * inherited
+    void divergence(const double* u_int, const double* u_bnd, double* out, bool rhs = false, double dt = 1.0,
+                    const double* inherited = nullptr, double weight = 0.0);
+    // `project!` (prepared = false: walls made impermeable first) or `_project_prepared!`
+    void project(double* u_int, double* u_bnd, double* p, double dt, double tolerance, int max_cycles,
+                 int compatibility, const double* inherited, double reference_dt, int precision, bool prepared,
+                 SolveStats& st);
+
+private:
+    int64_t nbfaces_ = -1;
+    DevArray<int> inc_ptr_, inc_code_, b_cell_, perr_;
+    DevArray<double> f_hm_, f_hp_, b_side_, b_area_, proj_b_, proj_phi_, proj_in_, proj_part_, proj_cvol_;
 };
 
 }  // namespace tpa

@@ -38,6 +38,16 @@ __global__ void kr_sqrt(int n, const double* __restrict__ k, double* __restrict_
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) sk[i] = sqrt(k[i]);
 }
 
+// new coefficients against the current ones: flags |= 1 for a value that is
+// not finite or negative, |= 2 where the set of zero coefficients differs
+__global__ void kr_check(int n, const double* __restrict__ k_new, const double* __restrict__ k_old, int* flags) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double v = k_new[i];
+        if (!(isfinite(v) && v >= 0.0)) atomicOr(flags, 1);
+        else if ((v == 0.0) != (k_old[i] == 0.0)) atomicOr(flags, 2);
+    }
+}
+
 // coarse face coefficients: overlap-weighted average of the fine ones
 __global__ void kr_restrict(int nfc, const int* __restrict__ rptr, const int* __restrict__ ridx,
                             const double* __restrict__ rw, const double* __restrict__ kf, double* __restrict__ kc) {
@@ -513,6 +523,8 @@ void DeviceSolver::prepare_refresh(const Hierarchy& h) {
         R.tg.upload(tg.data(), tg.size(), stream_);
         R.tc.upload(tc.data(), tc.size(), stream_);
         R.kappa.alloc(size_t(std::max<int64_t>(nf, 1)));
+        if (l == 0 && nf > 0)  // the current coefficients: the zero-set check of a device refresh
+            R.kappa.upload(op.kappa.data(), op.kappa.size(), stream_);
         R.sk.alloc(size_t(std::max<int64_t>(nf, 1)));
         const HostLevel& hl = h.levels[size_t(l)];
         if (size_t(l) < sdev_.size() && sdev_[size_t(l)].on) {
@@ -622,11 +634,33 @@ bool DeviceSolver::refresh_applicable(const Hierarchy& h) const {
 void DeviceSolver::refresh_on_device(const Hierarchy& h, const double* kappa_host) {
     TPA_CUDA(cudaSetDevice(device_));
     if (!rl_ready_) prepare_refresh(h);
+    std::memcpy(rstage_, kappa_host, sizeof(double) * size_t(rl_[0].nf));  // no copy is in flight here
+    TPA_CUDA(cudaMemcpyAsync(rl_[0].kappa.p, rstage_, sizeof(double) * size_t(rl_[0].nf), cudaMemcpyHostToDevice,
+                             stream_));
+    refresh_levels();
+}
+
+int DeviceSolver::refresh_from_device(const Hierarchy& h, const double* kappa_dev) {
+    TPA_CUDA(cudaSetDevice(device_));
+    if (!rl_ready_) prepare_refresh(h);
+    const int nf = rl_[0].nf;
+    int flags = 0;
+    TPA_CUDA(cudaMemsetAsync(rerr_.p, 0, sizeof(int), stream_));
+    if (nf > 0) kr_check<<<rgrid(nf), kRThreads, 0, stream_>>>(nf, kappa_dev, rl_[0].kappa.p, rerr_.p);
+    TPA_CUDA(cudaMemcpyAsync(&flags, rerr_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    TPA_CUDA(cudaStreamSynchronize(stream_));
+    if (flags & 1) throw Error(1, "face coefficients must be finite and nonnegative");
+    if (flags & 2) return 1;
+    TPA_CUDA(cudaMemcpyAsync(rl_[0].kappa.p, kappa_dev, sizeof(double) * size_t(nf), cudaMemcpyDeviceToDevice,
+                             stream_));
+    refresh_levels();
+    return 0;
+}
+
+void DeviceSolver::refresh_levels() {
     const int nl = int(levels_.size());
     cudaStream_t s = stream_;
     TPA_CUDA(cudaMemsetAsync(rerr_.p, 0, sizeof(int), s));
-    std::memcpy(rstage_, kappa_host, sizeof(double) * size_t(rl_[0].nf));  // no copy is in flight here
-    TPA_CUDA(cudaMemcpyAsync(rl_[0].kappa.p, rstage_, sizeof(double) * size_t(rl_[0].nf), cudaMemcpyHostToDevice, s));
     for (int l = 0; l < nl; ++l) {
         RefreshLevel& R = rl_[size_t(l)];
         DevLevel& L = levels_[size_t(l)];
@@ -706,9 +740,12 @@ void DeviceSolver::refresh_on_device(const Hierarchy& h, const double* kappa_hos
     // the level views (and the captured graphs, which hold them by value) change
     vd_dev_.upload(vd_.data(), vd_.size(), s);
     vf_dev_.upload(vf_.data(), vf_.size(), s);
+    // the face kernels' sqrt(kappa) (same faces, same zero set)
+    if (nfaces_ >= 0 && rl_[0].nf > 0)
+        TPA_CUDA(cudaMemcpyAsync(f_sqrtk_.p, rl_[0].sk.p, sizeof(double) * size_t(rl_[0].nf), cudaMemcpyDeviceToDevice,
+                                 s));
     TPA_CUDA(cudaStreamSynchronize(s));
     destroy_graphs();
-    invalidate_faces();
 }
 
 std::vector<double> DeviceSolver::level_weights() {

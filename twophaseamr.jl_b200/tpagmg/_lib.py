@@ -110,6 +110,14 @@ SIGNATURES = {
     "tpa_residual_norms": (C.c_int32, [P, P, f64p]),
     "tpa_residual_norms_noalloc": (C.c_int32, [P, P, P, C.c_int64, f64p]),
     "tpa_time_kernel": (C.c_int32, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, f64p]),
+    "tpa_refresh_device": (C.c_int32, [P, P]),
+    "tpa_conditional_fraction_device": (C.c_int32, [P, P, C.c_double, P, P]),
+    "tpa_face_coefficients_device": (C.c_int32, [P, P, C.c_double, C.c_double, P]),
+    "tpa_surface_tension_device": (C.c_int32, [P, P, C.c_double, C.c_double, C.c_int32, P, P]),
+    "tpa_weighted_gradient_device": (C.c_int32, [P, P, P, P]),
+    "tpa_divergence_device": (C.c_int32, [P, P, P, P]),
+    "tpa_project": (C.c_int32, [P, f64p, f64p, f64p, P, C.POINTER(StatsC)]),
+    "tpa_project_device": (C.c_int32, [P, P, P, P, P, C.POINTER(StatsC)]),
 }
 
 _lib = None

@@ -82,6 +82,7 @@ class EllipticSolver:
         self.multigrid = mg
         self.precision = precision
         mesh = operator.mesh
+        self.device = int(device)
         self.ctx = _lib.Context(device)
         self.ctx.call("tpa_set_mesh", *mesh._mesh_args())
         self._kappa = _lib.f64(operator.face_coefficient)
