@@ -39,12 +39,16 @@ typedef int32_t tpa_status;
 
 typedef struct tpa_context tpa_context;
 
-/* MultigridOptions (src/solvers/multigrid/options.jl:14-48). */
+/* MultigridOptions (src/solvers/multigrid/options.jl:14-48), plus the
+ * smoother: 0 = the reference's damped Jacobi, 1 = red-black Gauss-Seidel
+ * (colour (I + J) mod 2 at each cell's own level; red then black before the
+ * coarse correction, black then red after it; not in the reference). */
 typedef struct {
     int32_t coarse_size; /* default 64 */
     int32_t pre_sweeps;  /* default 2  */
     int32_t post_sweeps; /* default 2  */
     int32_t max_levels;  /* default 32 */
+    int32_t smoother;    /* default 0  */
 } tpa_multigrid_options;
 
 /* LinearSolverStats (src/solvers/multigrid/stats.jl:15-30) plus device timing. */
@@ -112,6 +116,10 @@ tpa_status tpa_level_owners(const tpa_context* ctx, int32_t level, int32_t* owne
 /* Level scalars: smoother weight, transfer weight, number of ungauged components. */
 tpa_status tpa_level_info(const tpa_context* ctx, int32_t level, double* smoother_weight, double* transfer_weight,
                           int32_t* components);
+/* Red-black smoother data of level `level` (host-side, no device call):
+ * colour per cell (0 red, 1 black: (I + J) mod 2 at the cell's own level) and
+ * the half-sweep weight.  Either output may be NULL. */
+tpa_status tpa_level_red_black(const tpa_context* ctx, int32_t level, uint8_t* colours, double* weight);
 /* Restricted face coefficients of level `level` (tree_coarsening.jl:538-555). */
 tpa_status tpa_level_face_coefficients(const tpa_context* ctx, int32_t level, double* kappa);
 

@@ -40,11 +40,16 @@ class MultigridOptions:
     pre_sweeps: int = 2
     post_sweeps: int = 2
     max_levels: int = 32
+    # not in the reference: "red_black" replaces its damped Jacobi sweeps by
+    # red-black Gauss-Seidel (see `red_black_colours`)
+    smoother: str = "jacobi"
 
     def __post_init__(self):
         for v in (self.coarse_size, self.pre_sweeps, self.post_sweeps, self.max_levels):
             if not isinstance(v, (int, np.integer)) or isinstance(v, bool):
                 raise TypeError("multigrid sizes and sweep counts must be integers")
+        if self.smoother not in ("jacobi", "red_black"):
+            raise ValueError("smoother must be 'jacobi' or 'red_black'")
         if self.coarse_size <= 0:
             raise ValueError("coarse_size must be positive")
         if self.pre_sweeps < 0 or self.post_sweeps < 0:
@@ -198,6 +203,35 @@ def smoothed_transfer(stiffness, owners, n_coarse):
     return P, w
 
 
+def red_black_colours(mesh):
+    """Red-black colouring of a level (no counterpart in the reference, which
+    smooths with damped Jacobi): colour (I + J) mod 2 of every cell, with (I, J)
+    its lattice coordinates at its own block's refinement level (0 red, 1 black)."""
+    nx, ny = mesh.block_size
+    ci = np.tile(np.arange(nx), ny)
+    cj = np.repeat(np.arange(ny), nx)
+    out = np.empty(mesh.ncells, dtype=np.int64)
+    for b, (_, bi, bj) in enumerate(mesh.keys):
+        out[b * nx * ny:(b + 1) * nx * ny] = (bi * nx + ci + bj * ny + cj) & 1
+    return out
+
+
+def red_black_weight(matrix, colours):
+    """Weight of a red-black half-sweep: `_jacobi_weight!`'s rule min(1, 4/(3 b))
+    applied to the rows restricted to their own colour, b = max_i sum over j of
+    the same colour of |a_ij| / a_ii (1, so weight 1, for an exact two-colouring;
+    above 1 where coarse-fine faces, hanging-vertex rows or odd periodic axes
+    couple cells of one colour)."""
+    A = matrix.tocoo()
+    same = colours[A.row] == colours[A.col]
+    rs = np.zeros(matrix.shape[0])
+    np.add.at(rs, A.row[same], np.abs(A.data[same]))
+    d = matrix.diagonal()
+    ok = d > 0
+    bound = float(np.max(rs[ok] / d[ok])) if np.any(ok) else 0.0
+    return 1.0 if bound == 0.0 else min(1.0, 4.0 / (3.0 * bound))
+
+
 class Level:
     """`MultigridLevel` (hierarchy.jl:248-274) built by `_multigrid_level`."""
 
@@ -213,6 +247,8 @@ class Level:
         self.slots = comp["slots"]
         self.component_volumes = comp["volumes"] if op.singular else np.zeros(0)
         self.n = op.mesh.ncells
+        self.colours = red_black_colours(op.mesh)
+        self.rb_weight = red_black_weight(op.matrix, self.colours)
 
     @property
     def singular(self):
@@ -301,11 +337,22 @@ class TreeGeometricMultigrid:
             return self.coarse_lu.solve(rhs)[:c.n]
         return self.coarse_lu.solve(b)
 
-    def smooth(self, lev: Level, x, b, sweeps):
-        """`_smooth!` (cycles.jl:8-24): damped Jacobi, means removed per sweep."""
+    def smooth(self, lev: Level, x, b, sweeps, order=(0, 1)):
+        """`_smooth!` (cycles.jl:8-24): damped Jacobi, means removed per sweep.
+        With the red-black smoother each sweep updates the colours in `order`
+        (red then black before the coarse correction, the reverse after it, so
+        that the V-cycle stays symmetric), each colour from the iterate left by
+        the previous one, with `red_black_weight`."""
         for _ in range(sweeps):
-            t = lev.matrix @ x
-            x += lev.weight * lev.inverse_diagonal * (b - t)
+            if self.options.smoother == "red_black":
+                om = lev.rb_weight
+                for c in order:
+                    t = lev.matrix @ x
+                    sel = lev.colours == c
+                    x[sel] += om * lev.inverse_diagonal[sel] * (b[sel] - t[sel])
+            else:
+                t = lev.matrix @ x
+                x += lev.weight * lev.inverse_diagonal * (b - t)
             if lev.singular:
                 lev.remove_means(x)
         return x
@@ -325,7 +372,7 @@ class TreeGeometricMultigrid:
         x += lev.prolongation @ xc
         if lev.singular:
             lev.remove_means(x)
-        self.smooth(lev, x, b, self.post_sweeps)
+        self.smooth(lev, x, b, self.post_sweeps, order=(1, 0))
         return x
 
     def ldiv(self, r):

@@ -381,7 +381,10 @@ tpa_status tpa_build_hierarchy(tpa_context* ctx, const tpa_multigrid_options* op
             o.pre_sweeps = opts->pre_sweeps;
             o.post_sweeps = opts->post_sweeps;
             o.max_levels = opts->max_levels;
+            o.smoother = opts->smoother;
         }
+        if (o.smoother != 0 && o.smoother != 1)
+            throw tpa::Error(TPA_ERR_INVALID_ARG, "smoother must be 0 (damped Jacobi) or 1 (red-black Gauss-Seidel)");
         if (o.pre_sweeps != o.post_sweeps)
             throw tpa::Error(TPA_ERR_INVALID_ARG,
                              "CG requires equal pre_sweeps and post_sweeps for a geometric multigrid preconditioner");
@@ -430,6 +433,17 @@ tpa_status tpa_level_info(const tpa_context* cctx, int32_t level, double* sw, do
         if (sw) *sw = l.weight;
         if (tw) *tw = l.transfer_weight;
         if (comps) *comps = l.op.singular ? int32_t(l.op.comp.volume.size()) : 0;
+    });
+}
+
+tpa_status tpa_level_red_black(const tpa_context* cctx, int32_t level, uint8_t* colours, double* weight) {
+    auto* ctx = const_cast<tpa_context*>(cctx);
+    return guard(ctx, [&] {
+        ensure_host_fresh(ctx);
+        const tpa::HostLevel& l = level_of(ctx, level);
+        std::vector<unsigned char> c = tpa::red_black_colours(l.op.mesh);
+        if (colours) std::memcpy(colours, c.data(), c.size());
+        if (weight) *weight = tpa::red_black_weight(l.op.A, c);
     });
 }
 
@@ -873,6 +887,8 @@ tpa_status tpa_batch_create(tpa_batch** out, tpa_context* const* ctxs, int32_t c
                 throw tpa::Error(TPA_ERR_STATE, "problem " + std::to_string(k) + " has no hierarchy");
             if (ctxs[k]->device != ctxs[0]->device) throw tpa::Error(TPA_ERR_INVALID_ARG, "contexts on different devices");
             ensure_host_fresh(ctxs[k]);
+            if (ctxs[k]->hier.opts.smoother != 0)
+                throw tpa::Error(TPA_ERR_UNSUPPORTED, "the merged batch smooths with damped Jacobi only");
             hs.push_back(&ctxs[k]->hier);
         }
         int devices = 0;

@@ -60,6 +60,15 @@ __global__ void k_jacobi(int n, const int* __restrict__ rp, const int* __restric
     if (i < n) xout[i] = xin[i] + w * dinv[i] * (b[i] - row_dot(rp, ci, v, xin, i));
 }
 
+// red-black half-sweep: cells of colour c updated from xin, the others copied
+template <typename T>
+__global__ void k_rb_sweep(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ v,
+                           const T* __restrict__ b, const T* __restrict__ dinv, const unsigned char* __restrict__ col,
+                           int c, T w, const T* __restrict__ xin, T* __restrict__ xout) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) xout[i] = col[i] == c ? xin[i] + w * dinv[i] * (b[i] - row_dot(rp, ci, v, xin, i)) : xin[i];
+}
+
 template <typename T>
 __global__ void k_residual(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ v,
                            const T* __restrict__ b, const T* __restrict__ x, const T* __restrict__ tinv,
@@ -424,6 +433,38 @@ DeviceSolver::~DeviceSolver() {
 template <> DevLevelT<double>& DeviceSolver::lv<double>(int l) { return levels_[size_t(l)].d; }
 template <> DevLevelT<float>& DeviceSolver::lv<float>(int l) { return levels_[size_t(l)].f; }
 
+// Red-black colouring of a level (the reference smooths with damped Jacobi and
+// has no colouring): colour (I + J) mod 2 of every cell, (I, J) its lattice
+// coordinates at its own block's refinement level; 0 red, 1 black.
+std::vector<unsigned char> red_black_colours(const Mesh& m) {
+    const int nx = m.bs[0], ny = m.bs[1];
+    std::vector<unsigned char> out(static_cast<size_t>(m.ncells()));
+    for (int64_t b = 0; b < m.nblocks(); ++b) {
+        const int64_t bi = key_i(m.keys[size_t(b)]) * nx, bj = key_j(m.keys[size_t(b)]) * ny;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i)
+                out[size_t(b * nx * ny + j * nx + i)] = static_cast<unsigned char>((bi + i + bj + j) & 1);
+    }
+    return out;
+}
+
+// Weight of a red-black half-sweep: the `_jacobi_weight!` rule min(1, 4/(3 b)),
+// b = max_i sum_{j of i's colour} |a_ij| / a_ii (rows with a_ii > 0); weight 1
+// for an exact two-colouring (b = 1) or without a bound.
+double red_black_weight(const Csr& A, const std::vector<unsigned char>& col) {
+    double bound = 0.0;
+    for (int64_t r = 0; r < A.n; ++r) {
+        double d = 0.0, rs = 0.0;
+        for (int64_t k = A.ptr[size_t(r)]; k < A.ptr[size_t(r + 1)]; ++k) {
+            const int32_t c = A.col[size_t(k)];
+            if (c == r) d = A.val[size_t(k)];
+            if (col[size_t(c)] == col[size_t(r)]) rs += std::fabs(A.val[size_t(k)]);
+        }
+        if (d > 0) bound = std::max(bound, rs / d);
+    }
+    return bound == 0.0 ? 1.0 : std::min(1.0, 4.0 / (3.0 * bound));
+}
+
 void DeviceSolver::upload(const Hierarchy& h) {
     TPA_CUDA(cudaSetDevice(device_));
     TPA_CUDA(cudaStreamSynchronize(stream_));
@@ -433,6 +474,7 @@ void DeviceSolver::upload(const Hierarchy& h) {
     levels_.resize(h.levels.size());
     pre_ = h.opts.pre_sweeps;
     post_ = h.opts.post_sweeps;
+    rb_ = h.opts.smoother == 1;
     for (size_t l = 0; l < h.levels.size(); ++l) {
         const HostLevel& hl = h.levels[l];
         DevLevel& d = levels_[l];
@@ -480,6 +522,11 @@ void DeviceSolver::upload(const Hierarchy& h) {
             d.f.tinv.upload(ft.data(), ft.size(), stream_);
             d.d.tw = hl.transfer_weight;
             d.f.tw = float(hl.transfer_weight);
+        }
+        if (rb_) {
+            std::vector<unsigned char> col = red_black_colours(hl.op.mesh);
+            d.rbw = red_black_weight(A, col);
+            d.colour.upload(col.data(), col.size(), stream_);
         }
         for (auto* a : {&d.d.x, &d.d.y, &d.d.b, &d.d.r, &d.d.s}) a->alloc(static_cast<size_t>(d.n));
         for (auto* a : {&d.f.x, &d.f.y, &d.f.b, &d.f.r, &d.f.s}) a->alloc(static_cast<size_t>(d.n));
@@ -540,7 +587,17 @@ void DeviceSolver::vcycle_t(int /*unused*/) {
         if (L.ncomp) project_rhs<T>(l, D.b.p);
         T* x = D.x.p;
         T* y = D.y.p;
-        if (pre_ == 0) {
+        if (rb_) {
+            // red then black per sweep, from x = 0
+            k_fill<T><<<grid_for(L.n), kThreads, 0, stream_>>>(L.n, x, T(0));
+            for (int k = 0; k < pre_; ++k)
+                for (int c : {0, 1}) {
+                    k_rb_sweep<T><<<grid_for(L.n), kThreads, 0, stream_>>>(L.n, L.rowptr.p, L.col.p, D.val.p, D.b.p,
+                                                                          D.dinv.p, L.colour.p, c, T(L.rbw), x, y);
+                    std::swap(x, y);
+                }
+            launches_ += 1 + pre_;  // with the count below: the fill and 2 pre_ half-sweeps
+        } else if (pre_ == 0) {
             k_fill<T><<<grid_for(L.n), kThreads, 0, stream_>>>(L.n, x, T(0));
         } else {
             k_jacobi_first<T><<<grid_for(L.n), kThreads, 0, stream_>>>(L.n, D.b.p, D.dinv.p, D.w, x);
@@ -588,6 +645,15 @@ void DeviceSolver::vcycle_t(int /*unused*/) {
                                                               xcur[size_t(l + 1)], D.tinv.p, D.tw, x);
         ++launches_;
         for (int k = 0; k < post_; ++k) {
+            if (rb_) {  // black then red: the reverse of the pre-smoothing
+                for (int c : {1, 0}) {
+                    k_rb_sweep<T><<<grid_for(L.n), kThreads, 0, stream_>>>(L.n, L.rowptr.p, L.col.p, D.val.p, D.b.p,
+                                                                          D.dinv.p, L.colour.p, c, T(L.rbw), x, y);
+                    std::swap(x, y);
+                    ++launches_;
+                }
+                continue;
+            }
             k_jacobi<T><<<grid_for(L.n), kThreads, 0, stream_>>>(L.n, L.rowptr.p, L.col.p, D.val.p, D.b.p, D.dinv.p,
                                                                  D.w, x, y);
             std::swap(x, y);

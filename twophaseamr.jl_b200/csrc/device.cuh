@@ -82,6 +82,8 @@ struct DevLevel {
     std::vector<double> comp_volume;
     DevLevelT<double> d;
     DevLevelT<float> f;
+    DevArray<unsigned char> colour;  // red-black smoother: 0 red, 1 black per cell
+    double rbw = 1.0;                // red-black half-sweep weight
 };
 
 // PCG scalars kept on the device between kernels.
@@ -109,6 +111,10 @@ struct SolveStats {
     double ms_total = 0;
     int restarts = 0;
 };
+
+// red-black smoother set-up (device.cu)
+std::vector<unsigned char> red_black_colours(const Mesh& m);
+double red_black_weight(const Csr& A, const std::vector<unsigned char>& colours);
 
 class DeviceSolver {
 public:
@@ -138,6 +144,7 @@ public:
     void residual_norms(const double* r, double out[2]);
 
     int kernel_launches() const { return launches_; }
+    bool red_black() const { return rb_; }
     void reset_launches() { launches_ = 0; }
 
 private:
@@ -154,6 +161,7 @@ private:
     DevArray<double> coarse_inv_, coarse_b_, coarse_x_;
     int coarse_n_ = 0;
     int pre_ = 2, post_ = 2;
+    bool rb_ = false;  // red-black Gauss-Seidel smoother in place of damped Jacobi
     // fine-level FP64 PCG workspace
     DevArray<double> b_, r_, p_, ap_, z_, tmp_, partial_;
     DevArray<CgScalars> sc_;

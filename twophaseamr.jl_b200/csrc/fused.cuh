@@ -62,6 +62,9 @@ struct LevelView {
     T* y;              // second iterate buffer
     T* r;              // residual
     T* s;              // Dt^-1 r
+    const unsigned char* colour;  // red-black smoother (rb != 0): 0 red, 1 black
+    int rb;
+    T rbw;             // red-black half-sweep weight
 };
 
 // fold partial[0..count) in fixed order by one block; returns the sum in thread 0
@@ -204,6 +207,36 @@ __device__ __forceinline__ void sweep_cell(const LevelView<T>& L, const T* in, T
     out[i] = in[i] + L.w * L.dinv[i] * (L.bp[i] - rowdot(L, in, i));
 }
 
+// Red-black Gauss-Seidel (an option; the reference smooths with damped
+// Jacobi).  A half-sweep updates the cells of one colour from the iterate `in`
+// into `out` and copies the other colour, so that coupled cells of one colour
+// (coarse-fine faces) read the values of the previous half-sweep.  Red then
+// black before the coarse correction, the reverse after it: the V-cycle stays
+// symmetric, as CG needs.
+
+// first sweep from x = 0: red x = w D^-1 bp; black x = w D^-1 (bp - A x_red),
+// the red values recomputed at the black cell's red neighbours
+template <typename T, typename TB>
+__device__ __forceinline__ void rb_first_cell(const LevelView<T>& L, const TB* b, double mean, int i) {
+    const T bi = proj_b<T, TB>(L, b, mean, i);
+    L.bp[i] = bi;
+    if (L.colour[i] == 0) {
+        L.x[i] = L.rbw * L.dinv[i] * bi;
+        return;
+    }
+    T acc = T(0);
+    for (int k = L.rp[i]; k < L.rp[i + 1]; ++k) {
+        const int j = L.ci[k];
+        if (L.colour[j] == 0) acc += L.val[k] * (L.rbw * L.dinv[j] * proj_b<T, TB>(L, b, mean, j));
+    }
+    L.x[i] = L.rbw * L.dinv[i] * (bi - acc);
+}
+
+template <typename T>
+__device__ __forceinline__ void rb_half_cell(const LevelView<T>& L, const T* in, T* out, int c, int i) {
+    out[i] = L.colour[i] == c ? in[i] + L.rbw * L.dinv[i] * (L.bp[i] - rowdot(L, in, i)) : in[i];
+}
+
 // ---------------------------------------------------------------------------------
 // multi-CTA kernels
 
@@ -215,6 +248,37 @@ __global__ void k_pre2(LevelView<T> L, const TB* __restrict__ b, const double* l
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
     if (i < L.n) pre2_cell<T, TB>(L, b, mean, i);
+}
+
+template <typename T, typename TB>
+__global__ void k_rb_pre(LevelView<T> L, const TB* __restrict__ b, const double* level_sum) {
+    pdl_entry();
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
+    if (i < L.n) rb_first_cell<T, TB>(L, b, mean, i);
+}
+
+// one red-black half-sweep in -> out (colour c); with `mean_out`, also the
+// volume-weighted mean of out (the last post-sweep of the finest level)
+template <typename T>
+__global__ void k_rb_half(LevelView<T> L, const T* __restrict__ in, T* __restrict__ out, int c, double* partial,
+                          unsigned* counter, double* mean_out) {
+    pdl_entry();
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0;
+    if (i < L.n) {
+        rb_half_cell(L, in, out, c, i);
+        v = double(L.vol[i]) * double(out[i]);
+    }
+    if (mean_out) {
+        if (publish_partial(v, partial, counter)) {
+            double s = fold_partials(partial, gridDim.x);
+            if (threadIdx.x == 0) {
+                *mean_out = s * L.cvol_inv;
+                *counter = 0;
+            }
+        }
+    }
 }
 
 template <typename T>
@@ -402,9 +466,20 @@ __device__ void tail_run(const LevelView<T>* __restrict__ levels, int first, int
             cl.sync();
             break;
         }
-        for (int i = gt; i < L.n; i += gs) {
-            if (top) pre2_cell<T, TB>(L, top_b, mean, i);
-            else pre2_cell<T, T>(L, L.b, mean, i);
+        if (L.rb) {
+            for (int i = gt; i < L.n; i += gs) {
+                if (top) rb_first_cell<T, TB>(L, top_b, mean, i);
+                else rb_first_cell<T, T>(L, L.b, mean, i);
+            }
+            cl.sync();
+            for (int i = gt; i < L.n; i += gs) rb_half_cell(L, L.x, L.y, 0, i);
+            cl.sync();
+            for (int i = gt; i < L.n; i += gs) rb_half_cell(L, L.y, L.x, 1, i);
+        } else {
+            for (int i = gt; i < L.n; i += gs) {
+                if (top) pre2_cell<T, TB>(L, top_b, mean, i);
+                else pre2_cell<T, T>(L, L.b, mean, i);
+            }
         }
         cl.sync();
         for (int i = gt; i < L.n; i += gs) residual_cell(L, i);
@@ -424,6 +499,15 @@ __device__ void tail_run(const LevelView<T>* __restrict__ levels, int first, int
         const T* xc = levels[l + 1].x;
         for (int i = gt; i < L.n; i += gs) prolong_cell(L, xc, i);
         cl.sync();
+        if (L.rb) {
+            for (int s = 0; s < 2; ++s) {
+                for (int i = gt; i < L.n; i += gs) rb_half_cell(L, L.x, L.y, 1, i);
+                cl.sync();
+                for (int i = gt; i < L.n; i += gs) rb_half_cell(L, L.y, L.x, 0, i);
+                cl.sync();
+            }
+            continue;
+        }
         for (int i = gt; i < L.n; i += gs) sweep_cell(L, L.x, L.y, i);
         cl.sync();
         for (int i = gt; i < L.n; i += gs) sweep_cell(L, L.y, L.x, i);

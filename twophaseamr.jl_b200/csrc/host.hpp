@@ -133,6 +133,7 @@ double jacobi_weight(std::vector<double>& inv_diag, const std::vector<double>& r
 
 struct HierarchyOptions {
     int coarse_size = 64, pre_sweeps = 2, post_sweeps = 2, max_levels = 32;
+    int smoother = 0;  // 0 damped Jacobi (the reference's), 1 red-black Gauss-Seidel
 };
 
 // One level of the tree hierarchy with everything the device V-cycle reads.

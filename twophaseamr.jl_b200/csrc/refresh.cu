@@ -75,20 +75,24 @@ __global__ void kr_assemble(int nnz, const int* __restrict__ tptr, const int* __
     }
 }
 
-// D^-1 and Dt^-1 per row and the two Jacobi bounds max_i sum_j |a_ij| / a_ii;
-// the last block writes w = min(1, 4/(3 bound)) (1 without a bound) and the
-// unclamped transfer weight 4/(3 bound) (0 without a bound) into wtw[0..1].
+// D^-1 and Dt^-1 per row and the Jacobi bounds max_i sum_j |a_ij| / a_ii;
+// the last block writes w = min(1, 4/(3 bound)) (1 without a bound), the
+// unclamped transfer weight 4/(3 bound) (0 without a bound) and, with a
+// red-black colouring, the half-sweep weight from the rows restricted to their
+// own colour into wtw[0..2].
 __global__ void kr_weights(int n, const int* __restrict__ rp, const int* __restrict__ ci,
-                           const double* __restrict__ val, int singular, double* __restrict__ dinv_d,
-                           float* __restrict__ dinv_f, double* __restrict__ tinv_d, float* __restrict__ tinv_f,
-                           double* partial, unsigned* counter, double* wtw, int* err) {
-    double bs = 0.0, bt = 0.0;
+                           const double* __restrict__ val, int singular, const unsigned char* __restrict__ colour,
+                           double* __restrict__ dinv_d, float* __restrict__ dinv_f, double* __restrict__ tinv_d,
+                           float* __restrict__ tinv_f, double* partial, unsigned* counter, double* wtw, int* err) {
+    double bs = 0.0, bt = 0.0, br = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double d = 0.0, rs = 0.0;
+        double d = 0.0, rs = 0.0, rc = 0.0;
         for (int k = rp[i]; k < rp[i + 1]; ++k) {
             rs += fabs(val[k]);
             if (ci[k] == i) d = val[k];
+            if (colour && colour[ci[k]] == colour[i]) rc += fabs(val[k]);
         }
+        if (d > 0) br = fmax(br, rc / d);
         double di = d;
         if (d == 0.0 && singular) {
             // an isolated cell of an ungauged component keeps D^-1 = 0
@@ -110,39 +114,45 @@ __global__ void kr_weights(int n, const int* __restrict__ rp, const int* __restr
             tinv_f[i] = float(ti);
         }
     }
-    __shared__ double sh[2][32];
+    __shared__ double sh[3][32];
     __shared__ bool last;
     for (int o = 16; o; o >>= 1) {
         bs = fmax(bs, __shfl_down_sync(0xffffffffu, bs, o));
         bt = fmax(bt, __shfl_down_sync(0xffffffffu, bt, o));
+        br = fmax(br, __shfl_down_sync(0xffffffffu, br, o));
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (!lane) {
         sh[0][wid] = bs;
         sh[1][wid] = bt;
+        sh[2][wid] = br;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double ms = 0.0, mt = 0.0;
+        double ms = 0.0, mt = 0.0, mr = 0.0;
         for (int w = 0; w < int(blockDim.x >> 5); ++w) {
             ms = fmax(ms, sh[0][w]);
             mt = fmax(mt, sh[1][w]);
+            mr = fmax(mr, sh[2][w]);
         }
         partial[blockIdx.x] = ms;
         partial[gridDim.x + blockIdx.x] = mt;
+        partial[2 * gridDim.x + blockIdx.x] = mr;
         __threadfence();
         last = atomicAdd(counter, 1u) == gridDim.x - 1;
     }
     __syncthreads();
     if (last && threadIdx.x == 0) {
         __threadfence();
-        double ms = 0.0, mt = 0.0;
+        double ms = 0.0, mt = 0.0, mr = 0.0;
         for (unsigned b = 0; b < gridDim.x; ++b) {
             ms = fmax(ms, ((volatile double*)partial)[b]);
             mt = fmax(mt, ((volatile double*)partial)[gridDim.x + b]);
+            mr = fmax(mr, ((volatile double*)partial)[2 * gridDim.x + b]);
         }
         wtw[0] = ms == 0.0 ? 1.0 : fmin(1.0, 4.0 / (3.0 * ms));
         wtw[1] = mt == 0.0 ? 0.0 : 4.0 / (3.0 * mt);
+        wtw[2] = mr == 0.0 ? 1.0 : fmin(1.0, 4.0 / (3.0 * mr));
         *counter = 0;
     }
 }
@@ -611,8 +621,8 @@ void DeviceSolver::prepare_refresh(const Hierarchy& h) {
     if (rstage_) cudaFreeHost(rstage_);
     rstage_ = nullptr;
     TPA_CUDA(cudaMallocHost(&rstage_, sizeof(double) * std::max<size_t>(1, size_t(rl_[0].nf))));
-    rwtw_.alloc(size_t(2 * nl));
-    rpart_.alloc(size_t(2 * 1184));
+    rwtw_.alloc(size_t(3 * nl));
+    rpart_.alloc(size_t(3 * 1184));
     rcnt_.alloc(1);
     rerr_.alloc(1);
     TPA_CUDA(cudaMemsetAsync(rcnt_.p, 0, sizeof(unsigned), stream_));
@@ -680,9 +690,10 @@ void DeviceSolver::refresh_levels() {
                                                                            R.rw.p, R.kappa.p,
                                                                            rl_[size_t(l + 1)].kappa.p);
         kr_weights<<<rgrid(L.n), kRThreads, 0, s>>>(L.n, L.rowptr.p, L.col.p, L.d.val.p, L.ncomp > 0 ? 1 : 0,
+                                                   rb_ ? L.colour.p : nullptr,
                                                    L.d.dinv.p, L.f.dinv.p, l + 1 < nl ? L.d.tinv.p : nullptr,
                                                    l + 1 < nl ? L.f.tinv.p : nullptr, rpart_.p, rcnt_.p,
-                                                   rwtw_.p + 2 * l, rerr_.p);
+                                                   rwtw_.p + 3 * l, rerr_.p);
     }
     const DevLevel& C = levels_.back();
     TPA_CUDA(cudaMemsetAsync(coarse_M_.p, 0, sizeof(double) * coarse_M_.n, s));
@@ -711,7 +722,7 @@ void DeviceSolver::refresh_levels() {
     kr_coarse_inv<<<(C.n + kInvWarps - 1) / kInvWarps, 32 * kInvWarps, inv_smem(N), s>>>(
         N, C.n, coarse_M_.p, coarse_piv_.p, coarse_inv_.p, rerr_.p);
     TPA_CUDA(cudaGetLastError());
-    std::vector<double> wtw(size_t(2 * nl));
+    std::vector<double> wtw(size_t(3 * nl));
     int err = 0;
     TPA_CUDA(cudaMemcpyAsync(wtw.data(), rwtw_.p, sizeof(double) * wtw.size(), cudaMemcpyDeviceToHost, s));
     TPA_CUDA(cudaMemcpyAsync(&err, rerr_.p, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -720,11 +731,16 @@ void DeviceSolver::refresh_levels() {
     if (err == 2) throw Error(1, "coarsest multigrid matrix is singular");
     for (int l = 0; l < nl; ++l) {
         DevLevel& L = levels_[size_t(l)];
-        L.d.w = wtw[size_t(2 * l)];
+        L.d.w = wtw[size_t(3 * l)];
         L.f.w = float(L.d.w);
         if (l + 1 < nl) {
-            L.d.tw = wtw[size_t(2 * l + 1)];
+            L.d.tw = wtw[size_t(3 * l + 1)];
             L.f.tw = float(L.d.tw);
+        }
+        if (rb_) {
+            L.rbw = wtw[size_t(3 * l + 2)];
+            vd_[size_t(l)].rbw = L.rbw;
+            vf_[size_t(l)].rbw = float(L.rbw);
         }
         vd_[size_t(l)].w = L.d.w;
         vf_[size_t(l)].w = L.f.w;

@@ -379,6 +379,10 @@ TuneConfig DeviceSolver::effective_tuning() const {
     if (tune_.fuse_restrict >= 0) c.fuse_restrict = tune_.fuse_restrict ? 1 : 0;
     c.persistent = std::getenv("TPAGMG_PERSISTENT") ? 1 : 0;
     if (tune_.persistent >= 0) c.persistent = tune_.persistent ? 1 : 0;
+    if (rb_) {  // the red-black sweeps exist for the CSR levels and the tail only
+        c.structured = 0;
+        c.persistent = 0;
+    }
     return c;
 }
 
@@ -438,6 +442,9 @@ void DeviceSolver::build_views() {
             v.y = D.y.p;
             v.r = D.r.p;
             v.s = D.s.p;
+            v.colour = L.colour.p;
+            v.rb = rb_ ? 1 : 0;
+            v.rbw = static_cast<decltype(v.w)>(L.rbw);
         };
         fill(vd_[size_t(l)], L.d);
         fill(vf_[size_t(l)], L.f);
@@ -530,8 +537,17 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
             launches_ += 3;
             continue;
         }
-        if (l == 0) go(k_pre2<T, double>, blocks_for(L.n), kThreads, 0, L, r, rsum);
-        else go(k_pre2<T, T>, blocks_for(L.n), kThreads, 0, L, L.b, lsum_.p + l);
+        if (L.rb) {
+            if (l == 0) go(k_rb_pre<T, double>, blocks_for(L.n), kThreads, 0, L, r, rsum);
+            else go(k_rb_pre<T, T>, blocks_for(L.n), kThreads, 0, L, L.b, lsum_.p + l);
+            go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.x, L.y, 0, nullptr, nullptr, nullptr);
+            go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.y, L.x, 1, nullptr, nullptr, nullptr);
+            launches_ += 2;
+        } else if (l == 0) {
+            go(k_pre2<T, double>, blocks_for(L.n), kThreads, 0, L, r, rsum);
+        } else {
+            go(k_pre2<T, T>, blocks_for(L.n), kThreads, 0, L, L.b, lsum_.p + l);
+        }
         const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
         const int rgrid = next_sum ? reduce_grid(4 * int64_t(L.nc)) : blocks_for(4 * int64_t(L.nc));
         if (fuse_rr_) {
@@ -580,6 +596,16 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
             continue;
         }
         go(k_prolong<T>, blocks_for(L.n), kThreads, 0, L, V[size_t(l + 1)].x);
+        if (L.rb) {
+            const bool last_mean = (l == 0) && L.singular;
+            go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.x, L.y, 1, nullptr, nullptr, nullptr);
+            go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.y, L.x, 0, nullptr, nullptr, nullptr);
+            go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.x, L.y, 1, nullptr, nullptr, nullptr);
+            go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.y, L.x, 0, fpartial_.p,
+               counters_.p + kPostMean, last_mean ? mean_out : nullptr);
+            launches_ += 5;
+            continue;
+        }
         go(k_post1<T>, blocks_for(L.n), kThreads, 0, L);
         const bool want_mean = (l == 0) && L.singular;
         go(k_post2<T>, blocks_for(L.n), kThreads, 0, L, fpartial_.p, counters_.p + kPostMean,

@@ -32,7 +32,7 @@ class TpaError(RuntimeError):
 
 class MultigridOptionsC(C.Structure):
     _fields_ = [("coarse_size", C.c_int32), ("pre_sweeps", C.c_int32),
-                ("post_sweeps", C.c_int32), ("max_levels", C.c_int32)]
+                ("post_sweeps", C.c_int32), ("max_levels", C.c_int32), ("smoother", C.c_int32)]
 
 
 class StatsC(C.Structure):
@@ -111,6 +111,7 @@ SIGNATURES = {
     "tpa_residual_norms_noalloc": (C.c_int32, [P, P, P, C.c_int64, f64p]),
     "tpa_time_kernel": (C.c_int32, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, f64p]),
     "tpa_refresh_device": (C.c_int32, [P, P]),
+    "tpa_level_red_black": (C.c_int32, [P, C.c_int32, C.POINTER(C.c_uint8), f64p]),
     "tpa_conditional_fraction_device": (C.c_int32, [P, P, C.c_double, P, P]),
     "tpa_face_coefficients_device": (C.c_int32, [P, P, C.c_double, C.c_double, P]),
     "tpa_surface_tension_device": (C.c_int32, [P, P, C.c_double, C.c_double, C.c_int32, P, P]),

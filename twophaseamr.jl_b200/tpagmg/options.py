@@ -27,8 +27,13 @@ class MultigridOptions:
     pre_sweeps: int = 2
     post_sweeps: int = 2
     max_levels: int = 32
+    # not in the reference: "red_black" replaces the damped Jacobi sweeps by
+    # red-black Gauss-Seidel half-sweeps (colour (I + J) mod 2 per level)
+    smoother: str = "jacobi"
 
     def __post_init__(self):
+        if self.smoother not in ("jacobi", "red_black"):
+            raise ValueError("smoother must be 'jacobi' or 'red_black'")
         if not all(_is_int(v) for v in (self.coarse_size, self.pre_sweeps, self.post_sweeps, self.max_levels)):
             raise TypeError("multigrid sizes and sweep counts must be integers")
         if self.coarse_size <= 0:

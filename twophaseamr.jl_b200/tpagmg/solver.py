@@ -68,7 +68,8 @@ class EllipticSolver:
         mg = MultigridOptions(coarse_size=mg.coarse_size if coarse_size is None else coarse_size,
                               pre_sweeps=mg.pre_sweeps if pre_sweeps is None else pre_sweeps,
                               post_sweeps=mg.post_sweeps if post_sweeps is None else post_sweeps,
-                              max_levels=mg.max_levels if max_levels is None else max_levels)
+                              max_levels=mg.max_levels if max_levels is None else max_levels,
+                              smoother=mg.smoother)
         if mg.pre_sweeps != mg.post_sweeps:
             raise ValueError(f"CG requires equal pre_sweeps and post_sweeps for a geometric multigrid "
                              f"preconditioner; got {mg.pre_sweeps} and {mg.post_sweeps}")
@@ -87,7 +88,8 @@ class EllipticSolver:
         self.ctx.call("tpa_set_mesh", *mesh._mesh_args())
         self._kappa = _lib.f64(operator.face_coefficient)
         self.ctx.call("tpa_set_operator", _lib.ptr(self._kappa, C.c_double))
-        o = _lib.MultigridOptionsC(mg.coarse_size, mg.pre_sweeps, mg.post_sweeps, mg.max_levels)
+        o = _lib.MultigridOptionsC(mg.coarse_size, mg.pre_sweeps, mg.post_sweeps, mg.max_levels,
+                                   1 if mg.smoother == "red_black" else 0)
         self.ctx.call("tpa_build_hierarchy", C.byref(o))
         self.stats = LinearSolverStats(precision=precision)
 
@@ -108,6 +110,13 @@ class EllipticSolver:
         sw, tw, nc = C.c_double(), C.c_double(), C.c_int32()
         self.ctx.call("tpa_level_info", int(level), C.byref(sw), C.byref(tw), C.byref(nc))
         return sw.value, tw.value, nc.value
+
+    def level_red_black(self, level, ncells):
+        """Red-black colours (0 red, 1 black) of a level and its half-sweep weight."""
+        col = np.zeros(ncells, dtype=np.uint8)
+        w = C.c_double()
+        self.ctx.call("tpa_level_red_black", int(level), col.ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(w))
+        return col, w.value
 
     def level_face_coefficients(self, level, nfaces):
         out = np.zeros(nfaces, dtype=np.float64)
