@@ -435,6 +435,41 @@ def main():
     peak, peak_kind = measured_peaks()
     achieved = alg32 / (sweep.value * 1e-3) / 1e9
 
+    # the same solve with the red-black Gauss-Seidel smoother (an option; the
+    # reference smooths with damped Jacobi), after the timed solves
+    red_black = None
+    if not args.profile:
+        from tpagmg import MultigridOptions
+        rb = EllipticSolver(PoissonOperator(mesh, kappa), device=local,
+                            multigrid=MultigridOptions(smoother="red_black"))
+        rb.ctx.call("tpa_set_stream", C.c_void_p(stream.cuda_stream))
+
+        def rb_timed(precision, steps):
+            ms, its = [], []
+            for k in range(steps + 2):
+                x_d.zero_()
+                flush.fill_(1.0)
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                st = rb.solve_device(rhs_d.data_ptr(), x_d.data_ptr(), rtol=RTOL, precision=precision)
+                e1.record(stream)
+                e1.synchronize()
+                assert st.converged, st
+                if k >= 2:
+                    ms.append(e0.elapsed_time(e1))
+                    its.append(st.cycles)
+            return float(np.mean(ms)), float(np.mean(its))
+        rb_mixed_ms, rb_mixed_it = rb_timed("mixed", args.steps)
+        rb_fp64_ms, rb_fp64_it = rb_timed("fp64", args.steps)
+        red_black = {"mixed_ms": rb_mixed_ms, "fp64_ms": rb_fp64_ms,
+                     "cg_iterations": {"mixed": rb_mixed_it, "fp64": rb_fp64_it},
+                     "mixed_value": world * n * rb_mixed_it / (rb_mixed_ms * 1e-3),
+                     "what": "red-black Gauss-Seidel smoother (MultigridOptions smoother='red_black'), "
+                             "same inputs and tolerance, default layout"}
+        del rb
+
     # the per-step coefficient refresh (`_refresh_geometric_multigrid!`), after
     # the timed solves: device path, then the host path, median wall ms
     refresh = None
@@ -549,6 +584,7 @@ def main():
         "cpu_baseline": cpu,
         "refresh": refresh,
         "two_phase_step": two_phase,
+        "red_black_smoother": red_black,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -162,6 +162,11 @@ private:
     int coarse_n_ = 0;
     int pre_ = 2, post_ = 2;
     bool rb_ = false;  // red-black Gauss-Seidel smoother in place of damped Jacobi
+    // red-black levels up to this many cells fuse each sweep's two half-sweeps
+    // into one pass (recomputing the first colour); larger levels use two.
+    // Measured slower at every threshold on the droplet (the recomputation
+    // costs more than the launch it saves), so 0 unless TPAGMG_RB_PAIR_CELLS.
+    int rb_pair_cells_ = 0;
     // fine-level FP64 PCG workspace
     DevArray<double> b_, r_, p_, ap_, z_, tmp_, partial_;
     DevArray<CgScalars> sc_;

@@ -209,19 +209,19 @@ __device__ __forceinline__ void sweep_cell(const LevelView<T>& L, const T* in, T
 
 // Red-black Gauss-Seidel (an option; the reference smooths with damped
 // Jacobi).  A half-sweep updates the cells of one colour from the iterate `in`
-// into `out` and copies the other colour, so that coupled cells of one colour
-// (coarse-fine faces) read the values of the previous half-sweep.  Red then
+// and keeps the other colour, so that coupled cells of one colour (coarse-fine
+// faces) read the values of the previous half-sweep.  Red then
 // black before the coarse correction, the reverse after it: the V-cycle stays
 // symmetric, as CG needs.
 
-// first sweep from x = 0: red x = w D^-1 bp; black x = w D^-1 (bp - A x_red),
+// first sweep from zero into `out`: red w D^-1 bp; black w D^-1 (bp - A x_red),
 // the red values recomputed at the black cell's red neighbours
 template <typename T, typename TB>
-__device__ __forceinline__ void rb_first_cell(const LevelView<T>& L, const TB* b, double mean, int i) {
+__device__ __forceinline__ void rb_first_cell(const LevelView<T>& L, const TB* b, double mean, T* out, int i) {
     const T bi = proj_b<T, TB>(L, b, mean, i);
     L.bp[i] = bi;
     if (L.colour[i] == 0) {
-        L.x[i] = L.rbw * L.dinv[i] * bi;
+        out[i] = L.rbw * L.dinv[i] * bi;
         return;
     }
     T acc = T(0);
@@ -229,12 +229,32 @@ __device__ __forceinline__ void rb_first_cell(const LevelView<T>& L, const TB* b
         const int j = L.ci[k];
         if (L.colour[j] == 0) acc += L.val[k] * (L.rbw * L.dinv[j] * proj_b<T, TB>(L, b, mean, j));
     }
-    L.x[i] = L.rbw * L.dinv[i] * (bi - acc);
+    out[i] = L.rbw * L.dinv[i] * (bi - acc);
 }
 
+// the half-sweep value of cell i of colour c from `in`
 template <typename T>
-__device__ __forceinline__ void rb_half_cell(const LevelView<T>& L, const T* in, T* out, int c, int i) {
-    out[i] = L.colour[i] == c ? in[i] + L.rbw * L.dinv[i] * (L.bp[i] - rowdot(L, in, i)) : in[i];
+__device__ __forceinline__ T rb_update(const LevelView<T>& L, const T* in, int i) {
+    return in[i] + L.rbw * L.dinv[i] * (L.bp[i] - rowdot(L, in, i));
+}
+
+// two half-sweeps, colour c then the other, from `in` into `out` in one pass:
+// a cell of the second colour recomputes its colour-c neighbours' first
+// half-sweep values (the same arithmetic, so the same bits, as the
+// half-sweep kernel writes); cells of one colour read only `in` values of
+// their own colour, as in two separate half-sweeps
+template <typename T>
+__device__ __forceinline__ void rb_pair_cell(const LevelView<T>& L, const T* in, T* out, int c, int i) {
+    if (L.colour[i] == c) {
+        out[i] = rb_update(L, in, i);
+        return;
+    }
+    T acc = T(0);
+    for (int k = L.rp[i]; k < L.rp[i + 1]; ++k) {
+        const int j = L.ci[k];
+        acc += L.val[k] * (L.colour[j] == c ? rb_update(L, in, j) : in[j]);
+    }
+    out[i] = in[i] + L.rbw * L.dinv[i] * (L.bp[i] - acc);
 }
 
 // ---------------------------------------------------------------------------------
@@ -250,16 +270,8 @@ __global__ void k_pre2(LevelView<T> L, const TB* __restrict__ b, const double* l
     if (i < L.n) pre2_cell<T, TB>(L, b, mean, i);
 }
 
-template <typename T, typename TB>
-__global__ void k_rb_pre(LevelView<T> L, const TB* __restrict__ b, const double* level_sum) {
-    pdl_entry();
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
-    if (i < L.n) rb_first_cell<T, TB>(L, b, mean, i);
-}
-
-// one red-black half-sweep in -> out (colour c); with `mean_out`, also the
-// volume-weighted mean of out (the last post-sweep of the finest level)
+// one red-black half-sweep (colour c) from in into out; with `mean_out`, also
+// the volume-weighted mean of out
 template <typename T>
 __global__ void k_rb_half(LevelView<T> L, const T* __restrict__ in, T* __restrict__ out, int c, double* partial,
                           unsigned* counter, double* mean_out) {
@@ -267,7 +279,39 @@ __global__ void k_rb_half(LevelView<T> L, const T* __restrict__ in, T* __restric
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v = 0;
     if (i < L.n) {
-        rb_half_cell(L, in, out, c, i);
+        out[i] = L.colour[i] == c ? rb_update(L, in, i) : in[i];
+        v = double(L.vol[i]) * double(out[i]);
+    }
+    if (mean_out) {
+        if (publish_partial(v, partial, counter)) {
+            double s = fold_partials(partial, gridDim.x);
+            if (threadIdx.x == 0) {
+                *mean_out = s * L.cvol_inv;
+                *counter = 0;
+            }
+        }
+    }
+}
+
+// first red-black sweep from zero into out
+template <typename T, typename TB>
+__global__ void k_rb_pre(LevelView<T> L, const TB* __restrict__ b, const double* level_sum, T* out) {
+    pdl_entry();
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
+    if (i < L.n) rb_first_cell<T, TB>(L, b, mean, out, i);
+}
+
+// one red-black sweep (colour c, then the other) from in into out; with
+// `mean_out`, also the volume-weighted mean of out
+template <typename T>
+__global__ void k_rb_pair(LevelView<T> L, const T* __restrict__ in, T* __restrict__ out, int c, double* partial,
+                          unsigned* counter, double* mean_out) {
+    pdl_entry();
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0;
+    if (i < L.n) {
+        rb_pair_cell(L, in, out, c, i);
         v = double(L.vol[i]) * double(out[i]);
     }
     if (mean_out) {
@@ -468,13 +512,11 @@ __device__ void tail_run(const LevelView<T>* __restrict__ levels, int first, int
         }
         if (L.rb) {
             for (int i = gt; i < L.n; i += gs) {
-                if (top) rb_first_cell<T, TB>(L, top_b, mean, i);
-                else rb_first_cell<T, T>(L, L.b, mean, i);
+                if (top) rb_first_cell<T, TB>(L, top_b, mean, L.y, i);
+                else rb_first_cell<T, T>(L, L.b, mean, L.y, i);
             }
             cl.sync();
-            for (int i = gt; i < L.n; i += gs) rb_half_cell(L, L.x, L.y, 0, i);
-            cl.sync();
-            for (int i = gt; i < L.n; i += gs) rb_half_cell(L, L.y, L.x, 1, i);
+            for (int i = gt; i < L.n; i += gs) rb_pair_cell(L, L.y, L.x, 0, i);
         } else {
             for (int i = gt; i < L.n; i += gs) {
                 if (top) pre2_cell<T, TB>(L, top_b, mean, i);
@@ -500,12 +542,10 @@ __device__ void tail_run(const LevelView<T>* __restrict__ levels, int first, int
         for (int i = gt; i < L.n; i += gs) prolong_cell(L, xc, i);
         cl.sync();
         if (L.rb) {
-            for (int s = 0; s < 2; ++s) {
-                for (int i = gt; i < L.n; i += gs) rb_half_cell(L, L.x, L.y, 1, i);
-                cl.sync();
-                for (int i = gt; i < L.n; i += gs) rb_half_cell(L, L.y, L.x, 0, i);
-                cl.sync();
-            }
+            for (int i = gt; i < L.n; i += gs) rb_pair_cell(L, L.x, L.y, 1, i);
+            cl.sync();
+            for (int i = gt; i < L.n; i += gs) rb_pair_cell(L, L.y, L.x, 1, i);
+            cl.sync();
             continue;
         }
         for (int i = gt; i < L.n; i += gs) sweep_cell(L, L.x, L.y, i);

@@ -400,6 +400,7 @@ void DeviceSolver::check_barrier() {
 
 void DeviceSolver::build_views() {
     const TuneConfig cfg = effective_tuning();
+    if (const char* e = std::getenv("TPAGMG_RB_PAIR_CELLS")) rb_pair_cells_ = std::atoi(e);
     pdl_ = cfg.pdl != 0;
     fuse_rr_ = cfg.fuse_restrict != 0;
     fused_ok_ = (pre_ == 2 && post_ == 2);
@@ -538,11 +539,20 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
             continue;
         }
         if (L.rb) {
-            if (l == 0) go(k_rb_pre<T, double>, blocks_for(L.n), kThreads, 0, L, r, rsum);
-            else go(k_rb_pre<T, T>, blocks_for(L.n), kThreads, 0, L, L.b, lsum_.p + l);
-            go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.x, L.y, 0, nullptr, nullptr, nullptr);
-            go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.y, L.x, 1, nullptr, nullptr, nullptr);
-            launches_ += 2;
+            // second sweep: one pass on a small level (the red values recomputed),
+            // two half-sweeps on a large one
+            const bool pair = L.n <= rb_pair_cells_;
+            T* first = pair ? L.y : L.x;
+            if (l == 0) go(k_rb_pre<T, double>, blocks_for(L.n), kThreads, 0, L, r, rsum, first);
+            else go(k_rb_pre<T, T>, blocks_for(L.n), kThreads, 0, L, L.b, lsum_.p + l, first);
+            if (pair) {
+                go(k_rb_pair<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.y, L.x, 0, nullptr, nullptr, nullptr);
+                ++launches_;
+            } else {
+                go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.x, L.y, 0, nullptr, nullptr, nullptr);
+                go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.y, L.x, 1, nullptr, nullptr, nullptr);
+                launches_ += 2;
+            }
         } else if (l == 0) {
             go(k_pre2<T, double>, blocks_for(L.n), kThreads, 0, L, r, rsum);
         } else {
@@ -598,12 +608,20 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
         go(k_prolong<T>, blocks_for(L.n), kThreads, 0, L, V[size_t(l + 1)].x);
         if (L.rb) {
             const bool last_mean = (l == 0) && L.singular;
-            go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.x, L.y, 1, nullptr, nullptr, nullptr);
-            go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.y, L.x, 0, nullptr, nullptr, nullptr);
-            go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.x, L.y, 1, nullptr, nullptr, nullptr);
-            go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.y, L.x, 0, fpartial_.p,
-               counters_.p + kPostMean, last_mean ? mean_out : nullptr);
-            launches_ += 5;
+            double* mo = last_mean ? mean_out : nullptr;
+            if (L.n <= rb_pair_cells_) {
+                go(k_rb_pair<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.x, L.y, 1, nullptr, nullptr, nullptr);
+                go(k_rb_pair<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.y, L.x, 1, fpartial_.p,
+                   counters_.p + kPostMean, mo);
+                launches_ += 3;
+            } else {
+                go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.x, L.y, 1, nullptr, nullptr, nullptr);
+                go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.y, L.x, 0, nullptr, nullptr, nullptr);
+                go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.x, L.y, 1, nullptr, nullptr, nullptr);
+                go(k_rb_half<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.y, L.x, 0, fpartial_.p,
+                   counters_.p + kPostMean, mo);
+                launches_ += 5;
+            }
             continue;
         }
         go(k_post1<T>, blocks_for(L.n), kThreads, 0, L);
