@@ -17,6 +17,9 @@
 // Reductions run on a fixed grid (kReduceBlocks) and fold their partials in a
 // fixed order, so every result is bitwise repeatable.
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -432,6 +435,23 @@ DeviceSolver::~DeviceSolver() {
 
 template <> DevLevelT<double>& DeviceSolver::lv<double>(int l) { return levels_[size_t(l)].d; }
 template <> DevLevelT<float>& DeviceSolver::lv<float>(int l) { return levels_[size_t(l)].f; }
+
+int resident_ctas(const void* fn, int block, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::tuple<const void*, int, size_t, int>, int> cache;
+    int dev = 0;
+    TPA_CUDA(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(fn, block, smem, dev);
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int occ = 0, sms = 0;
+    TPA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, smem));
+    TPA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int r = std::max(1, occ) * std::max(1, sms);
+    cache.emplace(key, r);
+    return r;
+}
 
 // Red-black colouring of a level (the reference smooths with damped Jacobi and
 // has no colouring): colour (I + J) mod 2 of every cell, (I, J) its lattice

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -111,6 +112,19 @@ struct SolveStats {
     double ms_total = 0;
     int restarts = 0;
 };
+
+// CTAs of `fn` (block threads, smem bytes) resident at once on the current
+// device: its occupancy times the SM count (cached per kernel and device).
+int resident_ctas(const void* fn, int block, size_t smem);
+
+// Grid of a grid-stride launch whose CTAs fold partial sums: every CTA resident
+// in one wave (a second wave of a few CTAs would run its whole grid-stride
+// share after the first), at most `cap` partials and at most `want` CTAs.
+template <typename K>
+int fold_grid(K kernel, int block, int64_t want, int cap, size_t smem = 0) {
+    const int64_t res = resident_ctas(reinterpret_cast<const void*>(kernel), block, smem);
+    return int(std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(cap, res))));
+}
 
 // red-black smoother set-up (device.cu)
 std::vector<unsigned char> red_black_colours(const Mesh& m);

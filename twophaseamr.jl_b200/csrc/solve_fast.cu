@@ -141,7 +141,7 @@ void DeviceSolver::solve_fast(const double* rhs, double* x_user, double rtol, do
     DevLevel& L = levels_[0];
     const int n = L.n;
     const LevelView<double>& A = vd_[0];
-    const int grid = int(std::min<int64_t>((int64_t(n) + kThreads - 1) / kThreads, kGrid));
+    const int64_t want = (int64_t(n) + kThreads - 1) / kThreads;
     double* out = spres_.p;
     const double cvol = L.ncomp == 1 ? L.comp_volume[0] : 0.0;
     double vt = 0;  // total volume of cells with V > 0
@@ -157,7 +157,7 @@ void DeviceSolver::solve_fast(const double* rhs, double* x_user, double rtol, do
     TPA_CUDA(cudaEventRecord(e0, stream_));
     st = SolveStats();
 
-    k_prep<<<grid, kThreads, 0, stream_>>>(n, rhs, x_user, A.vol, b_.p, tmp_.p, spartial_.p, counters_.p + kCPrep,
+    k_prep<<<fold_grid(k_prep, kThreads, want, kGrid), kThreads, 0, stream_>>>(n, rhs, x_user, A.vol, b_.p, tmp_.p, spartial_.p, counters_.p + kCPrep,
                                            out);
     ++launches_;
     read(3);
@@ -175,7 +175,7 @@ void DeviceSolver::solve_fast(const double* rhs, double* x_user, double rtol, do
         double l2, linf, floor;
     };
     auto pres = [&](double b_mean, double x_mean) {
-        k_pres<<<grid, kThreads, 0, stream_>>>(A, b_.p, tmp_.p, xw_.p, r_.p, b_mean, x_mean, spartial_.p,
+        k_pres<<<fold_grid(k_pres, kThreads, want, kGrid), kThreads, 0, stream_>>>(A, b_.p, tmp_.p, xw_.p, r_.p, b_mean, x_mean, spartial_.p,
                                                counters_.p + kCPres, out);
         ++launches_;
         read(4);
@@ -199,7 +199,7 @@ void DeviceSolver::solve_fast(const double* rhs, double* x_user, double rtol, do
             cg_fused(precision, target, max_cycles - total, niter, flags);
             total += niter;
             // gauge of the iterate, then the true residual and its norms
-            k_xmean<<<grid, kThreads, 0, stream_>>>(n, xw_.p, A.vol, tmp_.p, spartial_.p, counters_.p + kCMean,
+            k_xmean<<<fold_grid(k_xmean, kThreads, want, kGrid), kThreads, 0, stream_>>>(n, xw_.p, A.vol, tmp_.p, spartial_.p, counters_.p + kCMean,
                                                     out);
             ++launches_;
             double xm = 0;

@@ -33,7 +33,6 @@ inline int blocks_for(int64_t n) {
 }
 
 constexpr int kMaxGrid = 1184;  // 8 CTAs on each of 148 SMs: bounds the partials every fold reads
-inline int reduce_grid(int64_t n) { return int(std::min<int64_t>(blocks_for(n), kMaxGrid)); }
 #define TPA_GRID_STRIDE(i, n) for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += gridDim.x * blockDim.x)
 
 // Kernel launch on `s`, with programmatic dependent launch when `pdl`: the
@@ -517,7 +516,8 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
             if (l == 0) go(v_pre2<T, double>, groups, 256, 0, S, r, rsum);
             else go(v_pre2<T, T>, groups, 256, 0, S, S.b, lsum_.p + l);
             go(v_residual<T>, groups, 256, 0, S);
-            go(v_restrict<T>, next_sum ? std::min(groups, kMaxGrid) : groups, 256, 0, S, V[size_t(l + 1)].b,
+            go(v_restrict<T>, next_sum ? fold_grid(v_restrict<T>, 256, groups, kMaxGrid) : groups, 256, 0, S,
+               V[size_t(l + 1)].b,
                fpartial_.p, counters_.p + kRestrictSum, next_sum ? lsum_.p + l + 1 : nullptr);
             launches_ += 3;
             continue;
@@ -531,7 +531,8 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
                 if (l == 0) go(s_pre2<T, double, N>, g, th, 0, S, r, rsum);
                 else go(s_pre2<T, T, N>, g, th, 0, S, S.b, lsum_.p + l);
                 go(s_residual<T, N>, g, th, 0, S);
-                go(s_restrict<T, N>, next_sum ? std::min(g, kMaxGrid) : g, th, th * sizeof(T), 
+                go(s_restrict<T, N>, next_sum ? fold_grid(s_restrict<T, N>, th, g, kMaxGrid, th * sizeof(T)) : g,
+                   th, th * sizeof(T),
                     S, V[size_t(l + 1)].b, fpartial_.p, counters_.p + kRestrictSum,
                     next_sum ? lsum_.p + l + 1 : nullptr);
             });
@@ -559,7 +560,10 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
             go(k_pre2<T, T>, blocks_for(L.n), kThreads, 0, L, L.b, lsum_.p + l);
         }
         const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
-        const int rgrid = next_sum ? reduce_grid(4 * int64_t(L.nc)) : blocks_for(4 * int64_t(L.nc));
+        const int64_t quads = blocks_for(4 * int64_t(L.nc));
+        const int rgrid = !next_sum ? int(quads)
+                          : fuse_rr_ ? fold_grid(k_resrest<T>, kThreads, quads, kMaxGrid)
+                                     : fold_grid(k_restrict<T>, kThreads, quads, kMaxGrid);
         if (fuse_rr_) {
             go(k_resrest<T>, rgrid, kThreads, 0, L, V[size_t(l + 1)].b, fpartial_.p, counters_.p + kRestrictSum,
                next_sum ? lsum_.p + l + 1 : nullptr);
@@ -584,7 +588,8 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
             go(v_prolong<T>, groups, 256, 0, S, V[size_t(l + 1)].x);
             go(v_sweep<T, false>, groups, 256, 0, S, S.x, S.y, nullptr, nullptr, nullptr);
             if (want_mean)
-                go(v_sweep<T, true>, std::min(groups, kMaxGrid), 256, 0, S, S.y, S.x, fpartial_.p,
+                go(v_sweep<T, true>, fold_grid(v_sweep<T, true>, 256, groups, kMaxGrid), 256, 0, S, S.y, S.x,
+                   fpartial_.p,
                    counters_.p + kPostMean, mean_out);
             else
                 go(v_sweep<T, false>, groups, 256, 0, S, S.y, S.x, nullptr, nullptr, nullptr);
@@ -599,7 +604,7 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
                 constexpr int N = decltype(nxc)::value;
                 go(s_prolong<T, N>, g, th, 0, S, V[size_t(l + 1)].x);
                 go(s_post1<T, N>, g, th, 0, S);
-                go(s_post2<T, N>, want_mean ? std::min(g, kMaxGrid) : g, th, 0, 
+                go(s_post2<T, N>, want_mean ? fold_grid(s_post2<T, N>, th, g, kMaxGrid) : g, th, 0,
                     S, fpartial_.p, counters_.p + kPostMean, want_mean ? mean_out : nullptr);
             });
             launches_ += 3;
@@ -643,7 +648,8 @@ void DeviceSolver::vcycle_fused(const double* r, double* z, int precision) {
     const int nl = int(levels_.size());
     double* rsum = lsum_.p;  // slot 0: level-0 RHS sum
     double* mean = lsum_.p + nl;
-    go(k_sum_into, reduce_grid(n), kThreads, 0, n, r, fpartial_.p, counters_.p + kRsum, rsum);
+    go(k_sum_into, fold_grid(k_sum_into, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, r, fpartial_.p,
+       counters_.p + kRsum, rsum);
     ++launches_;
     if (precision == 0) enqueue_vcycle<double>(r, rsum, mean);
     else enqueue_vcycle<float>(r, rsum, mean);
@@ -663,25 +669,25 @@ void DeviceSolver::enqueue_cg_body(int precision, cudaGraphConditionalHandle han
     double* mean = lsum_.p + nl;
     const LevelView<double>& A = vd_[0];
     if (sdev_[0].vec)
-        go(v_cg_ap, std::min((sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0, sd_[0], p_.p, ap_.p, fpartial_.p,
+        go(v_cg_ap, fold_grid(v_cg_ap, 256, (sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0, sd_[0], p_.p, ap_.p, fpartial_.p,
            counters_.p + kCgAp, s);
     else if (sdev_[0].on)
         with_nxc(sd_[0], [&](auto nxc) {
             constexpr int N = decltype(nxc)::value;
-            go(s_cg_ap<N>, std::min(sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, sd_[0], p_.p, ap_.p,
+            go(s_cg_ap<N>, fold_grid(s_cg_ap<N>, sd_[0].cpb, sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, sd_[0], p_.p, ap_.p,
                                                                                        fpartial_.p, counters_.p + kCgAp, s);
         });
     else
-        go(k_cg_ap, reduce_grid(n), kThreads, 0, A, p_.p, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
-    go(k_cg_update, reduce_grid(n), kThreads, 0, n, xw_.p, r_.p, p_.p, ap_.p, A.vol, fpartial_.p,
+        go(k_cg_ap, fold_grid(k_cg_ap, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, A, p_.p, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
+    go(k_cg_update, fold_grid(k_cg_update, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, xw_.p, r_.p, p_.p, ap_.p, A.vol, fpartial_.p,
                                                           fpartial2_.p, counters_.p + kCgUpdate, s);
     if (precision == 0) {
         enqueue_vcycle<double>(r_.p, &s->rsum, mean);
-        go(k_cg_z<double>, reduce_grid(n), kThreads, 0, n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+        go(k_cg_z<double>, fold_grid(k_cg_z<double>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
                                                                 counters_.p + kCgZ, s, 0, handle, set_cond);
     } else {
         enqueue_vcycle<float>(r_.p, &s->rsum, mean);
-        go(k_cg_z<float>, reduce_grid(n), kThreads, 0, n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+        go(k_cg_z<float>, fold_grid(k_cg_z<float>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
                                                                counters_.p + kCgZ, s, 0, handle, set_cond);
     }
     go(k_cg_p, blocks_for(n), kThreads, 0, n, p_.p, z_.p, s);
@@ -739,26 +745,26 @@ void DeviceSolver::cg_fused(int precision, double target, int itmax, int& niter,
     cudaGraphExec_t exec = cg_graph(precision);
     go(k_cg_set, 1, 1, 0, s, target, itmax);
     if (sdev_[0].vec)
-        go(v_cg_residual, std::min((sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0, sd_[0], b_.p, xw_.p, r_.p,
+        go(v_cg_residual, fold_grid(v_cg_residual, 256, (sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0, sd_[0], b_.p, xw_.p, r_.p,
            fpartial_.p, counters_.p + kCgRes, s);
     else if (sdev_[0].on)
         with_nxc(sd_[0], [&](auto nxc) {
             constexpr int N = decltype(nxc)::value;
-            go(s_cg_residual<N>, std::min(sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, 
+            go(s_cg_residual<N>, fold_grid(s_cg_residual<N>, sd_[0].cpb, sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, 
                 sd_[0], b_.p, xw_.p, r_.p, fpartial_.p, counters_.p + kCgRes, s);
         });
     else
-        go(k_cg_residual, reduce_grid(n), kThreads, 0, vd_[0], b_.p, xw_.p, r_.p, fpartial_.p,
+        go(k_cg_residual, fold_grid(k_cg_residual, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, vd_[0], b_.p, xw_.p, r_.p, fpartial_.p,
                                                                 counters_.p + kCgRes, s);
     launches_ += 2;
     if (precision == 0) {
         enqueue_vcycle<double>(r_.p, &s->rsum, mean);
-        go(k_cg_z<double>, reduce_grid(n), kThreads, 0, n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+        go(k_cg_z<double>, fold_grid(k_cg_z<double>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
                                                                 counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(),
                                                                 0);
     } else {
         enqueue_vcycle<float>(r_.p, &s->rsum, mean);
-        go(k_cg_z<float>, reduce_grid(n), kThreads, 0, n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
+        go(k_cg_z<float>, fold_grid(k_cg_z<float>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
                                                                counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(),
                                                                0);
     }
@@ -847,17 +853,17 @@ double DeviceSolver::time_fused(int which, int level, int precision, int iters) 
             if (precision != 0 || level != 0) throw Error(1, "the CG operator runs in FP64 on the finest level");
             CgState* s = reinterpret_cast<CgState*>(cgs_.p);
             if (sdev_[0].vec)
-                v_cg_ap<<<std::min((sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0, stream_>>>(sd_[0], p_.p, ap_.p,
+                v_cg_ap<<<fold_grid(v_cg_ap, 256, (sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0, stream_>>>(sd_[0], p_.p, ap_.p,
                                                                                           fpartial_.p,
                                                                                           counters_.p + kCgAp, s);
             else if (sdev_[0].on)
                 with_nxc(sd_[0], [&](auto nxc) {
                     constexpr int N = decltype(nxc)::value;
-                    s_cg_ap<N><<<std::min(sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, stream_>>>(
+                    s_cg_ap<N><<<fold_grid(s_cg_ap<N>, sd_[0].cpb, sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, stream_>>>(
                         sd_[0], p_.p, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
                 });
             else
-                k_cg_ap<<<reduce_grid(vd_[0].n), kThreads, 0, stream_>>>(vd_[0], p_.p, ap_.p, fpartial_.p,
+                k_cg_ap<<<fold_grid(k_cg_ap, kThreads, blocks_for(vd_[0].n), kMaxGrid), kThreads, 0, stream_>>>(vd_[0], p_.p, ap_.p, fpartial_.p,
                                                                          counters_.p + kCgAp, s);
         } else if (sdev_[size_t(level)].on) {
             if (precision == 0) one_s(sd_, double(0));
