@@ -121,6 +121,56 @@ __global__ void k_pres(LevelView<double> A, double* __restrict__ b, const double
     publish_fold<4>(v, 0xEu, partial, counter, out);
 }
 
+// k_pres on a constant-coefficient 16x16 finest level (vectorized quads,
+// stencil4.cuh): the row is c0 (count x_c - sum of neighbours), so
+// |A| |x| = |c0| (count |x_c| + sum |neighbours|).
+__global__ void __launch_bounds__(256) v_pres(SView<double> S, double* __restrict__ b, const double* __restrict__ x0,
+                                              double* __restrict__ x, double* __restrict__ r, double mb, double mx,
+                                              double* partial, unsigned* counter, double* out) {
+    double v[4] = {0, 0, 0, 0};
+    const int groups = (S.nblocks + 3) / 4;
+    const double* vol = S.vol;
+    const double ac0 = fabs(S.c0);
+    for (int grp = blockIdx.x; grp < groups; grp += gridDim.x) {
+        const QPos p = q_pos(grp);
+        const bool valid = p.b < S.nblocks;
+        const QNb<double> g = q_gather<double>(
+            S, p, valid, [&](int c) { return q_ldv(x0 + c); },
+            [&](double xv, int c) { return vol[c] > 0 ? xv - mx : 0.0; });
+        if (!valid) continue;
+        const Quad<double> ax = q_apply(S, g);
+        const Quad<double> vq = q_ld(vol + p.c);
+        Quad<double> bq = q_ldv(b + p.c), rq;
+        for (int m = 0; m < 4; ++m) {
+            const bool hw = m > 0 || g.hw, he = m < 3 || g.he;
+            double nb = 0.0;
+            int cnt = 0;
+            if (hw) nb += fabs(m > 0 ? g.x.v[m - 1] : g.w), ++cnt;
+            if (he) nb += fabs(m < 3 ? g.x.v[m + 1] : g.e), ++cnt;
+            if (g.hs) nb += fabs(g.s.v[m]), ++cnt;
+            if (g.hn) nb += fabs(g.n.v[m]), ++cnt;
+            const double aacc = ac0 * (double(cnt) * fabs(g.x.v[m]) + nb);
+            const double V = vq.v[m];
+            double bi = bq.v[m];
+            if (mb != 0.0 && V > 0) bi -= V * mb;
+            bq.v[m] = bi;
+            const double ri = bi - ax.v[m];
+            rq.v[m] = ri;
+            if (V > 0) {
+                v[0] += ri * ri / V;
+                const double q = fabs(ri) / V;
+                v[1] = (q != q || v[1] != v[1]) ? NAN : fmax(v[1], q);
+                v[2] = fmax(v[2], aacc / V);
+                v[3] = fmax(v[3], fabs(bi) / V);
+            }
+        }
+        if (mb != 0.0) q_st(b + p.c, bq);
+        q_st(x + p.c, g.x);
+        q_st(r + p.c, rq);
+    }
+    publish_fold<4>(v, 0xEu, partial, counter, out);
+}
+
 // out = sum V x; x0 = x (the next k_pres reads x0 and writes x)
 __global__ void k_xmean(int n, const double* __restrict__ x, const double* __restrict__ vol,
                         double* __restrict__ x0, double* partial, unsigned* counter, double* out) {
@@ -175,8 +225,14 @@ void DeviceSolver::solve_fast(const double* rhs, double* x_user, double rtol, do
         double l2, linf, floor;
     };
     auto pres = [&](double b_mean, double x_mean) {
-        k_pres<<<fold_grid(k_pres, kThreads, want, kGrid), kThreads, 0, stream_>>>(A, b_.p, tmp_.p, xw_.p, r_.p, b_mean, x_mean, spartial_.p,
-                                               counters_.p + kCPres, out);
+        if (sdev_[0].vec) {
+            const int groups = (sd_[0].nblocks + 3) / 4;
+            v_pres<<<fold_grid(v_pres, 256, groups, kGrid), 256, 0, stream_>>>(
+                sd_[0], b_.p, tmp_.p, xw_.p, r_.p, b_mean, x_mean, spartial_.p, counters_.p + kCPres, out);
+        } else {
+            k_pres<<<fold_grid(k_pres, kThreads, want, kGrid), kThreads, 0, stream_>>>(
+                A, b_.p, tmp_.p, xw_.p, r_.p, b_mean, x_mean, spartial_.p, counters_.p + kCPres, out);
+        }
         ++launches_;
         read(4);
         Norms nm;
