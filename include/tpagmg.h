@@ -67,6 +67,7 @@ typedef struct {
     double device_ms;       /* CUDA-event time of the solve on the solver stream   */
     int32_t kernel_launches; /* kernels this call launched                         */
     int32_t precision;
+    double removed_rhs_max_component_mean; /* max over components of |removed strong mean| */
 } tpa_stats;
 
 /* Create a context for CUDA device `device`.  No CUDA call is made until the

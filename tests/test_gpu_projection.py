@@ -217,3 +217,35 @@ def test_argument_errors():
         assert e.value.code == 1
     with pytest.raises(TpaError):
         P.face_coefficients(raw, s, (0.0, 1.0))
+
+
+def test_projection_on_a_split_domain():
+    """Zero coefficients on every face crossing x = 0.5 split a walled box into
+    two components: the increment solve projects each component's RHS mean,
+    the pressure is re-gauged per component (`_accumulate_pressure_increment!`)
+    and `compatible` looks at the largest removed component mean."""
+    spec = dict(base_mesh=(32, 32), block_size=(8, 8), periodic=(False, False))
+    m = BlockTreeMesh(**spec)
+    om = block_tree_mesh(**spec)
+    cx, _ = m.face_centers()
+    cut = (m.face_axis == 1) & (np.abs(cx - 0.5) < 1e-12)
+    kappa = np.where(cut, 0.0, 1.0 + 0.5 * np.sin(np.arange(m.nfaces)))
+    s = EllipticSolver(PoissonOperator(m, kappa))
+    assert s.level_info(0)[2] == 2
+    oop = OOp(om, kappa)
+    rng = np.random.default_rng(12)
+    u0, ub0, p0 = rng.standard_normal(m.nfaces), rng.standard_normal(m.nboundary_faces), rng.standard_normal(m.ncells)
+    for prepared, tol in ((False, 1e-10), (True, 1e-10), (True, 1e-3)):
+        u = P.FaceVelocity(m, u0, ub0)
+        p = p0.copy()
+        st = P.project(u, p, s, 0.05, tolerance=tol, prepared=prepared)
+        ou, oub, opr, phi, ost = OP.project(oop, TreeGeometricMultigrid(oop, OMG()), u0, ub0, p0, 0.05,
+                                            tolerance=tol, prepared=prepared)
+        assert st.converged and ost.converged
+        assert st.compatible == ost.compatible
+        assert np.max(np.abs(u.interior - ou)) <= 1e-9 * np.max(np.abs(ou))
+        assert np.max(np.abs(p - opr)) <= 1e-9 * np.max(np.abs(opr))
+        # each component's pressure has volume mean zero
+        vol = m.cell_volumes()
+        for side in (m.cell_centers()[0] < 0.5, m.cell_centers()[0] > 0.5):
+            assert abs(np.sum(vol[side] * p[side])) <= 1e-12 * np.sum(vol[side] * np.abs(p[side]))

@@ -797,6 +797,7 @@ void BatchSolver::solve(const double* rhs, double* x_user, double rtol, double a
             }
             coef[size_t(k)] = s[size_t(k)] / comp_vol_[size_t(k)];
             stats[size_t(k)].removed_rhs_mean = coef[size_t(k)];
+            stats[size_t(k)].removed_max_component_mean = std::fabs(coef[size_t(k)]);
         }
         write(d_coef, coef);
         go(bk_sub, nfi_, kItemRows, 0, fitems_.p, b_.p, fvol_.p, d_coef);

@@ -843,6 +843,8 @@ void DeviceSolver::solve(const double* rhs, double* x_user, double rtol, double 
                 throw Error(1, "Poisson right-hand side has nonzero volume mean");
             total += ssum;
             tvol += L.comp_volume[size_t(s)];
+            const double cm = std::fabs(ssum / L.comp_volume[size_t(s)]);
+            if (!std::isfinite(cm) || cm > st.removed_max_component_mean) st.removed_max_component_mean = cm;
             k_sub_scaled<double><<<g, kThreads, 0, stream_>>>(n, b_.p, vol, slot, s, sums_.p + s,
                                                               L.comp_volume[size_t(s)]);
             ++launches_;

@@ -109,6 +109,7 @@ struct SolveStats {
     int cycles = 0, converged = 0;
     double initial_l2 = 0, initial_linf = 0, final_l2 = 0, final_linf = 0, target_linf = 0;
     double residual_scale = 1, removed_rhs_mean = 0;
+    double removed_max_component_mean = 0;  // largest |removed strong mean| over the components
     double ms_total = 0;
     int restarts = 0;
 };

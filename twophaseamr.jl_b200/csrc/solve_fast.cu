@@ -220,6 +220,7 @@ void DeviceSolver::solve_fast(const double* rhs, double* x_user, double rtol, do
         mb = host_d_[0] / cvol;
         mx = host_d_[2] / cvol;
         st.removed_rhs_mean = mb;
+        st.removed_max_component_mean = std::fabs(mb);
     }
     struct Norms {
         double l2, linf, floor;

@@ -40,7 +40,8 @@ class StatsC(C.Structure):
                 ("restarts", C.c_int32), ("initial_l2", C.c_double), ("initial_linf", C.c_double),
                 ("final_l2", C.c_double), ("final_linf", C.c_double), ("target_linf", C.c_double),
                 ("residual_scale", C.c_double), ("removed_rhs_mean", C.c_double),
-                ("device_ms", C.c_double), ("kernel_launches", C.c_int32), ("precision", C.c_int32)]
+                ("device_ms", C.c_double), ("kernel_launches", C.c_int32), ("precision", C.c_int32),
+                ("removed_rhs_max_component_mean", C.c_double)]
 
 
 class TuneC(C.Structure):
