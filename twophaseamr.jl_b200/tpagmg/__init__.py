@@ -10,6 +10,8 @@ meaning and error behaviour as in ronaldremmerswaal/TwoPhaseAMR.jl):
   EllipticSolver       src/solvers/multigrid/elliptic_solver.jl:211-302
   solve (solve!)       src/solvers/multigrid/elliptic_solver.jl:614-675
   LinearSolverStats    src/solvers/multigrid/stats.jl:100-135
+  project (project!)   src/navier_stokes/projection.jl:183-260, with divergence!,
+                       weighted_gradient!, surface_tension! and FaceVelocity
 
 Every solve runs on the GPU through `libtpagmg.so`; there is no CPU path.
 """
@@ -18,7 +20,9 @@ from .options import LinearSolverOptions, MultigridOptions
 from .operator import PoissonOperator, mixture_density, surface_tension_jumps
 from .solver import EllipticSolver, LinearSolverStats, solve, solve_batched
 from .batch import BatchedSolver
+from .projection import FaceVelocity, project, divergence, weighted_gradient, surface_tension
 
 __all__ = ["BlockTreeMesh", "PoissonOperator", "MultigridOptions", "LinearSolverOptions", "EllipticSolver",
            "LinearSolverStats", "solve", "solve_batched", "BatchedSolver", "mixture_density",
-           "surface_tension_jumps"]
+           "surface_tension_jumps", "FaceVelocity", "project", "divergence", "weighted_gradient",
+           "surface_tension"]
