@@ -212,7 +212,8 @@ tpa_status tpa_batch_solve_device(tpa_batch* batch, const double* rhs, double* x
  * stencil kernels on constant-coefficient levels without coarse-fine rows,
  * 2 stencil kernels wherever the transfer has a block map; vectorized: 4-cell
  * kernels on constant-coefficient 16x16 levels; pdl: programmatic dependent
- * launch between cycle kernels; fuse_restrict: on CSR levels, the residual is
+ * launch between cycle kernels; fuse_restrict: on CSR levels (every one for 1,
+ * those of at most fuse_restrict cells above 1), the residual is
  * recomputed inside the restriction (one launch instead of two); persistent:
  * when every multi-CTA level is a CSR level, the whole V-cycle runs as one
  * cooperative launch with grid barriers (bounded waits; a barrier that gives up

@@ -24,7 +24,7 @@ def droplet():
 
 
 @pytest.mark.parametrize("layout", [dict(tail_cells=512), dict(tail_cells=8192, tail_ctas=4),
-                                    dict(structured=0), dict(structured=2), dict(pdl=0), dict(fuse_restrict=1),
+                                    dict(structured=0), dict(structured=2), dict(pdl=0), dict(fuse_restrict=1), dict(fuse_restrict=16384),
                                     dict(persistent=1), dict(persistent=1, tail_cells=4096),
                                     dict(tail_cells=1024, tail_ctas=8, structured=2, pdl=0)])
 def test_every_layout_gives_the_same_vcycle(layout):

@@ -1052,11 +1052,16 @@ tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tp
         np.pdl = 0;
         tpa::TuneConfig fr = b0, pe = b0;
         fr.fuse_restrict = 1;
+        tpa::TuneConfig fr_small = b0, fr_mid = b0;  // fused on the small levels only
+        fr_small.fuse_restrict = 16384;
+        fr_mid.fuse_restrict = 65536;
         pe.persistent = 1;
         pe.tail_ctas = 1;
         run(nv);
         run(np);
         run(fr);
+        run(fr_small);
+        run(fr_mid);
         run(pe);
         const size_t b = best_of();
         d.reconfigure(ctx->hier, res[b].first);

@@ -101,7 +101,8 @@ struct CgScalars {
 // map allows it.
 struct TuneConfig {
     int tail_cells = -1, tail_ctas = -1, structured = -1, vectorized = -1, pdl = -1;
-    int fuse_restrict = -1;  // CSR levels: residual recomputed inside the restriction
+    int fuse_restrict = -1;  // CSR levels: residual recomputed inside the restriction (0 off,
+                             // 1 every level, above 1 levels of at most that many cells)
     int persistent = -1;     // all-CSR hierarchies: the V-cycle as one cooperative launch
 };
 
@@ -229,7 +230,7 @@ private:
 
     bool fused_ok_ = false;
     bool pdl_ = true;  // programmatic dependent launch between cycle kernels
-    bool fuse_rr_ = false;  // residual + restriction in one launch on CSR levels
+    int rr_cells_ = 0;  // CSR levels of at most this many cells: residual + restriction in one launch
     int coop_grid_ = 0;     // > 0: the V-cycle runs as one cooperative launch of this many CTAs
     DevArray<unsigned> bar_;  // grid barrier: arrivals, generation
     DevArray<int> err_;       // set when a grid barrier gave up waiting

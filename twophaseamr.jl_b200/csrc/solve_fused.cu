@@ -374,8 +374,9 @@ TuneConfig DeviceSolver::effective_tuning() const {
     if (tune_.structured >= 0) c.structured = std::min(2, tune_.structured);
     c.vectorized = std::getenv("TPAGMG_NO_VEC") ? 0 : 1;
     if (tune_.vectorized >= 0) c.vectorized = tune_.vectorized ? 1 : 0;
-    c.fuse_restrict = std::getenv("TPAGMG_FUSE_RESTRICT") ? 1 : 0;
-    if (tune_.fuse_restrict >= 0) c.fuse_restrict = tune_.fuse_restrict ? 1 : 0;
+    c.fuse_restrict = 0;
+    if (const char* e = std::getenv("TPAGMG_FUSE_RESTRICT")) c.fuse_restrict = std::max(1, std::atoi(e));
+    if (tune_.fuse_restrict >= 0) c.fuse_restrict = tune_.fuse_restrict;
     c.persistent = std::getenv("TPAGMG_PERSISTENT") ? 1 : 0;
     if (tune_.persistent >= 0) c.persistent = tune_.persistent ? 1 : 0;
     if (rb_) {  // the red-black sweeps exist for the CSR levels and the tail only
@@ -401,7 +402,8 @@ void DeviceSolver::build_views() {
     const TuneConfig cfg = effective_tuning();
     if (const char* e = std::getenv("TPAGMG_RB_PAIR_CELLS")) rb_pair_cells_ = std::atoi(e);
     pdl_ = cfg.pdl != 0;
-    fuse_rr_ = cfg.fuse_restrict != 0;
+    // 1: every CSR level; above 1: levels of at most that many cells
+    rr_cells_ = cfg.fuse_restrict == 1 ? INT32_MAX : cfg.fuse_restrict;
     fused_ok_ = (pre_ == 2 && post_ == 2);
     for (auto& L : levels_)
         if (L.ncomp > 1) fused_ok_ = false;
@@ -562,9 +564,9 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
         const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
         const int64_t quads = blocks_for(4 * int64_t(L.nc));
         const int rgrid = !next_sum ? int(quads)
-                          : fuse_rr_ ? fold_grid(k_resrest<T>, kThreads, quads, kMaxGrid)
+                          : L.n <= rr_cells_ ? fold_grid(k_resrest<T>, kThreads, quads, kMaxGrid)
                                      : fold_grid(k_restrict<T>, kThreads, quads, kMaxGrid);
-        if (fuse_rr_) {
+        if (L.n <= rr_cells_) {
             go(k_resrest<T>, rgrid, kThreads, 0, L, V[size_t(l + 1)].b, fpartial_.p, counters_.p + kRestrictSum,
                next_sum ? lsum_.p + l + 1 : nullptr);
             launches_ += 2;
