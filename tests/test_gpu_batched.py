@@ -140,3 +140,24 @@ def test_merged_batch_compatibility_error_marks_one_problem():
     parts = bs.split(x)
     assert np.any(parts[0] != 0) and np.any(parts[2] != 0)
     assert not np.any(parts[1] != 0)
+
+
+def test_merged_batch_after_device_refresh():
+    """A context refreshed on the device leaves its host levels stale; the
+    merged batch built from it recomputes them first and solves the refreshed
+    problem."""
+    from tpagmg import BatchedSolver
+    probs = make(small(3), precision="fp64")
+    p, m, kappa, rhs, s = probs[0]
+    s.set_tuning(structured=0)
+    k2 = kappa * np.exp(0.3 * np.sin(np.arange(m.nfaces)))
+    s.refresh(k2)
+    assert s.last_refresh()[0] == "device"
+    bs = BatchedSolver([q[-1] for q in probs])
+    x = np.zeros(bs.ncells)
+    st = bs.solve(x, bs.concat([q[3] for q in probs]), rtol=1e-12, precision="fp64")
+    assert all(t["converged"] for t in st)
+    oo = OOp(block_tree_mesh(**W.batch_spec(p)), k2)
+    ref, _ = osolve(oo, TreeGeometricMultigrid(oo, OMG()), rhs, rtol=1e-12)
+    x0 = bs.split(x)[0]
+    assert np.max(np.abs(x0 - ref)) <= 1e-10 * np.max(np.abs(ref))

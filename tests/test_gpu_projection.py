@@ -249,3 +249,29 @@ def test_projection_on_a_split_domain():
         vol = m.cell_volumes()
         for side in (m.cell_centers()[0] < 0.5, m.cell_centers()[0] > 0.5):
             assert abs(np.sum(vol[side] * p[side])) <= 1e-12 * np.sum(vol[side] * np.abs(p[side]))
+
+
+def test_projection_after_device_refresh_uses_the_new_coefficients():
+    """The face kernels' sqrt(kappa) follows a device refresh (copied on the
+    device, the faces stay uploaded)."""
+    spec, m, om, raw = setup("two_level")
+    rng = np.random.default_rng(21)
+    k0 = np.exp(rng.uniform(-1, 1, m.nfaces))
+    k1 = np.exp(rng.uniform(-1, 1, m.nfaces))
+    s = EllipticSolver(PoissonOperator(m, k0))
+    s.set_tuning(structured=0)
+    p = rng.standard_normal(m.ncells)
+    P.weighted_gradient(p, s)  # faces uploaded with k0
+    P.refresh_device(s, torch.from_numpy(k1).cuda())
+    assert s.last_refresh()[0] == "device"
+    g = P.weighted_gradient(p, s)
+    og, _ = OP.weighted_gradient(OOp(om, k1), p)
+    assert np.max(np.abs(g.interior - og)) <= 1e-14 * np.max(np.abs(og))
+    u0 = rng.standard_normal(m.nfaces)
+    u = P.FaceVelocity(m, u0)
+    pr = np.zeros(m.ncells)
+    P.project(u, pr, s, 0.05, tolerance=1e-10)
+    oop = OOp(om, k1)
+    ou, _, opr, _, _ = OP.project(oop, TreeGeometricMultigrid(oop, OMG()), u0, None, np.zeros(m.ncells), 0.05,
+                                  tolerance=1e-10)
+    assert np.max(np.abs(u.interior - ou)) <= 1e-9 * np.max(np.abs(ou))
