@@ -307,7 +307,7 @@ private:
     int coarse_N_ = 0, coarse_ncomp_ = 0;
     bool lu_cluster_ = false;  // coarse LU on a cluster with the rows in shared memory
     double* rstage_ = nullptr; // pinned staging of the finest-level coefficients
-    DevArray<double> coarse_M_, rwtw_, rpart_;
+    DevArray<double> coarse_M_, coarse_MT_, rwtw_, rpart_;
     DevArray<int> coarse_piv_, rerr_;
     DevArray<unsigned> rcnt_;
 

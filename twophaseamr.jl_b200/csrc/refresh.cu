@@ -19,7 +19,6 @@
 #include <cstring>
 
 #include <cooperative_groups.h>
-#include <cuda_pipeline.h>
 
 #include "device.cuh"
 #include "structure.hpp"
@@ -365,95 +364,112 @@ size_t lu_smem(int N, int C, bool cluster) {
     return ((cluster ? R * size_t(N) : 0) + 2 * size_t(C) * N + 2 * size_t(N)) * sizeof(double);
 }
 
-constexpr int kInvWarps = 8;  // columns of the inverse per CTA
-constexpr int kInvStages = 4; // factor rows in flight
+constexpr int kInvWarps = 4;  // columns of the inverse per CTA
 
-// The first n columns of M^-1 from the factors, one warp per column: e = P
-// e_col (a unit vector: only its position moves), forward substitution with
-// the unit lower factor (rows above the 1 stay zero), back substitution with
-// the upper factor; G[r][col] = e[r] for r < n.  The CTA streams the factor
-// rows through a ring of shared-memory stages (asynchronous copies kInvStages
-// - 1 rows ahead), every warp taking its dot product from the staged row; dot
-// products run across the lanes with a fixed shuffle tree (deterministic).
-__global__ void __launch_bounds__(32 * kInvWarps) kr_coarse_inv(int N, int n, const double* __restrict__ M,
+// MT = M' (the factors by columns), 32 x 32 tiles through shared memory
+__global__ void kr_transpose(int N, const double* __restrict__ M, double* __restrict__ MT, const int* err) {
+    __shared__ double tile[32][33];
+    if (*err) return;
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int r = by + j, c = bx + int(threadIdx.x);
+        if (r < N && c < N) tile[j][threadIdx.x] = M[size_t(r) * N + c];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int r = bx + j, c = by + int(threadIdx.x);
+        if (r < N && c < N) MT[size_t(r) * N + c] = tile[threadIdx.x][j];
+    }
+}
+
+// The first n columns of M^-1 from the factors, one warp per column, in
+// blocks of 32 rows: lane t owns row 32 B + t.  A block first subtracts the
+// solved blocks' contribution (lane t reads MT[k][32 B + t]: consecutive
+// addresses across the warp), then resolves its own 32 rows in order with the
+// solved value broadcast by a shuffle.  Forward with the unit lower factor
+// from the permuted unit vector (blocks above its 1 stay zero), back with the
+// upper factor; G[r][col] = e[r] for r < n.  The order of each row's sum is
+// fixed (deterministic).
+__global__ void __launch_bounds__(32 * kInvWarps) kr_coarse_inv(int N, int n, const double* __restrict__ MT,
                                                                const int* __restrict__ piv,
                                                                double* __restrict__ G,
                                                                const int* __restrict__ err) {
     extern __shared__ double inv_sm[];
-    __shared__ int first;
     if (*err) return;  // uniform over the grid
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int col = int(blockIdx.x) * kInvWarps + wid;
+    if (col >= n) return;  // whole warps; no block-wide barrier follows
     double* e = inv_sm + size_t(wid) * N;
-    double* ring = inv_sm + size_t(kInvWarps) * N;
-    if (threadIdx.x == 0) first = N;
-    __syncthreads();
-    int pos = N;  // warps past the last column idle through the barriers
-    if (col < n) {
-        pos = col;
-        for (int k = 0; k < N; ++k) {
-            const int p = piv[k];
-            if (pos == k) pos = p;
-            else if (pos == p) pos = k;
-        }
-        for (int r = lane; r < N; r += 32) e[r] = r == pos ? 1.0 : 0.0;
-        if (lane == 0) atomicMin(&first, pos);
+    int pos = col;
+    for (int k = 0; k < N; ++k) {
+        const int p = piv[k];
+        if (pos == k) pos = p;
+        else if (pos == p) pos = k;
     }
-    __syncthreads();
-    const int r0 = first + 1;  // rows above stay zero in every column of this CTA
-    // forward: row r of the lower factor, columns [first, r)
-    auto load_fwd = [&](int r) {
-        if (r < N) {
-            double* dst = ring + size_t(r % kInvStages) * N;
-            const double* srow = M + size_t(r) * N;
-            for (int c = first + int(threadIdx.x); c < r; c += blockDim.x) __pipeline_memcpy_async(dst + c, srow + c, 8);
+    const int nb = (N + 31) / 32;
+    // sum over k in [k0, k1) of MT[k][r] e[k]: four interleaved partial sums,
+    // combined in a fixed order (the loads of a row run ahead of its FMAs)
+    auto dot = [&](int r, int k0, int k1) {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int k = k0;
+        for (; k + 4 <= k1; k += 4) {
+            s0 += MT[size_t(k) * N + r] * e[k];
+            s1 += MT[size_t(k + 1) * N + r] * e[k + 1];
+            s2 += MT[size_t(k + 2) * N + r] * e[k + 2];
+            s3 += MT[size_t(k + 3) * N + r] * e[k + 3];
         }
-        __pipeline_commit();
+        for (; k < k1; ++k) s0 += MT[size_t(k) * N + r] * e[k];
+        return (s0 + s1) + (s2 + s3);
     };
-    for (int j = 0; j < kInvStages - 1; ++j) load_fwd(r0 + j);
-    for (int r = r0; r < N; ++r) {
-        __pipeline_wait_prior(kInvStages - 2);
-        __syncthreads();  // row r is staged; the stage refilled next was read by everyone
-        load_fwd(r + kInvStages - 1);
-        if (r > pos) {
-            const double* mr = ring + size_t(r % kInvStages) * N;
-            double s = 0.0;
-            for (int k = pos + lane; k < r; k += 32) s += mr[k] * e[k];
-            for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) e[r] -= s;
-            __syncwarp();
+    // the block's 32 x 32 tile of the factor in registers: lane t holds
+    // M[32 B + t][32 B + kk] in t[kk] (0 beyond N)
+    double tile[32];
+    auto load_tile = [&](int B, int r, bool ok) {
+#pragma unroll
+        for (int kk = 0; kk < 32; ++kk) {
+            const int k = 32 * B + kk;
+            tile[kk] = (ok && k < N) ? MT[size_t(k) * N + r] : 0.0;
         }
-    }
-    __pipeline_wait_prior(0);
-    __syncthreads();
-    // backward: row r of the upper factor, columns [r, N)
-    auto load_bwd = [&](int r) {
-        if (r >= 0) {
-            double* dst = ring + size_t(r % kInvStages) * N;
-            const double* srow = M + size_t(r) * N;
-            for (int c = r + int(threadIdx.x); c < N; c += blockDim.x) __pipeline_memcpy_async(dst + c, srow + c, 8);
-        }
-        __pipeline_commit();
     };
-    for (int j = 0; j < kInvStages - 1; ++j) load_bwd(N - 1 - j);
-    for (int r = N - 1; r >= 0; --r) {
-        __pipeline_wait_prior(kInvStages - 2);
-        __syncthreads();
-        load_bwd(r - (kInvStages - 1));
-        if (col < n) {
-            const double* mr = ring + size_t(r % kInvStages) * N;
-            double s = 0.0;
-            for (int k = r + 1 + lane; k < N; k += 32) s += mr[k] * e[k];
-            for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) e[r] = (e[r] - s) / mr[r];
-            __syncwarp();
+    // forward: L y = P e_col
+    for (int k = lane; k < N; k += 32) e[k] = 0.0;
+    __syncwarp();
+    for (int B = pos / 32; B < nb; ++B) {
+        const int r = 32 * B + lane;
+        const bool ok = r < N;
+        load_tile(B, r, ok);
+        double v = (r == pos) ? 1.0 : 0.0;
+        if (ok) v -= dot(r, (pos / 32) * 32, 32 * B);
+#pragma unroll
+        for (int kk = 0; kk < 32; ++kk) {
+            const double ek = __shfl_sync(0xffffffffu, v, kk);
+            if (lane > kk) v -= tile[kk] * ek;
         }
+        if (ok) e[r] = v;
+        __syncwarp();
     }
-    if (col < n)
-        for (int r = lane; r < n; r += 32) G[size_t(r) * n + col] = e[r];
+    // backward: U x = y (lane kk's tile[kk] is the diagonal U[k][k])
+    for (int B = nb - 1; B >= 0; --B) {
+        const int r = 32 * B + lane;
+        const bool ok = r < N;
+        load_tile(B, r, ok);
+        double v = ok ? e[r] : 0.0;
+        if (ok) v -= dot(r, 32 * (B + 1), N);
+#pragma unroll
+        for (int kk = 31; kk >= 0; --kk) {
+            if (32 * B + kk < N) {  // uniform over the warp
+                if (lane == kk) v = v / tile[kk];
+                const double ek = __shfl_sync(0xffffffffu, v, kk);
+                if (lane < kk) v -= tile[kk] * ek;
+            }
+        }
+        if (ok) e[r] = v;
+        __syncwarp();
+    }
+    for (int r = lane; r < n; r += 32) G[size_t(r) * n + col] = e[r];
 }
 
-size_t inv_smem(int N) { return size_t(kInvWarps + kInvStages) * size_t(N) * sizeof(double); }
+size_t inv_smem(int N) { return size_t(kInvWarps) * size_t(N) * sizeof(double); }
 
 constexpr int kLuCluster = 8;  // CTAs sharing the rows of the coarsest matrix
 constexpr int kLuClusterThreads = 512;
@@ -584,6 +600,7 @@ void DeviceSolver::prepare_refresh(const Hierarchy& h) {
     coarse_N_ = int(c.op.A.n + ncomp);
     coarse_ncomp_ = int(ncomp);
     coarse_M_.alloc(size_t(coarse_N_) * size_t(coarse_N_));
+    coarse_MT_.alloc(size_t(coarse_N_) * size_t(coarse_N_));
     {
         // the cluster LU when a cluster's shared memory holds the matrix
         const int N = coarse_N_;
@@ -719,8 +736,12 @@ void DeviceSolver::refresh_levels() {
     } else {
         kr_lu<false><<<1, 1024, lu_smem(N, 1, false), s>>>(N, coarse_M_.p, coarse_piv_.p, rerr_.p);
     }
+    {
+        const dim3 tg((N + 31) / 32, (N + 31) / 32), tb(32, 8);
+        kr_transpose<<<tg, tb, 0, s>>>(N, coarse_M_.p, coarse_MT_.p, rerr_.p);
+    }
     kr_coarse_inv<<<(C.n + kInvWarps - 1) / kInvWarps, 32 * kInvWarps, inv_smem(N), s>>>(
-        N, C.n, coarse_M_.p, coarse_piv_.p, coarse_inv_.p, rerr_.p);
+        N, C.n, coarse_MT_.p, coarse_piv_.p, coarse_inv_.p, rerr_.p);
     TPA_CUDA(cudaGetLastError());
     std::vector<double> wtw(size_t(3 * nl));
     int err = 0;
