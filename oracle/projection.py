@@ -156,6 +156,7 @@ class ProjectionStats:
     def __init__(self, stats, dt, tolerance):
         self.solve = stats
         self.residual_scale = 1.0 / dt ** 2
+        stats.residual_scale = self.residual_scale
         # the largest removed component mean (a non-finite one wins)
         m = 0.0
         for v in stats.removed_rhs_component_means:

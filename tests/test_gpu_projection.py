@@ -275,3 +275,31 @@ def test_projection_after_device_refresh_uses_the_new_coefficients():
     ou, _, opr, _, _ = OP.project(oop, TreeGeometricMultigrid(oop, OMG()), u0, None, np.zeros(m.ncells), 0.05,
                                   tolerance=1e-10)
     assert np.max(np.abs(u.interior - ou)) <= 1e-9 * np.max(np.abs(ou))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("coefficient", ["one", "harmonic"])
+def test_pressure_projection_known_answer(coefficient, precision):
+    """test/operators/poisson.jl:1704-1747 ("pressure projection") through
+    `tpa_project`: a sinusoidal velocity on the two-level tree of 8x8 blocks,
+    kappa = 1 or the harmonic face mean of (x < 1/2 ? 1 : 100), dt 0.1,
+    tolerance 1e-11, coarse_size 8."""
+    from test_oracle_projection import check_projection_known_answer, harmonic_face_coefficients
+    spec = spec_of("two_level")
+    m = BlockTreeMesh(**spec)
+    om = block_tree_mesh(**spec)
+    x, y = m.face_centers()
+    u0 = np.where(m.face_axis == 1, np.sin(2 * np.pi * x) * np.cos(2 * np.pi * y),
+                  np.cos(2 * np.pi * x) * np.sin(2 * np.pi * y))
+    if coefficient == "one":
+        kappa = np.ones(m.nfaces)
+    else:
+        cx, _ = om.cell_centers()
+        kappa = harmonic_face_coefficients(om, np.where(cx < 0.5, 1.0, 100.0))
+    s = EllipticSolver(PoissonOperator(m, kappa), multigrid=MultigridOptions(coarse_size=8),
+                       preconditioner_options={"precision": precision})
+    u = P.FaceVelocity(m, u0)
+    p = np.zeros(m.ncells)
+    st = P.project(u, p, s, 0.1, tolerance=1e-11)
+    check_projection_known_answer(st, P.divergence(P.FaceVelocity(m, u0), s), P.divergence(u, s), p,
+                                  m.cell_volumes())

@@ -1,15 +1,21 @@
 """The oracle's projection step against the reference's own known answers
-(test/two_phase/forces.jl:110-158 of ronaldremmerswaal/TwoPhaseAMR.jl):
+(ronaldremmerswaal/TwoPhaseAMR.jl):
 
+test/two_phase/forces.jl:110-158
 * the CSF / CGFM jump is sigma * kappa * jump * |f| bit for bit;
 * the weighted jump force equals the weighted gradient of the potential
   sigma * kappa * [c > 1/2] (CGFM) or sigma * kappa * c (CSF) to 5e-13;
 * a balanced force projects to a velocity below 1e-9 (dt 0.01, tolerance
   1e-11) at density ratios 1 and 1000 on a uniform, a two-level and a
-  band-refined tree.
+  band-refined tree.  The reference's third mesh is adapted by `adapt!`; here
+  the blocks cut by the circle are refined to the same depth instead.
 
-The reference's third mesh is adapted by `adapt!`; here the blocks cut by the
-circle are refined to the same depth instead.
+test/operators/poisson.jl:1704-1747 ("pressure projection")
+* a sinusoidal velocity on the two-level tree, kappa = 1 or the harmonic face
+  mean of a 1 / 100 cell field: converged, initial >= final residual,
+  residual_scale 100, final residual / scale <= 1e-11, dt times the final
+  divergence equal to the scaled final residual to 8 eps, the divergence
+  reduced below 2e-11 of its initial value, the pressure integral <= 2e-12.
 """
 import numpy as np
 import pytest
@@ -98,3 +104,47 @@ def test_conditional_fraction_floor_and_bounds():
     for bad in (-1e-6, 1.0 + 1e-6, np.nan):
         with pytest.raises(ValueError):
             P.conditional_fraction(np.array([0.5, bad]))
+
+
+def harmonic_face_coefficients(mesh, cell_value):
+    """`harmonic_face_coefficients` (src/operators/elliptic.jl:9-23): the
+    distance-weighted harmonic mean of the two cell values."""
+    nx, ny = mesh.block_size
+    a = mesh.face_axis.astype(np.int64) - 1
+    dm = mesh.spacing[mesh.face_minus // (nx * ny), a] / 2
+    dp = mesh.spacing[mesh.face_plus // (nx * ny), a] / 2
+    cm, cp = cell_value[mesh.face_minus], cell_value[mesh.face_plus]
+    return (dm + dp) / (dm / cm + dp / cp)
+
+
+def check_projection_known_answer(stats, u_div0, u_div, pressure, volumes):
+    """The assertions of test/operators/poisson.jl:1738-1745."""
+    initial = np.max(np.abs(u_div0))
+    final = np.max(np.abs(u_div))
+    assert stats.converged
+    assert stats.initial_linf >= stats.final_linf
+    assert abs(stats.residual_scale - 100) <= 1e-12 * 100
+    assert stats.final_linf / stats.residual_scale <= 1e-11
+    assert abs(0.1 * final - stats.final_linf / stats.residual_scale) <= 8 * np.finfo(float).eps
+    assert final <= 2e-11 * initial
+    assert abs(np.sum(volumes * pressure)) <= 2e-12
+
+
+@pytest.mark.parametrize("coefficient", ["one", "harmonic"])
+def test_pressure_projection_known_answer(coefficient):
+    """Two-level tree of 8x8 blocks, u = (sin 2 pi x cos 2 pi y, cos 2 pi x
+    sin 2 pi y) at the face centres, dt 0.1, tolerance 1e-11, coarse_size 8."""
+    mesh = block_tree_mesh(**mesh_of(2))
+    x, y = mesh.face_center[:, 0], mesh.face_center[:, 1]
+    u0 = np.where(mesh.face_axis == 1, np.sin(2 * np.pi * x) * np.cos(2 * np.pi * y),
+                  np.cos(2 * np.pi * x) * np.sin(2 * np.pi * y))
+    if coefficient == "one":
+        kappa = np.ones(mesh.nfaces)
+    else:
+        cx, _ = mesh.cell_centers()
+        kappa = harmonic_face_coefficients(mesh, np.where(cx < 0.5, 1.0, 100.0))
+    op = PoissonOperator(mesh, kappa)
+    mg = TreeGeometricMultigrid(op, MultigridOptions(coarse_size=8))
+    u, ub, p, phi, st = P.project(op, mg, u0, None, np.zeros(mesh.ncells), 0.1, tolerance=1e-11)
+    check_projection_known_answer(st.solve, P.divergence(mesh, u0, ub), P.divergence(mesh, u, ub), p,
+                                  mesh.cell_volumes())
