@@ -31,6 +31,16 @@ __device__ __forceinline__ double frow(const FineCsr& A, const double* v, int i)
     return acc;
 }
 
+// A x as sum_j a_ij (x_j - x_i) for the true residual: the rows sum to zero, and
+// this form rounds at the level of the face fluxes (x_j - x_i), as the
+// factorized action does, rather than at that of a_ii x_i
+__device__ __forceinline__ double frow_diff(const FineCsr& A, const double* v, int i) {
+    const double vi = v[i];
+    double acc = 0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) acc += A.val[k] * (v[A.ci[k]] - vi);
+    return acc;
+}
+
 // b = V f and x = x0 (zero where V = 0)
 __global__ void bk_prepare(const BFItem* __restrict__ fi, FineCsr A, const double* __restrict__ rhs,
                            const double* __restrict__ x0, double* __restrict__ b, double* __restrict__ x) {
@@ -81,7 +91,7 @@ __global__ void bk_residual64(const BFItem* __restrict__ fi, const int* __restri
     const int i = it.begin + int(threadIdx.x);
     double q = 0, l2 = 0, sum = 0;
     if (i < it.end) {
-        const double ri = b[i] - frow(A, x, i);
+        const double ri = b[i] - frow_diff(A, x, i);
         r[i] = ri;
         const double V = A.vol[i];
         if (V > 0) {

@@ -42,6 +42,19 @@ __device__ __forceinline__ T row_dot(const int* __restrict__ rp, const int* __re
     return acc;
 }
 
+// A x as sum_j a_ij (x_j - x_i).  Every row of the operator sums to zero (the
+// area-weighted jump maps constants to zero and no side is open), so this is
+// A x in exact arithmetic; in floating point its rounding scales with the
+// differences x_j - x_i, as in the factorized face-flux action (elliptic.jl:
+// 1125-1180), rather than with a_ii x_i.  True residuals use it.
+__device__ __forceinline__ double row_diff(const int* __restrict__ rp, const int* __restrict__ ci,
+                                           const double* __restrict__ v, const double* __restrict__ x, int i) {
+    const double xi = x[i];
+    double acc = 0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) acc += v[k] * (x[ci[k]] - xi);
+    return acc;
+}
+
 template <typename T>
 __global__ void k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ v,
                        const T* __restrict__ x, T* __restrict__ y) {
@@ -277,7 +290,7 @@ __global__ void k_scale_rhs(int n, const double* __restrict__ rhs, const double*
 __global__ void k_residual64(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
                              const double* __restrict__ b, const double* __restrict__ x, double* __restrict__ r) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) r[i] = b[i] - row_dot(rp, ci, v, x, i);
+    if (i < n) r[i] = b[i] - row_diff(rp, ci, v, x, i);
 }
 
 __global__ void k_abs_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,

@@ -88,7 +88,13 @@ __global__ void k_prep(int n, const double* __restrict__ rhs, const double* __re
 }
 
 // b -= V mb, x = x0 - mx (0 where V = 0), r = b - A x; out = {sum_V r^2 / V,
-// max |r| / V, max (|A| |x|) / V, max |b| / V} over cells with V > 0
+// max |r| / V, max (|A| |x|) / V, max |b| / V} over cells with V > 0.  A x is
+// summed as sum_j a_ij (x_j - x_i): the rows sum to zero (the area-weighted
+// jump maps constants to zero and no side is open), and this form rounds at
+// the level of the face fluxes, as the factorized action of elliptic.jl:
+// 1125-1180 does, not at the level of a_ii x_i.  The projection step relies on
+// it: dt max |div u| after the update equals the final residual over 1/dt^2 to
+// a few ulps only when both are evaluated from face differences.
 __global__ void k_pres(LevelView<double> A, double* __restrict__ b, const double* __restrict__ x0,
                        double* __restrict__ x, double* __restrict__ r, double mb, double mx, double* partial,
                        unsigned* counter, double* out) {
@@ -100,14 +106,15 @@ __global__ void k_pres(LevelView<double> A, double* __restrict__ b, const double
             bi -= V * mb;
             b[i] = bi;
         }
+        const double xi = V > 0 ? x0[i] - mx : 0.0;
         double acc = 0, aacc = 0;
         for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
             const int j = A.ci[k];
             const double xj = A.vol[j] > 0 ? x0[j] - mx : 0.0;
-            acc += A.val[k] * xj;
+            acc += A.val[k] * (xj - xi);
             aacc += fabs(A.val[k]) * fabs(xj);
         }
-        x[i] = V > 0 ? x0[i] - mx : 0.0;
+        x[i] = xi;
         const double ri = bi - acc;
         r[i] = ri;
         if (V > 0) {
@@ -122,8 +129,8 @@ __global__ void k_pres(LevelView<double> A, double* __restrict__ b, const double
 }
 
 // k_pres on a constant-coefficient 16x16 finest level (vectorized quads,
-// stencil4.cuh): the row is c0 (count x_c - sum of neighbours), so
-// |A| |x| = |c0| (count |x_c| + sum |neighbours|).
+// stencil4.cuh): the row is c0 (count x_c - sum of neighbours), evaluated as
+// c0 sum (x_c - x_nb) like k_pres; |A| |x| = |c0| (count |x_c| + sum |neighbours|).
 __global__ void __launch_bounds__(256) v_pres(SView<double> S, double* __restrict__ b, const double* __restrict__ x0,
                                               double* __restrict__ x, double* __restrict__ r, double mb, double mx,
                                               double* partial, unsigned* counter, double* out) {
@@ -138,23 +145,30 @@ __global__ void __launch_bounds__(256) v_pres(SView<double> S, double* __restric
             S, p, valid, [&](int c) { return q_ldv(x0 + c); },
             [&](double xv, int c) { return vol[c] > 0 ? xv - mx : 0.0; });
         if (!valid) continue;
-        const Quad<double> ax = q_apply(S, g);
         const Quad<double> vq = q_ld(vol + p.c);
         Quad<double> bq = q_ldv(b + p.c), rq;
         for (int m = 0; m < 4; ++m) {
             const bool hw = m > 0 || g.hw, he = m < 3 || g.he;
-            double nb = 0.0;
+            const double xc = g.x.v[m];
+            double nb = 0.0, diff = 0.0;
             int cnt = 0;
-            if (hw) nb += fabs(m > 0 ? g.x.v[m - 1] : g.w), ++cnt;
-            if (he) nb += fabs(m < 3 ? g.x.v[m + 1] : g.e), ++cnt;
-            if (g.hs) nb += fabs(g.s.v[m]), ++cnt;
-            if (g.hn) nb += fabs(g.n.v[m]), ++cnt;
-            const double aacc = ac0 * (double(cnt) * fabs(g.x.v[m]) + nb);
+            if (hw) {
+                const double t = m > 0 ? g.x.v[m - 1] : g.w;
+                nb += fabs(t), diff += xc - t, ++cnt;
+            }
+            if (he) {
+                const double t = m < 3 ? g.x.v[m + 1] : g.e;
+                nb += fabs(t), diff += xc - t, ++cnt;
+            }
+            if (g.hs) nb += fabs(g.s.v[m]), diff += xc - g.s.v[m], ++cnt;
+            if (g.hn) nb += fabs(g.n.v[m]), diff += xc - g.n.v[m], ++cnt;
+            const double aacc = ac0 * (double(cnt) * fabs(xc) + nb);
+            const double axm = S.c0 * diff;
             const double V = vq.v[m];
             double bi = bq.v[m];
             if (mb != 0.0 && V > 0) bi -= V * mb;
             bq.v[m] = bi;
-            const double ri = bi - ax.v[m];
+            const double ri = bi - axm;
             rq.v[m] = ri;
             if (V > 0) {
                 v[0] += ri * ri / V;
