@@ -344,7 +344,7 @@ tpa_status tpa_divergence_device(tpa_context* ctx, const double* u_interior, con
 typedef struct {
     double dt;                          /* > 0 */
     double tolerance;                   /* in (0, 1); the reference's default is sqrt(eps) */
-    double reference_dt;                /* >= dt, or 0 for dt (`_reference_dt`) */
+    double reference_dt;                /* >= dt and finite, or 0 for dt (`_reference_dt`) */
     const double* inherited_divergence; /* NULL, or the `_inherited_divergence` cell array */
     int32_t max_cycles;                 /* default 100 */
     int32_t compatibility;              /* 0 :project, 1 :error */

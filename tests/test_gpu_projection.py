@@ -303,3 +303,63 @@ def test_pressure_projection_known_answer(coefficient, precision):
     st = P.project(u, p, s, 0.1, tolerance=1e-11)
     check_projection_known_answer(st, P.divergence(P.FaceVelocity(m, u0), s), P.divergence(u, s), p,
                                   m.cell_volumes())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_incremental_pressure_projection_known_answer(precision):
+    """test/operators/poisson.jl:1749-1771: u = -dt G_k p projects to |u| <
+    1e-10 and the pressure to |p| < 1e-9 (one periodic 8x8 block, kappa = 1 +
+    cos(2 pi x_f) / 4, tolerance 1e-13)."""
+    from test_oracle_projection import incremental_case
+    m = BlockTreeMesh(block_size=(8, 8))
+    kappa, p0 = incremental_case(block_tree_mesh(block_size=(8, 8)))
+    s = EllipticSolver(PoissonOperator(m, kappa), multigrid=MultigridOptions(coarse_size=8),
+                       preconditioner_options={"precision": precision})
+    g = P.weighted_gradient(p0, s)
+    u = P.FaceVelocity(m, -0.1 * g.interior)
+    p = p0.copy()
+    st = P.project(u, p, s, 0.1, tolerance=1e-13, max_cycles=100)
+    assert st.converged
+    assert np.max(np.abs(u.interior)) < 1e-10
+    assert np.max(np.abs(p)) < 1e-9
+
+
+def test_projection_argument_validation_leaves_the_velocity():
+    """test/operators/poisson.jl:1773-1797 through `tpa_project`."""
+    m = BlockTreeMesh(block_size=(4, 4))
+    s = EllipticSolver(PoissonOperator(m, np.ones(m.nfaces)), multigrid=MultigridOptions(coarse_size=4))
+    u = P.FaceVelocity(m, np.ones(m.nfaces))
+    original = u.interior.copy()
+    with pytest.raises(ValueError):
+        P.project(u, np.zeros(m.ncells), s, 0.1, compatibility="invalid")
+    for bad in (0.05, np.inf, np.nan):
+        with pytest.raises(TpaError) as e:
+            P.project(u, np.zeros(m.ncells), s, 0.1, reference_dt=bad)
+        assert e.value.code == 1
+        assert np.array_equal(u.interior, original)
+    for bad in (0.0, -np.finfo(float).eps, 1.0, np.inf, np.nan):
+        with pytest.raises(TpaError) as e:
+            P.project(u, np.zeros(m.ncells), s, 0.1, tolerance=bad)
+        assert e.value.code == 1
+        assert np.array_equal(u.interior, original)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_mixed_level_no_permeation_projection_known_answer(precision):
+    """test/operators/poisson.jl:1799-1823: a walled two-level tree of 4x4
+    blocks, u = (0.3 + sin cos, -0.2 + cos sin), dt 0.05, tolerance 1e-10, 80
+    cycles: converged, max |div u| <= 1e-8, zero boundary velocity, pressure
+    integral <= 2e-11."""
+    from test_oracle_projection import no_permeation_case
+    spec, om, u0, ub0 = no_permeation_case()
+    m = BlockTreeMesh(**spec)
+    assert np.array_equal(m.face_axis, om.face_axis) and np.array_equal(m.bface_cell, om.bface_cell)
+    s = EllipticSolver(PoissonOperator(m, np.ones(m.nfaces)), multigrid=MultigridOptions(coarse_size=8),
+                       preconditioner_options={"precision": precision})
+    u = P.FaceVelocity(m, u0, ub0)
+    p = np.zeros(m.ncells)
+    st = P.project(u, p, s, 0.05, tolerance=1e-10, max_cycles=80)
+    assert st.converged
+    assert np.max(np.abs(P.divergence(u, s))) <= 1e-8
+    assert not np.any(u.boundary)
+    assert abs(np.sum(m.cell_volumes() * p)) <= 2e-11

@@ -16,6 +16,21 @@ test/operators/poisson.jl:1704-1747 ("pressure projection")
   residual_scale 100, final residual / scale <= 1e-11, dt times the final
   divergence equal to the scaled final residual to 8 eps, the divergence
   reduced below 2e-11 of its initial value, the pressure integral <= 2e-12.
+
+test/operators/poisson.jl:1749-1771 ("incremental pressure projection")
+* u = -dt G_k p for p = sin 2 pi x cos 2 pi y on one periodic 8x8 block with
+  kappa = 1 + cos(2 pi x_f) / 4: the projection (tolerance 1e-13) returns
+  |u| < 1e-10 and |p| < 1e-9.
+
+test/operators/poisson.jl:1773-1797 (tolerance validation)
+* an unknown compatibility mode, a reference dt of 0.05 (< dt), inf or nan,
+  and a tolerance of 0, -eps, 1, inf or nan are argument errors that leave the
+  velocity as it was.
+
+test/operators/poisson.jl:1799-1823 ("mixed-level no-permeation projection")
+* a walled two-level tree of 4x4 blocks with u = (0.3 + sin cos, -0.2 + cos sin):
+  converged, max |div u| <= 1e-8, zero boundary velocity, pressure integral
+  <= 2e-11.
 """
 import numpy as np
 import pytest
@@ -148,3 +163,65 @@ def test_pressure_projection_known_answer(coefficient):
     u, ub, p, phi, st = P.project(op, mg, u0, None, np.zeros(mesh.ncells), 0.1, tolerance=1e-11)
     check_projection_known_answer(st.solve, P.divergence(mesh, u0, ub), P.divergence(mesh, u, ub), p,
                                   mesh.cell_volumes())
+
+
+def incremental_case(mesh):
+    """Coefficients and the velocity -dt G_k p of test/operators/poisson.jl:1749-1762."""
+    kappa = 1 + 0.25 * np.cos(2 * np.pi * mesh.face_center[:, 0])
+    x, y = mesh.cell_centers()
+    return kappa, np.sin(2 * np.pi * x) * np.cos(2 * np.pi * y)
+
+
+def test_incremental_pressure_projection_known_answer():
+    mesh = block_tree_mesh(block_size=(8, 8))
+    kappa, p0 = incremental_case(mesh)
+    op = PoissonOperator(mesh, kappa)
+    g, _ = P.weighted_gradient(op, p0)
+    u0 = -0.1 * g
+    mg = TreeGeometricMultigrid(op, MultigridOptions(coarse_size=8))
+    u, ub, p, phi, st = P.project(op, mg, u0, None, p0, 0.1, tolerance=1e-13, max_cycles=100)
+    assert st.converged
+    assert np.max(np.abs(u)) < 1e-10
+    assert np.max(np.abs(p)) < 1e-9
+
+
+def test_projection_argument_validation():
+    mesh = block_tree_mesh(block_size=(4, 4))
+    op = PoissonOperator(mesh)
+    mg = TreeGeometricMultigrid(op, MultigridOptions(coarse_size=4))
+    u = np.ones(mesh.nfaces)
+    original = u.copy()
+    with pytest.raises(ValueError):
+        P.project(op, mg, u, None, np.zeros(mesh.ncells), 0.1, compatibility="invalid")
+    for bad in (0.05, np.inf, np.nan):
+        with pytest.raises(ValueError):
+            P.project(op, mg, u, None, np.zeros(mesh.ncells), 0.1, reference_dt=bad)
+    for bad in (0.0, -np.finfo(float).eps, 1.0, np.inf, np.nan):
+        with pytest.raises(ValueError):
+            P.project(op, mg, u, None, np.zeros(mesh.ncells), 0.1, tolerance=bad)
+    assert np.array_equal(u, original)
+
+
+def no_permeation_case():
+    """Mesh and velocity of test/operators/poisson.jl:1799-1811."""
+    spec = dict(block_size=(4, 4), periodic=(False, False), max_level=2,
+                refine=lambda k, o, e: k[0] == 0 or (k[0] == 1 and k[1] == 0 and k[2] == 0))
+    mesh = block_tree_mesh(**spec)
+
+    def field(center, axis):
+        x, y = center[:, 0], center[:, 1]
+        return np.where(axis == 1, 0.3 + np.sin(2 * np.pi * x) * np.cos(2 * np.pi * y),
+                        -0.2 + np.cos(2 * np.pi * x) * np.sin(2 * np.pi * y))
+    return spec, mesh, field(mesh.face_center, mesh.face_axis), field(mesh.bface_center, mesh.bface_axis)
+
+
+def test_mixed_level_no_permeation_projection_known_answer():
+    _, mesh, u0, ub0 = no_permeation_case()
+    assert len(ub0) > 0 and np.any(ub0)
+    op = PoissonOperator(mesh)
+    mg = TreeGeometricMultigrid(op, MultigridOptions(coarse_size=8))
+    u, ub, p, phi, st = P.project(op, mg, u0, ub0, np.zeros(mesh.ncells), 0.05, tolerance=1e-10, max_cycles=80)
+    assert st.converged
+    assert np.max(np.abs(P.divergence(mesh, u, ub))) <= 1e-8
+    assert not np.any(ub)
+    assert abs(np.sum(mesh.cell_volumes() * p)) <= 2e-11

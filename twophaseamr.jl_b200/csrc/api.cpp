@@ -750,7 +750,8 @@ void project_body(tpa_context* ctx, double* u_int, double* u_bnd, double* p, con
         throw tpa::Error(TPA_ERR_INVALID_ARG, "compatibility must be :project or :error");
     if (o->precision != 0 && o->precision != 1) throw tpa::Error(TPA_ERR_INVALID_ARG, "bad precision");
     if (o->max_cycles < 0) throw tpa::Error(TPA_ERR_INVALID_ARG, "max_cycles must be nonnegative");
-    const double reference_dt = o->reference_dt > 0 ? o->reference_dt : o->dt;
+    // 0 stands for "not given"; any other value (negative, inf, nan) is checked
+    const double reference_dt = o->reference_dt == 0.0 ? o->dt : o->reference_dt;
     tpa::SolveStats st;
     ctx->dev->reset_launches();
     ctx->dev->project(u_int, u_bnd, p, o->dt, o->tolerance, o->max_cycles, o->compatibility, inherited,

@@ -52,7 +52,11 @@ class ProjectionOptions(C.Structure):
 
 
 def _options(solver, dt, tolerance, max_cycles, compatibility, precision, prepared, reference_dt, inherited_ptr):
-    return ProjectionOptions(float(dt), float(tolerance), float(reference_dt or 0.0), inherited_ptr,
+    if reference_dt is not None and float(reference_dt) == 0.0:
+        # 0 means "not given" at the C-ABI; an explicit 0 is below dt
+        raise ValueError("reference dt must be finite and at least dt")
+    return ProjectionOptions(float(dt), float(tolerance), 0.0 if reference_dt is None else float(reference_dt),
+                             inherited_ptr,
                              int(max_cycles), _compat(compatibility), _PRECISION[precision or solver.precision],
                              1 if prepared else 0)
 
