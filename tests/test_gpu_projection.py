@@ -284,7 +284,8 @@ def test_pressure_projection_known_answer(coefficient, precision):
     `tpa_project`: a sinusoidal velocity on the two-level tree of 8x8 blocks,
     kappa = 1 or the harmonic face mean of (x < 1/2 ? 1 : 100), dt 0.1,
     tolerance 1e-11, coarse_size 8."""
-    from test_oracle_projection import check_projection_known_answer, harmonic_face_coefficients
+    from reference_cases import harmonic_face_coefficients
+    from test_oracle_projection import check_projection_known_answer
     spec = spec_of("two_level")
     m = BlockTreeMesh(**spec)
     om = block_tree_mesh(**spec)

@@ -184,3 +184,65 @@ def test_periodic_nullspace_convention():
     assert abs(st.removed_rhs_mean - 3) < 1e-12
     assert abs(np.sum(p * op.volumes)) <= 16 * np.finfo(float).eps
     assert np.max(np.abs(p)) <= 16 * np.finfo(float).eps
+
+
+def test_root_block_vcycle_cg_comparison():
+    """test/operators/poisson.jl:672-720: capping the hierarchy at four levels
+    leaves the 8x8-cell root level as the coarsest (five levels uncapped, down
+    to a single 4x4 block); both CG solves of the manufactured field converge
+    at rtol 1e-8 to within 1e-6 of it, the uncapped one in no more cycles."""
+    from reference_cases import chain_exact, chain_spec
+    mesh = block_tree_mesh(**chain_spec())
+    op = PoissonOperator(mesh)
+    capped = TreeGeometricMultigrid(op, MultigridOptions(coarse_size=16, max_levels=4, pre_sweeps=4, post_sweeps=4))
+    full = TreeGeometricMultigrid(op, MultigridOptions(coarse_size=16, pre_sweeps=4, post_sweeps=4))
+    assert len(capped.level_sizes) == 4 and len(full.level_sizes) == 5
+    assert capped.level_sizes[-1] == 64 and full.level_sizes[-1] == 16
+    x, y = mesh.cell_centers()
+    exact = chain_exact(x, y)
+    rhs = op.apply(exact) / op.volumes  # `apply!`: the strong form
+    exact = exact - np.dot(op.volumes, exact) / np.sum(op.volumes)
+    (p0, s0), (p1, s1) = (solve(op, mg, rhs, rtol=1e-8, max_cycles=100) for mg in (capped, full))
+    assert s0.converged and s1.converged
+    assert s0.cycles > 1 and s1.cycles <= s0.cycles
+    assert np.max(np.abs(p0 - exact)) <= 1e-6 and np.max(np.abs(p1 - exact)) <= 1e-6
+
+
+def test_variable_coefficient_operator():
+    """test/operators/poisson.jl:788-818: harmonic face means of a 1 / 25 cell
+    field lie in [1, 25]; the strong-form action equals minus the divergence of
+    the weighted gradient (atol 2e-11, rtol 2e-13); symmetric, positive
+    semi-definite with one zero eigenvalue."""
+    from oracle import projection as OP
+    from reference_cases import harmonic_face_coefficients, two_level_spec
+    mesh = block_tree_mesh(**two_level_spec(4))
+    cx, cy = mesh.cell_centers()
+    kappa = harmonic_face_coefficients(mesh, np.where(cx < 0.5, 1.0, 25.0))
+    assert np.all(kappa > 0) and kappa.min() >= 1 and kappa.max() <= 25
+    op = PoissonOperator(mesh, kappa)
+    p = np.sin(2 * np.pi * cx) * np.cos(2 * np.pi * cy)
+    applied = op.apply(p) / op.volumes
+    g, gb = OP.weighted_gradient(op, p)
+    div = OP.divergence(mesh, g, gb)
+    assert np.allclose(applied, -div, atol=2e-11, rtol=2e-13)
+    dense = op.matrix.toarray()
+    assert np.allclose(dense, dense.T, atol=2e-13, rtol=2e-13)
+    w = np.linalg.eigvalsh(dense)
+    tol = 5e-12 * w.max()
+    assert w[0] >= -tol and np.sum(np.abs(w) <= tol) == 1
+
+
+def test_preconditioned_and_plain_cg():
+    """test/operators/poisson.jl:833-882: on a tree refined to level 4 the
+    preconditioned CG (coarse_size 32) converges at rtol 1e-10, and plain CG
+    (rtol 1e-8, 500 cycles) converges in more cycles."""
+    from reference_cases import deep_rhs, deep_spec
+    mesh = block_tree_mesh(**deep_spec())
+    op = PoissonOperator(mesh)
+    x, y = mesh.cell_centers()
+    rhs = deep_rhs(x, y)
+    p, st = solve(op, TreeGeometricMultigrid(op, MultigridOptions(coarse_size=32)), rhs, rtol=1e-10, max_cycles=100)
+    assert st.converged
+    q, plain = solve(op, None, rhs, rtol=1e-8, max_cycles=500, preconditioner=False)
+    assert plain.converged and plain.preconditioner == "none"
+    assert st.cycles < plain.cycles

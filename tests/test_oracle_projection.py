@@ -42,6 +42,8 @@ from oracle.operator import PoissonOperator
 
 from tpagmg import workloads as W
 
+from reference_cases import harmonic_face_coefficients  # noqa: F401  (also used by the GPU tests)
+
 CENTER, RADIUS = (0.5, 0.5), 0.2
 
 
@@ -119,17 +121,6 @@ def test_conditional_fraction_floor_and_bounds():
     for bad in (-1e-6, 1.0 + 1e-6, np.nan):
         with pytest.raises(ValueError):
             P.conditional_fraction(np.array([0.5, bad]))
-
-
-def harmonic_face_coefficients(mesh, cell_value):
-    """`harmonic_face_coefficients` (src/operators/elliptic.jl:9-23): the
-    distance-weighted harmonic mean of the two cell values."""
-    nx, ny = mesh.block_size
-    a = mesh.face_axis.astype(np.int64) - 1
-    dm = mesh.spacing[mesh.face_minus // (nx * ny), a] / 2
-    dp = mesh.spacing[mesh.face_plus // (nx * ny), a] / 2
-    cm, cp = cell_value[mesh.face_minus], cell_value[mesh.face_plus]
-    return (dm + dp) / (dm / cm + dp / cp)
 
 
 def check_projection_known_answer(stats, u_div0, u_div, pressure, volumes):
