@@ -139,11 +139,21 @@ __global__ void k_cg_ap(LevelView<double> A, const double* __restrict__ p, doubl
     }
 }
 
-// x += alpha p, r -= alpha Ap; folds max|r_i|/V_i and sum(r)
-__global__ void k_cg_update(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+// Search directions of iteration `iter` in the ping-pong pair (pa, pb): the
+// previous one (read by the operator product) and the new one (written by it,
+// read by the update).
+__device__ __forceinline__ const double* dir_old(const double* pa, const double* pb, int iter) {
+    return (iter & 1) ? pb : pa;
+}
+__device__ __forceinline__ double* dir_new(double* pa, double* pb, int iter) { return (iter & 1) ? pa : pb; }
+
+// x += alpha p, r -= alpha Ap (p: this iteration's direction); folds
+// max|r_i|/V_i and sum(r)
+__global__ void k_cg_update(int n, double* __restrict__ x, double* __restrict__ r, double* pa, double* pb,
                             const double* __restrict__ ap, const double* __restrict__ vol, double* pmax, double* psum,
                             unsigned* counter, CgState* s) {
     pdl_entry();
+    const double* __restrict__ p = dir_new(pa, pb, s->iter);
     __shared__ bool last;
     const bool skip = s->flags & 2;
     const double alpha = s->alpha;
@@ -280,19 +290,19 @@ void with_nxc(const SView<T>& S, F f) {
     else f(std::integral_constant<int, 0>{});
 }
 
-// z = x0 - mean, gamma_next = r'z and the stopping rules; `init` starts a run
-// (p = z, gamma = r'z).  With `set_cond`, sets the graph loop condition.
+// gamma_next = r'z for z = x0 - mean (the V-cycle's output, not stored: the
+// next operator product forms z and p where it reads them) and the stopping
+// rules; `init` starts a run (gamma = r'z, iter 0: the first direction is z).
+// With `set_cond`, sets the graph loop condition.
 template <typename T>
 __global__ void k_cg_z(int n, const T* __restrict__ xv, const double* mean, const double* __restrict__ r,
-                       double* __restrict__ z, double* __restrict__ p, double* partial, unsigned* counter, CgState* s,
-                       int init, cudaGraphConditionalHandle handle, int set_cond) {
+                       double* partial, unsigned* counter, CgState* s, int init, cudaGraphConditionalHandle handle,
+                       int set_cond) {
     pdl_entry();
     const double m = mean ? *mean : 0.0;
     double v = 0;
     TPA_GRID_STRIDE(i, n) {
         double zi = double(xv[i]) - m;
-        z[i] = zi;
-        if (init) p[i] = zi;
         v += r[i] * zi;
     }
     if (publish_partial(v, partial, counter)) {
@@ -331,11 +341,89 @@ __global__ void k_cg_z(int n, const T* __restrict__ xv, const double* mean, cons
     }
 }
 
-__global__ void k_cg_p(int n, double* __restrict__ p, const double* __restrict__ z, const CgState* s) {
+// The next search direction p = z + beta p_old, formed where the
+// operator product reads it: z_j = x_j - mean from the V-cycle's finest-level
+// output (FP32 or FP64) and p_old from the other buffer of the ping-pong pair;
+// the first iteration of a run (iter 0) takes p = z.  So neither z nor a
+// separate p pass goes through memory, and no launch of its own is needed.
+template <typename T>
+struct NextDir {
+    const T* __restrict__ x;
+    const double* __restrict__ pold;
+    double mean, beta;
+    bool first;
+    __device__ __forceinline__ double operator()(int j) const {
+        const double z = double(x[j]) - mean;
+        return first ? z : z + beta * pold[j];
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ NextDir<T> next_dir(const T* xv, const double* mean, const double* pa, const double* pb,
+                                               const CgState* s) {
+    const int k = s->iter;
+    return NextDir<T>{xv, dir_old(pa, pb, k), *mean, s->beta, k == 0};
+}
+
+// p = z + beta p_old, Ap and alpha = gamma / p'Ap (CSR finest level)
+template <typename T>
+__global__ void k_cg_dir_ap(LevelView<double> A, const T* __restrict__ xv, const double* mean, double* pa,
+                            double* pb, double* __restrict__ ap, double* partial, unsigned* counter, CgState* s) {
     pdl_entry();
-    if (s->flags & 6) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) p[i] = z[i] + s->beta * p[i];
+    const NextDir<T> d = next_dir(xv, mean, pa, pb, s);
+    double* __restrict__ pn = dir_new(pa, pb, s->iter);
+    double v = 0;
+    TPA_GRID_STRIDE(i, A.n) {
+        double y = 0;
+        for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) y += A.val[k] * d(A.ci[k]);
+        const double pi = d(i);
+        pn[i] = pi;
+        ap[i] = y;
+        v += pi * y;
+    }
+    if (publish_partial(v, partial, counter)) {
+        double pAp = fold_partials(partial, gridDim.x);
+        if (threadIdx.x == 0) {
+            alpha_from(pAp, s);
+            *counter = 0;
+        }
+    }
+}
+
+// the same on a block-structured finest level
+template <typename T, int NXC>
+__global__ void s_cg_dir_ap(SView<double> L, const T* __restrict__ xv, const double* mean, double* pa, double* pb,
+                            double* __restrict__ ap, double* partial, unsigned* counter, CgState* s) {
+    pdl_entry();
+    const NextDir<T> d = next_dir(xv, mean, pa, pb, s);
+    double* __restrict__ pn = dir_new(pa, pb, s->iter);
+    s_apply_dot_ld<double, NXC>(L, d, [&](int c, double v) { pn[c] = v; }, ap, partial, counter,
+                                [&](double pAp) { alpha_from(pAp, s); });
+}
+
+// the same on a constant-coefficient 16x16 finest level (vectorized quads)
+template <typename T>
+__global__ void __launch_bounds__(256) v_cg_dir_ap(SView<double> L, const T* __restrict__ xv, const double* mean,
+                                                   double* pa, double* pb, double* __restrict__ ap, double* partial,
+                                                   unsigned* counter, CgState* s) {
+    pdl_entry();
+    const int k = s->iter;
+    const double* __restrict__ po = dir_old(pa, pb, k);
+    double* __restrict__ pn = dir_new(pa, pb, k);
+    const double mu = *mean, beta = s->beta;
+    const bool first = k == 0;
+    auto ld = [&](int c) {
+        const Quad<T> xq = q_ldv(xv + c);
+        Quad<double> q;
+        if (first) {
+            for (int m = 0; m < 4; ++m) q.v[m] = double(xq.v[m]) - mu;
+        } else {
+            const Quad<double> pq = q_ldv(po + c);
+            for (int m = 0; m < 4; ++m) q.v[m] = (double(xq.v[m]) - mu) + beta * pq.v[m];
+        }
+        return q;
+    };
+    v_apply_dot_ld(L, ld, pn, ap, partial, counter, [&](double pAp) { alpha_from(pAp, s); });
 }
 
 __global__ void k_cg_set(CgState* s, double target, int itmax) {
@@ -661,8 +749,9 @@ void DeviceSolver::vcycle_fused(const double* r, double* z, int precision) {
     TPA_CUDA(cudaGetLastError());
 }
 
-// One CG iteration: Ap and alpha, the x / r update, the V-cycle, z and the
-// stopping rules (which set the loop condition when `set_cond`), p = z + beta p.
+// One CG iteration: the direction p = z + beta p (from the previous V-cycle)
+// with Ap and alpha, the x / r update, the V-cycle, r'z and the stopping rules
+// (which set the loop condition when `set_cond`).
 void DeviceSolver::enqueue_cg_body(int precision, cudaGraphConditionalHandle handle, int set_cond) {
     const Launch go{stream_, pdl_};
     const int n = levels_[0].n;
@@ -670,38 +759,42 @@ void DeviceSolver::enqueue_cg_body(int precision, cudaGraphConditionalHandle han
     CgState* s = reinterpret_cast<CgState*>(cgs_.p);
     double* mean = lsum_.p + nl;
     const LevelView<double>& A = vd_[0];
-    if (sdev_[0].vec)
-        go(v_cg_ap, fold_grid(v_cg_ap, 256, (sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0, sd_[0], p_.p, ap_.p, fpartial_.p,
-           counters_.p + kCgAp, s);
-    else if (sdev_[0].on)
-        with_nxc(sd_[0], [&](auto nxc) {
-            constexpr int N = decltype(nxc)::value;
-            go(s_cg_ap<N>, fold_grid(s_cg_ap<N>, sd_[0].cpb, sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0, sd_[0], p_.p, ap_.p,
-                                                                                       fpartial_.p, counters_.p + kCgAp, s);
-        });
-    else
-        go(k_cg_ap, fold_grid(k_cg_ap, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, A, p_.p, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
-    go(k_cg_update, fold_grid(k_cg_update, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, xw_.p, r_.p, p_.p, ap_.p, A.vol, fpartial_.p,
-                                                          fpartial2_.p, counters_.p + kCgUpdate, s);
+    double* const pa = p_.p;  // the ping-pong pair of search directions
+    double* const pb = z_.p;
+    // p = z + beta p_old from the last V-cycle's output, Ap and alpha
+    auto dir_ap = [&](auto* xv) {
+        using T = std::remove_pointer_t<decltype(xv)>;
+        if (sdev_[0].vec)
+            go(v_cg_dir_ap<T>, fold_grid(v_cg_dir_ap<T>, 256, (sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0, sd_[0], xv,
+               mean, pa, pb, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
+        else if (sdev_[0].on)
+            with_nxc(sd_[0], [&](auto nxc) {
+                constexpr int N = decltype(nxc)::value;
+                go(s_cg_dir_ap<T, N>, fold_grid(s_cg_dir_ap<T, N>, sd_[0].cpb, sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0,
+                   sd_[0], xv, mean, pa, pb, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
+            });
+        else
+            go(k_cg_dir_ap<T>, fold_grid(k_cg_dir_ap<T>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, A, xv, mean, pa,
+               pb, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
+    };
+    if (precision == 0) dir_ap(vd_[0].x);
+    else dir_ap(vf_[0].x);
+    go(k_cg_update, fold_grid(k_cg_update, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, xw_.p, r_.p, pa, pb,
+       ap_.p, A.vol, fpartial_.p, fpartial2_.p, counters_.p + kCgUpdate, s);
     if (precision == 0) {
         enqueue_vcycle<double>(r_.p, &s->rsum, mean);
-        go(k_cg_z<double>, fold_grid(k_cg_z<double>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
-                                                                counters_.p + kCgZ, s, 0, handle, set_cond);
+        go(k_cg_z<double>, fold_grid(k_cg_z<double>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vd_[0].x,
+           mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 0, handle, set_cond);
     } else {
         enqueue_vcycle<float>(r_.p, &s->rsum, mean);
-        go(k_cg_z<float>, fold_grid(k_cg_z<float>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
-                                                               counters_.p + kCgZ, s, 0, handle, set_cond);
+        go(k_cg_z<float>, fold_grid(k_cg_z<float>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vf_[0].x,
+           mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 0, handle, set_cond);
     }
-    go(k_cg_p, blocks_for(n), kThreads, 0, n, p_.p, z_.p, s);
     TPA_CUDA(cudaGetLastError());
 }
 
 cudaGraphExec_t DeviceSolver::cg_graph(int precision) {
     if (cg_exec_[precision]) return cg_exec_[precision];
-    const int n = levels_[0].n;
-    const int nl = int(levels_.size());
-    CgState* s = reinterpret_cast<CgState*>(cgs_.p);
-    double* mean = lsum_.p + nl;
     cudaGraph_t g;
     TPA_CUDA(cudaGraphCreate(&g, 0));
     cudaGraphConditionalHandle handle;
@@ -724,7 +817,7 @@ cudaGraphExec_t DeviceSolver::cg_graph(int precision) {
     cudaGraph_t captured;
     cudaError_t ce = cudaStreamEndCapture(stream_, &captured);
     stream_ = saved;
-    graph_body_launches_[precision] = launches_ - saved_launches + 5;
+    graph_body_launches_[precision] = launches_ - saved_launches + 3;  // + direction/Ap, update, z
     launches_ = saved_launches;
     if (ce != cudaSuccess) {
         cudaGraphDestroy(g);
@@ -761,14 +854,12 @@ void DeviceSolver::cg_fused(int precision, double target, int itmax, int& niter,
     launches_ += 2;
     if (precision == 0) {
         enqueue_vcycle<double>(r_.p, &s->rsum, mean);
-        go(k_cg_z<double>, fold_grid(k_cg_z<double>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vd_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
-                                                                counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(),
-                                                                0);
+        go(k_cg_z<double>, fold_grid(k_cg_z<double>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vd_[0].x,
+           mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(), 0);
     } else {
         enqueue_vcycle<float>(r_.p, &s->rsum, mean);
-        go(k_cg_z<float>, fold_grid(k_cg_z<float>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vf_[0].x, mean, r_.p, z_.p, p_.p, fpartial_.p,
-                                                               counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(),
-                                                               0);
+        go(k_cg_z<float>, fold_grid(k_cg_z<float>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vf_[0].x,
+           mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(), 0);
     }
     ++launches_;
     CgState hs;

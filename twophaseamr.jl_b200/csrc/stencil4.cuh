@@ -427,6 +427,32 @@ __device__ __forceinline__ void v_apply_dot(const SView<double>& L, const double
     }
 }
 
+// v_apply_dot with the operand formed where it is read: ld(c) is the quad of
+// the operand at cells c .. c+3, and the CTA's own quads are stored to `keep`
+template <typename Ld, typename Fold>
+__device__ __forceinline__ void v_apply_dot_ld(const SView<double>& L, Ld ld, double* keep, double* y,
+                                               double* partial, unsigned* counter, Fold fold) {
+    const int groups = (L.nblocks + 3) / 4;
+    double part = 0;
+    TPA_Q_LOOP(groups) {
+        const QPos p = q_pos(grp);
+        const bool valid = p.b < L.nblocks;
+        const QNb<double> g = q_gather<double>(L, p, valid, ld, [](double v, int) { return v; });
+        if (!valid) continue;
+        const Quad<double> ax = q_apply(L, g);
+        q_st(keep + p.c, g.x);
+        q_st(y + p.c, ax);
+        for (int m = 0; m < 4; ++m) part += g.x.v[m] * ax.v[m];
+    }
+    if (publish_partial(part, partial, counter)) {
+        const double s = fold_partials(partial, gridDim.x);
+        if (threadIdx.x == 0) {
+            fold(s);
+            *counter = 0;
+        }
+    }
+}
+
 #undef TPA_Q_LOOP
 
 }  // namespace tpa
