@@ -301,10 +301,16 @@ __global__ void k_cg_z(int n, const T* __restrict__ xv, const double* mean, cons
     pdl_entry();
     const double m = mean ? *mean : 0.0;
     double v = 0;
-    TPA_GRID_STRIDE(i, n) {
-        double zi = double(xv[i]) - m;
-        v += r[i] * zi;
+    // whole quads by 16-byte loads (both vectors are allocation-aligned), so a
+    // thread keeps 4 cells' loads in flight; then the last n mod 4 cells
+    const int nq = n >> 2;
+    TPA_GRID_STRIDE(k, nq) {
+        const Quad<T> xq = q_ldv(xv + 4 * k);
+        const Quad<double> rq = q_ldv(r + 4 * k);
+        for (int c = 0; c < 4; ++c) v += rq.v[c] * (double(xq.v[c]) - m);
     }
+    for (int i = 4 * nq + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        v += r[i] * (double(xv[i]) - m);
     if (publish_partial(v, partial, counter)) {
         double g = fold_partials(partial, gridDim.x);
         if (threadIdx.x == 0) {
@@ -783,12 +789,12 @@ void DeviceSolver::enqueue_cg_body(int precision, cudaGraphConditionalHandle han
        ap_.p, A.vol, fpartial_.p, fpartial2_.p, counters_.p + kCgUpdate, s);
     if (precision == 0) {
         enqueue_vcycle<double>(r_.p, &s->rsum, mean);
-        go(k_cg_z<double>, fold_grid(k_cg_z<double>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vd_[0].x,
-           mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 0, handle, set_cond);
+        go(k_cg_z<double>, fold_grid(k_cg_z<double>, kThreads, blocks_for((n + 3) / 4), kMaxGrid), kThreads, 0, n,
+           vd_[0].x, mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 0, handle, set_cond);
     } else {
         enqueue_vcycle<float>(r_.p, &s->rsum, mean);
-        go(k_cg_z<float>, fold_grid(k_cg_z<float>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vf_[0].x,
-           mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 0, handle, set_cond);
+        go(k_cg_z<float>, fold_grid(k_cg_z<float>, kThreads, blocks_for((n + 3) / 4), kMaxGrid), kThreads, 0, n,
+           vf_[0].x, mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 0, handle, set_cond);
     }
     TPA_CUDA(cudaGetLastError());
 }
@@ -854,12 +860,12 @@ void DeviceSolver::cg_fused(int precision, double target, int itmax, int& niter,
     launches_ += 2;
     if (precision == 0) {
         enqueue_vcycle<double>(r_.p, &s->rsum, mean);
-        go(k_cg_z<double>, fold_grid(k_cg_z<double>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vd_[0].x,
-           mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(), 0);
+        go(k_cg_z<double>, fold_grid(k_cg_z<double>, kThreads, blocks_for((n + 3) / 4), kMaxGrid), kThreads, 0, n,
+           vd_[0].x, mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(), 0);
     } else {
         enqueue_vcycle<float>(r_.p, &s->rsum, mean);
-        go(k_cg_z<float>, fold_grid(k_cg_z<float>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, vf_[0].x,
-           mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(), 0);
+        go(k_cg_z<float>, fold_grid(k_cg_z<float>, kThreads, blocks_for((n + 3) / 4), kMaxGrid), kThreads, 0, n,
+           vf_[0].x, mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(), 0);
     }
     ++launches_;
     CgState hs;
