@@ -226,11 +226,16 @@ def batch_main(args):
     x64 = x_all.clone()
     step("mixed")
     errs = [float((x_all[a:b] - x64[a:b]).abs().max() / x64[a:b].abs().max()) for a, b in zip(offs[:-1], offs[1:])]
-    # end to end: host arrays through the public batched entry point, copies inside
-    xs = [np.zeros(n) for n in sizes]
-    rh = [r for _, _, r in built]
-    xcat = np.zeros(int(offs[-1]))
-    rcat = np.concatenate(rh)
+    # end to end: pinned host arrays through the public batched entry point,
+    # copies inside
+    def pinned(a):
+        t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory()
+        return t, t.numpy()
+    keep = [pinned(np.zeros(n)) for n in sizes] + [pinned(r) for _, _, r in built]
+    xs = [a for _, a in keep[:len(sizes)]]
+    rh = [a for _, a in keep[len(sizes):]]
+    xcat_t, xcat = pinned(np.zeros(int(offs[-1])))
+    rcat_t, rcat = pinned(np.concatenate([r for _, _, r in built]))
     e2e = []
     for k in range(args.steps + 1):
         torch.cuda.synchronize()

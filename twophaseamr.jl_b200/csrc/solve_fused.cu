@@ -1043,6 +1043,8 @@ void DeviceSolver::upload_structured(const Hierarchy& h) {
             TPA_CUDA(cudaStreamSynchronize(stream_));
         }
         DevLevel& L = levels_[size_t(l)];
+        const std::vector<double>& hv = hl.op.volumes;
+        const bool const_vol = !hv.empty() && std::all_of(hv.begin(), hv.end(), [&](double v) { return v == hv[0]; });
         auto fill = [&](auto& v, auto& DL, auto* cx, auto* cy, auto* exv, auto cast) {
             v.nx = hl.op.mesh.bs[0];
             v.ny = hl.op.mesh.bs[1];
@@ -1061,6 +1063,8 @@ void DeviceSolver::upload_structured(const Hierarchy& h) {
             v.ex_val = exv;
             v.map = D.map.p;
             v.vol = DL.vol.p;
+            v.const_vol = const_vol ? 1 : 0;
+            v.vol0 = cast(hl.op.volumes.empty() ? 0.0 : hl.op.volumes[0]);
             v.w = DL.w;
             v.tw = DL.tw;
             v.singular = L.ncomp == 1;

@@ -33,6 +33,8 @@ struct SView {
     const T* ex_val;
     const int* map;  // 4 per block: coarse block, x offset, y offset, scale
     const T* vol;
+    T vol0;          // every cell's volume when const_vol (the vectorized kernels skip the loads)
+    int const_vol;
     T w, tw;
     int singular;
     double cvol_inv;

@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(256) v_pre2(SView<T> L, const TB* __restrict__
             const Quad<TB> a = q_ldv(bin + c);
             for (int m = 0; m < 4; ++m) r.v[m] = T(a.v[m]);
             if (mean != 0.0) {
-                const Quad<T> v = q_ld(L.vol + c);
+                const Quad<T> v = L.const_vol ? Quad<T>{{L.vol0, L.vol0, L.vol0, L.vol0}} : q_ld(L.vol + c);
                 for (int m = 0; m < 4; ++m) r.v[m] = T(double(a.v[m]) - double(v.v[m]) * mean);
             }
             return r;
@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(256) v_sweep(SView<T> L, const T* __restrict__
         for (int m = 0; m < 4; ++m) o.v[m] = g.x.v[m] + L.w * d.v[m] * (bp.v[m] - ax.v[m]);
         q_st(out + p.c, o);
         if (Fold && mean_out) {
-            const Quad<T> v = q_ld(L.vol + p.c);
+            const Quad<T> v = L.const_vol ? Quad<T>{{L.vol0, L.vol0, L.vol0, L.vol0}} : q_ld(L.vol + p.c);
             for (int m = 0; m < 4; ++m) part += double(v.v[m]) * double(o.v[m]);
         }
     }
