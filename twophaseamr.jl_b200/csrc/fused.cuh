@@ -497,30 +497,15 @@ __device__ void tail_run(const LevelView<T>* __restrict__ levels, int first, int
             for (int i = gt; i < L.n; i += gs)
                 L.bp[i] = top ? proj_b<T, TB>(L, top_b, mean, i) : proj_b<T, T>(L, L.b, mean, i);
             cl.sync();
-            // a warp takes kCoarseRows consecutive rows, lanes striding them
-            // together: coalesced reads of G with one independent load per row
-            // in flight (a row's sum runs in the same order as one row alone)
-            constexpr int kCoarseRows = 8;
+            // one warp per row, lanes striding the row: coalesced reads of G
             const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
             const int warp = rank * nwarps + (threadIdx.x >> 5);
-            for (int i0 = kCoarseRows * warp; i0 < gn; i0 += kCoarseRows * nb * nwarps) {
-                const int nr = min(kCoarseRows, gn - i0);
-                const double* row = G + size_t(i0) * gn;
-                double acc[kCoarseRows];
-#pragma unroll
-                for (int q = 0; q < kCoarseRows; ++q) acc[q] = 0;
-                for (int k = lane; k < gn; k += 32) {
-                    const double bk = double(L.bp[k]);
-#pragma unroll
-                    for (int q = 0; q < kCoarseRows; ++q)
-                        if (q < nr) acc[q] += row[size_t(q) * gn + k] * bk;
-                }
-#pragma unroll
-                for (int q = 0; q < kCoarseRows; ++q) {
-                    double a = acc[q];
-                    for (int o = 16; o; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
-                    if (!lane && q < nr) L.x[i0 + q] = T(a);
-                }
+            for (int i = warp; i < gn; i += nb * nwarps) {
+                const double* row = G + size_t(i) * gn;
+                double acc = 0;
+                for (int k = lane; k < gn; k += 32) acc += row[k] * double(L.bp[k]);
+                for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+                if (!lane) L.x[i] = T(acc);
             }
             cl.sync();
             break;
