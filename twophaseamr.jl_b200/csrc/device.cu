@@ -529,6 +529,10 @@ void DeviceSolver::upload(const Hierarchy& h) {
         d.f.vol.upload(fvol.data(), fvol.size(), stream_);
         d.d.w = hl.weight;
         d.f.w = float(hl.weight);
+        d.vol0 = hl.op.volumes.empty() ? 0.0 : hl.op.volumes[0];
+        d.const_vol = !hl.op.volumes.empty() && d.vol0 > 0 &&
+                      std::all_of(hl.op.volumes.begin(), hl.op.volumes.end(), [&](double v) { return v == d.vol0; });
+        d.any_void = std::any_of(hl.op.volumes.begin(), hl.op.volumes.end(), [](double v) { return !(v > 0); });
         if (hl.op.singular) {
             d.ncomp = int(hl.op.comp.volume.size());
             if (d.ncomp > kMaxComponents) throw Error(5, "more ungauged components than the device supports");

@@ -85,6 +85,9 @@ struct DevLevel {
     DevLevelT<float> f;
     DevArray<unsigned char> colour;  // red-black smoother: 0 red, 1 black per cell
     double rbw = 1.0;                // red-black half-sweep weight
+    double vol0 = 0;                 // every cell's volume when const_vol
+    bool const_vol = false;
+    bool any_void = false;           // some cell has volume <= 0 (masked out of sums and rows)
 };
 
 // PCG scalars kept on the device between kernels.

@@ -69,13 +69,14 @@ __device__ __forceinline__ void publish_fold(const double (&v)[N], unsigned max_
     if (threadIdx.x == 0) *counter = 0;
 }
 
-// b = V f (0 where V = 0), x0 = x_in (0 where V = 0); out = {sum b, sum |b|, sum V x0}
+// b = V f (0 where V = 0), x0 = x_in (0 where V = 0); out = {sum b, sum |b|, sum V x0}.
+// vol null: every cell's volume is vol0.
 __global__ void k_prep(int n, const double* __restrict__ rhs, const double* __restrict__ xin,
-                       const double* __restrict__ vol, double* __restrict__ b, double* __restrict__ x0,
+                       const double* __restrict__ vol, double vol0, double* __restrict__ b, double* __restrict__ x0,
                        double* partial, unsigned* counter, double* out) {
     double v[3] = {0, 0, 0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const double V = vol[i];
+        const double V = vol ? vol[i] : vol0;
         const double bi = V > 0 ? rhs[i] * V : 0.0;
         const double xi = V > 0 ? xin[i] : 0.0;
         b[i] = bi;
@@ -96,8 +97,8 @@ __global__ void k_prep(int n, const double* __restrict__ rhs, const double* __re
 // it: dt max |div u| after the update equals the final residual over 1/dt^2 to
 // a few ulps only when both are evaluated from face differences.
 __global__ void k_pres(LevelView<double> A, double* __restrict__ b, const double* __restrict__ x0,
-                       double* __restrict__ x, double* __restrict__ r, double mb, double mx, double* partial,
-                       unsigned* counter, double* out) {
+                       double* __restrict__ x, double* __restrict__ r, double mb, double mx, int masked,
+                       double* partial, unsigned* counter, double* out) {
     double v[4] = {0, 0, 0, 0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
         const double V = A.vol[i];
@@ -110,7 +111,7 @@ __global__ void k_pres(LevelView<double> A, double* __restrict__ b, const double
         double acc = 0, aacc = 0;
         for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
             const int j = A.ci[k];
-            const double xj = A.vol[j] > 0 ? x0[j] - mx : 0.0;
+            const double xj = (!masked || A.vol[j] > 0) ? x0[j] - mx : 0.0;
             acc += A.val[k] * (xj - xi);
             aacc += fabs(A.val[k]) * fabs(xj);
         }
@@ -141,11 +142,13 @@ __global__ void __launch_bounds__(256) v_pres(SView<double> S, double* __restric
     for (int grp = blockIdx.x; grp < groups; grp += gridDim.x) {
         const QPos p = q_pos(grp);
         const bool valid = p.b < S.nblocks;
+        // a level of equal positive volumes needs no per-cell volume loads
+        const bool uniform = S.const_vol && S.vol0 > 0;
         const QNb<double> g = q_gather<double>(
             S, p, valid, [&](int c) { return q_ldv(x0 + c); },
-            [&](double xv, int c) { return vol[c] > 0 ? xv - mx : 0.0; });
+            [&](double xv, int c) { return (uniform || vol[c] > 0) ? xv - mx : 0.0; });
         if (!valid) continue;
-        const Quad<double> vq = q_ld(vol + p.c);
+        const Quad<double> vq = uniform ? Quad<double>{{S.vol0, S.vol0, S.vol0, S.vol0}} : q_ld(vol + p.c);
         Quad<double> bq = q_ldv(b + p.c), rq;
         for (int m = 0; m < 4; ++m) {
             const bool hw = m > 0 || g.hw, he = m < 3 || g.he;
@@ -185,14 +188,15 @@ __global__ void __launch_bounds__(256) v_pres(SView<double> S, double* __restric
     publish_fold<4>(v, 0xEu, partial, counter, out);
 }
 
-// out = sum V x; x0 = x (the next k_pres reads x0 and writes x)
-__global__ void k_xmean(int n, const double* __restrict__ x, const double* __restrict__ vol,
+// out = sum V x; x0 = x (the next k_pres reads x0 and writes x).  vol null:
+// every cell's volume is vol0.
+__global__ void k_xmean(int n, const double* __restrict__ x, const double* __restrict__ vol, double vol0,
                         double* __restrict__ x0, double* partial, unsigned* counter, double* out) {
     double v[1] = {0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const double xi = x[i];
         x0[i] = xi;
-        v[0] += vol[i] * xi;
+        v[0] += (vol ? vol[i] : vol0) * xi;
     }
     publish_fold<1>(v, 0u, partial, counter, out);
 }
@@ -221,7 +225,7 @@ void DeviceSolver::solve_fast(const double* rhs, double* x_user, double rtol, do
     TPA_CUDA(cudaEventRecord(e0, stream_));
     st = SolveStats();
 
-    k_prep<<<fold_grid(k_prep, kThreads, want, kGrid), kThreads, 0, stream_>>>(n, rhs, x_user, A.vol, b_.p, tmp_.p, spartial_.p, counters_.p + kCPrep,
+    k_prep<<<fold_grid(k_prep, kThreads, want, kGrid), kThreads, 0, stream_>>>(n, rhs, x_user, L.const_vol ? nullptr : A.vol, L.vol0, b_.p, tmp_.p, spartial_.p, counters_.p + kCPrep,
                                            out);
     ++launches_;
     read(3);
@@ -246,7 +250,8 @@ void DeviceSolver::solve_fast(const double* rhs, double* x_user, double rtol, do
                 sd_[0], b_.p, tmp_.p, xw_.p, r_.p, b_mean, x_mean, spartial_.p, counters_.p + kCPres, out);
         } else {
             k_pres<<<fold_grid(k_pres, kThreads, want, kGrid), kThreads, 0, stream_>>>(
-                A, b_.p, tmp_.p, xw_.p, r_.p, b_mean, x_mean, spartial_.p, counters_.p + kCPres, out);
+                A, b_.p, tmp_.p, xw_.p, r_.p, b_mean, x_mean, L.any_void ? 1 : 0, spartial_.p, counters_.p + kCPres,
+                out);
         }
         ++launches_;
         read(4);
@@ -270,7 +275,7 @@ void DeviceSolver::solve_fast(const double* rhs, double* x_user, double rtol, do
             cg_fused(precision, target, max_cycles - total, niter, flags);
             total += niter;
             // gauge of the iterate, then the true residual and its norms
-            k_xmean<<<fold_grid(k_xmean, kThreads, want, kGrid), kThreads, 0, stream_>>>(n, xw_.p, A.vol, tmp_.p, spartial_.p, counters_.p + kCMean,
+            k_xmean<<<fold_grid(k_xmean, kThreads, want, kGrid), kThreads, 0, stream_>>>(n, xw_.p, L.const_vol ? nullptr : A.vol, L.vol0, tmp_.p, spartial_.p, counters_.p + kCMean,
                                                     out);
             ++launches_;
             double xm = 0;

@@ -148,10 +148,10 @@ __device__ __forceinline__ const double* dir_old(const double* pa, const double*
 __device__ __forceinline__ double* dir_new(double* pa, double* pb, int iter) { return (iter & 1) ? pa : pb; }
 
 // x += alpha p, r -= alpha Ap (p: this iteration's direction); folds
-// max|r_i|/V_i and sum(r)
+// max|r_i|/V_i and sum(r).  vol null: every cell's volume is vol0.
 __global__ void k_cg_update(int n, double* __restrict__ x, double* __restrict__ r, double* pa, double* pb,
-                            const double* __restrict__ ap, const double* __restrict__ vol, double* pmax, double* psum,
-                            unsigned* counter, CgState* s) {
+                            const double* __restrict__ ap, const double* __restrict__ vol, double vol0, double* pmax,
+                            double* psum, unsigned* counter, CgState* s) {
     pdl_entry();
     const double* __restrict__ p = dir_new(pa, pb, s->iter);
     __shared__ bool last;
@@ -166,7 +166,7 @@ __global__ void k_cg_update(int n, double* __restrict__ x, double* __restrict__ 
             ri -= alpha * ap[i];
             r[i] = ri;
         }
-        double V = vol[i];
+        double V = vol ? vol[i] : vol0;
         if (V > 0) {
             double q = fabs(ri) / V;
             if (q != q) nan = true;
@@ -785,8 +785,9 @@ void DeviceSolver::enqueue_cg_body(int precision, cudaGraphConditionalHandle han
     };
     if (precision == 0) dir_ap(vd_[0].x);
     else dir_ap(vf_[0].x);
+    const DevLevel& L0 = levels_[0];
     go(k_cg_update, fold_grid(k_cg_update, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, xw_.p, r_.p, pa, pb,
-       ap_.p, A.vol, fpartial_.p, fpartial2_.p, counters_.p + kCgUpdate, s);
+       ap_.p, L0.const_vol ? nullptr : A.vol, L0.vol0, fpartial_.p, fpartial2_.p, counters_.p + kCgUpdate, s);
     if (precision == 0) {
         enqueue_vcycle<double>(r_.p, &s->rsum, mean);
         go(k_cg_z<double>, fold_grid(k_cg_z<double>, kThreads, blocks_for((n + 3) / 4), kMaxGrid), kThreads, 0, n,
