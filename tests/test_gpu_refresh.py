@@ -90,6 +90,27 @@ def test_device_refresh_matches_host_refresh(case, lu, monkeypatch):
 
 
 @pytest.mark.parametrize("case", ["pruned_b8", "droplet_l2"])
+def test_lu_forms_agree_bitwise(case, monkeypatch):
+    """The cluster LU and the one-CTA LU apply the same operations to every
+    element in the same order, so the refreshed V-cycles agree bit for bit."""
+    spec, coarse = CASES[case]
+    m = BlockTreeMesh(**spec)
+    k1, k2 = coefficients(m, 1), coefficients(m, 2)
+    r = zero_mean_residual(m, 3)
+    out = []
+    for one_cta in (False, True):
+        if one_cta:
+            monkeypatch.setenv("TPAGMG_LU_ONE_CTA", "1")
+        s = solver(m, k1, coarse)
+        s.vcycle(r)
+        s.refresh(k2)
+        assert s.last_refresh()[0] == "device"
+        out.append(s.vcycle(r, "fp64"))
+    monkeypatch.delenv("TPAGMG_LU_ONE_CTA")
+    assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("case", ["pruned_b8", "droplet_l2"])
 def test_device_refresh_solves_match_oracle(case):
     """A chain of device refreshes, then solves at the last coefficients agree
     with the oracle's hierarchy built on them."""
