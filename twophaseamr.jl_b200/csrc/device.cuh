@@ -202,6 +202,9 @@ public:
 private:
     void build_views();
     template <typename T> void enqueue_vcycle(const double* r, const double* rsum, double* mean_out);
+    template <typename T, typename Epi>
+    void enqueue_vcycle_epi(const double* r, const double* rsum, double* mean_out, const Epi& epi);
+    bool rz_foldable() const;
     // CG from the current xw_/b_: returns iterations and flags (Krylov.jl cg! loop)
     void cg_fused(int precision, double target, int itmax, int& niter, int& flags);
     void vcycle_fused(const double* r, double* z, int precision);

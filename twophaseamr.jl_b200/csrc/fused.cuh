@@ -137,6 +137,58 @@ __device__ __forceinline__ bool publish_partial(double v, double* partial, unsig
     return last;
 }
 
+// publish_partial of two block sums (v into p1, w into p2) under one counter
+__device__ __forceinline__ bool publish_partial2(double v, double w, double* p1, double* p2, unsigned* counter) {
+    __shared__ bool last;
+    v = block_sum_all(v);
+    w = block_sum_all(w);
+    if (threadIdx.x == 0) {
+        p1[blockIdx.x] = v;
+        p2[blockIdx.x] = w;
+        __threadfence();
+        unsigned t = atomicAdd(counter, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    return last;
+}
+
+// Epilogue of the finest level's last post-smoothing, which folds the volume
+// mean of x: nothing more (MeanOnly), or -- inside the CG loop -- also the sum
+// of r_i x_i, handed with the mean to the CG's own step (kRz), so that r'z of
+// z = x - mean needs no pass of its own.
+struct MeanOnly {
+    static constexpr bool kRz = false;
+    const double* r = nullptr;
+    double* partial = nullptr;
+    __device__ void operator()(double, double) const {}
+};
+
+// The last block folds sum V x (partial) and, with kRz, sum r x (epi.partial);
+// thread 0 writes the mean and calls the epilogue.
+template <typename Epi>
+__device__ __forceinline__ void fold_mean(double v, double w, double* partial, unsigned* counter, double* mean_out,
+                                          double cvol_inv, const Epi& epi) {
+    if constexpr (Epi::kRz) {
+        if (publish_partial2(v, w, partial, epi.partial, counter)) {
+            const double s = fold_partials(partial, gridDim.x);
+            const double rx = fold_partials(epi.partial, gridDim.x);
+            if (threadIdx.x == 0) {
+                const double mean = s * cvol_inv;
+                *mean_out = mean;
+                epi(mean, rx);
+                *counter = 0;
+            }
+        }
+    } else if (publish_partial(v, partial, counter)) {
+        const double s = fold_partials(partial, gridDim.x);
+        if (threadIdx.x == 0) {
+            *mean_out = s * cvol_inv;
+            *counter = 0;
+        }
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ T rowdot(const LevelView<T>& L, const T* v, int i) {
     T acc = T(0);
@@ -418,24 +470,18 @@ __global__ void k_post1(LevelView<T> L) {
 }
 
 // second post-sweep x = sweep(y); with `mean_out`, also the volume-weighted mean
-template <typename T>
-__global__ void k_post2(LevelView<T> L, double* partial, unsigned* counter, double* mean_out) {
+template <typename T, typename Epi = MeanOnly>
+__global__ void k_post2(LevelView<T> L, double* partial, unsigned* counter, double* mean_out, Epi epi = Epi()) {
     pdl_entry();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double v = 0;
+    double v = 0, w = 0;
     if (i < L.n) {
         sweep_cell(L, L.y, L.x, i);
-        v = double(L.vol[i]) * double(L.x[i]);
+        const double xi = double(L.x[i]);
+        v = double(L.vol[i]) * xi;
+        if constexpr (Epi::kRz) w = epi.r[i] * xi;
     }
-    if (mean_out) {
-        if (publish_partial(v, partial, counter)) {
-            double s = fold_partials(partial, gridDim.x);
-            if (threadIdx.x == 0) {
-                *mean_out = s * L.cvol_inv;
-                *counter = 0;
-            }
-        }
-    }
+    if (mean_out) fold_mean(v, w, partial, counter, mean_out, L.cvol_inv, epi);
 }
 
 // ---------------------------------------------------------------------------------

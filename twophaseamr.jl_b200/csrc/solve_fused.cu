@@ -290,6 +290,8 @@ void with_nxc(const SView<T>& S, F f) {
     else f(std::integral_constant<int, 0>{});
 }
 
+__device__ void cg_after_z(CgState* s, double g, int init, cudaGraphConditionalHandle handle, int set_cond);
+
 // gamma_next = r'z for z = x0 - mean (the V-cycle's output, not stored: the
 // next operator product forms z and p where it reads them) and the stopping
 // rules; `init` starts a run (gamma = r'z, iter 0: the first direction is z).
@@ -315,37 +317,58 @@ __global__ void k_cg_z(int n, const T* __restrict__ xv, const double* mean, cons
         double g = fold_partials(partial, gridDim.x);
         if (threadIdx.x == 0) {
             *counter = 0;
-            bool stop;
-            if (init) {
-                s->gamma = g;
-                s->pnorm2 = g;
-                s->rnorm = sqrt(g);
-                s->beta = 0;
-                s->iter = 0;
-                s->flags = g == 0 ? 8 : 0;
-                stop = g == 0 || s->itmax <= 0;
-            } else if (s->flags & 2) {
-                stop = true;  // zero curvature: the iteration is abandoned
-            } else {
-                double rnorm = sqrt(g);
-                s->rnorm = rnorm;
-                bool solved = rnorm + 1.0 <= 1.0;
-                if (!solved) {
-                    double beta = g / s->gamma;
-                    s->beta = beta;
-                    s->pnorm2 = g + beta * beta * s->pnorm2;
-                    s->gamma = g;
-                } else {
-                    s->flags |= 4;
-                }
-                s->iter += 1;
-                if (s->strong_max <= s->target) s->flags |= 1;
-                stop = solved || s->iter >= s->itmax || (s->flags & 1);
-            }
-            if (set_cond) cudaGraphSetConditional(handle, stop ? 0u : 1u);
+            cg_after_z(s, g, init, handle, set_cond);
         }
     }
 }
+
+// gamma_next = g = r'z: the stopping rules and beta (a run starts with `init`);
+// with `set_cond`, sets the graph loop condition.  One thread.
+__device__ void cg_after_z(CgState* s, double g, int init, cudaGraphConditionalHandle handle, int set_cond) {
+    bool stop;
+    if (init) {
+        s->gamma = g;
+        s->pnorm2 = g;
+        s->rnorm = sqrt(g);
+        s->beta = 0;
+        s->iter = 0;
+        s->flags = g == 0 ? 8 : 0;
+        stop = g == 0 || s->itmax <= 0;
+    } else if (s->flags & 2) {
+        stop = true;  // zero curvature: the iteration is abandoned
+    } else {
+        double rnorm = sqrt(g);
+        s->rnorm = rnorm;
+        bool solved = rnorm + 1.0 <= 1.0;
+        if (!solved) {
+            double beta = g / s->gamma;
+            s->beta = beta;
+            s->pnorm2 = g + beta * beta * s->pnorm2;
+            s->gamma = g;
+        } else {
+            s->flags |= 4;
+        }
+        s->iter += 1;
+        if (s->strong_max <= s->target) s->flags |= 1;
+        stop = solved || s->iter >= s->itmax || (s->flags & 1);
+    }
+    if (set_cond) cudaGraphSetConditional(handle, stop ? 0u : 1u);
+}
+
+// r'z folded into the finest post-smoothing of the CG loop's V-cycle:
+// r'z = sum r_i (x_i - mean) = sum r_i x_i - mean sum r_i, with sum r_i from
+// the x / r update (s->rsum)
+struct CgRz {
+    static constexpr bool kRz = true;
+    const double* r;
+    double* partial;
+    CgState* s;
+    cudaGraphConditionalHandle handle;
+    int set_cond;
+    __device__ void operator()(double mean, double rx) const {
+        cg_after_z(s, rx - mean * s->rsum, 0, handle, set_cond);
+    }
+};
 
 // The next search direction p = z + beta p_old, formed where the
 // operator product reads it: z_j = x_j - mean from the V-cycle's finest-level
@@ -547,8 +570,9 @@ void DeviceSolver::build_views() {
     }
     vd_dev_.upload(vd_.data(), vd_.size(), stream_);
     vf_dev_.upload(vf_.data(), vf_.size(), stream_);
+    // every folding launch has at most max(maxgrid, kMaxGrid) CTAs
     fpartial_.alloc(size_t(std::max<int64_t>(maxgrid, kMaxGrid)));
-    fpartial2_.alloc(size_t(maxgrid));
+    fpartial2_.alloc(size_t(std::max<int64_t>(maxgrid, kMaxGrid)));
     lsum_.alloc(size_t(nl + 2));
     xw_.alloc(size_t(levels_[0].n));
     counters_.alloc(16);
@@ -578,6 +602,14 @@ void DeviceSolver::destroy_graphs() {
 // (device pointer); result in view 0's x, level-0 mean in *mean_out.
 template <typename T>
 void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* mean_out) {
+    enqueue_vcycle_epi<T>(r, rsum, mean_out, MeanOnly());
+}
+
+// The same, with `epi` run by the finest level's last post-smoothing after it
+// folds the mean (see MeanOnly).  The caller checks rz_foldable() first when
+// the epilogue must run.
+template <typename T, typename Epi>
+void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, double* mean_out, const Epi& epi) {
     const Launch go{stream_, pdl_};
     const int nl = int(levels_.size());
     const int t = tail_first_;
@@ -682,13 +714,12 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
             const int groups = (S.nblocks + 3) / 4;
             const bool want_mean = (l == 0) && L.singular;
             go(v_prolong<T>, groups, 256, 0, S, V[size_t(l + 1)].x);
-            go(v_sweep<T, false>, groups, 256, 0, S, S.x, S.y, nullptr, nullptr, nullptr);
+            go(v_sweep<T, false>, groups, 256, 0, S, S.x, S.y, nullptr, nullptr, nullptr, MeanOnly());
             if (want_mean)
-                go(v_sweep<T, true>, fold_grid(v_sweep<T, true>, 256, groups, kMaxGrid), 256, 0, S, S.y, S.x,
-                   fpartial_.p,
-                   counters_.p + kPostMean, mean_out);
+                go(v_sweep<T, true, Epi>, fold_grid(v_sweep<T, true, Epi>, 256, groups, kMaxGrid), 256, 0, S, S.y,
+                   S.x, fpartial_.p, counters_.p + kPostMean, mean_out, epi);
             else
-                go(v_sweep<T, false>, groups, 256, 0, S, S.y, S.x, nullptr, nullptr, nullptr);
+                go(v_sweep<T, false>, groups, 256, 0, S, S.y, S.x, nullptr, nullptr, nullptr, MeanOnly());
             launches_ += 3;
             continue;
         }
@@ -700,8 +731,8 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
                 constexpr int N = decltype(nxc)::value;
                 go(s_prolong<T, N>, g, th, 0, S, V[size_t(l + 1)].x);
                 go(s_post1<T, N>, g, th, 0, S);
-                go(s_post2<T, N>, want_mean ? fold_grid(s_post2<T, N>, th, g, kMaxGrid) : g, th, 0,
-                    S, fpartial_.p, counters_.p + kPostMean, want_mean ? mean_out : nullptr);
+                go(s_post2<T, N, Epi>, want_mean ? fold_grid(s_post2<T, N, Epi>, th, g, kMaxGrid) : g, th, 0, S,
+                   fpartial_.p, counters_.p + kPostMean, want_mean ? mean_out : nullptr, epi);
             });
             launches_ += 3;
             continue;
@@ -727,8 +758,8 @@ void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* m
         }
         go(k_post1<T>, blocks_for(L.n), kThreads, 0, L);
         const bool want_mean = (l == 0) && L.singular;
-        go(k_post2<T>, blocks_for(L.n), kThreads, 0, L, fpartial_.p, counters_.p + kPostMean,
-                                                              want_mean ? mean_out : nullptr);
+        go(k_post2<T, Epi>, blocks_for(L.n), kThreads, 0, L, fpartial_.p, counters_.p + kPostMean,
+           want_mean ? mean_out : nullptr, epi);
         launches_ += 3;
     }
     if (!V[0].singular) TPA_CUDA(cudaMemsetAsync(mean_out, 0, sizeof(double), stream_));
@@ -788,7 +819,12 @@ void DeviceSolver::enqueue_cg_body(int precision, cudaGraphConditionalHandle han
     const DevLevel& L0 = levels_[0];
     go(k_cg_update, fold_grid(k_cg_update, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, xw_.p, r_.p, pa, pb,
        ap_.p, L0.const_vol ? nullptr : A.vol, L0.vol0, fpartial_.p, fpartial2_.p, counters_.p + kCgUpdate, s);
-    if (precision == 0) {
+    if (rz_foldable()) {
+        // r'z and the stopping rules in the V-cycle's last kernel
+        const CgRz epi{r_.p, fpartial2_.p, s, handle, set_cond};
+        if (precision == 0) enqueue_vcycle_epi<double>(r_.p, &s->rsum, mean, epi);
+        else enqueue_vcycle_epi<float>(r_.p, &s->rsum, mean, epi);
+    } else if (precision == 0) {
         enqueue_vcycle<double>(r_.p, &s->rsum, mean);
         go(k_cg_z<double>, fold_grid(k_cg_z<double>, kThreads, blocks_for((n + 3) / 4), kMaxGrid), kThreads, 0, n,
            vd_[0].x, mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 0, handle, set_cond);
@@ -798,6 +834,19 @@ void DeviceSolver::enqueue_cg_body(int precision, cudaGraphConditionalHandle han
            vf_[0].x, mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 0, handle, set_cond);
     }
     TPA_CUDA(cudaGetLastError());
+}
+
+// The finest level is a CSR level swept by the multi-CTA kernels (not the tail
+// or the cooperative cycle), with the damped-Jacobi post-smoothing, and is
+// singular (its last post-smoothing folds the mean): r'z can ride on that fold.
+// The structured and vectorized post-smoothings can carry it too (s_post2,
+// v_sweep take the epilogue), but their folding grids are capped and stride
+// over the level.  On the vectorized 2048^2 level the extra r stream cost more
+// than the separate pass it replaces (3.35 -> 3.38 ms), and the structured
+// kernel, with the same capped grid, is left out with it.  The CSR
+// post-smoothing has one thread per cell and gains (droplet: 2.56 -> 2.49 ms).
+bool DeviceSolver::rz_foldable() const {
+    return tail_first_ > 0 && coop_grid_ == 0 && !rb_ && levels_[0].ncomp == 1 && !sdev_.empty() && !sdev_[0].on;
 }
 
 cudaGraphExec_t DeviceSolver::cg_graph(int precision) {
@@ -824,7 +873,8 @@ cudaGraphExec_t DeviceSolver::cg_graph(int precision) {
     cudaGraph_t captured;
     cudaError_t ce = cudaStreamEndCapture(stream_, &captured);
     stream_ = saved;
-    graph_body_launches_[precision] = launches_ - saved_launches + 3;  // + direction/Ap, update, z
+    // + direction/Ap, update and (unless folded) z
+    graph_body_launches_[precision] = launches_ - saved_launches + (rz_foldable() ? 2 : 3);
     launches_ = saved_launches;
     if (ce != cudaSuccess) {
         cudaGraphDestroy(g);

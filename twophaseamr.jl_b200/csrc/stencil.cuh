@@ -204,26 +204,19 @@ __global__ void s_post1(SView<T> L) {
     L.y[c] = x[c] + L.w * s_dinv(L, c) * (L.bp[c] - s_apply<NXC>(L, b, i, j, c, [&](int q) { return x[q]; }));
 }
 
-template <typename T, int NXC>
-__global__ void s_post2(SView<T> L, double* partial, unsigned* counter, double* mean_out) {
+template <typename T, int NXC, typename Epi = MeanOnly>
+__global__ void s_post2(SView<T> L, double* partial, unsigned* counter, double* mean_out, Epi epi = Epi()) {
     pdl_entry();
     const T* y = L.y;
-    double part = 0;
+    double part = 0, rx = 0;
     for (int b = blockIdx.x; b < L.nblocks; b += gridDim.x) {
         TPA_S_CELL(b);
         T v = y[c] + L.w * s_dinv(L, c) * (L.bp[c] - s_apply<NXC>(L, b, i, j, c, [&](int q) { return y[q]; }));
         L.x[c] = v;
         part += double(L.vol[c]) * double(v);
+        if constexpr (Epi::kRz) rx += epi.r[c] * double(v);
     }
-    if (mean_out) {
-        if (publish_partial(part, partial, counter)) {
-            double s = fold_partials(partial, gridDim.x);
-            if (threadIdx.x == 0) {
-                *mean_out = s * L.cvol_inv;
-                *counter = 0;
-            }
-        }
-    }
+    if (mean_out) fold_mean(part, rx, partial, counter, mean_out, L.cvol_inv, epi);
 }
 
 // y = A x on the finest level with the partial x'y, folded by `fold(sum)` in the

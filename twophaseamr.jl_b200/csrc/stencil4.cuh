@@ -369,12 +369,13 @@ __global__ void __launch_bounds__(256) v_prolong(SView<T> L, const T* __restrict
 
 // out = in + w D^-1 (bp - A in); with `partial`, folds the volume-weighted sum of
 // out into mean_out (times cvol_inv)
-template <typename T, bool Fold>
+template <typename T, bool Fold, typename Epi = MeanOnly>
 __global__ void __launch_bounds__(256) v_sweep(SView<T> L, const T* __restrict__ in, T* __restrict__ out,
-                                               double* partial, unsigned* counter, double* mean_out) {
+                                               double* partial, unsigned* counter, double* mean_out,
+                                               Epi epi = Epi()) {
     pdl_entry();
     const int groups = (L.nblocks + 3) / 4;
-    double part = 0;
+    double part = 0, rx = 0;
     TPA_Q_LOOP(groups) {
         const QPos p = q_pos(grp);
         const bool valid = p.b < L.nblocks;
@@ -389,17 +390,13 @@ __global__ void __launch_bounds__(256) v_sweep(SView<T> L, const T* __restrict__
         if (Fold && mean_out) {
             const Quad<T> v = L.const_vol ? Quad<T>{{L.vol0, L.vol0, L.vol0, L.vol0}} : q_ld(L.vol + p.c);
             for (int m = 0; m < 4; ++m) part += double(v.v[m]) * double(o.v[m]);
-        }
-    }
-    if (Fold && mean_out) {
-        if (publish_partial(part, partial, counter)) {
-            const double s = fold_partials(partial, gridDim.x);
-            if (threadIdx.x == 0) {
-                *mean_out = s * L.cvol_inv;
-                *counter = 0;
+            if constexpr (Epi::kRz) {
+                const Quad<double> rq = q_ldv(epi.r + p.c);
+                for (int m = 0; m < 4; ++m) rx += rq.v[m] * double(o.v[m]);
             }
         }
     }
+    if (Fold && mean_out) fold_mean(part, rx, partial, counter, mean_out, L.cvol_inv, epi);
 }
 
 // finest level, FP64: y = A x with x'y folded by `fold`
