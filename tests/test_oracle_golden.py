@@ -246,3 +246,72 @@ def test_preconditioned_and_plain_cg():
     q, plain = solve(op, None, rhs, rtol=1e-8, max_cycles=500, preconditioner=False)
     assert plain.converged and plain.preconditioner == "none"
     assert st.cycles < plain.cycles
+
+
+class _ComponentLevel:
+    """The level data the multigrid component projections read: per-cell
+    component slots (-1: inactive), volumes and per-component volumes."""
+
+    def __init__(self, slots, volumes, component_volumes):
+        self.slots = slots
+        self.volumes = volumes
+        self.component_volumes = component_volumes
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("n", [19, 4 * 1024 + 17])
+def test_multigrid_component_projections(dtype, n):
+    """test/operators/poisson.jl:1245-1357: `_multigrid_remove_component_means!`
+    and `_multigrid_project_component_rhs!` on interleaved components with
+    inactive cells: the expected projections to 64 eps, zero component sums,
+    idempotence, Q and Q' adjoint (256 eps), inactive entries (also non-finite
+    ones) untouched, and nothing done on a completely inactive level."""
+    from oracle.multigrid import Level
+    eps = np.finfo(dtype).eps
+    cells = np.arange(1, n + 1)
+    index = np.where(cells == n, 4, np.where(cells % 17 == 0, 0, (cells - 1) % 3 + 1))
+    volumes = np.where(index == 0, 0, (1 + (5 * cells) % 7) / 8).astype(dtype)
+    groups = [np.nonzero(index == c)[0] for c in range(1, 5)]
+    inactive = np.nonzero(index == 0)[0]
+    active = np.nonzero(index != 0)[0]
+    level = _ComponentLevel(index - 1, volumes, np.array([volumes[g].sum() for g in groups], dtype=dtype))
+    solution = (((7 * cells) % 31 - 13) / 8).astype(dtype)
+    rhs = (((11 * cells) % 37 - 17) / 16).astype(dtype)
+    exp_x, exp_b = solution.copy(), rhs.copy()
+    for g in groups:
+        vol = volumes[g].sum()
+        exp_x[g] -= np.dot(volumes[g], solution[g]) / vol
+        exp_b[g] -= volumes[g] * (rhs[g].sum() / vol)
+    remove = lambda v: Level.remove_means(level, v)  # noqa: E731
+    project = lambda v: Level.project_rhs(level, v)  # noqa: E731
+    px, pb = remove(solution.copy()), project(rhs.copy())
+    tol = 64 * eps
+    assert np.allclose(px, exp_x, rtol=tol, atol=tol) and np.allclose(pb, exp_b, rtol=tol, atol=tol)
+    assert np.array_equal(px[inactive], solution[inactive]) and np.array_equal(pb[inactive], rhs[inactive])
+    for g in groups:
+        assert abs(np.dot(volumes[g], px[g])) <= tol * max(np.sum(np.abs(volumes[g] * solution[g])), 1)
+        assert abs(np.sum(pb[g])) <= tol * max(np.sum(np.abs(rhs[g])), 1)
+    assert np.allclose(remove(px.copy()), px, rtol=tol, atol=tol)
+    assert np.allclose(project(pb.copy()), pb, rtol=tol, atol=tol)
+    big = 256 * eps * max(np.sqrt(float(np.dot(solution, solution)) * float(np.dot(rhs, rhs))), 1)
+    assert np.isclose(np.dot(px, rhs), np.dot(solution, pb), rtol=256 * eps, atol=big)
+    normal_x = project(px.copy())
+    normal_b = project(remove(rhs.copy()))
+    assert np.isclose(np.dot(solution, normal_b), np.dot(rhs, normal_x), rtol=256 * eps, atol=big)
+    assert np.isclose(np.dot(solution, normal_x), np.dot(px, px), rtol=256 * eps, atol=big)
+    assert np.dot(solution, normal_x) > 0
+    # covered entries are neither read nor overwritten
+    sentinels = [dtype(np.nan), dtype(np.inf), dtype(-np.inf), dtype(-0.0)]
+    for fn, source, expected in ((remove, solution, px), (project, rhs, pb)):
+        v = source.copy()
+        v[inactive] = [sentinels[k % 4] for k in range(len(inactive))]
+        out = fn(v.copy())
+        assert np.array_equal(out[inactive], v[inactive], equal_nan=True)
+        assert np.array_equal(np.signbit(out[inactive]), np.signbit(v[inactive]))
+        assert np.allclose(out[active], expected[active], rtol=tol, atol=tol)
+    # a completely inactive level has nothing to normalise
+    empty = _ComponentLevel(np.full(n, -1), np.zeros(n, dtype=dtype), np.zeros(0, dtype=dtype))
+    v = solution.copy()
+    v[0] = np.nan
+    for fn in (Level.remove_means, Level.project_rhs):
+        assert np.array_equal(fn(empty, v.copy()), v, equal_nan=True)
