@@ -120,7 +120,9 @@ __device__ __forceinline__ void alpha_from(double pAp, CgState* s) {
     }
 }
 
-// Ap = A p and alpha = gamma / p'Ap with the zero-curvature guard
+// Ap = A p and alpha = gamma / p'Ap with the zero-curvature guard: the CG
+// operator product alone, as time_fused times it (the CG loop runs the
+// *_cg_dir_ap kernels, which also form p)
 __global__ void k_cg_ap(LevelView<double> A, const double* __restrict__ p, double* __restrict__ ap, double* partial,
                         unsigned* counter, CgState* s) {
     pdl_entry();
