@@ -195,6 +195,16 @@ def batch_main(args):
         return st[0]["device_ms"], [s["cycles"] for s in st], st[0]["kernel_launches"]
 
     step = step_merged if merged else step_streams
+    if args.profile:
+        # only W warm-up and K mixed solves of the batch (for ncu launch lists)
+        launches = 0
+        for _ in range(args.warmup + args.steps):
+            launches += step("mixed")[2]
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"profile": f"batch_{args.batch} mixed", "solves": args.steps,
+                              "kernel_launches": launches}))
+        return 0
     streams_ms = None
     if merged:
         # the per-problem-stream path on the same problems, for comparison

@@ -8,6 +8,7 @@
 #include "batch.hpp"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 
@@ -644,7 +645,7 @@ void BatchSolver::enqueue_z(int precision, int init) {
     ++launches_;
 }
 
-void BatchSolver::enqueue_body(int precision, cudaGraphConditionalHandle handle) {
+void BatchSolver::enqueue_body(int precision, cudaGraphConditionalHandle handle, bool in_graph) {
     const Launch go{stream_, true};
     BState* st = state_.p;
     const FineCsr A{frp_.p, fci_.p, fval_.p, fvol_.p};
@@ -658,8 +659,11 @@ void BatchSolver::enqueue_body(int precision, cudaGraphConditionalHandle handle)
     else enqueue_vcycle<float>(r_.p);
     enqueue_z(precision, 0);
     go(bk_cg_p, nfi_, kItemRows, 0, fitems_.p, p_.p, z_.p, st, active_.p);
-    go(bk_cg_cond, 1, 256, 0, active_.p, K_, handle);
-    launches_ += 2;
+    ++launches_;
+    if (in_graph) {
+        go(bk_cg_cond, 1, 256, 0, active_.p, K_, handle);
+        ++launches_;
+    }
 }
 
 cudaGraphExec_t BatchSolver::graph(int precision) {
@@ -682,7 +686,7 @@ cudaGraphExec_t BatchSolver::graph(int precision) {
     stream_ = own_stream_;
     const int before = launches_;
     TPA_CUDA(cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    enqueue_body(precision, handle);
+    enqueue_body(precision, handle, true);
     cudaGraph_t captured;
     cudaError_t ce = cudaStreamEndCapture(stream_, &captured);
     stream_ = saved;
@@ -848,9 +852,23 @@ void BatchSolver::solve(const double* rhs, double* x_user, double rtol, double a
         std::vector<int> act(static_cast<size_t>(K));
         TPA_CUDA(cudaMemcpyAsync(act.data(), active_.p, size_t(K) * sizeof(int), cudaMemcpyDeviceToHost, stream_));
         TPA_CUDA(cudaStreamSynchronize(stream_));
+        const bool no_graph = std::getenv("TPAGMG_NO_GRAPH") != nullptr;
         if (std::any_of(act.begin(), act.end(), [](int v) { return v != 0; })) {
-            cudaGraphExec_t exec = graph(precision);
-            TPA_CUDA(cudaGraphLaunch(exec, stream_));
+            if (no_graph) {
+                // the same body launched kernel by kernel, the loop condition
+                // read on the host after each body (profiling and diagnosis);
+                // every problem stops within its iteration limit
+                for (int body = 0; body <= max_cycles; ++body) {
+                    enqueue_body(precision, cudaGraphConditionalHandle(), false);
+                    TPA_CUDA(cudaMemcpyAsync(act.data(), active_.p, size_t(K) * sizeof(int), cudaMemcpyDeviceToHost,
+                                             stream_));
+                    TPA_CUDA(cudaStreamSynchronize(stream_));
+                    if (std::none_of(act.begin(), act.end(), [](int v) { return v != 0; })) break;
+                }
+            } else {
+                cudaGraphExec_t exec = graph(precision);
+                TPA_CUDA(cudaGraphLaunch(exec, stream_));
+            }
         }
         std::vector<BState> hs(static_cast<size_t>(K));
         TPA_CUDA(cudaMemcpyAsync(hs.data(), st, size_t(K) * sizeof(BState), cudaMemcpyDeviceToHost, stream_));
@@ -858,7 +876,7 @@ void BatchSolver::solve(const double* rhs, double* x_user, double rtol, double a
         int max_iter = 0;
         for (int k = 0; k < K; ++k)
             if (run[size_t(k)]) max_iter = std::max(max_iter, hs[size_t(k)].iter + ((hs[size_t(k)].flags & 2) ? 1 : 0));
-        launches_ += max_iter * body_launches_[precision];
+        if (!no_graph) launches_ += max_iter * body_launches_[precision];
         remove_means(run);
         std::vector<double> fin, fl;
         residual_norms(fin, nullptr);

@@ -54,7 +54,7 @@ private:
     void build(const std::vector<const Hierarchy*>& hierarchies);
     template <typename T> void enqueue_vcycle(const double* r);
     void enqueue_z(int precision, int init);
-    void enqueue_body(int precision, cudaGraphConditionalHandle handle);
+    void enqueue_body(int precision, cudaGraphConditionalHandle handle, bool in_graph);
     cudaGraphExec_t graph(int precision);
     double total_volume(int k) const;
 
