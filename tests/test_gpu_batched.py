@@ -161,3 +161,37 @@ def test_merged_batch_after_device_refresh():
     ref, _ = osolve(oo, TreeGeometricMultigrid(oo, OMG()), rhs, rtol=1e-12)
     x0 = bs.split(x)[0]
     assert np.max(np.abs(x0 - ref)) <= 1e-10 * np.max(np.abs(ref))
+
+
+def test_merged_batch_host_driven_loop_matches_graph(monkeypatch):
+    """TPAGMG_NO_GRAPH (kernel-by-kernel Krylov loop, condition read on the host;
+    the profiling mode) runs the same kernels in the same order as the graph's
+    WHILE loop: bit-identical solutions and iteration counts."""
+    probs = make(small(4) + [p for p in W.batch_problems() if p["depth"] == 4][:2])
+    bs = BatchedSolver([s for *_, s in probs])
+    rhs = bs.concat([r for _, _, _, r, _ in probs])
+    x1 = np.zeros(bs.ncells)
+    st1 = bs.solve(x1, rhs, rtol=1e-10)
+    monkeypatch.setenv("TPAGMG_NO_GRAPH", "1")
+    x2 = np.zeros(bs.ncells)
+    st2 = bs.solve(x2, rhs, rtol=1e-10)
+    monkeypatch.delenv("TPAGMG_NO_GRAPH")
+    assert [s["cycles"] for s in st1] == [s["cycles"] for s in st2]
+    assert np.array_equal(x1, x2)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_single_solve_host_driven_loop_matches_graph(precision, monkeypatch):
+    """The same for one solve (graph WHILE loop against kernel-by-kernel)."""
+    p = [q for q in W.batch_problems() if q["depth"] == 4][0]
+    m = BlockTreeMesh(**W.batch_spec(p))
+    kappa, rhs = W.batch_inputs(m, p)
+    s = EllipticSolver(PoissonOperator(m, kappa), preconditioner_options={"precision": precision})
+    x1 = np.zeros(m.ncells)
+    st1 = solve(x1, s, rhs, rtol=1e-10)
+    monkeypatch.setenv("TPAGMG_NO_GRAPH", "1")
+    x2 = np.zeros(m.ncells)
+    st2 = solve(x2, s, rhs, rtol=1e-10)
+    monkeypatch.delenv("TPAGMG_NO_GRAPH")
+    assert st1.converged and st1.cycles == st2.cycles
+    assert np.array_equal(x1, x2)
