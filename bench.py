@@ -23,6 +23,7 @@ import os
 import pathlib
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -32,6 +33,8 @@ sys.path[:0] = [str(ROOT), str(ROOT / "twophaseamr.jl_b200")]
 
 RTOL = 1e-10
 HBM_FALLBACK = 6650.0
+# one metric string for both arms (the precision is carried by `dtype`)
+DROPLET_METRIC = "cell-updates/s to rel. residual 1e-10 (droplet AMR pressure solve)"
 
 
 def measured_peaks():
@@ -74,14 +77,16 @@ def reference_arm(args):
     from oracle import cgmg
     res = cgmg.bench_droplet(steps=args.steps, warmup=args.warmup, levels=args.levels)
     line = {
-        "impl": "reference", "metric": "cell-updates/s to rel. residual 1e-10 (droplet AMR pressure solve)",
+        "impl": "reference", "metric": DROPLET_METRIC,
         "value": res["cell_updates_per_s"], "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Philox)",
         "config": {"workload": f"droplet_amr levels={args.levels}", "fine_cells": res["cells"],
                    "cg_iterations": res["iterations"], "threads": res["threads"]},
         "cpu_baseline": {"value": res["cell_updates_per_s"], "unit": "cell-updates/s", "cores": res["threads"],
-                         "kind": "port", "sample": f"{args.steps} full solves of the droplet workload"},
+                         "kind": "port",
+                         "sample": f"median of {args.steps} warm full solves of the droplet workload "
+                                   f"({args.warmup} untimed), {res['threads']} OpenMP threads"},
         "e2e": {"value": res["cell_updates_per_s"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -94,12 +99,11 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        self.path = pathlib.Path(tempfile.gettempdir()) / f"tpagmg_clocks_{os.getpid()}.csv"
 
     def __enter__(self):
         self.t0 = time.perf_counter()
         try:
-            self.path.parent.mkdir(exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index),
@@ -553,12 +557,24 @@ def main():
                              "(all fields on the device; dt 1e-3, tolerance sqrt(eps))"}
         solver.refresh(kappa)
 
-    cpu = None
+    cpu, oracle_err = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "droplet_amr":
+        # the C/OpenMP restatement on this host's cores: the same measurement as
+        # `--impl reference` (median of warm solves), then the FP64 oracle
+        # solution of the very RHS the GPU solved, to rtol 1e-12, against which
+        # both GPU solutions (rtol 1e-10) are compared
         from oracle import cgmg
-        res = cgmg.bench_droplet(steps=1, warmup=0, levels=args.levels, threads=os.cpu_count())
+        problem = cgmg.droplet_problem(args.levels)
+        res = cgmg.bench_droplet(steps=10, warmup=3, threads=os.cpu_count(), problem=problem)
         cpu = {"value": res["cell_updates_per_s"], "unit": "cell-updates/s", "cores": res["threads"],
-               "kind": "port", "sample": "1 full solve of the same droplet workload (setup excluded)"}
+               "kind": "port", "sample": f"median of 10 warm full solves of the same droplet workload "
+                                         f"(3 untimed), {res['threads']} OpenMP threads, setup excluded"}
+        x_oracle, ost = res["runner"].solve(rhs_h, rtol=1e-12, threads=os.cpu_count())
+        ref_max = float(np.max(np.abs(x_oracle)))
+        oracle_err = {"mixed": float(np.max(np.abs(x_mixed.cpu().numpy() - x_oracle)) / ref_max),
+                      "fp64": float(np.max(np.abs(x_ref.cpu().numpy() - x_oracle)) / ref_max),
+                      "norm": "max |x_gpu - x_oracle| / max |x_oracle|",
+                      "oracle": f"C restatement solved to rtol 1e-12 ({ost.cycles} CG iterations) on the same RHS"}
     # DRAM bytes per launch of the roofline kernel from a committed ncu capture
     traffic = None
     tp = ROOT / "profiles" / "roofline_traffic.json"
@@ -570,7 +586,7 @@ def main():
     cells_updates = n * mixed_it
     value = world * cells_updates / (mixed_ms * 1e-3)
     if args.workload == "droplet_amr":
-        metric = "cell-updates/s to rel. residual 1e-10 (droplet AMR pressure solve, mixed FP32/FP64 GMG)"
+        metric = DROPLET_METRIC
         wname = f"droplet_amr levels={args.levels} (unit square, 4x4 roots of 16x16, circle band)"
     else:
         metric = f"cell-updates/s to rel. residual 1e-10 ({args.size}^2 uniform periodic solve, mixed FP32/FP64 GMG)"
@@ -588,6 +604,7 @@ def main():
         "cg_iterations": {"mixed": mixed_it, "fp64": fp64_it},
         "fp64_value": world * n * fp64_it / (fp64_ms * 1e-3),
         "mixed_error_vs_fp64": mixed_err,
+        "error_vs_fp64_oracle": oracle_err,
         "e2e": {"value": world * n * e2e_it / (e2e_ms_mean * 1e-3), "unit": "cell-updates/s",
                 "ms_per_step": e2e_ms_mean, "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 8 * n},
         "gpu_launches": mixed_launches,

@@ -272,20 +272,22 @@ tpa_status tpa_synchronize(tpa_context* ctx);
  * over cells of positive volume.  Uses the context's device scratch; out is a
  * host array. */
 tpa_status tpa_residual_norms(tpa_context* ctx, const double* r, double out[2]);
-/* The same two norms for callers that cannot allocate device memory (code
- * running under CUDA graph capture, memory owned by a pool or arena that must
- * not be bypassed, hosts that forbid runtime allocation).  This entry point has
- * no counterpart in the reference, which has no device code.  r and volumes
- * are device pointers of n cells on the current device; out is a host array.
- * It calls no cudaMalloc or cudaFree: its scratch is one static device array
- * of about 14 KiB, held by every GPU that loads this library until the process
- * exits.  n must lie in [1, 2^31 - 1]; larger sizes are rejected with
- * TPA_ERR_INVALID_ARG.  The first call on a device looks up the scratch's
- * device address and clears its counter, so make that first call before any
- * stream capture.  Every call shares the scratch: calls that overlap on the
- * GPU (from several threads or streams) race and must be serialised by the
- * caller.  The call runs on the legacy default stream and waits for it.  ctx
- * is used only for the error message and may be NULL. */
+/* The same two norms for callers that cannot allocate device memory (memory
+ * owned by a pool or arena that must not be bypassed, hosts that forbid
+ * runtime allocation).  This entry point has no counterpart in the reference,
+ * which has no device code.  r and volumes are device pointers of n cells on
+ * the current device; out is a host array.  It calls no cudaMalloc or
+ * cudaFree: its scratch is one static device array of about 14 KiB, held by
+ * every GPU that loads this library until the process exits.  n must lie in
+ * [1, 2^31 - 1]; other sizes are rejected with TPA_ERR_INVALID_ARG before any
+ * CUDA call.  The first call on a device looks up the scratch's device address
+ * (make that first call before any stream capture); the address is cached for
+ * the process and does not survive cudaDeviceReset.  Every call clears the
+ * scratch's counter, launches on the legacy default stream and waits for it
+ * (a synchronous copy of the two norms).  Every call shares the scratch: calls
+ * that overlap on the GPU (from several threads or streams) race and must be
+ * serialised by the caller.  ctx is used only for the error message and may
+ * be NULL. */
 tpa_status tpa_residual_norms_noalloc(tpa_context* ctx, const double* r, const double* volumes, int64_t n,
                                       double out[2]);
 /* Device layout of the uploaded hierarchy: out = {levels on the block-

@@ -147,9 +147,12 @@ def droplet_problem(levels=4):
     return mesh, op, mg, rhs
 
 
-def bench_droplet(steps=1, warmup=0, levels=4, threads=None):
+def bench_droplet(steps=10, warmup=3, levels=4, threads=None, problem=None):
+    """Time `steps` warm solves of the droplet workload (after `warmup`
+    untimed ones) with `threads` OpenMP threads; ms_per_step is their median.
+    `problem` is an already built `droplet_problem(levels)`."""
     threads = threads or os.cpu_count()
-    mesh, op, mg, rhs = droplet_problem(levels)
+    mesh, op, mg, rhs = problem or droplet_problem(levels)
     run = Runner(op, mg)
     for _ in range(warmup):
         run.solve(rhs, threads=threads)
@@ -160,6 +163,6 @@ def bench_droplet(steps=1, warmup=0, levels=4, threads=None):
         ts.append(time.perf_counter() - t0)
         its.append(st.cycles)
         assert st.converged
-    ms = 1e3 * float(np.mean(ts))
-    return {"cells": mesh.ncells, "iterations": float(np.mean(its)), "ms_per_step": ms, "threads": threads,
-            "cell_updates_per_s": mesh.ncells * float(np.mean(its)) / (ms * 1e-3)}
+    ms = 1e3 * float(np.median(ts))
+    return {"cells": mesh.ncells, "iterations": float(np.median(its)), "ms_per_step": ms, "threads": threads,
+            "cell_updates_per_s": mesh.ncells * float(np.median(its)) / (ms * 1e-3), "runner": run}

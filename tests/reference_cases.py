@@ -42,3 +42,51 @@ def harmonic_face_coefficients(mesh, cell_value):
     dp = mesh.spacing[mesh.face_plus // (nx * ny), a] / 2
     cm, cp = cell_value[mesh.face_minus], cell_value[mesh.face_plus]
     return (dm + dp) / (dm / cm + dp / cp)
+
+
+# Chapter 11 fixtures of the technical reference (docs/techref/figures/solvers.jl
+# of the reference): walls, 8x8 blocks, a drop circle and a deterministic noise RHS.
+TECHREF_CENTRE = (0.513, 0.468)   # SOLV_DROP, solvers.jl:19
+TECHREF_RADIUS = 0.2371
+TECHREF_BAND = 0.02
+TECHREF_DENSITY = (1000.0, 1.0)   # SOLV_DENSITY, solvers.jl:16
+
+
+def techref_noise(n):
+    """`solv_noise(index)` (solvers.jl:24) for the 1-based cell indices 1..n."""
+    idx = np.arange(1, n + 1, dtype=np.float64)
+    v = np.sin(12.9898 * idx) * 43758.5453
+    return v - np.floor(v) - 0.5
+
+
+def techref_uniform(n):
+    """`solv_uniform(n)` (solvers.jl:26-28)."""
+    return dict(base_mesh=(n, n), block_size=(8, 8), periodic=(False, False))
+
+
+def _techref_near_circle(origin, extent):
+    """`solv_near_circle` (solvers.jl:31-38): the block box comes within the band of the circle."""
+    xs = (origin[0], origin[0] + extent[0])
+    ys = (origin[1], origin[1] + extent[1])
+    cx, cy = TECHREF_CENTRE
+    nearest = np.hypot(min(max(cx, xs[0]), xs[1]) - cx, min(max(cy, ys[0]), ys[1]) - cy)
+    farthest = max(np.hypot(x - cx, y - cy) for x in xs for y in ys)
+    return nearest - TECHREF_BAND <= TECHREF_RADIUS <= farthest + TECHREF_BAND
+
+
+def techref_amr(n, levels=2):
+    """`solv_amr(n)` (solvers.jl:40-45)."""
+    return dict(base_mesh=(n, n), block_size=(8, 8), periodic=(False, False), max_level=levels,
+                refine=lambda k, o, e: _techref_near_circle(o, e))
+
+
+TECHREF_CASES = {
+    "uniform64": (techref_uniform, 64, False), "uniform128": (techref_uniform, 128, False),
+    "uniform256": (techref_uniform, 256, False), "amr32": (techref_amr, 32, False),
+    "amr64": (techref_amr, 64, False), "drop128": (techref_uniform, 128, True),
+    "dropamr": (techref_amr, 64, True),
+}
+TECHREF_VCYCLE_CASES = {
+    "uniform16": (techref_uniform, 16, False), "uniform32": (techref_uniform, 32, False),
+    "amr16": (techref_amr, 16, False), "drop32": (techref_uniform, 32, True),
+}

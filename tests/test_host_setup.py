@@ -110,3 +110,24 @@ def test_invalid_mesh_arguments():
         BlockTreeMesh(block_size=(3, 3))
     with pytest.raises(_lib.TpaError):
         BlockTreeMesh(base_mesh=(32, 32), block_size=(16, 16), leaves=[(0, 0, 0)])
+
+
+def test_noalloc_norms_reject_sizes_before_any_cuda_call():
+    """tpa_residual_norms_noalloc checks its size (1 <= n <= 2^31 - 1, the
+    library's 32-bit cell indices) and its pointers before touching the
+    device, so the rejection holds on a host without a GPU.  The pointers
+    passed here are never dereferenced."""
+    import ctypes as C
+    lib = _lib.lib()
+    ctx = _lib.Context(0)  # no CUDA call until the first device operation
+    out = np.zeros(2)
+    fake = C.c_void_p(256)
+    for n in (2 ** 31, 2 ** 40, 0, -5):
+        st = lib.tpa_residual_norms_noalloc(ctx.handle, fake, fake, n, out.ctypes.data_as(C.POINTER(C.c_double)))
+        assert st == _lib.TPA_ERR_INVALID_ARG
+        assert b"[1, 2147483647]" in lib.tpa_last_error(ctx.handle)
+    st = lib.tpa_residual_norms_noalloc(ctx.handle, None, fake, 10, out.ctypes.data_as(C.POINTER(C.c_double)))
+    assert st == _lib.TPA_ERR_INVALID_ARG
+    # without a context the status alone reports the rejection
+    assert lib.tpa_residual_norms_noalloc(None, fake, fake, 2 ** 31, out.ctypes.data_as(C.POINTER(C.c_double))) \
+        == _lib.TPA_ERR_INVALID_ARG

@@ -10,6 +10,9 @@ from oracle.mesh import block_tree_mesh
 from oracle.operator import PoissonOperator
 from oracle.multigrid import MultigridOptions, TreeGeometricMultigrid, jacobi_weight
 from oracle.krylov import solve
+from oracle import projection as OP
+from tpagmg import workloads as W
+import reference_cases as RC
 
 GOLD = json.loads((pathlib.Path(__file__).parent / "golden" / "known_answers.json").read_text())
 
@@ -36,8 +39,12 @@ def test_manufactured_errors_match_published_table(row):
     l2 = np.sqrt(np.sum(v * err ** 2) / np.sum(v))
     assert float(f"{l2:.3e}") == row["l2"]
     assert float(f"{err.max():.3e}") == row["linf"]
-    # The published PCG counts are not asserted by the reference's own test
-    # (which checks a spread <= 3); this restatement takes at most two more.
+    # The PCG column of this hand-written table (8/8/9) is not asserted by the
+    # reference's own test (test/operators/poisson.jl:820-831 checks a spread
+    # <= 3), and it disagrees with the reference's machine-generated solver
+    # checks: the restatement reproduces those exactly on seven solves and four
+    # V-cycle spectra (`test_techref_*` below), and takes 9/10/10 here.
+    assert st.cycles == {4: 9, 8: 10, 16: 10}[row["block"]]
     assert row["pcg_iterations"] <= st.cycles <= row["pcg_iterations"] + 2
 
 
@@ -315,3 +322,93 @@ def test_multigrid_component_projections(dtype, n):
     v[0] = np.nan
     for fn in (Level.remove_means, Level.project_rhs):
         assert np.array_equal(fn(empty, v.copy()), v, equal_nan=True)
+
+
+TECH = GOLD["techref_pressure_solves"]
+
+
+def techref_operator(maker, n, drop):
+    """A fixture of the reference's Chapter 11 solver checks: the mesh and the
+    operator (kappa = 1, or 1/rho_f of the drop's mixture density)."""
+    mesh = block_tree_mesh(**maker(n))
+    if drop:
+        frac = W.circle_fractions(mesh, RC.TECHREF_CENTRE, RC.TECHREF_RADIUS)
+        _, cond = OP.conditional_fraction(frac)
+        return mesh, PoissonOperator(mesh, OP.face_coefficients(mesh, cond, RC.TECHREF_DENSITY))
+    return mesh, PoissonOperator(mesh)
+
+
+@pytest.mark.parametrize("name", list(RC.TECHREF_CASES))
+def test_techref_preconditioned_solves(name):
+    """`solv_poisson` (docs/techref/figures/solvers.jl:72-93) on the cases of
+    `solv_pressure_cases` (:95-113): unknowns, levels, PCG iterations and the
+    convergence factor (final_l2 / initial_l2)^(1/cycles) that the reference's
+    own run wrote into checks.tex (chkSolv*Cycles/Factor/Levels/Unknowns).
+    These pin the V-cycle and the Krylov loop with its strong-residual stop."""
+    ref = TECH["solves"][name]
+    mesh, op = techref_operator(*RC.TECHREF_CASES[name])
+    mg = TreeGeometricMultigrid(op, MultigridOptions())
+    _, st = solve(op, mg, RC.techref_noise(mesh.ncells), rtol=1e-10, max_cycles=20000)
+    assert st.converged
+    assert mesh.ncells == ref["unknowns"]
+    assert len(mg.levels) == ref["levels"]
+    assert st.cycles == ref["cycles"]
+    factor = (st.final_l2 / st.initial_l2) ** (1.0 / st.cycles)
+    assert f"{factor:.2f}" == ref["factor"]
+    assert f"{mg.levels[0].weight:.3f}" == TECH["omega_uniform128"]
+
+
+@pytest.mark.parametrize("name", ["uniform64", "uniform128", "amr32", "amr64", "drop128"])
+def test_techref_plain_cg(name):
+    """The same solves without a preconditioner (chkSolv*Plain): the restated
+    Krylov.jl `cg!` recurrence takes exactly the reference's iteration counts
+    on the constant-coefficient cases.  At density ratio 1000 thousands of
+    unpreconditioned iterations amplify rounding (dot-product order, the
+    circle fractions to 1e-10), so the count agrees to 1 %."""
+    ref = TECH["solves"][name]
+    mesh, op = techref_operator(*RC.TECHREF_CASES[name])
+    _, st = solve(op, None, RC.techref_noise(mesh.ncells), rtol=1e-10, max_cycles=20000, preconditioner=False)
+    assert st.converged
+    if name.startswith("drop"):
+        assert abs(st.cycles - ref["plain_cycles"]) <= 0.01 * ref["plain_cycles"]
+    else:
+        assert st.cycles == ref["plain_cycles"]
+
+
+def test_techref_vcycle_spectra():
+    """`solv_vcycle_check` (solvers.jl:117-165): the V-cycle as a matrix B on
+    the compatible subspace, the spectrum of L'(Z'BZ)L with Z'AZ = LL', its
+    condition number kappa (chkSolvKappa*), the CG bound (sqrt(kappa) - 1) /
+    (sqrt(kappa) + 1), the symmetry of B and the PCG count of each case."""
+    import scipy.linalg as sl
+    lam_min, lam_max = np.inf, 0.0
+    for name, case in RC.TECHREF_VCYCLE_CASES.items():
+        ref = TECH["vcycle"][name]
+        mesh, op = techref_operator(*case)
+        mg = TreeGeometricMultigrid(op, MultigridOptions())
+        n = mesh.ncells
+        B = np.empty((n, n))
+        for j in range(n):
+            e = np.zeros(n)
+            e[j] = 1.0
+            B[:, j] = mg.ldiv(e)
+        Z = sl.null_space(op.volumes[None, :])
+        L = np.linalg.cholesky(Z.T @ op.matrix.toarray() @ Z)
+        M = L.T @ (Z.T @ B @ Z) @ L
+        lam = np.linalg.eigvalsh((M + M.T) / 2)
+        kappa = lam.max() / lam.min()
+        assert f"{kappa:.2f}" == ref["kappa"], name
+        assert np.max(np.abs(B - B.T)) <= 1e-14 * np.max(np.abs(B))
+        if "bound" in ref:
+            assert f"{(np.sqrt(kappa) - 1) / (np.sqrt(kappa) + 1):.2f}" == ref["bound"]
+        if "cells" in ref:
+            assert n == ref["cells"]
+        if "cycles" in ref:
+            _, st = solve(op, mg, RC.techref_noise(n), rtol=1e-10, max_cycles=20000)
+            assert st.cycles == ref["cycles"]
+            assert f"{(st.final_l2 / st.initial_l2) ** (1.0 / st.cycles):.2f}" == ref["factor"]
+        lam_min, lam_max = min(lam_min, lam.min()), max(lam_max, lam.max())
+    # the published extremes also cover an embedded-solid case that is not on
+    # this path; the four cases here lie inside them, the drop at the minimum
+    assert f"{lam_min:.3f}" == TECH["lambda_min_all"]
+    assert lam_max <= float(TECH["lambda_max_all"])

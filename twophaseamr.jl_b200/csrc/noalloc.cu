@@ -1,14 +1,18 @@
 // Residual norms without any device allocation.
 //
-// Some callers cannot call cudaMalloc: code running while a CUDA graph is being
-// captured around it, callers whose device memory is owned by a pool or
-// arena they must not bypass, or embedded hosts that forbid runtime
+// Some callers cannot call cudaMalloc: callers whose device memory is owned by
+// a pool or arena they must not bypass, and embedded hosts that forbid runtime
 // allocation.  `tpa_residual_norms_noalloc` gives them the two norms of
 // `_integrated_residual_norms` (src/solvers/multigrid/cycles.jl:210-221 in
 // ronaldremmerswaal/TwoPhaseAMR.jl) with all scratch in one file-scope
 // `__device__` array of fixed size (kNoAllocBlocks partial sums per norm, about
 // 14 KiB), which every GPU that loads this library holds until the process
 // exits.  No tpa_context state is used, so no hierarchy upload is triggered.
+//
+// Per call, on the legacy default stream: the fold counter is cleared with
+// cudaMemsetAsync (so a launch that was aborted, or two calls that overlapped,
+// cannot leave it nonzero for the next call), the kernel runs, and a
+// synchronous cudaMemcpy returns the two norms.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -32,7 +36,7 @@ struct NormsScratch {
     double vol[kNoAllocBlocks];
     double mx[kNoAllocBlocks];
     double result[2];
-    unsigned counter;  // blocks done; returned to zero by the last block
+    unsigned counter;  // blocks done; cleared by the host before every launch
 };
 
 // The scratch of every call on this device.  In host code this name is only a
@@ -40,13 +44,15 @@ struct NormsScratch {
 static __device__ __align__(256) NormsScratch g_norms_scratch;
 
 __global__ void __launch_bounds__(kNoAllocThreads)
-    k_norms_noalloc(const double* __restrict__ r, const double* __restrict__ vol, int n, NormsScratch* S) {
+    k_norms_noalloc(const double* __restrict__ r, const double* __restrict__ vol, int64_t n, NormsScratch* S) {
     __shared__ double sa[32], sv[32], sm[32];
     __shared__ int nan_seen;
     __shared__ bool last;
     double a = 0, v = 0, m = 0;
     bool nan = false;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    // 64-bit index: the grid stride must not overflow for n near the maximum
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
         const double V = vol[i];
         if (!(V > 0)) continue;
         const double s = r[i] / V;
@@ -93,7 +99,6 @@ __global__ void __launch_bounds__(kNoAllocThreads)
     if (threadIdx.x == 0) {
         S->result[0] = sqrt(fa / fv);
         S->result[1] = fm;
-        S->counter = 0;
     }
 }
 
@@ -132,7 +137,9 @@ extern "C" tpa_status tpa_residual_norms_noalloc(tpa_context* ctx, const double*
     NormsScratch* S = nullptr;
     {
         // Set-up, once per device with that device current: the device address
-        // of the static scratch, and its counter cleared.
+        // of the static scratch (the host-side name is only a stand-in).  The
+        // cached address belongs to this process's context on the device; it
+        // does not survive cudaDeviceReset.
         std::lock_guard<std::mutex> lock(g_setup_mutex);
         if (!g_scratch_ptr[dev]) {
             void* p = nullptr;
@@ -142,18 +149,16 @@ extern "C" tpa_status tpa_residual_norms_noalloc(tpa_context* ctx, const double*
                                    cudaGetErrorString(e));
                 return TPA_ERR_CUDA;
             }
-            e = cudaMemset(static_cast<char*>(p) + offsetof(NormsScratch, counter), 0, sizeof(unsigned));
-            if (e != cudaSuccess) {
-                set_error(ctx, std::string("tpa_residual_norms_noalloc: clearing the scratch failed: ") +
-                                   cudaGetErrorString(e));
-                return TPA_ERR_CUDA;
-            }
             g_scratch_ptr[dev] = static_cast<NormsScratch*>(p);
         }
         S = g_scratch_ptr[dev];
     }
-    k_norms_noalloc<<<kNoAllocBlocks, kNoAllocThreads>>>(r, volumes, int(n), S);
-    e = cudaGetLastError();
+    // the last-block fold needs a zero counter: cleared before every launch
+    e = cudaMemsetAsync(reinterpret_cast<char*>(S) + offsetof(NormsScratch, counter), 0, sizeof(unsigned), 0);
+    if (e == cudaSuccess) {
+        k_norms_noalloc<<<kNoAllocBlocks, kNoAllocThreads>>>(r, volumes, n, S);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess)
         e = cudaMemcpy(out, reinterpret_cast<const char*>(S) + offsetof(NormsScratch, result), 2 * sizeof(double),
                        cudaMemcpyDeviceToHost);
