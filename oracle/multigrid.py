@@ -22,6 +22,7 @@ factorization agrees to rounding).
 """
 from __future__ import annotations
 
+import bisect
 from dataclasses import dataclass
 
 import numpy as np
@@ -149,14 +150,21 @@ def face_coefficient_restriction(coarse, fine):
     lines = {}
     for f in range(fine.nfaces):
         lines.setdefault((int(fine.face_axis[f]), int(fn[f])), []).append((int(flo[f]), int(fhi[f]), f))
-    for v in lines.values():
+    starts = {}
+    for key, v in lines.items():
         v.sort(key=lambda t: t[0])
+        starts[key] = [t[0] for t in v]
     cn, clo, chi = coarse.face_lattice_geometry(lattice)
     ptr = [0]; idx = []; w = []
     for f in range(coarse.nfaces):
         lo, hi = int(clo[f]), int(chi[f])
         covered = 0
-        for (a, b, k) in lines.get((int(coarse.face_axis[f]), int(cn[f])), []):
+        key = (int(coarse.face_axis[f]), int(cn[f]))
+        line = lines.get(key, [])
+        # fine faces on a line are disjoint and sorted: start at the one that
+        # contains lo (the scan order, and so the sums, are unchanged)
+        first = max(bisect.bisect_right(starts[key], lo) - 1, 0) if line else 0
+        for (a, b, k) in line[first:]:
             if a >= hi:
                 break
             overlap = min(hi, b) - max(lo, a)
