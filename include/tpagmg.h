@@ -217,16 +217,19 @@ tpa_status tpa_batch_solve_device(tpa_batch* batch, const double* rhs, double* x
  * recomputed inside the restriction (one launch instead of two); persistent:
  * when every multi-CTA level is a CSR level, the whole V-cycle runs as one
  * cooperative launch with grid barriers (bounded waits; a barrier that gives up
- * makes the solve return TPA_ERR_TIMEOUT).  Every layout gives the same V-cycle
- * to rounding. */
+ * makes the solve return TPA_ERR_TIMEOUT); tiles: each CSR level of the
+ * multi-CTA part runs as two launches on haloed block tiles (both pre-sweeps,
+ * the residual and the restriction in one, the prolongation and both
+ * post-sweeps in the other; the halo is recomputed in each tile).  Every
+ * layout gives the same V-cycle to rounding. */
 typedef struct {
-    int32_t tail_cells, tail_ctas, structured, vectorized, pdl, fuse_restrict, persistent;
+    int32_t tail_cells, tail_ctas, structured, vectorized, pdl, fuse_restrict, persistent, tiles;
     double ms_per_vcycle; /* measured time (tpa_autotune), else 0 */
 } tpa_tune_config;
 /* Autotuner: times `vcycles` V-cycles (precision 0 FP64, 1 mixed) of every
  * candidate layout on the uploaded hierarchy (tail size x tail CTAs x stencil
  * policy, then the best without vectorized kernels, without PDL, with the
- * fused restriction and as one cooperative launch), keeps the
+ * fused restriction, as one cooperative launch and on block tiles), keeps the
  * fastest and returns it in *best; tried (capacity entries, may be NULL)
  * receives every measurement and *ntried their count.  The choice persists
  * across tpa_refresh; a new hierarchy starts from the defaults. */
@@ -295,6 +298,11 @@ tpa_status tpa_residual_norms_noalloc(tpa_context* ctx, const double* r, const d
  * of the single-CTA coarse tail, 1 if the fused default cycle is used}.
  * Uploads the hierarchy if needed. */
 tpa_status tpa_device_info(tpa_context* ctx, int64_t out[4]);
+/* Number of levels whose V-cycle phases run on haloed block tiles under the
+ * layout in effect (tpa_tune_config.tiles; a level keeps the unfused kernels
+ * when its tiles do not fit).  Uploads the hierarchy if needed.  Measurement
+ * support; no reference counterpart. */
+tpa_status tpa_tiled_levels(tpa_context* ctx, int32_t* count);
 /* Run subsequent device work on the caller's CUDA stream (a cudaStream_t
  * passed as void*; NULL restores the context's own stream).  Replaces nothing
  * in the reference (it has no device); it lets a caller order the solve with

@@ -20,7 +20,7 @@ STRUCTS = {
                   "kernel_launches", "precision", "removed_rhs_max_component_mean"],
     "tpa_multigrid_options": ["coarse_size", "pre_sweeps", "post_sweeps", "max_levels", "smoother"],
     "tpa_tune_config": ["tail_cells", "tail_ctas", "structured", "vectorized", "pdl", "fuse_restrict",
-                        "persistent", "ms_per_vcycle"],
+                        "persistent", "tiles", "ms_per_vcycle"],
     "tpa_projection_options": ["dt", "tolerance", "reference_dt", "inherited_divergence", "max_cycles",
                                "compatibility", "precision", "prepared"],
 }

@@ -1,0 +1,100 @@
+"""The V-cycle on haloed block tiles (two launches per CSR level,
+csrc/tiles.cuh) against the unfused kernels and the oracle.
+
+Both layouts run the CSR kernels on every multi-CTA level (structured = 0),
+so the only difference is the tiling.  Tolerances: one FP64 V-cycle to 1e-13
+of max |z| (the rows are summed in the same order; only the coarse RHS sums
+fold their partials in another order), one mixed V-cycle to 1e-5, solutions
+to the oracle's to 1e-10 (FP64, rtol 1e-12) and 1e-9 (mixed).
+"""
+import numpy as np
+import pytest
+
+from oracle.krylov import solve as osolve
+from oracle.mesh import block_tree_mesh
+from oracle.multigrid import MultigridOptions as OMG, TreeGeometricMultigrid
+from oracle.operator import PoissonOperator as OOp
+
+pytestmark = pytest.mark.gpu
+
+from tpagmg import BlockTreeMesh, EllipticSolver, MultigridOptions, PoissonOperator, solve  # noqa: E402
+from tpagmg import workloads as W  # noqa: E402
+import reference_cases as RC  # noqa: E402
+
+
+def two_level(bs):
+    return dict(block_size=(bs, bs), max_level=2,
+                refine=lambda k, o, e: k[0] == 0 or (k[0] == 1 and k[1] == 0 and k[2] == 0))
+
+
+CASES = {
+    "droplet_l2": (W.droplet_spec(levels=2), 64, "droplet"),
+    "droplet_l3": (W.droplet_spec(levels=3), 64, "droplet"),
+    "two_level_b16": (two_level(16), 8, None),
+    "walls_varcoef_b16": (dict(base_mesh=(128, 128), block_size=(16, 16), periodic=(False, False)), 64,
+                          lambda m: np.exp(0.5 * np.sin(0.3 * np.arange(m.nfaces)))),
+    "periodic_b16": (dict(base_mesh=(128, 64), block_size=(16, 16), extent=(2.0, 1.0), periodic=(True, True)), 64,
+                     None),
+    "techref_amr32_b8": (RC.techref_amr(32), 64, None),
+}
+
+
+def build(name, tiles):
+    spec, coarse, coef = CASES[name]
+    m = BlockTreeMesh(**spec)
+    if coef == "droplet":
+        _, kappa, _ = W.droplet_inputs(m)
+    elif coef is None:
+        kappa = np.ones(m.nfaces)
+    else:
+        kappa = coef(m)
+    s = EllipticSolver(PoissonOperator(m, kappa), multigrid=MultigridOptions(coarse_size=coarse))
+    s.set_tuning(structured=0, tiles=tiles, tail_cells=1024)
+    return spec, m, kappa, coarse, s
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_tiled_vcycle_matches_unfused(name):
+    spec, m, kappa, coarse, s = build(name, 1)
+    _, _, _, _, s0 = build(name, 0)
+    assert s.tiled_levels() >= 1 and s0.tiled_levels() == 0
+    rng = np.random.default_rng(9)
+    vol = m.cell_volumes()
+    for trial in range(2):  # twice: the tile buffers are reused
+        r = rng.standard_normal(m.ncells) * vol
+        r -= vol * np.sum(r) / np.sum(vol)
+        for precision, tol in (("fp64", 1e-13), ("mixed", 1e-5)):
+            z, z0 = s.vcycle(r, precision=precision), s0.vcycle(r, precision=precision)
+            assert np.max(np.abs(z - z0)) <= tol * np.max(np.abs(z0)), (precision, trial)
+
+
+@pytest.mark.parametrize("name", ["droplet_l2", "walls_varcoef_b16", "techref_amr32_b8"])
+def test_tiled_solve_matches_oracle(name):
+    spec, m, kappa, coarse, s = build(name, 1)
+    _, _, _, _, s0 = build(name, 0)
+    oo = OOp(block_tree_mesh(**spec), kappa)
+    rhs = W.gaussian_rhs(m, 21)
+    po, so = osolve(oo, TreeGeometricMultigrid(oo, OMG(coarse_size=coarse)), rhs, rtol=1e-12)
+    x, x0 = np.zeros(m.ncells), np.zeros(m.ncells)
+    st, st0 = solve(x, s, rhs, rtol=1e-12), solve(x0, s0, rhs, rtol=1e-12)
+    assert st.converged and st.cycles == st0.cycles and abs(st.cycles - so.cycles) <= 1
+    assert np.max(np.abs(x - po)) <= 1e-10 * np.max(np.abs(po))
+    xm = np.zeros(m.ncells)
+    stm = solve(xm, s, rhs, rtol=1e-10, precision="mixed")
+    assert stm.converged
+    assert np.max(np.abs(xm - po)) <= 1e-9 * np.max(np.abs(po))
+
+
+def test_tiled_refresh_matches_rebuild():
+    """A device refresh updates the tile copies of the level values."""
+    spec, m, kappa, coarse, s = build("droplet_l2", 1)
+    k2 = kappa * (1.0 + 0.2 * np.cos(np.arange(m.nfaces)))
+    s.refresh(k2)
+    fresh = EllipticSolver(PoissonOperator(m, k2), multigrid=MultigridOptions(coarse_size=coarse))
+    fresh.set_tuning(structured=0, tiles=0, tail_cells=1024)
+    rng = np.random.default_rng(2)
+    vol = m.cell_volumes()
+    r = rng.standard_normal(m.ncells) * vol
+    r -= vol * np.sum(r) / np.sum(vol)
+    z, z0 = s.vcycle(r, precision="fp64"), fresh.vcycle(r, precision="fp64")
+    assert np.max(np.abs(z - z0)) <= 1e-12 * np.max(np.abs(z0))

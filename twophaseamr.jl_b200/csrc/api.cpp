@@ -994,6 +994,7 @@ tpa::TuneConfig from_c(const tpa_tune_config& c) {
     t.pdl = c.pdl;
     t.fuse_restrict = c.fuse_restrict;
     t.persistent = c.persistent;
+    t.tiles = c.tiles;
     return t;
 }
 tpa_tune_config to_c(const tpa::TuneConfig& t, double ms) {
@@ -1005,6 +1006,7 @@ tpa_tune_config to_c(const tpa::TuneConfig& t, double ms) {
     c.pdl = t.pdl;
     c.fuse_restrict = t.fuse_restrict;
     c.persistent = t.persistent;
+    c.tiles = t.tiles;
     c.ms_per_vcycle = ms;
     return c;
 }
@@ -1032,6 +1034,7 @@ tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tp
                     c.pdl = 1;
                     c.fuse_restrict = 0;
                     c.persistent = 0;
+                    c.tiles = 0;
                     cand.push_back(c);
                 }
         std::vector<std::pair<tpa::TuneConfig, double>> res;
@@ -1064,6 +1067,14 @@ tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tp
         run(fr_small);
         run(fr_mid);
         run(pe);
+        // the CSR levels on haloed block tiles (two launches per level), with
+        // the tail sizes around the best one
+        for (int cells : {1024, 2048, 4096}) {
+            tpa::TuneConfig tl = b0;
+            tl.tiles = 1;
+            tl.tail_cells = cells;
+            run(tl);
+        }
         const size_t b = best_of();
         d.reconfigure(ctx->hier, res[b].first);
         if (best) *best = to_c(res[b].first, res[b].second);
@@ -1080,6 +1091,14 @@ tpa_status tpa_set_tuning(tpa_context* ctx, const tpa_tune_config* cfg) {
         ensure_device(ctx);
         ensure_host_fresh(ctx);  // stencil copies come from the host levels
         ctx->dev->reconfigure(ctx->hier, from_c(*cfg));
+    });
+}
+
+tpa_status tpa_tiled_levels(tpa_context* ctx, int32_t* count) {
+    return guard(ctx, [&] {
+        if (!count) throw tpa::Error(TPA_ERR_INVALID_ARG, "null output");
+        ensure_device(ctx);
+        *count = ctx->dev->tiled_levels();
     });
 }
 

@@ -25,6 +25,7 @@ void DeviceSolver::reconfigure(const Hierarchy& h, const TuneConfig& c) {
     tune_ = c;
     build_views();
     upload_structured(h);
+    upload_tiles(h);
 }
 
 double DeviceSolver::time_vcycles(int precision, int count) {

@@ -578,6 +578,7 @@ void DeviceSolver::upload(const Hierarchy& h) {
     TPA_CUDA(cudaStreamSynchronize(stream_));
     build_views();
     upload_structured(h);
+    upload_tiles(h);
 }
 
 void DeviceSolver::apply(const double* x, double* y) {

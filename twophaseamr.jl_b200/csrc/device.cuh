@@ -13,6 +13,8 @@
 #include "stencil.cuh"
 #include "stencil4.cuh"
 #include "structure.hpp"
+#include "tiles.cuh"
+#include "tiles.hpp"
 
 namespace tpa {
 
@@ -107,6 +109,7 @@ struct TuneConfig {
     int fuse_restrict = -1;  // CSR levels: residual recomputed inside the restriction (0 off,
                              // 1 every level, above 1 levels of at most that many cells)
     int persistent = -1;     // all-CSR hierarchies: the V-cycle as one cooperative launch
+    int tiles = -1;          // CSR levels: two launches per level on haloed block tiles (tiles.cuh)
 };
 
 struct SolveStats {
@@ -273,9 +276,27 @@ private:
     std::vector<SView<float>> sf_;
     void upload_structured(const Hierarchy& h);
 
+    // haloed block tiles of CSR levels (tiles.hpp, tiles.cuh)
+    struct TileDev {
+        bool on = false;
+        int ntiles = 0, n3max = 0, n2max = 0, n1max = 0, nent = 0;
+        DevArray<int> cell, cell_off, ring, lrp, lrp_off, ent_off, pos, co, co_off;
+        DevArray<int16_t> lcol, ch;
+        DevArray<double> val_d;
+        DevArray<float> val_f;
+    };
+    std::vector<TileDev> tdev_;
+    std::vector<TileView<double>> td_;
+    std::vector<TileView<float>> tf_;
+    void upload_tiles(const Hierarchy& h);
+    template <typename T> const TileView<T>& tile_view(int l) const;
+    void gather_tile_values();  // tile copies of the level CSR values (after an upload or a refresh)
+
 public:
     // Levels on the block-structured path and their exception-row counts.
     int structured_levels() const;
+    // Levels whose V-cycle phases run on haloed block tiles.
+    int tiled_levels() const;
     int64_t exception_rows() const;
 
     // ---- coefficient refresh on the device (csrc/refresh.cu) ----

@@ -782,6 +782,7 @@ void DeviceSolver::refresh_levels() {
         TPA_CUDA(cudaMemcpyAsync(f_sqrtk_.p, rl_[0].sk.p, sizeof(double) * size_t(rl_[0].nf), cudaMemcpyDeviceToDevice,
                                  s));
     TPA_CUDA(cudaStreamSynchronize(s));
+    gather_tile_values();  // the tile copies of the refreshed level values
     destroy_graphs();
 }
 

@@ -498,9 +498,12 @@ TuneConfig DeviceSolver::effective_tuning() const {
     if (tune_.fuse_restrict >= 0) c.fuse_restrict = tune_.fuse_restrict;
     c.persistent = std::getenv("TPAGMG_PERSISTENT") ? 1 : 0;
     if (tune_.persistent >= 0) c.persistent = tune_.persistent ? 1 : 0;
+    c.tiles = std::getenv("TPAGMG_TILES") ? std::atoi(std::getenv("TPAGMG_TILES")) != 0 : 0;
+    if (tune_.tiles >= 0) c.tiles = tune_.tiles ? 1 : 0;
     if (rb_) {  // the red-black sweeps exist for the CSR levels and the tail only
         c.structured = 0;
         c.persistent = 0;
+        c.tiles = 0;
     }
     return c;
 }
@@ -669,6 +672,22 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
             launches_ += 3;
             continue;
         }
+        if (tdev_.size() > size_t(l) && tdev_[size_t(l)].on) {
+            // both pre-sweeps, the residual and the restriction in one launch
+            const TileDev& D = tdev_[size_t(l)];
+            const TileView<T>& TV = tile_view<T>(l);
+            const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
+            const size_t sm = tile_down_smem<T>(D.n3max, D.n2max, D.n1max);
+            if (l == 0)
+                go(k_tile_down<T, double>, D.ntiles, kTileThreads, sm, L, TV, r, rsum, V[size_t(l + 1)].b,
+                   fpartial_.p, counters_.p + kRestrictSum, next_sum ? lsum_.p + l + 1 : nullptr);
+            else
+                go(k_tile_down<T, T>, D.ntiles, kTileThreads, sm, L, TV, (const T*)L.b, (const double*)(lsum_.p + l),
+                   V[size_t(l + 1)].b, fpartial_.p, counters_.p + kRestrictSum,
+                   next_sum ? lsum_.p + l + 1 : nullptr);
+            ++launches_;
+            continue;
+        }
         if (L.rb) {
             // second sweep: one pass on a small level (the red values recomputed),
             // two half-sweeps on a large one
@@ -737,6 +756,16 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
                    fpartial_.p, counters_.p + kPostMean, want_mean ? mean_out : nullptr, epi);
             });
             launches_ += 3;
+            continue;
+        }
+        if (tdev_.size() > size_t(l) && tdev_[size_t(l)].on) {
+            // prolongation and both post-sweeps in one launch
+            const TileDev& D = tdev_[size_t(l)];
+            const bool want_mean = (l == 0) && L.singular;
+            go(k_tile_up<T, Epi>, D.ntiles, kTileThreads, tile_up_smem<T>(D.n3max, D.n2max, D.n1max), L,
+               tile_view<T>(l), (const T*)V[size_t(l + 1)].x, fpartial_.p, counters_.p + kPostMean,
+               want_mean ? mean_out : nullptr, epi);
+            ++launches_;
             continue;
         }
         go(k_prolong<T>, blocks_for(L.n), kThreads, 0, L, V[size_t(l + 1)].x);
@@ -1042,6 +1071,127 @@ double DeviceSolver::time_fused(int which, int level, int precision, int iters) 
 }  // namespace tpa
 
 namespace tpa {
+
+template <typename T>
+const TileView<T>& DeviceSolver::tile_view(int l) const {
+    if constexpr (std::is_same<T, double>::value) return td_[size_t(l)];
+    else return tf_[size_t(l)];
+}
+
+template <typename T, typename TB>
+static void allow_tile_down_smem(size_t bytes) {
+    TPA_CUDA(cudaFuncSetAttribute(k_tile_down<T, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+}
+template <typename T, typename Epi>
+static void allow_tile_up_smem(size_t bytes) {
+    TPA_CUDA(cudaFuncSetAttribute(k_tile_up<T, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+}
+
+// Tiles of every CSR level of the multi-CTA part of the default cycle (not the
+// stencil levels, the tail, the red-black smoother or the cooperative cycle).
+void DeviceSolver::upload_tiles(const Hierarchy& h) {
+    const int nl = int(levels_.size());
+    const TuneConfig cfg = effective_tuning();
+    tdev_.clear();
+    tdev_.resize(size_t(nl));
+    td_.assign(size_t(nl), TileView<double>{});
+    tf_.assign(size_t(nl), TileView<float>{});
+    if (!cfg.tiles || rb_ || !fused_ok_ || coop_grid_ > 0) return;
+    // a tile's arrays live in shared memory: at most this many cells (rings <= 3)
+    constexpr int kTileMaxCells = 1536;
+    size_t down_d = 0, up_d = 0;
+    for (int l = 0; l < tail_first_ && l + 1 < nl; ++l) {
+        if (sdev_[size_t(l)].on) continue;
+        const HostLevel& hl = h.levels[size_t(l)];
+        const TileLevelHost T = build_tiles(hl.op.A, hl.op.mesh.nblocks(), hl.op.mesh.cells_per_block(), hl.owner,
+                                            h.levels[size_t(l + 1)].op.A.n, kTileMaxCells);
+        if (!T.ok) continue;
+        TileDev& D = tdev_[size_t(l)];
+        D.ntiles = T.ntiles;
+        D.n3max = T.n3max;
+        D.n2max = T.n2max;
+        D.n1max = T.n1max;
+        D.nent = int(T.pos.size());
+        D.cell.upload(T.cell.data(), T.cell.size(), stream_);
+        D.cell_off.upload(T.cell_off.data(), T.cell_off.size(), stream_);
+        D.ring.upload(T.ring.data(), T.ring.size(), stream_);
+        D.lrp.upload(T.lrp.data(), T.lrp.size(), stream_);
+        D.lrp_off.upload(T.lrp_off.data(), T.lrp_off.size(), stream_);
+        D.ent_off.upload(T.ent_off.data(), T.ent_off.size(), stream_);
+        D.pos.upload(T.pos.data(), T.pos.size(), stream_);
+        D.lcol.upload(T.lcol.data(), T.lcol.size(), stream_);
+        D.co.upload(T.co.data(), T.co.size(), stream_);
+        D.co_off.upload(T.co_off.data(), T.co_off.size(), stream_);
+        D.ch.upload(T.ch.data(), T.ch.size(), stream_);
+        D.val_d.alloc(T.pos.size());
+        D.val_f.alloc(T.pos.size());
+        TPA_CUDA(cudaStreamSynchronize(stream_));  // the host arrays go out of scope
+        auto fill = [&](auto& v, auto* val) {
+            v.ntiles = D.ntiles;
+            v.n3max = D.n3max;
+            v.n2max = D.n2max;
+            v.n1max = D.n1max;
+            v.cell = D.cell.p;
+            v.cell_off = D.cell_off.p;
+            v.ring = reinterpret_cast<const int4*>(D.ring.p);
+            v.lrp = D.lrp.p;
+            v.lrp_off = D.lrp_off.p;
+            v.ent_off = D.ent_off.p;
+            v.val = val;
+            v.lcol = reinterpret_cast<const short*>(D.lcol.p);
+            v.co = D.co.p;
+            v.co_off = D.co_off.p;
+            v.ch = reinterpret_cast<const short4*>(D.ch.p);
+        };
+        fill(td_[size_t(l)], D.val_d.p);
+        fill(tf_[size_t(l)], D.val_f.p);
+        down_d = std::max(down_d, tile_down_smem<double>(D.n3max, D.n2max, D.n1max));
+        up_d = std::max(up_d, tile_up_smem<double>(D.n3max, D.n2max, D.n1max));
+        D.on = true;
+    }
+    if (down_d == 0) return;
+    // one partial sum per tile in the folds of the tile kernels
+    size_t ntiles = 0;
+    for (const auto& D : tdev_) ntiles = std::max(ntiles, size_t(D.on ? D.ntiles : 0));
+    if (ntiles > fpartial_.n) {
+        fpartial_.alloc(ntiles);
+        fpartial2_.alloc(ntiles);
+    }
+    int optin = 0;
+    TPA_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
+    if (down_d > size_t(optin) || up_d > size_t(optin)) {
+        for (auto& D : tdev_) D.on = false;
+        return;
+    }
+    allow_tile_down_smem<double, double>(down_d);
+    allow_tile_down_smem<float, double>(down_d);
+    allow_tile_down_smem<float, float>(down_d);
+    allow_tile_up_smem<double, MeanOnly>(up_d);
+    allow_tile_up_smem<float, MeanOnly>(up_d);
+    allow_tile_up_smem<double, CgRz>(up_d);
+    allow_tile_up_smem<float, CgRz>(up_d);
+    gather_tile_values();
+    destroy_graphs();
+}
+
+void DeviceSolver::gather_tile_values() {
+    for (size_t l = 0; l < tdev_.size(); ++l) {
+        TileDev& D = tdev_[l];
+        if (!D.on || D.nent == 0) continue;
+        const DevLevel& L = levels_[l];
+        const int g = int(std::min<int64_t>((D.nent + kThreads - 1) / kThreads, kMaxGrid));
+        k_tile_gather<double><<<g, kThreads, 0, stream_>>>(D.nent, D.pos.p, L.d.val.p, D.val_d.p);
+        k_tile_gather<float><<<g, kThreads, 0, stream_>>>(D.nent, D.pos.p, L.f.val.p, D.val_f.p);
+    }
+    TPA_CUDA(cudaGetLastError());
+    TPA_CUDA(cudaStreamSynchronize(stream_));
+}
+
+int DeviceSolver::tiled_levels() const {
+    int k = 0;
+    for (const auto& d : tdev_) k += d.on ? 1 : 0;
+    return k;
+}
 
 // Block-structured copies of every level that qualifies: 16x16-style blocks
 // (32 to 1024 cells, a multiple of 32), a valid block map of the transfer and

@@ -47,7 +47,7 @@ class StatsC(C.Structure):
 class TuneC(C.Structure):
     _fields_ = [("tail_cells", C.c_int32), ("tail_ctas", C.c_int32), ("structured", C.c_int32),
                 ("vectorized", C.c_int32), ("pdl", C.c_int32), ("fuse_restrict", C.c_int32),
-                ("persistent", C.c_int32),
+                ("persistent", C.c_int32), ("tiles", C.c_int32),
                 ("ms_per_vcycle", C.c_double)]
 
 
@@ -108,6 +108,7 @@ SIGNATURES = {
     "tpa_synchronize": (C.c_int32, [P]),
     "tpa_set_stream": (C.c_int32, [P, P]),
     "tpa_device_info": (C.c_int32, [P, i64p]),
+    "tpa_tiled_levels": (C.c_int32, [P, i32p]),
     "tpa_residual_norms": (C.c_int32, [P, P, f64p]),
     "tpa_residual_norms_noalloc": (C.c_int32, [P, P, P, C.c_int64, f64p]),
     "tpa_time_kernel": (C.c_int32, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, f64p]),

@@ -135,7 +135,7 @@ class EllipticSolver:
     def _tune_dict(t):
         return {"tail_cells": t.tail_cells, "tail_ctas": t.tail_ctas, "structured": t.structured,
                 "vectorized": t.vectorized, "pdl": t.pdl, "fuse_restrict": t.fuse_restrict, "persistent": t.persistent,
-                "ms_per_vcycle": t.ms_per_vcycle}
+                "tiles": t.tiles, "ms_per_vcycle": t.ms_per_vcycle}
 
     def autotune(self, precision=None, vcycles=20):
         """Time the candidate device layouts of the V-cycle and keep the
@@ -152,10 +152,16 @@ class EllipticSolver:
         self.ctx.call("tpa_get_tuning", C.byref(t))
         return self._tune_dict(t)
 
+    def tiled_levels(self):
+        """Levels whose V-cycle phases run on haloed block tiles."""
+        n = C.c_int32()
+        self.ctx.call("tpa_tiled_levels", C.byref(n))
+        return int(n.value)
+
     def set_tuning(self, **fields):
         """Apply a layout (tail_cells, tail_ctas, structured, vectorized, pdl,
-        fuse_restrict, persistent; omitted fields: default)."""
-        keys = ("tail_cells", "tail_ctas", "structured", "vectorized", "pdl", "fuse_restrict", "persistent")
+        fuse_restrict, persistent, tiles; omitted fields: default)."""
+        keys = ("tail_cells", "tail_ctas", "structured", "vectorized", "pdl", "fuse_restrict", "persistent", "tiles")
         unknown = set(fields) - set(keys)
         if unknown:
             raise ValueError(f"unknown layout fields: {sorted(unknown)}")
