@@ -93,6 +93,29 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def model_bytes_per_cell_iteration(s, s_kappa):
+    """Compulsory HBM bytes per fine cell and CG iteration of the solve: a
+    V-cycle (hierarchy factor 4/3; two pre-sweeps reading x, b and two face
+    coefficients and writing x; residual + restriction; prolongation +
+    correction) in value size s with coefficient size s_kappa (0 when
+    constant), plus 56 bytes of the FP64 CG (operator product and the fused
+    vector updates)."""
+    vcycle = 4.0 / 3.0 * (4 * (3 * s + 2 * s_kappa) + (2 * s + 2 * s_kappa + s / 4) + (2 * s + s / 4))
+    return vcycle + 56.0
+
+
+def whole_solve_roofline(n, variable_kappa, mixed, fp64, peak, peak_kind, world=1):
+    """Model bytes of whole solves (per-iteration model times iterations) over
+    their measured time, against the measured HBM bandwidth."""
+    out = {"peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+           "what": "model bytes per cell and CG iteration x cells x iterations / solve time"}
+    for name, (its, ms), s in (("mixed", mixed, 4), ("fp64", fp64, 8)):
+        b = model_bytes_per_cell_iteration(s, s if variable_kappa else 0)
+        gbs = world * n * its * b / (ms * 1e-3) / 1e9
+        out[name] = {"bytes_per_cell_iteration": b, "achieved": gbs, "frac": gbs / peak}
+    return out
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle sampling during the timed region."""
 
@@ -612,6 +635,8 @@ def main():
                      "traffic": traffic, "kernel": "damped-Jacobi sweep, finest level, FP32",
                      "kernel_ms": sweep.value, "kernel_ms_fp64": sweep64.value,
                      "algorithmic_bytes": alg32, "peak_kind": peak_kind},
+        "whole_solve_roofline": whole_solve_roofline(n, skappa, (mixed_it, mixed_ms), (fp64_it, fp64_ms), peak,
+                                                     peak_kind, world),
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
         "refresh": refresh,

@@ -243,6 +243,7 @@ private:
     int coop_grid_ = 0;     // > 0: the V-cycle runs as one cooperative launch of this many CTAs
     DevArray<unsigned> bar_;  // grid barrier: arrivals, generation
     DevArray<int> err_;       // set when a grid barrier gave up waiting
+    unsigned long long barrier_spins_ = 0;  // poll limit of a grid barrier
 
 public:
     // throws (status 3) if a grid barrier of the cooperative V-cycle gave up

@@ -524,6 +524,10 @@ void DeviceSolver::build_views() {
     const TuneConfig cfg = effective_tuning();
     if (const char* e = std::getenv("TPAGMG_RB_PAIR_CELLS")) rb_pair_cells_ = std::atoi(e);
     pdl_ = cfg.pdl != 0;
+    // grid-barrier poll limit of the cooperative cycle (TPAGMG_BARRIER_SPINS
+    // lowers it; 0 makes every barrier that has to wait give up)
+    barrier_spins_ = kBarrierSpins;
+    if (const char* e = std::getenv("TPAGMG_BARRIER_SPINS")) barrier_spins_ = std::strtoull(e, nullptr, 10);
     // 1: every CSR level; above 1: levels of at most that many cells
     rr_cells_ = cfg.fuse_restrict == 1 ? INT32_MAX : cfg.fuse_restrict;
     fused_ok_ = (pre_ == 2 && post_ == 2);
@@ -632,7 +636,7 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
         // the whole cycle in one cooperative launch (persistent.cuh)
         const Launch gc{stream_, false, 1, true};
         gc(k_vcycle_grid<T>, coop_grid_, kTailThreads, 0, Vdev, t, nl, r, rsum, mean_out, coarse_inv_.p, coarse_n_,
-           fpartial_.p, bar_.p, lsum_.p, err_.p);
+           fpartial_.p, bar_.p, lsum_.p, err_.p, barrier_spins_);
         ++launches_;
         if (!V[0].singular) TPA_CUDA(cudaMemsetAsync(mean_out, 0, sizeof(double), stream_));
         return;
