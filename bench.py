@@ -621,7 +621,7 @@ def main():
         "dtype": "f32/f64", "data": "synthetic (seeded Philox)",
         "config": {"workload": wname,
                    "fine_cells": n, "levels": solver.level_sizes(), "parallelism": "replicas" if world > 1 else "1 GPU",
-                   "l2": "flushed between steps (256 MiB write)", "device_layout": solver.device_info(),
+                   "l2": "flushed between steps (256 MiB write)", "device_layout": dict(solver.device_info(), tiled_levels=solver.tiled_levels()),
                    "autotuned_layout": layout, "autotune_s": tune_s},
         "time_to_tolerance_ms": {"mixed": mixed_ms, "fp64": fp64_ms, "speedup_mixed_over_fp64": fp64_ms / mixed_ms},
         "cg_iterations": {"mixed": mixed_it, "fp64": fp64_it},

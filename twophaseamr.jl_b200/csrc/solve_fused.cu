@@ -650,6 +650,18 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
             const SView<T>& S = (*Sp)[size_t(l)];
             const int groups = (S.nblocks + 3) / 4;
             const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
+            if (tdev_.size() > size_t(l) && tdev_[size_t(l)].vec) {
+                // both pre-sweeps, the residual and the restriction on 22 x 22 tiles
+                if (l == 0)
+                    go(v_tile_down<T, double>, S.nblocks, kTileThreads, 0, S, r, rsum, V[size_t(l + 1)].b, fpartial_.p,
+                       counters_.p + kRestrictSum, next_sum ? lsum_.p + l + 1 : nullptr);
+                else
+                    go(v_tile_down<T, T>, S.nblocks, kTileThreads, 0, S, (const T*)S.b,
+                       (const double*)(lsum_.p + l), V[size_t(l + 1)].b, fpartial_.p, counters_.p + kRestrictSum,
+                       next_sum ? lsum_.p + l + 1 : nullptr);
+                ++launches_;
+                continue;
+            }
             if (l == 0) go(v_pre2<T, double>, groups, 256, 0, S, r, rsum);
             else go(v_pre2<T, T>, groups, 256, 0, S, S.b, lsum_.p + l);
             go(v_residual<T>, groups, 256, 0, S);
@@ -738,6 +750,13 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
             const SView<T>& S = (*Sp)[size_t(l)];
             const int groups = (S.nblocks + 3) / 4;
             const bool want_mean = (l == 0) && L.singular;
+            if (tdev_.size() > size_t(l) && tdev_[size_t(l)].vec) {
+                // prolongation and both post-sweeps on 22 x 22 tiles
+                go(v_tile_up<T, Epi>, S.nblocks, kTileThreads, 0, S, (const T*)V[size_t(l + 1)].x, fpartial_.p,
+                   counters_.p + kPostMean, want_mean ? mean_out : nullptr, epi);
+                ++launches_;
+                continue;
+            }
             go(v_prolong<T>, groups, 256, 0, S, V[size_t(l + 1)].x);
             go(v_sweep<T, false>, groups, 256, 0, S, S.x, S.y, nullptr, nullptr, nullptr, MeanOnly());
             if (want_mean)
@@ -1105,6 +1124,10 @@ void DeviceSolver::upload_tiles(const Hierarchy& h) {
     constexpr int kTileMaxCells = 1536;
     size_t down_d = 0, up_d = 0;
     for (int l = 0; l < tail_first_ && l + 1 < nl; ++l) {
+        if (sdev_[size_t(l)].vec) {
+            tdev_[size_t(l)].vec = true;  // stencil tiles need no lists
+            continue;
+        }
         if (sdev_[size_t(l)].on) continue;
         const HostLevel& hl = h.levels[size_t(l)];
         const TileLevelHost T = build_tiles(hl.op.A, hl.op.mesh.nblocks(), hl.op.mesh.cells_per_block(), hl.owner,
@@ -1193,7 +1216,7 @@ void DeviceSolver::gather_tile_values() {
 
 int DeviceSolver::tiled_levels() const {
     int k = 0;
-    for (const auto& d : tdev_) k += d.on ? 1 : 0;
+    for (const auto& d : tdev_) k += (d.on || d.vec) ? 1 : 0;
     return k;
 }
 

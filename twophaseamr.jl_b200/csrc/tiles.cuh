@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include "fused.cuh"
+#include "stencil.cuh"
 
 namespace tpa {
 
@@ -207,6 +208,215 @@ __global__ void __launch_bounds__(kTileThreads)
 template <typename T>
 __global__ void k_tile_gather(int m, const int* __restrict__ pos, const T* __restrict__ val, T* __restrict__ out) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) out[k] = val[pos[k]];
+}
+
+// ---------------------------------------------------------------------------------
+// The same two launches per level on constant-coefficient 16x16 levels (the
+// levels of the vectorized kernels, stencil4.cuh: every block and its
+// neighbours the same size, every coupling c0): the tile is the block plus a
+// three-cell frame, a 22 x 22 square taken from the block and its eight
+// neighbours (W, E, S, N from the neighbour table, the corners through them;
+// cells of missing blocks -- walls -- do not exist), with no index lists.
+// Each phase works on a square one cell smaller than the last.  The row
+// arithmetic is that of the vectorized kernels (q_apply: the existing
+// neighbours summed west, east, south, north).
+
+namespace vt {
+constexpr int R = 22;  // region side: 16 + 2 * 3
+__device__ __forceinline__ int at(int i, int j) { return (j + 3) * R + (i + 3); }
+}  // namespace vt
+
+// the nine blocks around block b (index (by + 1) * 3 + (bx + 1), -1: none)
+template <typename T>
+__device__ __forceinline__ void vt_blocks(const SView<T>& L, int b, int* nb9) {
+    if (threadIdx.x == 0) {
+        const int4 c = *reinterpret_cast<const int4*>(L.nbr + 4 * b);
+        const int4 none = make_int4(-1, -1, -1, -1);
+        const int4 w = c.x >= 0 ? *reinterpret_cast<const int4*>(L.nbr + 4 * c.x) : none;
+        const int4 e = c.y >= 0 ? *reinterpret_cast<const int4*>(L.nbr + 4 * c.y) : none;
+        const int4 s = c.z >= 0 ? *reinterpret_cast<const int4*>(L.nbr + 4 * c.z) : none;
+        const int4 n = c.w >= 0 ? *reinterpret_cast<const int4*>(L.nbr + 4 * c.w) : none;
+        nb9[0] = c.x >= 0 ? w.z : s.x;  // south-west
+        nb9[1] = c.z;
+        nb9[2] = c.y >= 0 ? e.z : s.y;  // south-east
+        nb9[3] = c.x;
+        nb9[4] = b;
+        nb9[5] = c.y;
+        nb9[6] = c.x >= 0 ? w.w : n.x;  // north-west
+        nb9[7] = c.w;
+        nb9[8] = c.y >= 0 ? e.w : n.y;  // north-east
+    }
+}
+
+// global cell of region cell (i, j), i, j in [-3, 18], or -1 when it does not exist
+__device__ __forceinline__ int vt_cell(const int* nb9, int i, int j) {
+    const int bx = i < 0 ? -1 : (i > 15 ? 1 : 0), by = j < 0 ? -1 : (j > 15 ? 1 : 0);
+    const int B = nb9[(by + 1) * 3 + bx + 1];
+    if (B < 0) return -1;
+    return B * 256 + (j - 16 * by) * 16 + (i - 16 * bx);
+}
+
+// c0 (count * v - sum of the existing neighbours), neighbours in the order of q_apply
+template <typename T>
+__device__ __forceinline__ T vt_apply(const SView<T>& L, const T* v, const unsigned char* ex, int k) {
+    T off = T(0);
+    int cnt = 0;
+    if (ex[k - 1]) off += v[k - 1], ++cnt;
+    if (ex[k + 1]) off += v[k + 1], ++cnt;
+    if (ex[k - vt::R]) off += v[k - vt::R], ++cnt;
+    if (ex[k + vt::R]) off += v[k + vt::R], ++cnt;
+    return L.c0 * (T(cnt) * v[k] - off);
+}
+
+template <typename T, typename TB>
+__global__ void __launch_bounds__(kTileThreads)
+    v_tile_down(SView<T> L, const TB* __restrict__ bin, const double* level_sum, T* __restrict__ bc, double* partial,
+                unsigned* counter, double* coarse_sum) {
+    pdl_entry();
+    constexpr int N = vt::R * vt::R;
+    __shared__ T sb[N], sd[N], sx[N], sy[N], sr[N], ss[N];
+    __shared__ unsigned char ex[N];
+    __shared__ int nb9[9];
+    const int b = blockIdx.x;
+    vt_blocks(L, b, nb9);
+    const double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
+    __syncthreads();
+    for (int q = threadIdx.x; q < N; q += blockDim.x) {
+        const int i = q % vt::R - 3, j = q / vt::R - 3;
+        const int c = vt_cell(nb9, i, j);
+        T bv = T(0), d = T(0);
+        if (c >= 0) {
+            const TB a = bin[c];
+            if (mean != 0.0) {
+                const double v = L.const_vol ? double(L.vol0) : double(L.vol[c]);
+                bv = T(double(a) - v * mean);
+            } else {
+                bv = T(a);
+            }
+            d = L.dinv ? L.dinv[c] : L.dinv0;
+        }
+        ex[q] = c >= 0;
+        sb[q] = bv;
+        sd[q] = d;
+        sx[q] = L.w * d * bv;  // the first sweep from zero, pointwise
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < 20 * 20; q += blockDim.x) {
+        const int k = vt::at(q % 20 - 2, q / 20 - 2);
+        if (ex[k]) sy[k] = sx[k] + L.w * sd[k] * (sb[k] - vt_apply(L, sx, ex, k));
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < 18 * 18; q += blockDim.x) {
+        const int k = vt::at(q % 18 - 1, q / 18 - 1);
+        if (ex[k]) {
+            const T r = sb[k] - vt_apply(L, sy, ex, k);
+            sr[k] = r;
+            ss[k] = sd[k] * r;
+        }
+    }
+    __syncthreads();
+    // t = r - wt A s on the block (into sx, no longer needed), and the block's
+    // iterate (into L.y, read by v_tile_up) and projected right-hand side
+    for (int q = threadIdx.x; q < 256; q += blockDim.x) {
+        const int k = vt::at(q & 15, q >> 4);
+        sx[k] = sr[k] - L.tw * vt_apply(L, ss, ex, k);
+        L.y[b * 256 + q] = sy[k];
+        L.bp[b * 256 + q] = sb[k];
+    }
+    __syncthreads();
+    const int4 mp = *reinterpret_cast<const int4*>(L.map + 4 * b);
+    double part = 0;
+    if (mp.w == 1) {
+        for (int q = threadIdx.x; q < 256; q += blockDim.x) {
+            const int i = q & 15, j = q >> 4;
+            const T t = sx[vt::at(i, j)];
+            bc[mp.x * 256 + (mp.z + j) * 16 + mp.y + i] = t;
+            part += double(t);
+        }
+    } else {
+        // 2 x 2 aggregation in the order of v_restrict: row pairs, then the row above
+        for (int q = threadIdx.x; q < 64; q += blockDim.x) {
+            const int i = 2 * (q & 7), j = 2 * (q >> 3);
+            const T h0 = sx[vt::at(i, j)] + sx[vt::at(i + 1, j)];
+            const T d0 = sx[vt::at(i, j + 1)] + sx[vt::at(i + 1, j + 1)];
+            const T t = h0 + d0;
+            bc[mp.x * 256 + (mp.z + (j >> 1)) * 16 + mp.y + (i >> 1)] = t;
+            part += double(t);
+        }
+    }
+    if (coarse_sum) {
+        if (publish_partial(part, partial, counter)) {
+            const double s = fold_partials(partial, gridDim.x);
+            if (threadIdx.x == 0) {
+                *coarse_sum = s;
+                *counter = 0;
+            }
+        }
+    }
+}
+
+// e = P_tent x_c at the cell (li, lj) of block B (its map: coarse block, x / y offset, scale)
+template <typename T>
+__device__ __forceinline__ T vt_coarse(const SView<T>& L, const T* xc, int B, int li, int lj) {
+    const int4 mp = *reinterpret_cast<const int4*>(L.map + 4 * B);
+    if (mp.w == 1) return xc[mp.x * 256 + (mp.z + lj) * 16 + mp.y + li];
+    return xc[mp.x * 256 + (mp.z + (lj >> 1)) * 16 + mp.y + (li >> 1)];
+}
+
+template <typename T, typename Epi>
+__global__ void __launch_bounds__(kTileThreads)
+    v_tile_up(SView<T> L, const T* __restrict__ xc, double* partial, unsigned* counter, double* mean_out, Epi epi) {
+    pdl_entry();
+    constexpr int N = vt::R * vt::R;
+    __shared__ T se[N], sp[N], sq[N], sd[N], sb[N];
+    __shared__ unsigned char ex[N];
+    __shared__ int nb9[9];
+    const int b = blockIdx.x;
+    vt_blocks(L, b, nb9);
+    __syncthreads();
+    for (int q = threadIdx.x; q < N; q += blockDim.x) {
+        const int i = q % vt::R - 3, j = q / vt::R - 3;
+        const int bx = i < 0 ? -1 : (i > 15 ? 1 : 0), by = j < 0 ? -1 : (j > 15 ? 1 : 0);
+        const int B = nb9[(by + 1) * 3 + bx + 1];
+        ex[q] = B >= 0;
+        T e = T(0), x = T(0), d = T(0), bp = T(0);
+        if (B >= 0) {
+            const int li = i - 16 * bx, lj = j - 16 * by, c = B * 256 + lj * 16 + li;
+            e = vt_coarse(L, xc, B, li, lj);
+            if (i >= -2 && i <= 17 && j >= -2 && j <= 17) {
+                x = L.y[c];
+                d = L.dinv ? L.dinv[c] : L.dinv0;
+                if (i >= -1 && i <= 16 && j >= -1 && j <= 16) bp = L.bp[c];
+            }
+        }
+        se[q] = e;
+        sp[q] = x;
+        sd[q] = d;
+        sb[q] = bp;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < 20 * 20; q += blockDim.x) {
+        const int k = vt::at(q % 20 - 2, q / 20 - 2);
+        if (ex[k]) sp[k] += se[k] - L.tw * sd[k] * vt_apply(L, se, ex, k);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < 18 * 18; q += blockDim.x) {
+        const int k = vt::at(q % 18 - 1, q / 18 - 1);
+        if (ex[k]) sq[k] = sp[k] + L.w * sd[k] * (sb[k] - vt_apply(L, sp, ex, k));
+    }
+    __syncthreads();
+    double v = 0, w = 0;
+    for (int q = threadIdx.x; q < 256; q += blockDim.x) {
+        const int k = vt::at(q & 15, q >> 4);
+        const T o = sq[k] + L.w * sd[k] * (sb[k] - vt_apply(L, sq, ex, k));
+        const int c = b * 256 + q;
+        L.x[c] = o;
+        if (mean_out) {
+            v += (L.const_vol ? double(L.vol0) : double(L.vol[c])) * double(o);
+            if constexpr (Epi::kRz) w += epi.r[c] * double(o);
+        }
+    }
+    if (mean_out) fold_mean(v, w, partial, counter, mean_out, L.cvol_inv, epi);
 }
 
 }  // namespace tpa
