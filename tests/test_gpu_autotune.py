@@ -69,4 +69,4 @@ def test_bad_layouts_are_rejected():
     with pytest.raises(TpaError):
         s.set_tuning(tail_ctas=9)
     with pytest.raises(ValueError):
-        s.set_tuning(tiles=3)
+        s.set_tuning(tiling=3)  # not a layout field

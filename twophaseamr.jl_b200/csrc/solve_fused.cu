@@ -693,7 +693,7 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
             const TileDev& D = tdev_[size_t(l)];
             const TileView<T>& TV = tile_view<T>(l);
             const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
-            const size_t sm = tile_down_smem<T>(D.n3max, D.n2max, D.n1max);
+            const size_t sm = tile_down_smem<T>(D.n3max, D.n2max, D.n1max, D.emax);
             if (l == 0)
                 go(k_tile_down<T, double>, D.ntiles, kTileThreads, sm, L, TV, r, rsum, V[size_t(l + 1)].b,
                    fpartial_.p, counters_.p + kRestrictSum, next_sum ? lsum_.p + l + 1 : nullptr);
@@ -785,7 +785,7 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
             // prolongation and both post-sweeps in one launch
             const TileDev& D = tdev_[size_t(l)];
             const bool want_mean = (l == 0) && L.singular;
-            go(k_tile_up<T, Epi>, D.ntiles, kTileThreads, tile_up_smem<T>(D.n3max, D.n2max, D.n1max), L,
+            go(k_tile_up<T, Epi>, D.ntiles, kTileThreads, tile_up_smem<T>(D.n3max, D.n2max, D.n1max, D.emax), L,
                tile_view<T>(l), (const T*)V[size_t(l + 1)].x, fpartial_.p, counters_.p + kPostMean,
                want_mean ? mean_out : nullptr, epi);
             ++launches_;
@@ -1138,6 +1138,7 @@ void DeviceSolver::upload_tiles(const Hierarchy& h) {
         D.n3max = T.n3max;
         D.n2max = T.n2max;
         D.n1max = T.n1max;
+        D.emax = T.emax;
         D.nent = int(T.pos.size());
         D.cell.upload(T.cell.data(), T.cell.size(), stream_);
         D.cell_off.upload(T.cell_off.data(), T.cell_off.size(), stream_);
@@ -1158,6 +1159,7 @@ void DeviceSolver::upload_tiles(const Hierarchy& h) {
             v.n3max = D.n3max;
             v.n2max = D.n2max;
             v.n1max = D.n1max;
+            v.emax = D.emax;
             v.cell = D.cell.p;
             v.cell_off = D.cell_off.p;
             v.ring = reinterpret_cast<const int4*>(D.ring.p);
@@ -1172,8 +1174,8 @@ void DeviceSolver::upload_tiles(const Hierarchy& h) {
         };
         fill(td_[size_t(l)], D.val_d.p);
         fill(tf_[size_t(l)], D.val_f.p);
-        down_d = std::max(down_d, tile_down_smem<double>(D.n3max, D.n2max, D.n1max));
-        up_d = std::max(up_d, tile_up_smem<double>(D.n3max, D.n2max, D.n1max));
+        down_d = std::max(down_d, tile_down_smem<double>(D.n3max, D.n2max, D.n1max, D.emax));
+        up_d = std::max(up_d, tile_up_smem<double>(D.n3max, D.n2max, D.n1max, D.emax));
         D.on = true;
     }
     if (down_d == 0) return;

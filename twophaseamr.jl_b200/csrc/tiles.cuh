@@ -34,7 +34,7 @@ constexpr int kTileThreads = 256;
 template <typename T>
 struct TileView {
     int ntiles;
-    int n3max, n2max, n1max;
+    int n3max, n2max, n1max, emax;
     const int* cell;
     const int* cell_off;
     const int4* ring;  // per tile: cells of rings <= 0, 1, 2, 3
@@ -48,14 +48,33 @@ struct TileView {
     const short4* ch;  // per coarse cell: local indices of its children (-1: none)
 };
 
+// Shared memory of a tile: the cell arrays in precision T, the tile's CSR
+// values (T), its local row pointers (int) and local columns (short), so that
+// every phase after the prologue reads shared memory only.
 template <typename T>
-__host__ __device__ inline size_t tile_down_smem(int n3, int n2, int n1) {
-    return sizeof(T) * (3 * size_t(n3) + size_t(n2) + 3 * size_t(n1)) + sizeof(int) * (size_t(n2) + 1);
+__host__ __device__ inline size_t tile_down_smem(int n3, int n2, int n1, int e) {
+    return sizeof(T) * (3 * size_t(n3) + size_t(n2) + 3 * size_t(n1) + size_t(e)) + sizeof(int) * (size_t(n2) + 1) +
+           sizeof(short) * size_t(e);
 }
 
 template <typename T>
-__host__ __device__ inline size_t tile_up_smem(int n3, int n2, int n1) {
-    return sizeof(T) * (size_t(n3) + 3 * size_t(n2) + 2 * size_t(n1)) + sizeof(int) * (size_t(n2) + 1);
+__host__ __device__ inline size_t tile_up_smem(int n3, int n2, int n1, int e) {
+    return sizeof(T) * (size_t(n3) + 3 * size_t(n2) + 2 * size_t(n1) + size_t(e)) + sizeof(int) * (size_t(n2) + 1) +
+           sizeof(short) * size_t(e);
+}
+
+// the tile's local CSR into shared memory (coalesced copies)
+template <typename T>
+__device__ __forceinline__ void tile_stage_csr(const TileView<T>& V, int t, int n2, T* sval, int* slrp, short* slc) {
+    const int* rowp = V.lrp + V.lrp_off[t];
+    const int e0 = V.ent_off[t], ne = V.ent_off[t + 1] - e0;
+    const T* val = V.val + e0;
+    const short* lc = V.lcol + e0;
+    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+        sval[e] = val[e];
+        slc[e] = lc[e];
+    }
+    for (int k = threadIdx.x; k <= n2; k += blockDim.x) slrp[k] = rowp[k];
 }
 
 template <typename T>
@@ -85,13 +104,13 @@ __global__ void __launch_bounds__(kTileThreads)
     T* ti = xb + V.n2max;
     T* rr = ti + V.n1max;
     T* ss = rr + V.n1max;
-    int* lrp = reinterpret_cast<int*>(ss + V.n1max);
+    T* val = ss + V.n1max;
+    int* lrp = reinterpret_cast<int*>(val + V.emax);
+    short* lc = reinterpret_cast<short*>(lrp + V.n2max + 1);
     const int t = blockIdx.x;
     const int4 R = V.ring[t];
     const int* cell = V.cell + V.cell_off[t];
-    const int* rowp = V.lrp + V.lrp_off[t];
-    const T* val = V.val + V.ent_off[t];
-    const short* lc = V.lcol + V.ent_off[t];
+    tile_stage_csr(V, t, R.z, val, lrp, lc);
     const double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
     for (int k = threadIdx.x; k < R.w; k += blockDim.x) {
         const int g = cell[k];
@@ -102,7 +121,6 @@ __global__ void __launch_bounds__(kTileThreads)
         xa[k] = L.w * dk * bk;
         if (k < R.y) ti[k] = L.tinv[g];
     }
-    for (int k = threadIdx.x; k <= R.z; k += blockDim.x) lrp[k] = rowp[k];
     __syncthreads();
     for (int k = threadIdx.x; k < R.z; k += blockDim.x) {
         const T acc = tile_rowdot(val, lc, lrp, xa, k);
@@ -164,13 +182,13 @@ __global__ void __launch_bounds__(kTileThreads)
     T* ti = dv + V.n2max;
     T* bp = ti + V.n2max;
     T* xq = bp + V.n1max;
-    int* lrp = reinterpret_cast<int*>(xq + V.n1max);
+    T* val = xq + V.n1max;
+    int* lrp = reinterpret_cast<int*>(val + V.emax);
+    short* lc = reinterpret_cast<short*>(lrp + V.n2max + 1);
     const int t = blockIdx.x;
     const int4 R = V.ring[t];
     const int* cell = V.cell + V.cell_off[t];
-    const int* rowp = V.lrp + V.lrp_off[t];
-    const T* val = V.val + V.ent_off[t];
-    const short* lc = V.lcol + V.ent_off[t];
+    tile_stage_csr(V, t, R.z, val, lrp, lc);
     for (int k = threadIdx.x; k < R.w; k += blockDim.x) {
         const int g = cell[k];
         e[k] = xc[L.owner[g]];
@@ -181,7 +199,6 @@ __global__ void __launch_bounds__(kTileThreads)
         }
         if (k < R.y) bp[k] = L.bp[g];
     }
-    for (int k = threadIdx.x; k <= R.z; k += blockDim.x) lrp[k] = rowp[k];
     __syncthreads();
     for (int k = threadIdx.x; k < R.z; k += blockDim.x) {
         const T ae = tile_rowdot(val, lc, lrp, e, k);
