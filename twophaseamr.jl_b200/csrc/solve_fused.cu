@@ -1121,7 +1121,7 @@ void DeviceSolver::upload_tiles(const Hierarchy& h) {
     tf_.assign(size_t(nl), TileView<float>{});
     if (!cfg.tiles || rb_ || !fused_ok_ || coop_grid_ > 0) return;
     // a tile's arrays live in shared memory: at most this many cells (rings <= 3)
-    constexpr int kTileMaxCells = 1536;
+    constexpr int kTileMaxCells = kTileCellsPerThread * kTileThreads;
     size_t down_d = 0, up_d = 0;
     for (int l = 0; l < tail_first_ && l + 1 < nl; ++l) {
         if (sdev_[size_t(l)].vec) {
@@ -1141,6 +1141,7 @@ void DeviceSolver::upload_tiles(const Hierarchy& h) {
         D.emax = T.emax;
         D.nent = int(T.pos.size());
         D.cell.upload(T.cell.data(), T.cell.size(), stream_);
+        D.own.upload(T.own.data(), T.own.size(), stream_);
         D.cell_off.upload(T.cell_off.data(), T.cell_off.size(), stream_);
         D.ring.upload(T.ring.data(), T.ring.size(), stream_);
         D.lrp.upload(T.lrp.data(), T.lrp.size(), stream_);
@@ -1161,6 +1162,7 @@ void DeviceSolver::upload_tiles(const Hierarchy& h) {
             v.n1max = D.n1max;
             v.emax = D.emax;
             v.cell = D.cell.p;
+            v.own = D.own.p;
             v.cell_off = D.cell_off.p;
             v.ring = reinterpret_cast<const int4*>(D.ring.p);
             v.lrp = D.lrp.p;

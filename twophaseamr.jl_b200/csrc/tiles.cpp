@@ -96,6 +96,7 @@ TileLevelHost build_tiles(const Csr& A, int64_t nblocks, int64_t cpb, const std:
         for (int32_t g : cells) loc[size_t(g)] = -1;
         if (!fits) return TileLevelHost();
         T.cell.insert(T.cell.end(), cells.begin(), cells.end());
+        for (int32_t g : cells) T.own.push_back(owner[size_t(g)]);
         for (int r = 0; r < 4; ++r) T.ring.push_back(ring[r]);
         T.cell_off.push_back(int32_t(T.cell.size()));
         T.lrp_off.push_back(int32_t(T.lrp.size()));

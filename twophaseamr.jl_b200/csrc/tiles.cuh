@@ -36,6 +36,7 @@ struct TileView {
     int ntiles;
     int n3max, n2max, n1max, emax;
     const int* cell;
+    const int* own;    // parallel to cell: tentative owner on the coarse level
     const int* cell_off;
     const int4* ring;  // per tile: cells of rings <= 0, 1, 2, 3
     const int* lrp;
@@ -63,16 +64,39 @@ __host__ __device__ inline size_t tile_up_smem(int n3, int n2, int n1, int e) {
            sizeof(short) * size_t(e);
 }
 
-// the tile's local CSR into shared memory (coalesced copies)
+// Loads in flight per thread in the prologues: a CTA's latency is that of its
+// dependent load chains, so every batch of independent loads is issued before
+// any of them is used.
+constexpr int kTileCellsPerThread = 6;   // cells of a tile: at most 6 x 256 = 1536
+constexpr int kTileEntriesPerThread = 8;
+
+// the tile's local CSR into shared memory (coalesced copies, 8 entries in flight)
 template <typename T>
 __device__ __forceinline__ void tile_stage_csr(const TileView<T>& V, int t, int n2, T* sval, int* slrp, short* slc) {
     const int* rowp = V.lrp + V.lrp_off[t];
     const int e0 = V.ent_off[t], ne = V.ent_off[t + 1] - e0;
     const T* val = V.val + e0;
     const short* lc = V.lcol + e0;
-    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-        sval[e] = val[e];
-        slc[e] = lc[e];
+    constexpr int U = kTileEntriesPerThread;
+    for (int base = threadIdx.x; base < ne; base += U * kTileThreads) {
+        T v[U];
+        short c[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = base + u * kTileThreads;
+            if (e < ne) {
+                v[u] = val[e];
+                c[u] = lc[e];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = base + u * kTileThreads;
+            if (e < ne) {
+                sval[e] = v[u];
+                slc[e] = c[u];
+            }
+        }
     }
     for (int k = threadIdx.x; k <= n2; k += blockDim.x) slrp[k] = rowp[k];
 }
@@ -110,16 +134,39 @@ __global__ void __launch_bounds__(kTileThreads)
     const int t = blockIdx.x;
     const int4 R = V.ring[t];
     const int* cell = V.cell + V.cell_off[t];
+    constexpr int CU = kTileCellsPerThread;
+    int g[CU];
+#pragma unroll
+    for (int u = 0; u < CU; ++u) {
+        const int k = threadIdx.x + u * kTileThreads;
+        g[u] = k < R.w ? cell[k] : -1;
+    }
     tile_stage_csr(V, t, R.z, val, lrp, lc);
     const double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
-    for (int k = threadIdx.x; k < R.w; k += blockDim.x) {
-        const int g = cell[k];
-        const T bk = proj_b<T, TB>(L, b, mean, g);
-        const T dk = L.dinv[g];
-        bp[k] = bk;
-        dv[k] = dk;
-        xa[k] = L.w * dk * bk;
-        if (k < R.y) ti[k] = L.tinv[g];
+    TB bb[CU];
+    T vv[CU], dd[CU], tt[CU];
+#pragma unroll
+    for (int u = 0; u < CU; ++u) {
+        if (g[u] >= 0) {
+            bb[u] = b[g[u]];
+            vv[u] = L.singular ? L.vol[g[u]] : T(0);
+            dd[u] = L.dinv[g[u]];
+            tt[u] = L.tinv[g[u]];
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < CU; ++u) {
+        const int k = threadIdx.x + u * kTileThreads;
+        if (g[u] >= 0) {
+            // the projected RHS as proj_b forms it
+            double v = double(bb[u]);
+            if (L.singular) v -= double(vv[u]) * mean;
+            const T bk = T(v);
+            bp[k] = bk;
+            dv[k] = dd[u];
+            xa[k] = L.w * dd[u] * bk;
+            if (k < R.y) ti[k] = tt[u];
+        }
     }
     __syncthreads();
     for (int k = threadIdx.x; k < R.z; k += blockDim.x) {
@@ -188,16 +235,42 @@ __global__ void __launch_bounds__(kTileThreads)
     const int t = blockIdx.x;
     const int4 R = V.ring[t];
     const int* cell = V.cell + V.cell_off[t];
+    const int* own = V.own + V.cell_off[t];
+    constexpr int CU = kTileCellsPerThread;
+    int g[CU], o[CU];
+#pragma unroll
+    for (int u = 0; u < CU; ++u) {
+        const int k = threadIdx.x + u * kTileThreads;
+        g[u] = k < R.w ? cell[k] : -1;
+        o[u] = k < R.w ? own[k] : -1;
+    }
     tile_stage_csr(V, t, R.z, val, lrp, lc);
-    for (int k = threadIdx.x; k < R.w; k += blockDim.x) {
-        const int g = cell[k];
-        e[k] = xc[L.owner[g]];
-        if (k < R.z) {
-            xp[k] = L.y[g];
-            dv[k] = L.dinv[g];
-            ti[k] = L.tinv[g];
+    T ee[CU], yy[CU], dd[CU], tt[CU], bb[CU];
+#pragma unroll
+    for (int u = 0; u < CU; ++u) {
+        const int k = threadIdx.x + u * kTileThreads;
+        if (g[u] >= 0) {
+            ee[u] = xc[o[u]];
+            if (k < R.z) {
+                yy[u] = L.y[g[u]];
+                dd[u] = L.dinv[g[u]];
+                tt[u] = L.tinv[g[u]];
+            }
+            if (k < R.y) bb[u] = L.bp[g[u]];
         }
-        if (k < R.y) bp[k] = L.bp[g];
+    }
+#pragma unroll
+    for (int u = 0; u < CU; ++u) {
+        const int k = threadIdx.x + u * kTileThreads;
+        if (g[u] >= 0) {
+            e[k] = ee[u];
+            if (k < R.z) {
+                xp[k] = yy[u];
+                dv[k] = dd[u];
+                ti[k] = tt[u];
+            }
+            if (k < R.y) bp[k] = bb[u];
+        }
     }
     __syncthreads();
     for (int k = threadIdx.x; k < R.z; k += blockDim.x) {
@@ -298,21 +371,34 @@ __global__ void __launch_bounds__(kTileThreads)
     vt_blocks(L, b, nb9);
     const double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
     __syncthreads();
-    for (int q = threadIdx.x; q < N; q += blockDim.x) {
-        const int i = q % vt::R - 3, j = q / vt::R - 3;
-        const int c = vt_cell(nb9, i, j);
-        T bv = T(0), d = T(0);
-        if (c >= 0) {
-            const TB a = bin[c];
-            if (mean != 0.0) {
-                const double v = L.const_vol ? double(L.vol0) : double(L.vol[c]);
-                bv = T(double(a) - v * mean);
-            } else {
-                bv = T(a);
-            }
-            d = L.dinv ? L.dinv[c] : L.dinv0;
+    // the region's loads, all issued before any is used
+    constexpr int QU = (N + kTileThreads - 1) / kTileThreads;
+    int c[QU];
+    TB a[QU];
+    T vo[QU], dd[QU];
+#pragma unroll
+    for (int u = 0; u < QU; ++u) {
+        const int q = threadIdx.x + u * kTileThreads;
+        c[u] = q < N ? vt_cell(nb9, q % vt::R - 3, q / vt::R - 3) : -1;
+    }
+#pragma unroll
+    for (int u = 0; u < QU; ++u) {
+        if (c[u] >= 0) {
+            a[u] = bin[c[u]];
+            vo[u] = (mean != 0.0 && !L.const_vol) ? L.vol[c[u]] : L.vol0;
+            dd[u] = L.dinv ? L.dinv[c[u]] : L.dinv0;
         }
-        ex[q] = c >= 0;
+    }
+#pragma unroll
+    for (int u = 0; u < QU; ++u) {
+        const int q = threadIdx.x + u * kTileThreads;
+        if (q >= N) continue;
+        T bv = T(0), d = T(0);
+        if (c[u] >= 0) {
+            bv = mean != 0.0 ? T(double(a[u]) - double(vo[u]) * mean) : T(a[u]);
+            d = dd[u];
+        }
+        ex[q] = c[u] >= 0;
         sb[q] = bv;
         sd[q] = d;
         sx[q] = L.w * d * bv;  // the first sweep from zero, pointwise
@@ -391,25 +477,52 @@ __global__ void __launch_bounds__(kTileThreads)
     const int b = blockIdx.x;
     vt_blocks(L, b, nb9);
     __syncthreads();
-    for (int q = threadIdx.x; q < N; q += blockDim.x) {
-        const int i = q % vt::R - 3, j = q / vt::R - 3;
-        const int bx = i < 0 ? -1 : (i > 15 ? 1 : 0), by = j < 0 ? -1 : (j > 15 ? 1 : 0);
-        const int B = nb9[(by + 1) * 3 + bx + 1];
-        ex[q] = B >= 0;
-        T e = T(0), x = T(0), d = T(0), bp = T(0);
-        if (B >= 0) {
-            const int li = i - 16 * bx, lj = j - 16 * by, c = B * 256 + lj * 16 + li;
-            e = vt_coarse(L, xc, B, li, lj);
-            if (i >= -2 && i <= 17 && j >= -2 && j <= 17) {
-                x = L.y[c];
-                d = L.dinv ? L.dinv[c] : L.dinv0;
-                if (i >= -1 && i <= 16 && j >= -1 && j <= 16) bp = L.bp[c];
+    // the region's loads, all issued before any is used
+    constexpr int QU = (N + kTileThreads - 1) / kTileThreads;
+    int4 mp[QU];
+    int c[QU], li[QU], lj[QU], ring[QU];
+#pragma unroll
+    for (int u = 0; u < QU; ++u) {
+        const int q = threadIdx.x + u * kTileThreads;
+        c[u] = -1;
+        if (q < N) {
+            const int i = q % vt::R - 3, j = q / vt::R - 3;
+            const int bx = i < 0 ? -1 : (i > 15 ? 1 : 0), by = j < 0 ? -1 : (j > 15 ? 1 : 0);
+            const int B = nb9[(by + 1) * 3 + bx + 1];
+            li[u] = i - 16 * bx;
+            lj[u] = j - 16 * by;
+            // 3: the outer frame (e only), 2: x and D^-1 too, 1: also bp
+            ring[u] = max(max(-i, i - 15), max(-j, j - 15));
+            if (B >= 0) {
+                c[u] = B * 256 + lj[u] * 16 + li[u];
+                mp[u] = *reinterpret_cast<const int4*>(L.map + 4 * B);
             }
         }
-        se[q] = e;
-        sp[q] = x;
-        sd[q] = d;
-        sb[q] = bp;
+    }
+    T e[QU], x[QU], d[QU], bp[QU];
+#pragma unroll
+    for (int u = 0; u < QU; ++u) {
+        e[u] = x[u] = d[u] = bp[u] = T(0);
+        if (c[u] >= 0) {
+            const int4 m = mp[u];
+            e[u] = m.w == 1 ? xc[m.x * 256 + (m.z + lj[u]) * 16 + m.y + li[u]]
+                            : xc[m.x * 256 + (m.z + (lj[u] >> 1)) * 16 + m.y + (li[u] >> 1)];
+            if (ring[u] <= 2) {
+                x[u] = L.y[c[u]];
+                d[u] = L.dinv ? L.dinv[c[u]] : L.dinv0;
+                if (ring[u] <= 1) bp[u] = L.bp[c[u]];
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < QU; ++u) {
+        const int q = threadIdx.x + u * kTileThreads;
+        if (q >= N) continue;
+        ex[q] = c[u] >= 0;
+        se[q] = e[u];
+        sp[q] = x[u];
+        sd[q] = d[u];
+        sb[q] = bp[u];
     }
     __syncthreads();
     for (int q = threadIdx.x; q < 20 * 20; q += blockDim.x) {

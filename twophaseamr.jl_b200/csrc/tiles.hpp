@@ -30,6 +30,7 @@ struct TileLevelHost {
     // order (n0 of them), then ring 1, ring 2, ring 3; ring[4 t + r] = cells of
     // rings <= r (ring[4 t] = n0)
     std::vector<int32_t> cell, cell_off, ring;
+    std::vector<int32_t> own;  // parallel to cell: the tentative owner (coarse cell) of each tile cell
     // local rows 0 .. n2 - 1 of tile t: entries lrp[lrp_off[t] + k] ..
     // lrp[lrp_off[t] + k + 1] (relative to ent_off[t]) in CSR order; pos is the
     // entry's position in the level CSR, lcol its column as a local cell index
