@@ -282,6 +282,7 @@ private:
         bool on = false;   // CSR tiles (k_tile_*)
         bool vec = false;  // constant-coefficient 16x16 level: stencil tiles (v_tile_*)
         int ntiles = 0, n3max = 0, n2max = 0, n1max = 0, emax = 0, nent = 0;
+        int nt = 256;  // threads per CTA
         DevArray<int> cell, own, cell_off, ring, lrp, lrp_off, ent_off, pos, co, co_off;
         DevArray<int16_t> lcol, ch;
         DevArray<double> val_d;

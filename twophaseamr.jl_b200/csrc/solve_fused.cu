@@ -286,6 +286,16 @@ __global__ void __launch_bounds__(256) v_cg_residual(SView<double> L, const doub
     }
 }
 
+// CTA size of a level's CSR tiles: every tile resident in one wave with as
+// many warps per tile as that allows (a tile's phases are dependent chains,
+// so its latency falls with the warps that share them)
+template <typename F>
+void with_tile_threads(int nt, F f) {
+    if (nt == 1024) f(std::integral_constant<int, 1024>());
+    else if (nt == 512) f(std::integral_constant<int, 512>());
+    else f(std::integral_constant<int, 256>());
+}
+
 template <typename T, typename F>
 void with_nxc(const SView<T>& S, F f) {
     if (S.nx == 16 && S.ny == 16) f(std::integral_constant<int, 16>{});
@@ -694,13 +704,16 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
             const TileView<T>& TV = tile_view<T>(l);
             const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
             const size_t sm = tile_down_smem<T>(D.n3max, D.n2max, D.n1max, D.emax);
-            if (l == 0)
-                go(k_tile_down<T, double>, D.ntiles, kTileThreads, sm, L, TV, r, rsum, V[size_t(l + 1)].b,
-                   fpartial_.p, counters_.p + kRestrictSum, next_sum ? lsum_.p + l + 1 : nullptr);
-            else
-                go(k_tile_down<T, T>, D.ntiles, kTileThreads, sm, L, TV, (const T*)L.b, (const double*)(lsum_.p + l),
-                   V[size_t(l + 1)].b, fpartial_.p, counters_.p + kRestrictSum,
-                   next_sum ? lsum_.p + l + 1 : nullptr);
+            with_tile_threads(D.nt, [&](auto nt) {
+                constexpr int NT = decltype(nt)::value;
+                if (l == 0)
+                    go(k_tile_down<T, double, NT>, D.ntiles, NT, sm, L, TV, r, rsum, V[size_t(l + 1)].b, fpartial_.p,
+                       counters_.p + kRestrictSum, next_sum ? lsum_.p + l + 1 : nullptr);
+                else
+                    go(k_tile_down<T, T, NT>, D.ntiles, NT, sm, L, TV, (const T*)L.b, (const double*)(lsum_.p + l),
+                       V[size_t(l + 1)].b, fpartial_.p, counters_.p + kRestrictSum,
+                       next_sum ? lsum_.p + l + 1 : nullptr);
+            });
             ++launches_;
             continue;
         }
@@ -785,9 +798,12 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
             // prolongation and both post-sweeps in one launch
             const TileDev& D = tdev_[size_t(l)];
             const bool want_mean = (l == 0) && L.singular;
-            go(k_tile_up<T, Epi>, D.ntiles, kTileThreads, tile_up_smem<T>(D.n3max, D.n2max, D.n1max, D.emax), L,
-               tile_view<T>(l), (const T*)V[size_t(l + 1)].x, fpartial_.p, counters_.p + kPostMean,
-               want_mean ? mean_out : nullptr, epi);
+            with_tile_threads(D.nt, [&](auto nt) {
+                constexpr int NT = decltype(nt)::value;
+                go(k_tile_up<T, Epi, NT>, D.ntiles, NT, tile_up_smem<T>(D.n3max, D.n2max, D.n1max, D.emax), L,
+                   tile_view<T>(l), (const T*)V[size_t(l + 1)].x, fpartial_.p, counters_.p + kPostMean,
+                   want_mean ? mean_out : nullptr, epi);
+            });
             ++launches_;
             continue;
         }
@@ -1103,11 +1119,15 @@ const TileView<T>& DeviceSolver::tile_view(int l) const {
 
 template <typename T, typename TB>
 static void allow_tile_down_smem(size_t bytes) {
-    TPA_CUDA(cudaFuncSetAttribute(k_tile_down<T, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    TPA_CUDA(cudaFuncSetAttribute(k_tile_down<T, TB, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    TPA_CUDA(cudaFuncSetAttribute(k_tile_down<T, TB, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    TPA_CUDA(cudaFuncSetAttribute(k_tile_down<T, TB, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
 }
 template <typename T, typename Epi>
 static void allow_tile_up_smem(size_t bytes) {
-    TPA_CUDA(cudaFuncSetAttribute(k_tile_up<T, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    TPA_CUDA(cudaFuncSetAttribute(k_tile_up<T, Epi, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    TPA_CUDA(cudaFuncSetAttribute(k_tile_up<T, Epi, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    TPA_CUDA(cudaFuncSetAttribute(k_tile_up<T, Epi, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
 }
 
 // Tiles of every CSR level of the multi-CTA part of the default cycle (not the
@@ -1121,7 +1141,8 @@ void DeviceSolver::upload_tiles(const Hierarchy& h) {
     tf_.assign(size_t(nl), TileView<float>{});
     if (!cfg.tiles || rb_ || !fused_ok_ || coop_grid_ > 0) return;
     // a tile's arrays live in shared memory: at most this many cells (rings <= 3)
-    constexpr int kTileMaxCells = kTileCellsPerThread * kTileThreads;
+    int sms = 148;
+    TPA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
     size_t down_d = 0, up_d = 0;
     for (int l = 0; l < tail_first_ && l + 1 < nl; ++l) {
         if (sdev_[size_t(l)].vec) {
@@ -1139,6 +1160,8 @@ void DeviceSolver::upload_tiles(const Hierarchy& h) {
         D.n2max = T.n2max;
         D.n1max = T.n1max;
         D.emax = T.emax;
+        // 2 CTAs of 1024 threads, 4 of 512 fit an SM (by threads)
+        D.nt = T.ntiles <= 2 * sms ? 1024 : T.ntiles <= 4 * sms ? 512 : 256;
         D.nent = int(T.pos.size());
         D.cell.upload(T.cell.data(), T.cell.size(), stream_);
         D.own.upload(T.own.data(), T.own.size(), stream_);

@@ -28,7 +28,8 @@
 
 namespace tpa {
 
-constexpr int kTileThreads = 256;
+constexpr int kTileThreads = 256;  // stencil tiles; CSR tiles take NT = 256, 512 or 1024
+constexpr int kTileMaxCells = 1536;  // cells of a CSR tile (rings <= 3) at most
 
 // One level's tiles in precision T (device pointers).
 template <typename T>
@@ -67,23 +68,22 @@ __host__ __device__ inline size_t tile_up_smem(int n3, int n2, int n1, int e) {
 // Loads in flight per thread in the prologues: a CTA's latency is that of its
 // dependent load chains, so every batch of independent loads is issued before
 // any of them is used.
-constexpr int kTileCellsPerThread = 6;   // cells of a tile: at most 6 x 256 = 1536
 constexpr int kTileEntriesPerThread = 8;
 
 // the tile's local CSR into shared memory (coalesced copies, 8 entries in flight)
-template <typename T>
+template <typename T, int NT>
 __device__ __forceinline__ void tile_stage_csr(const TileView<T>& V, int t, int n2, T* sval, int* slrp, short* slc) {
     const int* rowp = V.lrp + V.lrp_off[t];
     const int e0 = V.ent_off[t], ne = V.ent_off[t + 1] - e0;
     const T* val = V.val + e0;
     const short* lc = V.lcol + e0;
     constexpr int U = kTileEntriesPerThread;
-    for (int base = threadIdx.x; base < ne; base += U * kTileThreads) {
+    for (int base = threadIdx.x; base < ne; base += U * NT) {
         T v[U];
         short c[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const int e = base + u * kTileThreads;
+            const int e = base + u * NT;
             if (e < ne) {
                 v[u] = val[e];
                 c[u] = lc[e];
@@ -91,7 +91,7 @@ __device__ __forceinline__ void tile_stage_csr(const TileView<T>& V, int t, int 
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const int e = base + u * kTileThreads;
+            const int e = base + u * NT;
             if (e < ne) {
                 sval[e] = v[u];
                 slc[e] = c[u];
@@ -115,8 +115,8 @@ __device__ __forceinline__ int short4_at(short4 v, int q) {
 // b: this level's raw right-hand side (the FP64 residual on the finest level);
 // level_sum: its sum (projection, may be null); bc: the coarse right-hand side;
 // coarse_sum (may be null): receives the sum of bc, folded by the last CTA.
-template <typename T, typename TB>
-__global__ void __launch_bounds__(kTileThreads)
+template <typename T, typename TB, int NT>
+__global__ void __launch_bounds__(NT)
     k_tile_down(LevelView<T> L, TileView<T> V, const TB* __restrict__ b, const double* level_sum,
                 T* __restrict__ bc, double* partial, unsigned* counter, double* coarse_sum) {
     pdl_entry();
@@ -134,14 +134,14 @@ __global__ void __launch_bounds__(kTileThreads)
     const int t = blockIdx.x;
     const int4 R = V.ring[t];
     const int* cell = V.cell + V.cell_off[t];
-    constexpr int CU = kTileCellsPerThread;
+    constexpr int CU = (kTileMaxCells + NT - 1) / NT;
     int g[CU];
 #pragma unroll
     for (int u = 0; u < CU; ++u) {
-        const int k = threadIdx.x + u * kTileThreads;
+        const int k = threadIdx.x + u * NT;
         g[u] = k < R.w ? cell[k] : -1;
     }
-    tile_stage_csr(V, t, R.z, val, lrp, lc);
+    tile_stage_csr<T, NT>(V, t, R.z, val, lrp, lc);
     const double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
     TB bb[CU];
     T vv[CU], dd[CU], tt[CU];
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kTileThreads)
     }
 #pragma unroll
     for (int u = 0; u < CU; ++u) {
-        const int k = threadIdx.x + u * kTileThreads;
+        const int k = threadIdx.x + u * NT;
         if (g[u] >= 0) {
             // the projected RHS as proj_b forms it
             double v = double(bb[u]);
@@ -217,8 +217,8 @@ __global__ void __launch_bounds__(kTileThreads)
 
 // xc: the coarse level's correction; mean_out (may be null): the volume mean
 // of the result, folded by the last CTA, which then runs `epi`.
-template <typename T, typename Epi>
-__global__ void __launch_bounds__(kTileThreads)
+template <typename T, typename Epi, int NT>
+__global__ void __launch_bounds__(NT)
     k_tile_up(LevelView<T> L, TileView<T> V, const T* __restrict__ xc, double* partial, unsigned* counter,
               double* mean_out, Epi epi) {
     pdl_entry();
@@ -236,19 +236,19 @@ __global__ void __launch_bounds__(kTileThreads)
     const int4 R = V.ring[t];
     const int* cell = V.cell + V.cell_off[t];
     const int* own = V.own + V.cell_off[t];
-    constexpr int CU = kTileCellsPerThread;
+    constexpr int CU = (kTileMaxCells + NT - 1) / NT;
     int g[CU], o[CU];
 #pragma unroll
     for (int u = 0; u < CU; ++u) {
-        const int k = threadIdx.x + u * kTileThreads;
+        const int k = threadIdx.x + u * NT;
         g[u] = k < R.w ? cell[k] : -1;
         o[u] = k < R.w ? own[k] : -1;
     }
-    tile_stage_csr(V, t, R.z, val, lrp, lc);
+    tile_stage_csr<T, NT>(V, t, R.z, val, lrp, lc);
     T ee[CU], yy[CU], dd[CU], tt[CU], bb[CU];
 #pragma unroll
     for (int u = 0; u < CU; ++u) {
-        const int k = threadIdx.x + u * kTileThreads;
+        const int k = threadIdx.x + u * NT;
         if (g[u] >= 0) {
             ee[u] = xc[o[u]];
             if (k < R.z) {
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(kTileThreads)
     }
 #pragma unroll
     for (int u = 0; u < CU; ++u) {
-        const int k = threadIdx.x + u * kTileThreads;
+        const int k = threadIdx.x + u * NT;
         if (g[u] >= 0) {
             e[k] = ee[u];
             if (k < R.z) {
