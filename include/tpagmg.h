@@ -217,11 +217,12 @@ tpa_status tpa_batch_solve_device(tpa_batch* batch, const double* rhs, double* x
  * recomputed inside the restriction (one launch instead of two); persistent:
  * when every multi-CTA level is a CSR level, the whole V-cycle runs as one
  * cooperative launch with grid barriers (bounded waits; a barrier that gives up
- * makes the solve return TPA_ERR_TIMEOUT); tiles: each CSR level of the
- * multi-CTA part runs as two launches on haloed block tiles (both pre-sweeps,
- * the residual and the restriction in one, the prolongation and both
- * post-sweeps in the other; the halo is recomputed in each tile).  Every
- * layout gives the same V-cycle to rounding. */
+ * makes the solve return TPA_ERR_TIMEOUT); tiles: 1 (the default) runs each
+ * CSR level of the multi-CTA part as two launches on haloed block tiles (both
+ * pre-sweeps, the residual and the restriction in one, the prolongation and
+ * both post-sweeps in the other; the halo is recomputed in each tile), 2 also
+ * the constant-coefficient 16x16 levels (on 22 x 22 stencil tiles), 0 none.
+ * Every layout gives the same V-cycle to rounding. */
 typedef struct {
     int32_t tail_cells, tail_ctas, structured, vectorized, pdl, fuse_restrict, persistent, tiles;
     double ms_per_vcycle; /* measured time (tpa_autotune), else 0 */

@@ -115,7 +115,7 @@ def test_stencil_tiles_match_vectorized_kernels(name):
     m = BlockTreeMesh(**spec)
     s = EllipticSolver(PoissonOperator(m), multigrid=MultigridOptions(coarse_size=64))
     s0 = EllipticSolver(PoissonOperator(m), multigrid=MultigridOptions(coarse_size=64))
-    s.set_tuning(tiles=1, tail_cells=1024)
+    s.set_tuning(tiles=2, tail_cells=1024)
     s0.set_tuning(tiles=0, tail_cells=1024)
     assert s.device_info()["structured_levels"] >= 1
     assert s.tiled_levels() >= 1 and s0.tiled_levels() == 0

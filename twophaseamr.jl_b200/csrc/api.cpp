@@ -1069,12 +1069,13 @@ tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tp
         run(pe);
         // the CSR levels on haloed block tiles (two launches per level), with
         // the tail sizes around the best one
-        for (int cells : {1024, 2048, 4096}) {
-            tpa::TuneConfig tl = b0;
-            tl.tiles = 1;
-            tl.tail_cells = cells;
-            run(tl);
-        }
+        for (int tiles : {1, 2})
+            for (int cells : {1024, 2048, 4096}) {
+                tpa::TuneConfig tl = b0;
+                tl.tiles = tiles;
+                tl.tail_cells = cells;
+                run(tl);
+            }
         const size_t b = best_of();
         d.reconfigure(ctx->hier, res[b].first);
         if (best) *best = to_c(res[b].first, res[b].second);
@@ -1087,7 +1088,8 @@ tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tp
 tpa_status tpa_set_tuning(tpa_context* ctx, const tpa_tune_config* cfg) {
     return guard(ctx, [&] {
         if (!cfg) throw tpa::Error(TPA_ERR_INVALID_ARG, "null configuration");
-        if (cfg->tail_ctas > 8 || cfg->structured > 2) throw tpa::Error(TPA_ERR_INVALID_ARG, "bad configuration");
+        if (cfg->tail_ctas > 8 || cfg->structured > 2 || cfg->tiles > 2)
+            throw tpa::Error(TPA_ERR_INVALID_ARG, "bad configuration");
         ensure_device(ctx);
         ensure_host_fresh(ctx);  // stencil copies come from the host levels
         ctx->dev->reconfigure(ctx->hier, from_c(*cfg));

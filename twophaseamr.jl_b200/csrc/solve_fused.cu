@@ -508,8 +508,12 @@ TuneConfig DeviceSolver::effective_tuning() const {
     if (tune_.fuse_restrict >= 0) c.fuse_restrict = tune_.fuse_restrict;
     c.persistent = std::getenv("TPAGMG_PERSISTENT") ? 1 : 0;
     if (tune_.persistent >= 0) c.persistent = tune_.persistent ? 1 : 0;
-    c.tiles = std::getenv("TPAGMG_TILES") ? std::atoi(std::getenv("TPAGMG_TILES")) != 0 : 0;
-    if (tune_.tiles >= 0) c.tiles = tune_.tiles ? 1 : 0;
+    // 1: CSR levels on tiles (the default: measured faster on the droplet),
+    // 2: the constant-coefficient 16x16 levels on stencil tiles as well
+    // (measured slower than the vectorized kernels on uniform 2048^2), 0: none
+    c.tiles = 1;
+    if (const char* e = std::getenv("TPAGMG_TILES")) c.tiles = std::min(2, std::max(0, std::atoi(e)));
+    if (tune_.tiles >= 0) c.tiles = std::min(2, tune_.tiles);
     if (rb_) {  // the red-black sweeps exist for the CSR levels and the tail only
         c.structured = 0;
         c.persistent = 0;
@@ -1146,7 +1150,7 @@ void DeviceSolver::upload_tiles(const Hierarchy& h) {
     size_t down_d = 0, up_d = 0;
     for (int l = 0; l < tail_first_ && l + 1 < nl; ++l) {
         if (sdev_[size_t(l)].vec) {
-            tdev_[size_t(l)].vec = true;  // stencil tiles need no lists
+            tdev_[size_t(l)].vec = cfg.tiles >= 2;  // stencil tiles need no lists
             continue;
         }
         if (sdev_[size_t(l)].on) continue;
