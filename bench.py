@@ -464,16 +464,26 @@ def main():
         e2e_it = st.cycles
     e2e_ms_mean = float(np.mean(e2e_ms))
 
-    # roofline: fine-level smoothing sweep of the mixed cycle, timed alone
-    sweep = C.c_double()
-    solver.ctx.call("tpa_time_kernel", 0, 0, 1, 200, C.byref(sweep))
-    sweep64 = C.c_double()
-    solver.ctx.call("tpa_time_kernel", 0, 0, 0, 200, C.byref(sweep64))
-    # algorithmic bytes of one damped-Jacobi sweep: read x and b, write x, plus
-    # two face coefficients per cell when they vary (3 s + 2 s_kappa)
+    # roofline of the dominant kernel, timed alone (CUDA events, 200 launches):
+    # with the finest level on CSR tiles its down kernel (both pre-sweeps, the
+    # residual and the restriction), else the smoothing sweep
     skappa = 0 if args.workload == "uniform_2048" else 1
-    alg32 = n * (3 * 4 + 2 * 4 * skappa)
-    alg64 = n * (3 * 8 + 2 * 8 * skappa)
+    sweep, sweep64 = C.c_double(), C.c_double()
+    try:
+        solver.ctx.call("tpa_time_kernel", 6, 0, 1, 200, C.byref(sweep))
+        solver.ctx.call("tpa_time_kernel", 6, 0, 0, 200, C.byref(sweep64))
+        # read the FP64 residual and two face coefficients, write the
+        # pre-smoothed iterate, the projected RHS and the coarse RHS (a quarter
+        # of a value per fine cell): 8 + 2 s_kappa + 2 s + s / 4
+        kname = "k_tile_down, finest level, FP32 cycle (both pre-sweeps, residual, restriction)"
+        alg32 = n * (8 + 2 * 4 * skappa + 2 * 4 + 1)
+    except _lib.TpaError:
+        solver.ctx.call("tpa_time_kernel", 0, 0, 1, 200, C.byref(sweep))
+        solver.ctx.call("tpa_time_kernel", 0, 0, 0, 200, C.byref(sweep64))
+        # one damped-Jacobi sweep: read x and b, write x, plus two face
+        # coefficients per cell when they vary (3 s + 2 s_kappa)
+        kname = "damped-Jacobi sweep, finest level, FP32"
+        alg32 = n * (3 * 4 + 2 * 4 * skappa)
     peak, peak_kind = measured_peaks()
     achieved = alg32 / (sweep.value * 1e-3) / 1e9
 
@@ -632,7 +642,7 @@ def main():
                 "ms_per_step": e2e_ms_mean, "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 8 * n},
         "gpu_launches": mixed_launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "damped-Jacobi sweep, finest level, FP32",
+                     "traffic": traffic, "kernel": kname,
                      "kernel_ms": sweep.value, "kernel_ms_fp64": sweep64.value,
                      "algorithmic_bytes": alg32, "peak_kind": peak_kind},
         "whole_solve_roofline": whole_solve_roofline(n, skappa, (mixed_it, mixed_ms), (fp64_it, fp64_ms), peak,

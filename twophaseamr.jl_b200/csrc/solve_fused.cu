@@ -1072,7 +1072,36 @@ double DeviceSolver::time_fused(int which, int level, int precision, int iters) 
             }
         });
     };
+    // 6 / 7: the down / up tile kernel of a tiled CSR level
+    auto one_tile = [&](const auto& V, auto tag) {
+        using T = decltype(tag);
+        const TileDev& D = tdev_[size_t(level)];
+        const LevelView<T>& L = V[size_t(level)];
+        const TileView<T>& TV = tile_view<T>(level);
+        with_tile_threads(D.nt, [&](auto nt) {
+            constexpr int NT = decltype(nt)::value;
+            const size_t sm = tile_down_smem<T>(D.n3max, D.n2max, D.n1max, D.emax);
+            if (which == 6 && level == 0)  // the finest level reads the FP64 residual, as in the cycle
+                k_tile_down<T, double, NT><<<D.ntiles, NT, sm, stream_>>>(
+                    L, TV, (const double*)r_.p, nullptr, V[size_t(level + 1)].b, fpartial_.p, counters_.p, nullptr);
+            else if (which == 6)
+                k_tile_down<T, T, NT><<<D.ntiles, NT, sm, stream_>>>(L, TV, (const T*)L.b, nullptr,
+                                                                     V[size_t(level + 1)].b, fpartial_.p,
+                                                                     counters_.p, nullptr);
+            else
+                k_tile_up<T, MeanOnly, NT><<<D.ntiles, NT, tile_up_smem<T>(D.n3max, D.n2max, D.n1max, D.emax),
+                                            stream_>>>(L, TV, (const T*)V[size_t(level + 1)].x, fpartial_.p,
+                                                       counters_.p, nullptr, MeanOnly());
+        });
+    };
     auto launch = [&]() {
+        if (which == 6 || which == 7) {
+            if (size_t(level) >= tdev_.size() || !tdev_[size_t(level)].on)
+                throw Error(1, "level does not run on CSR tiles");
+            if (precision == 0) one_tile(vd_, double(0));
+            else one_tile(vf_, float(0));
+            return;
+        }
         if (which == 3) {
             if (precision != 0 || level != 0) throw Error(1, "the CG operator runs in FP64 on the finest level");
             CgState* s = reinterpret_cast<CgState*>(cgs_.p);
