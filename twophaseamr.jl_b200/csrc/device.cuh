@@ -110,6 +110,7 @@ struct TuneConfig {
                              // 1 every level, above 1 levels of at most that many cells)
     int persistent = -1;     // all-CSR hierarchies: the V-cycle as one cooperative launch
     int tiles = -1;          // CSR levels: two launches per level on haloed block tiles (tiles.cuh)
+    int tail_smem = -1;      // 0: the coarse tail reads its levels from global memory
 };
 
 struct SolveStats {
@@ -252,6 +253,7 @@ public:
 private:
     int tail_first_ = 0;
     int tail_ctas_ = 1;  // CTAs of the coarse-tail cluster
+    size_t tail_smem_[2] = {0, 0};  // > 0: dynamic shared bytes of the staged tail (FP64, FP32 cycle)
     std::vector<LevelView<double>> vd_;
     std::vector<LevelView<float>> vf_;
     DevArray<LevelView<double>> vd_dev_;

@@ -15,6 +15,7 @@
 
 #include "device.cuh"
 #include "persistent.cuh"
+#include "tail_smem.cuh"
 
 namespace tpa {
 namespace {
@@ -593,6 +594,33 @@ void DeviceSolver::build_views() {
     }
     vd_dev_.upload(vd_.data(), vd_.size(), stream_);
     vf_dev_.upload(vf_.data(), vf_.size(), stream_);
+    // the coarse tail in shared memory when its levels fit (one CTA, Jacobi);
+    // TPAGMG_NO_TAIL_SMEM keeps the global-memory tail
+    tail_smem_[0] = tail_smem_[1] = 0;
+    if (fused_ok_ && !rb_ && tail_ctas_ == 1 && nl <= kTailSmemMaxLevels && !std::getenv("TPAGMG_NO_TAIL_SMEM") &&
+        (tune_.tail_smem != 0)) {
+        size_t bd = 0, bf = 0;
+        for (int l = tail_first_; l < nl; ++l) {
+            const DevLevel& L = levels_[size_t(l)];
+            const bool last = l == nl - 1;
+            bd += tail_level_bytes<double>(L.n, int(L.nnz), last ? 0 : L.nc, last);
+            bf += tail_level_bytes<float>(L.n, int(L.nnz), last ? 0 : L.nc, last);
+        }
+        int optin = 0;
+        TPA_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
+        // room for the kernel's static shared memory (views, reductions)
+        const size_t room = size_t(optin) > 16384 ? size_t(optin) - 16384 : 0;
+        if (bd <= room) {
+            TPA_CUDA(cudaFuncSetAttribute(k_tail_smem<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(bd)));
+            tail_smem_[0] = bd;
+        }
+        if (bf <= room) {
+            TPA_CUDA(cudaFuncSetAttribute(k_tail_smem<float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(bf)));
+            tail_smem_[1] = bf;
+        }
+    }
     // every folding launch has at most max(maxgrid, kMaxGrid) CTAs
     fpartial_.alloc(size_t(std::max<int64_t>(maxgrid, kMaxGrid)));
     fpartial2_.alloc(size_t(std::max<int64_t>(maxgrid, kMaxGrid)));
@@ -757,10 +785,18 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
            next_sum ? lsum_.p + l + 1 : nullptr);
         launches_ += 3;
     }
+    const size_t tsm = tail_smem_[std::is_same<T, double>::value ? 0 : 1];
+    if (tsm > 0) {
+        // the tail's levels staged in shared memory (tail_smem.cuh)
+        go(k_tail_smem<T, double>, 1, kTailThreads, tsm, Vdev, t, nl, t == 0 ? r : nullptr, coarse_inv_.p, coarse_n_,
+           t == 0 && V[0].singular ? mean_out : nullptr);
+        ++launches_;
+    } else {
     const Launch gt{stream_, pdl_, tail_ctas_};
     gt(k_tail<T, double>, tail_ctas_, kTailThreads, 0, Vdev, t, nl, t == 0 ? r : nullptr, coarse_inv_.p, coarse_n_,
                                                          t == 0 && V[0].singular ? mean_out : nullptr);
     ++launches_;
+    }
     for (int l = t - 1; l >= 0; --l) {
         const LevelView<T>& L = V[size_t(l)];
         if (sdev_[size_t(l)].vec) {
