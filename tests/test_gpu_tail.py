@@ -1,5 +1,6 @@
-"""The coarse tail staged in shared memory (csrc/tail_smem.cuh) against the
-tail that reads its levels from global memory.  Both run the same phase code
+"""The coarse tail staged in shared memory (csrc/tail_smem.cuh, on request:
+TPAGMG_TAIL_SMEM) against the default tail that reads its levels from global
+memory.  Both run the same phase code
 on the same values, so V-cycles and solves agree bit for bit; the cases cover
 a tail below tiled levels, 8x8 blocks, and a hierarchy that lies entirely in
 the tail (its first level is the finest, read from the caller's residual)."""
@@ -38,15 +39,15 @@ def test_staged_tail_equals_global_tail(name, monkeypatch):
     out = {}
     for staged in (True, False):
         if staged:
-            monkeypatch.delenv("TPAGMG_NO_TAIL_SMEM", raising=False)
+            monkeypatch.setenv("TPAGMG_TAIL_SMEM", "1")
         else:
-            monkeypatch.setenv("TPAGMG_NO_TAIL_SMEM", "1")
+            monkeypatch.delenv("TPAGMG_TAIL_SMEM", raising=False)
         s.set_tuning()  # rebuild the views under the environment
         zs = [s.vcycle(r, precision=p) for p in ("fp64", "mixed", "fp64")]
         x = np.zeros(m.ncells)
         st = solve(x, s, rhs, rtol=1e-10, precision="mixed")
         out[staged] = (zs, x, st.cycles)
-    monkeypatch.delenv("TPAGMG_NO_TAIL_SMEM", raising=False)
+    monkeypatch.delenv("TPAGMG_TAIL_SMEM", raising=False)
     s.set_tuning()
     for a, b in zip(out[True][0], out[False][0]):
         assert np.array_equal(a, b)

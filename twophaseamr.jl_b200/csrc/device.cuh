@@ -110,7 +110,7 @@ struct TuneConfig {
                              // 1 every level, above 1 levels of at most that many cells)
     int persistent = -1;     // all-CSR hierarchies: the V-cycle as one cooperative launch
     int tiles = -1;          // CSR levels: two launches per level on haloed block tiles (tiles.cuh)
-    int tail_smem = -1;      // 0: the coarse tail reads its levels from global memory
+    int tail_smem = -1;      // 1: the coarse tail staged in shared memory (default: global memory)
 };
 
 struct SolveStats {

@@ -594,11 +594,13 @@ void DeviceSolver::build_views() {
     }
     vd_dev_.upload(vd_.data(), vd_.size(), stream_);
     vf_dev_.upload(vf_.data(), vf_.size(), stream_);
-    // the coarse tail in shared memory when its levels fit (one CTA, Jacobi);
-    // TPAGMG_NO_TAIL_SMEM keeps the global-memory tail
+    // the coarse tail staged in shared memory when its levels fit (one CTA,
+    // Jacobi), on request only (TPAGMG_TAIL_SMEM or tail_smem = 1): measured on
+    // the droplet its copy-in costs more than the global-load chains it removes
+    // (V-cycle 101.6 against 97.9 us)
     tail_smem_[0] = tail_smem_[1] = 0;
-    if (fused_ok_ && !rb_ && tail_ctas_ == 1 && nl <= kTailSmemMaxLevels && !std::getenv("TPAGMG_NO_TAIL_SMEM") &&
-        (tune_.tail_smem != 0)) {
+    const bool want_tail_smem = tune_.tail_smem >= 0 ? tune_.tail_smem != 0 : std::getenv("TPAGMG_TAIL_SMEM") != nullptr;
+    if (fused_ok_ && !rb_ && tail_ctas_ == 1 && nl <= kTailSmemMaxLevels && want_tail_smem) {
         size_t bd = 0, bf = 0;
         for (int l = tail_first_; l < nl; ++l) {
             const DevLevel& L = levels_[size_t(l)];
