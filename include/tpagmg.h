@@ -101,6 +101,22 @@ tpa_status tpa_mesh_boundary_faces(const tpa_context* ctx, int32_t* cell, int8_t
  * one nonnegative coefficient per interior face (kappa = 1/rho_f for the
  * two-phase operator, two_phase/forces.jl:113-140). */
 tpa_status tpa_set_operator(tpa_context* ctx, const double* face_coefficient);
+/* Open (pressure Dirichlet 0) sides, `velocity_boundary` of PoissonOperator:
+ * open_sides = {left, right, bottom, top}, nonzero for a side whose velocity
+ * condition is Outflow or ZeroGradientVelocity (`_pressure_boundary_sides`,
+ * src/operators/elliptic.jl:76-87); periodic axes have none.
+ * boundary_coefficient: one per boundary face (tpa_mesh_boundary_faces order,
+ * `boundary_face_coefficient`), or NULL to extend the interior coefficients
+ * to the open faces (`_boundary_material`, elliptic.jl:91-134).  Each open face
+ * adds the conductance 2 k_b / h |f| to its cell's diagonal and anchors that
+ * cell's component (`_elliptic_boundary_data!`, elliptic.jl:136-152): such a
+ * component has no nullspace and its RHS is not projected.  May be called
+ * before or after tpa_set_operator; an existing operator is assembled again
+ * and the hierarchy must be rebuilt.  A coefficient refresh keeps the boundary
+ * coefficients (`_replace_face_coefficient`, elliptic.jl:809-824) and runs on
+ * the host.  The merged batch and the adjoint reject operators with open
+ * sides (TPA_ERR_UNSUPPORTED). */
+tpa_status tpa_set_open_boundaries(tpa_context* ctx, const int32_t open_sides[4], const double* boundary_coefficient);
 /* Number of stored off-diagonal inverse-metric entries (0 when K is diagonal),
  * operators/gradient.jl:369-393. */
 tpa_status tpa_metric_offdiagonal_count(const tpa_context* ctx, int64_t* count);

@@ -142,24 +142,32 @@ def cell_owners(fine, coarse):
     return owners
 
 
-def face_coefficient_restriction(coarse, fine):
+def face_coefficient_restriction(coarse, fine, boundary=False):
     """`_face_coefficient_restriction` (tree_coarsening.jl:347-398): CSR rows of
-    coarse faces over fine faces on the same lattice line, weighted by overlap."""
+    coarse faces over fine faces on the same lattice line, weighted by overlap;
+    with `boundary`, the same over the boundary faces."""
     lattice = common_lattice(fine, coarse)
-    fn, flo, fhi = fine.face_lattice_geometry(lattice)
+    if boundary:
+        fn, flo, fhi = fine.bface_lattice_geometry(lattice)
+        faxis, nfine = fine.bface_axis, len(fine.bface_cell)
+        cgeo, caxis, ncoarse = coarse.bface_lattice_geometry(lattice), coarse.bface_axis, len(coarse.bface_cell)
+    else:
+        fn, flo, fhi = fine.face_lattice_geometry(lattice)
+        faxis, nfine = fine.face_axis, fine.nfaces
+        cgeo, caxis, ncoarse = coarse.face_lattice_geometry(lattice), coarse.face_axis, coarse.nfaces
     lines = {}
-    for f in range(fine.nfaces):
-        lines.setdefault((int(fine.face_axis[f]), int(fn[f])), []).append((int(flo[f]), int(fhi[f]), f))
+    for f in range(nfine):
+        lines.setdefault((int(faxis[f]), int(fn[f])), []).append((int(flo[f]), int(fhi[f]), f))
     starts = {}
     for key, v in lines.items():
         v.sort(key=lambda t: t[0])
         starts[key] = [t[0] for t in v]
-    cn, clo, chi = coarse.face_lattice_geometry(lattice)
+    cn, clo, chi = cgeo
     ptr = [0]; idx = []; w = []
-    for f in range(coarse.nfaces):
+    for f in range(ncoarse):
         lo, hi = int(clo[f]), int(chi[f])
         covered = 0
-        key = (int(coarse.face_axis[f]), int(cn[f]))
+        key = (int(caxis[f]), int(cn[f]))
         line = lines.get(key, [])
         # fine faces on a line are disjoint and sorted: start at the one that
         # contains lo (the scan order, and so the sums, are unchanged)
@@ -174,7 +182,7 @@ def face_coefficient_restriction(coarse, fine):
             raise RuntimeError("tree hierarchy could not cover a coarse face with fine faces")
         ptr.append(len(idx))
     return sp.csr_matrix((np.array(w), np.array(idx, dtype=np.int64), np.array(ptr)),
-                         shape=(coarse.nfaces, fine.nfaces))
+                         shape=(ncoarse, nfine))
 
 
 def jacobi_weight(diagonal, row_sums, *, skip_nonpositive=False, allow_zero=False,
@@ -289,6 +297,7 @@ class TreeGeometricMultigrid:
         self.prolongations = []
         self.transfer_weights = []
         self.restrictions = []
+        self.boundary_restrictions = []
         current = op.mesh
         while True:
             coarse = next_coarse_mesh(current, options.coarse_size, options.max_levels, len(ops))
@@ -302,7 +311,15 @@ class TreeGeometricMultigrid:
             self.prolongations.append(P)
             self.transfer_weights.append(w)
             self.restrictions.append(R)
-            ops.append(PoissonOperator(coarse, kappa_c))
+            # open sides keep their Dirichlet conductance on every level: the
+            # boundary coefficients are restricted like the interior ones
+            # (geometric_preconditioner.jl:256-300)
+            kb_c = None
+            if any(op.open_sides):
+                Rb = face_coefficient_restriction(coarse, current, boundary=True)
+                self.boundary_restrictions.append(Rb)
+                kb_c = Rb @ ops[-1].boundary_coefficient
+            ops.append(PoissonOperator(coarse, kappa_c, open_sides=op.open_sides, boundary_coefficient=kb_c))
             current = coarse
         self.operators = ops
         self.levels = [Level(o, self.prolongations[k] if k < len(self.prolongations) else None)
@@ -327,6 +344,11 @@ class TreeGeometricMultigrid:
         """`_refresh_geometric_multigrid!` (geometric_preconditioner.jl:483-594)."""
         self.operators[0].refresh(kappa)
         for k in range(1, len(self.operators)):
+            if self.boundary_restrictions:
+                # the fine level's (possibly updated) open-face coefficients,
+                # restricted again (geometric_preconditioner.jl:505-515)
+                self.operators[k].update_boundary_coefficient(
+                    self.boundary_restrictions[k - 1] @ self.operators[k - 1].boundary_coefficient)
             self.operators[k].refresh(self.restrictions[k - 1] @ self.operators[k - 1].face_coefficient)
         for k in range(len(self.prolongations)):
             P, w = smoothed_transfer(self.operators[k].matrix, self.owners[k], self.operators[k + 1].mesh.ncells)

@@ -105,10 +105,11 @@ def weighted_jump_force(op, jumps):
 
 def weighted_gradient(op, p):
     """`weighted_gradient!`: interior sqrt(k) K sqrt(k) |f| (p+ - p-); on a
-    boundary face -side * 0 * p (no open sides: the boundary gradient is zero)."""
+    boundary face `_elliptic_boundary_gradient!` (elliptic.jl:1254-1262),
+    -side * (2 k_b / h) * p on open faces and -side * 0 * p on closed ones."""
     mesh = op.mesh
     interior = op.weighted_gradient(p)
-    boundary = (-mesh.bface_side.astype(np.float64) * 0.0) * p[mesh.bface_cell]
+    boundary = (-mesh.bface_side.astype(np.float64) * op.boundary_gradient) * p[mesh.bface_cell]
     return interior, boundary
 
 
@@ -185,7 +186,14 @@ def project(op, mg, u_interior, u_boundary, pressure, dt, *, tolerance=np.sqrt(E
     if not (np.isfinite(tolerance) and 0 < tolerance < 1):
         raise ValueError("tolerance must be finite and lie in (0, 1)")
     u_int = np.array(u_interior, dtype=np.float64)
-    u_bnd = np.zeros(len(op.mesh.bface_cell)) if not prepared else np.array(u_boundary, dtype=np.float64)
+    nb = len(op.mesh.bface_cell)
+    u_bnd = np.zeros(nb) if u_boundary is None or np.ndim(u_boundary) == 0 \
+        else np.array(u_boundary, dtype=np.float64)
+    if not prepared:
+        # no permeation through the closed sides; open faces keep their
+        # velocity (`enforce_velocity_boundary!(...; preserve_open = true)`)
+        from .operator import open_face_mask
+        u_bnd[~open_face_mask(op.mesh, op.open_sides)] = 0.0
     b = projection_rhs(divergence(op.mesh, u_int, u_bnd), dt, inherited, reference_dt)
     phi, st = _solve(op, mg, b, np.zeros(op.mesh.ncells), rtol=0.0, atol=tolerance / dt ** 2,
                      max_cycles=max_cycles, compatibility=compatibility)

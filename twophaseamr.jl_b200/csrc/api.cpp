@@ -30,6 +30,10 @@ struct tpa_context {
     bool host_stale = false;
     int refresh_path = 0;  // 1 host, 2 device (tpa_last_refresh)
     double refresh_ms = 0;
+    // open sides (left, right, bottom, top) and their explicit boundary
+    // coefficients (empty: extended from the interior ones)
+    bool open[4] = {false, false, false, false};
+    std::vector<double> bcoef;
 };
 
 namespace tpa {
@@ -55,6 +59,18 @@ tpa_status guard(tpa_context* ctx, F&& f) {
         ctx->error = e.what();
         return TPA_ERR_INVALID_ARG;
     }
+}
+
+// the context's open sides on a fine operator (kappa set): explicit boundary
+// coefficients, or the interior ones extended (`_boundary_material`)
+void apply_open_sides(const tpa_context* ctx, tpa::LevelOperator& op) {
+    std::copy(ctx->open, ctx->open + 4, op.open);
+    if (!op.any_open()) {
+        op.bkappa.assign(op.mesh.bcell.size(), 0.0);
+        return;
+    }
+    if (!ctx->bcoef.empty()) op.bkappa = ctx->bcoef;
+    else tpa::extend_boundary_material(op);
 }
 
 const tpa::LevelOperator& fine_op(const tpa_context* ctx) {
@@ -98,7 +114,12 @@ void ensure_faces(tpa_context* ctx) {
 
 void ensure_projection(tpa_context* ctx) {
     ensure_faces(ctx);
-    if (!ctx->dev->projection_ready()) ctx->dev->upload_projection(ctx->hier.levels[0].op.mesh);
+    if (!ctx->dev->projection_ready()) {
+        const tpa::LevelOperator& op = ctx->hier.levels[0].op;
+        std::vector<unsigned char> open(op.mesh.bcell.size());
+        for (size_t b = 0; b < open.size(); ++b) open[b] = op.open_face(int64_t(b)) ? 1 : 0;
+        ctx->dev->upload_projection(op.mesh, op.bgrad, open);
+    }
 }
 
 void fill_stats(const tpa::SolveStats& s, int precision, int launches, tpa_stats* out) {
@@ -360,10 +381,48 @@ tpa_status tpa_set_operator(tpa_context* ctx, const double* face_coefficient) {
             if (!std::isfinite(face_coefficient[f])) throw tpa::Error(TPA_ERR_NONFINITE, "face coefficients must be finite");
         op.kappa.assign(face_coefficient, face_coefficient + nf);
         op.metric = tpa::assemble_metric(op.mesh);
+        apply_open_sides(ctx, op);
         tpa::assemble_operator(op);
         ctx->op = std::move(op);
         ctx->have_operator = true;
         ctx->have_hierarchy = ctx->uploaded = false;
+    });
+}
+
+tpa_status tpa_set_open_boundaries(tpa_context* ctx, const int32_t open_sides[4], const double* boundary_coefficient) {
+    return guard(ctx, [&] {
+        if (!ctx->have_mesh) throw tpa::Error(TPA_ERR_STATE, "no mesh: call tpa_set_mesh first");
+        if (!open_sides) throw tpa::Error(TPA_ERR_INVALID_ARG, "null open sides");
+        const tpa::Mesh& m = ctx->have_hierarchy ? ctx->hier.levels[0].op.mesh
+                                                 : (ctx->have_operator ? ctx->op.mesh : ctx->mesh);
+        const size_t nb = m.bcell.size();
+        std::vector<double> bc;
+        if (boundary_coefficient) {
+            bc.assign(boundary_coefficient, boundary_coefficient + nb);
+            for (double v : bc)
+                if (!std::isfinite(v) || v < 0)
+                    throw tpa::Error(TPA_ERR_INVALID_ARG, "boundary coefficients must be finite and nonnegative");
+        }
+        for (int a = 0; a < 2; ++a)
+            if (m.periodic[a] && (open_sides[2 * a] || open_sides[2 * a + 1]))
+                throw tpa::Error(TPA_ERR_INVALID_ARG, "a periodic axis has no open sides");
+        bool open[4];
+        for (int k = 0; k < 4; ++k) open[k] = open_sides[k] != 0;
+        // a fine operator that exists is assembled again (the hierarchy must be
+        // rebuilt): `_update_elliptic_boundary_coefficient!` (elliptic.jl:826-845)
+        if (ctx->have_operator || ctx->have_hierarchy) {
+            tpa::LevelOperator op = ctx->have_hierarchy ? ctx->hier.levels[0].op : ctx->op;
+            std::copy(open, open + 4, ctx->open);
+            ctx->bcoef = bc;
+            apply_open_sides(ctx, op);
+            tpa::assemble_operator(op);
+            ctx->op = std::move(op);
+            ctx->have_operator = true;
+            ctx->have_hierarchy = ctx->uploaded = false;
+        } else {
+            std::copy(open, open + 4, ctx->open);
+            ctx->bcoef = std::move(bc);
+        }
     });
 }
 
@@ -616,6 +675,8 @@ tpa_status tpa_face_coefficient_gradient(tpa_context* ctx, const double* p, cons
 static void adjoint_on_device(tpa_context* ctx, const double* p, const double* pbar, double* rhs_bar,
                               double* kappa_bar, double rtol, double atol, int32_t max_cycles, int32_t precision,
                               tpa_stats* stats) {
+    if (ctx->have_hierarchy && ctx->hier.levels[0].op.any_open())
+        throw tpa::Error(TPA_ERR_UNSUPPORTED, "the adjoint takes closed sides only (no open pressure sides)");
     ensure_faces(ctx);
     tpa::DeviceSolver& d = *ctx->dev;
     size_t n = size_t(d.ncells());
@@ -891,6 +952,8 @@ tpa_status tpa_batch_create(tpa_batch** out, tpa_context* const* ctxs, int32_t c
             ensure_host_fresh(ctxs[k]);
             if (ctxs[k]->hier.opts.smoother != 0)
                 throw tpa::Error(TPA_ERR_UNSUPPORTED, "the merged batch smooths with damped Jacobi only");
+            if (ctxs[k]->hier.levels[0].op.any_open())
+                throw tpa::Error(TPA_ERR_UNSUPPORTED, "the merged batch takes closed sides only (no open pressure sides)");
             hs.push_back(&ctxs[k]->hier);
         }
         int devices = 0;

@@ -288,9 +288,10 @@ __global__ void k_scale_rhs(int n, const double* __restrict__ rhs, const double*
 }
 
 __global__ void k_residual64(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
-                             const double* __restrict__ b, const double* __restrict__ x, double* __restrict__ r) {
+                             const double* __restrict__ b, const double* __restrict__ x, double* __restrict__ r,
+                             const double* __restrict__ bdiag) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) r[i] = b[i] - row_diff(rp, ci, v, x, i);
+    if (i < n) r[i] = b[i] - (row_diff(rp, ci, v, x, i) + (bdiag ? bdiag[i] * x[i] : 0.0));
 }
 
 __global__ void k_abs_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
@@ -559,6 +560,14 @@ void DeviceSolver::upload(const Hierarchy& h) {
             d.f.tinv.upload(ft.data(), ft.size(), stream_);
             d.d.tw = hl.transfer_weight;
             d.f.tw = float(hl.transfer_weight);
+        }
+        if (l == 0) {
+            // open-face conductances of the finest level (true residuals)
+            if (std::any_of(hl.op.bdiag.begin(), hl.op.bdiag.end(), [](double v) { return v != 0.0; }))
+                bdiag_.upload(hl.op.bdiag.data(), hl.op.bdiag.size(), stream_);
+            else
+                bdiag_.free();
+            open_sides_ = hl.op.any_open();
         }
         if (rb_) {
             std::vector<unsigned char> col = red_black_colours(hl.op.mesh);
@@ -871,7 +880,7 @@ void DeviceSolver::solve(const double* rhs, double* x_user, double rtol, double 
         remove_means<double>(0, x);
     }
     auto residual = [&](const double* xx, double* rr) {
-        k_residual64<<<g, kThreads, 0, stream_>>>(n, L.rowptr.p, L.col.p, L.d.val.p, b_.p, xx, rr);
+        k_residual64<<<g, kThreads, 0, stream_>>>(n, L.rowptr.p, L.col.p, L.d.val.p, b_.p, xx, rr, bdiag_.p);
         ++launches_;
     };
     auto norms = [&](const double* rr, double& l2, double& linf) {

@@ -192,6 +192,8 @@ private:
     int rb_pair_cells_ = 0;
     // fine-level FP64 PCG workspace
     DevArray<double> b_, r_, p_, ap_, z_, tmp_, partial_;
+    DevArray<double> bdiag_;   // finest level's open-face conductance per cell (empty: none)
+    bool open_sides_ = false;  // the finest operator has an open side
     DevArray<CgScalars> sc_;
     DevArray<double> sums_;   // component sums scratch
     CgScalars* host_sc_ = nullptr;
@@ -369,7 +371,10 @@ public:
     // ---- the projection step around the solve (csrc/projection.cu) ----
     // Boundary faces, each cell's incident faces in face order and the face
     // spacings (after upload_faces).
-    void upload_projection(const Mesh& mesh);
+    // bgrad: the open-face gradient factor 2 k_b / h per boundary face (0 on
+    // closed faces); open: 1 on a face of an open side
+    void upload_projection(const Mesh& mesh, const std::vector<double>& bgrad, const std::vector<unsigned char>& open);
+    bool has_open_sides() const { return open_sides_; }
     bool projection_ready() const { return nbfaces_ >= 0 && nfaces_ >= 0; }
     int64_t nboundary_faces() const { return nbfaces_; }
     // `_refresh_conditional_fraction!` (no embedded geometry); physical may be null
@@ -394,6 +399,8 @@ private:
     int64_t nbfaces_ = -1;
     DevArray<int> inc_ptr_, inc_code_, b_cell_, perr_;
     DevArray<double> f_hm_, f_hp_, b_side_, b_area_, proj_b_, proj_phi_, proj_in_, proj_part_, proj_cvol_;
+    DevArray<double> b_grad_;          // open-face gradient factor per boundary face
+    DevArray<unsigned char> b_open_;   // 1 on faces of open sides
 };
 
 }  // namespace tpa

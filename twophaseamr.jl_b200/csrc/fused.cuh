@@ -65,6 +65,10 @@ struct LevelView {
     const unsigned char* colour;  // red-black smoother (rb != 0): 0 red, 1 black
     int rb;
     T rbw;             // red-black half-sweep weight
+    // open-face conductance per cell (finest level, FP64 view; null: no open
+    // side).  The operator's diagonal holds it; the true-residual kernels, which
+    // sum rows as a_ij (x_j - x_i), add it back as bdiag_i x_i.
+    const double* bdiag;
 };
 
 // fold partial[0..count) in fixed order by one block; returns the sum in thread 0

@@ -4,8 +4,10 @@
 //   src/operators/elliptic.jl:157-257   symmetric stiffness (A + A')/2 of J' M J with
 //                                       M = k K (diagonal K) or sqrt(k) K sqrt(k)
 //   src/solvers/multigrid/elliptic_solver.jl:1-129, two_phase/projection/common.jl:53-83
-//                                       open-face components; all ungauged here (no open
-//                                       Dirichlet sides, no inactive cells)
+//                                       open-face components; a component touching an open
+//                                       (Dirichlet) side is anchored, the others ungauged
+//   src/operators/elliptic.jl:76-152, 757-764   open sides: boundary material, the
+//                                       conductance 2 k_b / h |f| added to the diagonal
 //   src/solvers/multigrid/hierarchy.jl:8-30        `_jacobi_weight!`
 //   src/solvers/multigrid/hierarchy.jl:631-721     smoothed transfer weights
 //   src/solvers/multigrid/hierarchy.jl:786-817     `_multigrid_level` (row sums, weight)
@@ -17,6 +19,7 @@
 #include <cmath>
 #include <map>
 #include <numeric>
+#include <tuple>
 
 #include "host.hpp"
 
@@ -38,6 +41,30 @@ int32_t find_root(std::vector<int32_t>& parent, int32_t x) {
     return x;
 }
 
+// `_elliptic_boundary_data!` (elliptic.jl:136-152) with unit apertures and
+// no inactive cells: the gradient factor 2 k_b / h of every open boundary face
+// and the diagonal term |f| times it of its cell
+void boundary_data(LevelOperator& op) {
+    const Mesh& m = op.mesh;
+    const int64_t nb = int64_t(m.bcell.size());
+    op.bdiag.clear();
+    op.bgrad.assign(size_t(nb), 0.0);
+    if (!op.any_open()) return;
+    if (int64_t(op.bkappa.size()) != nb) throw Error(1, "one coefficient is required per boundary face");
+    op.bdiag.assign(size_t(m.ncells()), 0.0);
+    const int64_t cpb = m.cells_per_block();
+    for (int64_t b = 0; b < nb; ++b) {
+        if (!op.open_face(b)) continue;
+        const int32_t cell = m.bcell[size_t(b)];
+        if (!(op.volumes[size_t(cell)] > 0)) continue;
+        const int64_t blk = cell / cpb;
+        const double h = m.bax[size_t(b)] == 1 ? m.bsx[size_t(blk)] : m.bsy[size_t(blk)];
+        const double factor = 2 * op.bkappa[size_t(b)] / h;
+        op.bgrad[size_t(b)] = factor;
+        op.bdiag[size_t(cell)] += m.barea[size_t(b)] * factor;
+    }
+}
+
 Components components(const LevelOperator& op) {
     const Mesh& m = op.mesh;
     const int64_t nc = m.ncells();
@@ -51,9 +78,15 @@ Components components(const LevelOperator& op) {
     Components c;
     c.slot.assign(static_cast<size_t>(nc), -1);
     std::vector<int32_t> root_slot(static_cast<size_t>(nc), -1);
+    // a cell with an open-face conductance anchors its component
+    // (elliptic_solver.jl:80-82)
+    std::vector<char> anchored(static_cast<size_t>(nc), 0);
+    for (size_t i = 0; i < op.bdiag.size(); ++i)
+        if (op.bdiag[i] != 0.0) anchored[size_t(find_root(parent, int32_t(i)))] = 1;
     for (int64_t i = 0; i < nc; ++i) {
         if (!(op.volumes[size_t(i)] > 0)) continue;
         int32_t r = find_root(parent, int32_t(i));
+        if (anchored[size_t(r)]) continue;
         if (root_slot[size_t(r)] < 0) {
             root_slot[size_t(r)] = int32_t(c.anchor.size());
             c.anchor.push_back(r);
@@ -66,6 +99,37 @@ Components components(const LevelOperator& op) {
 }
 
 }  // namespace
+
+bool LevelOperator::open_face(int64_t b) const {
+    return open[2 * (mesh.bax[size_t(b)] - 1) + (mesh.bside[size_t(b)] > 0 ? 1 : 0)];
+}
+
+void extend_boundary_material(LevelOperator& op) {
+    const Mesh& m = op.mesh;
+    const int64_t nb = int64_t(m.bcell.size());
+    op.bkappa.assign(size_t(nb), 0.0);
+    if (!op.any_open()) return;
+    if (int64_t(op.kappa.size()) != m.nfaces()) throw Error(1, "one coefficient is required per interior face");
+    std::map<std::tuple<int32_t, int, int>, int64_t> index;
+    for (int64_t b = 0; b < nb; ++b)
+        if (op.open_face(b)) index[{m.bcell[size_t(b)], int(m.bax[size_t(b)]), int(m.bside[size_t(b)])}] = b;
+    std::vector<double> weights(size_t(nb), 0.0);
+    for (int64_t f = 0; f < m.nfaces(); ++f) {
+        const std::pair<int32_t, int> ends[2] = {{m.fm[size_t(f)], -1}, {m.fp[size_t(f)], 1}};
+        for (const auto& [cell, side] : ends) {
+            auto it = index.find({cell, int(m.fax[size_t(f)]), side});
+            if (it == index.end()) continue;
+            op.bkappa[size_t(it->second)] += m.farea[size_t(f)] * op.kappa[size_t(f)];
+            weights[size_t(it->second)] += m.farea[size_t(f)];
+        }
+    }
+    for (const auto& [key, b] : index) {
+        if (!(weights[size_t(b)] > 0))
+            throw Error(1, "cannot extend an interior coefficient to an open face without an opposite interior "
+                           "face; supply boundary face coefficients");
+        op.bkappa[size_t(b)] /= weights[size_t(b)];
+    }
+}
 
 void assemble_operator(LevelOperator& op) {
     const Mesh& m = op.mesh;
@@ -147,6 +211,14 @@ void assemble_operator(LevelOperator& op) {
             sym[size_t(k)] = v == 0.0 ? 0.0 : v;
         }
     A.val.swap(sym);
+    // open-face conductances on the diagonal, after the symmetric average
+    // (elliptic.jl:757-764)
+    boundary_data(op);
+    for (size_t r = 0; r < op.bdiag.size(); ++r) {
+        if (op.bdiag[r] == 0.0) continue;
+        for (int64_t k = A.ptr[r]; k < A.ptr[r + 1]; ++k)
+            if (A.col[size_t(k)] == int32_t(r)) A.val[size_t(k)] += op.bdiag[r];
+    }
     op.A = std::move(A);
     op.comp = components(op);
     op.singular = !op.comp.anchor.empty();
@@ -271,7 +343,7 @@ std::vector<int32_t> owners(const Mesh& fine, const Mesh& coarse) {
 }
 
 void face_restriction(const Mesh& coarse, const Mesh& fine, std::vector<int64_t>& ptr, std::vector<int32_t>& idx,
-                      std::vector<double>& w) {
+                      std::vector<double>& w, bool boundary = false) {
     int64_t lf[2], lc[2], lat[2];
     fine.lattice(fine.active, lf);
     coarse.lattice(coarse.active, lc);
@@ -279,20 +351,24 @@ void face_restriction(const Mesh& coarse, const Mesh& fine, std::vector<int64_t>
     lat[1] = std::max(lf[1], lc[1]);
     struct Seg { int64_t lo, hi; int32_t f; };
     std::map<std::pair<int, int64_t>, std::vector<Seg>> lines;
-    for (int64_t f = 0; f < fine.nfaces(); ++f) {
+    const int64_t nfine = boundary ? int64_t(fine.bcell.size()) : fine.nfaces();
+    for (int64_t f = 0; f < nfine; ++f) {
         int64_t n, lo, hi;
-        fine.face_lattice(f, lat, n, lo, hi);
-        lines[{fine.fax[size_t(f)], n}].push_back({lo, hi, int32_t(f)});
+        if (boundary) fine.bface_lattice(f, lat, n, lo, hi);
+        else fine.face_lattice(f, lat, n, lo, hi);
+        lines[{boundary ? fine.bax[size_t(f)] : fine.fax[size_t(f)], n}].push_back({lo, hi, int32_t(f)});
     }
     for (auto& kv : lines)
         std::sort(kv.second.begin(), kv.second.end(), [](const Seg& a, const Seg& b) { return a.lo < b.lo; });
     ptr.assign(1, 0);
     idx.clear();
     w.clear();
-    for (int64_t f = 0; f < coarse.nfaces(); ++f) {
+    const int64_t ncoarse = boundary ? int64_t(coarse.bcell.size()) : coarse.nfaces();
+    for (int64_t f = 0; f < ncoarse; ++f) {
         int64_t n, lo, hi;
-        coarse.face_lattice(f, lat, n, lo, hi);
-        auto it = lines.find({coarse.fax[size_t(f)], n});
+        if (boundary) coarse.bface_lattice(f, lat, n, lo, hi);
+        else coarse.face_lattice(f, lat, n, lo, hi);
+        auto it = lines.find({boundary ? coarse.bax[size_t(f)] : coarse.fax[size_t(f)], n});
         int64_t covered = 0;
         if (it != lines.end()) {
             const auto& segs = it->second;
@@ -317,6 +393,17 @@ std::vector<double> restrict_faces(const HostLevel& fine) {
     for (size_t f = 0; f + 1 < fine.rptr.size(); ++f) {
         double v = 0.0;
         for (int64_t k = fine.rptr[f]; k < fine.rptr[f + 1]; ++k) v += fine.rw[size_t(k)] * fine.op.kappa[size_t(fine.ridx[size_t(k)])];
+        out[f] = v;
+    }
+    return out;
+}
+
+std::vector<double> restrict_boundary_faces(const HostLevel& fine) {
+    std::vector<double> out(fine.brptr.empty() ? 0 : fine.brptr.size() - 1);
+    for (size_t f = 0; f < out.size(); ++f) {
+        double v = 0.0;
+        for (int64_t k = fine.brptr[f]; k < fine.brptr[f + 1]; ++k)
+            v += fine.brw[size_t(k)] * fine.op.bkappa[size_t(fine.bridx[size_t(k)])];
         out[f] = v;
     }
     return out;
@@ -409,6 +496,14 @@ Hierarchy build_hierarchy(LevelOperator fine, const HierarchyOptions& opts) {
         face_restriction(coarse, cur.op.mesh, cur.rptr, cur.ridx, cur.rw);
         std::vector<double> kc = restrict_faces(cur);
         HostLevel next;
+        // open sides keep their conductance on every level, with the boundary
+        // coefficients restricted like the interior ones
+        // (geometric_preconditioner.jl:256-300)
+        for (int s = 0; s < 4; ++s) next.op.open[s] = cur.op.open[s];
+        if (cur.op.any_open()) {
+            face_restriction(coarse, cur.op.mesh, cur.brptr, cur.bridx, cur.brw, true);
+            next.op.bkappa = restrict_boundary_faces(cur);
+        }
         next.op.mesh = std::move(coarse);
         next.op.metric = assemble_metric(next.op.mesh);
         next.op.kappa = std::move(kc);
@@ -425,6 +520,7 @@ void refresh_hierarchy(Hierarchy& h, const std::vector<double>& kappa) {
     assemble_operator(h.levels[0].op);
     for (size_t l = 1; l < h.levels.size(); ++l) {
         h.levels[l].op.kappa = restrict_faces(h.levels[l - 1]);
+        if (h.levels[l].op.any_open()) h.levels[l].op.bkappa = restrict_boundary_faces(h.levels[l - 1]);
         assemble_operator(h.levels[l].op);
     }
     for (size_t l = 0; l + 1 < h.levels.size(); ++l) transfer_weights(h.levels[l]);

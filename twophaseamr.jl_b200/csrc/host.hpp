@@ -77,6 +77,8 @@ struct Mesh {
     void cell_lattice(int64_t cell, const int64_t lat[2], int64_t low[2], int64_t sc[2]) const;
     // `_face_lattice_geometry` (mesh.jl:461-474)
     void face_lattice(int64_t f, const int64_t lat[2], int64_t& normal, int64_t& lo, int64_t& hi) const;
+    // its boundary-face form (mesh.jl:476-485)
+    void bface_lattice(int64_t b, const int64_t lat[2], int64_t& normal, int64_t& lo, int64_t& hi) const;
     std::vector<double> cell_volumes() const;
 };
 
@@ -124,7 +126,18 @@ struct LevelOperator {
     Csr A;
     Components comp;
     bool singular = false;
+    // open sides (left, right, bottom, top): pressure Dirichlet 0 on their
+    // faces (`_pressure_boundary_sides`, elliptic.jl:76-87)
+    bool open[4] = {false, false, false, false};
+    std::vector<double> bkappa;  // coefficient per boundary face (used on open faces)
+    std::vector<double> bdiag;   // open-face conductance 2 k_b / h |f| per cell (empty: none)
+    std::vector<double> bgrad;   // 2 k_b / h per boundary face (0 on closed faces)
+    bool any_open() const { return open[0] || open[1] || open[2] || open[3]; }
+    bool open_face(int64_t b) const;  // `_pressure_open_face` (elliptic.jl:86-87)
 };
+// `_boundary_material` (elliptic.jl:91-134): open-face coefficients extended
+// from the interior coefficients of the opposite faces (area-weighted).
+void extend_boundary_material(LevelOperator& op);
 void assemble_operator(LevelOperator& op);
 
 // `_jacobi_weight!` (solvers/multigrid/hierarchy.jl:8-30)
@@ -149,6 +162,10 @@ struct HostLevel {
     std::vector<int64_t> rptr;
     std::vector<int32_t> ridx;
     std::vector<double> rw;
+    // the same over the boundary faces (open sides only)
+    std::vector<int64_t> brptr;
+    std::vector<int32_t> bridx;
+    std::vector<double> brw;
 };
 
 struct Hierarchy {

@@ -108,6 +108,15 @@ void Mesh::face_lattice(int64_t f, const int64_t lat[2], int64_t& normal, int64_
     hi = std::min(ml[t] + ms[t], pl[t] + ps[t]);
 }
 
+void Mesh::bface_lattice(int64_t b, const int64_t lat[2], int64_t& normal, int64_t& lo, int64_t& hi) const {
+    int64_t low[2], sc[2];
+    cell_lattice(bcell[size_t(b)], lat, low, sc);
+    const int a = bax[size_t(b)] - 1, t = 1 - a;
+    normal = low[a] + (bside[size_t(b)] > 0 ? sc[a] : 0);
+    lo = low[t];
+    hi = low[t] + sc[t];
+}
+
 std::vector<double> Mesh::cell_volumes() const {
     std::vector<double> v(static_cast<size_t>(ncells()));
     int64_t cpb = cells_per_block();

@@ -101,13 +101,15 @@ __global__ void kp_face_out(int nf, const int* __restrict__ kptr, const int* __r
     }
 }
 
-// boundary faces of the weighted gradient: -side * 0 * p (no open sides), and
-// the velocity update u_b -= dt g_b; zero = 1 writes the zero force instead
+// boundary faces of the weighted gradient, `_elliptic_boundary_gradient!`
+// (elliptic.jl:1254-1262): -side * (2 k_b / h) * p on open faces, -side * 0 * p
+// on closed ones, and the velocity update u_b -= dt g_b; zero = 1 writes the
+// zero force instead
 __global__ void kp_boundary(int nb, const int* __restrict__ bcell, const double* __restrict__ bside,
-                            const double* __restrict__ p, double* __restrict__ g, double* __restrict__ u, double dt,
-                            int zero) {
+                            const double* __restrict__ bgrad, const double* __restrict__ p, double* __restrict__ g,
+                            double* __restrict__ u, double dt, int zero) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
-        const double w = zero ? 0.0 : __dmul_rn(__dmul_rn(-bside[k], 0.0), p[bcell[k]]);
+        const double w = zero ? 0.0 : __dmul_rn(__dmul_rn(-bside[k], bgrad[k]), p[bcell[k]]);
         if (g) g[k] = w;
         if (u) u[k] = __dsub_rn(u[k], __dmul_rn(dt, w));
     }
@@ -192,7 +194,16 @@ __global__ void kp_slot_apply(int n, double* __restrict__ p, const int* __restri
 
 }  // namespace
 
-void DeviceSolver::upload_projection(const Mesh& mesh) {
+// `enforce_no_permeation!` of the closed sides only: the normal velocity of
+// every boundary face that is not on an open side is zeroed (open faces keep
+// theirs, `preserve_open`)
+__global__ void kp_close_walls(int nb, const unsigned char* __restrict__ open, double* __restrict__ u) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x)
+        if (!open[k]) u[k] = 0.0;
+}
+
+void DeviceSolver::upload_projection(const Mesh& mesh, const std::vector<double>& bgrad,
+                                     const std::vector<unsigned char>& open) {
     TPA_CUDA(cudaSetDevice(device_));
     if (nfaces_ < 0) throw Error(7, "face data not uploaded");
     const int64_t nf = mesh.nfaces(), nb = int64_t(mesh.bcell.size()), n = mesh.ncells();
@@ -229,6 +240,9 @@ void DeviceSolver::upload_projection(const Mesh& mesh) {
     b_cell_.upload(bcell.data(), bcell.size(), stream_);
     b_side_.upload(side.data(), side.size(), stream_);
     b_area_.upload(mesh.barea.data(), mesh.barea.size(), stream_);
+    if (bgrad.size() != size_t(nb) || open.size() != size_t(nb)) throw Error(1, "boundary data size mismatch");
+    b_grad_.upload(bgrad.data(), bgrad.size(), stream_);
+    b_open_.upload(open.data(), open.size(), stream_);
     proj_b_.alloc(size_t(n));
     proj_phi_.alloc(size_t(n));
     proj_in_.alloc(size_t(std::max<int64_t>(nf, 1)));
@@ -282,7 +296,8 @@ void DeviceSolver::surface_tension(const double* conditional, double sigma, doub
         launches_ += 2;
     }
     if (nbfaces_ > 0 && a_bnd) {
-        kp_boundary<<<pgrid(nbfaces_), kPThreads, 0, stream_>>>(int(nbfaces_), b_cell_.p, b_side_.p, nullptr, a_bnd,
+        kp_boundary<<<pgrid(nbfaces_), kPThreads, 0, stream_>>>(int(nbfaces_), b_cell_.p, b_side_.p, b_grad_.p, nullptr,
+                                                                a_bnd,
                                                                 nullptr, 0.0, 1);
         ++launches_;
     }
@@ -300,7 +315,8 @@ void DeviceSolver::weighted_gradient(const double* p, double* g_int, double* g_b
         launches_ += 2;
     }
     if (nbfaces_ > 0 && (g_bnd || u_bnd)) {
-        kp_boundary<<<pgrid(nbfaces_), kPThreads, 0, stream_>>>(int(nbfaces_), b_cell_.p, b_side_.p, p, g_bnd, u_bnd,
+        kp_boundary<<<pgrid(nbfaces_), kPThreads, 0, stream_>>>(int(nbfaces_), b_cell_.p, b_side_.p, b_grad_.p, p,
+                                                                g_bnd, u_bnd,
                                                                 dt, 0);
         ++launches_;
     }
@@ -329,7 +345,14 @@ void DeviceSolver::project(double* u_int, double* u_bnd, double* p, double dt, d
         throw Error(1, "tolerance must be finite and lie in (0, 1)");
     const int n = ncells();
     // `project!` without a velocity boundary: no permeation through the walls
-    if (!prepared && nbfaces_ > 0) TPA_CUDA(cudaMemsetAsync(u_bnd, 0, sizeof(double) * size_t(nbfaces_), stream_));
+    if (!prepared && nbfaces_ > 0) {
+        if (open_sides_) {
+            kp_close_walls<<<pgrid(nbfaces_), kPThreads, 0, stream_>>>(int(nbfaces_), b_open_.p, u_bnd);
+            ++launches_;
+        } else {
+            TPA_CUDA(cudaMemsetAsync(u_bnd, 0, sizeof(double) * size_t(nbfaces_), stream_));
+        }
+    }
     const double weight = (reference_dt - dt) / (dt * reference_dt);
     divergence(u_int, u_bnd, proj_b_.p, true, dt, inherited, weight);
     TPA_CUDA(cudaMemsetAsync(proj_phi_.p, 0, sizeof(double) * size_t(n), stream_));

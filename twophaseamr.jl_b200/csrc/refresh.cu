@@ -649,6 +649,10 @@ void DeviceSolver::prepare_refresh(const Hierarchy& h) {
 }
 
 bool DeviceSolver::refresh_applicable(const Hierarchy& h) const {
+    // the entry term lists hold the face couplings only; levels with open-face
+    // conductances on their diagonal are refreshed on the host
+    for (const HostLevel& l : h.levels)
+        if (l.op.any_open()) return false;
     // stencil copies are gathered from the refreshed operator; a level kept as
     // one constant coupling or diagonal would change layout, so it needs the host
     for (const StructDev& D : sdev_)

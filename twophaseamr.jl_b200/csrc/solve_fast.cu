@@ -90,8 +90,9 @@ __global__ void k_prep(int n, const double* __restrict__ rhs, const double* __re
 
 // b -= V mb, x = x0 - mx (0 where V = 0), r = b - A x; out = {sum_V r^2 / V,
 // max |r| / V, max (|A| |x|) / V, max |b| / V} over cells with V > 0.  A x is
-// summed as sum_j a_ij (x_j - x_i): the rows sum to zero (the area-weighted
-// jump maps constants to zero and no side is open), and this form rounds at
+// summed as sum_j a_ij (x_j - x_i) (+ bdiag_i x_i at open sides): the rows
+// sum to that conductance (the area-weighted jump maps constants to zero), and
+// this form rounds at
 // the level of the face fluxes, as the factorized action of elliptic.jl:
 // 1125-1180 does, not at the level of a_ii x_i.  The projection step relies on
 // it: dt max |div u| after the update equals the final residual over 1/dt^2 to
@@ -115,6 +116,7 @@ __global__ void k_pres(LevelView<double> A, double* __restrict__ b, const double
             acc += A.val[k] * (xj - xi);
             aacc += fabs(A.val[k]) * fabs(xj);
         }
+        if (A.bdiag) acc += A.bdiag[i] * xi;  // rows at open sides do not sum to zero
         x[i] = xi;
         const double ri = bi - acc;
         r[i] = ri;

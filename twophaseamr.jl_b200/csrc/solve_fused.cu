@@ -588,9 +588,11 @@ void DeviceSolver::build_views() {
             v.colour = L.colour.p;
             v.rb = rb_ ? 1 : 0;
             v.rbw = static_cast<decltype(v.w)>(L.rbw);
+            v.bdiag = nullptr;
         };
         fill(vd_[size_t(l)], L.d);
         fill(vf_[size_t(l)], L.f);
+        if (l == 0) vd_[0].bdiag = bdiag_.p;
     }
     vd_dev_.upload(vd_.data(), vd_.size(), stream_);
     vf_dev_.upload(vf_.data(), vf_.size(), stream_);
@@ -1333,7 +1335,10 @@ void DeviceSolver::upload_structured(const Hierarchy& h) {
     for (int l = 0; l < nl; ++l) {
         const HostLevel& hl = h.levels[size_t(l)];
         const int cpb = hl.op.mesh.bs[0] * hl.op.mesh.bs[1];
-        if (disabled || l >= tail_first_ || l + 1 >= nl || cpb < 32 || cpb > 1024 || cpb % 32) continue;
+        // a stencil row is c0 (count x_c - neighbours): not a row with an
+        // open-face conductance on its diagonal
+        const bool open_diag = std::any_of(hl.op.bdiag.begin(), hl.op.bdiag.end(), [](double v) { return v != 0.0; });
+        if (disabled || open_diag || l >= tail_first_ || l + 1 >= nl || cpb < 32 || cpb > 1024 || cpb % 32) continue;
         StructLevel st = build_struct(hl, &h.levels[size_t(l + 1)].op.mesh);
         if (!st.has_map || !st.tinv_same) continue;
         // Variable-coefficient levels with coarse-fine exception rows are small and

@@ -67,6 +67,7 @@ SIGNATURES = {
     "tpa_mesh_faces": (C.c_int32, [P, i32p, i32p, i8p, f64p]),
     "tpa_mesh_boundary_faces": (C.c_int32, [P, i32p, i8p, i8p, f64p]),
     "tpa_set_operator": (C.c_int32, [P, f64p]),
+    "tpa_set_open_boundaries": (C.c_int32, [P, i32p, f64p]),
     "tpa_metric_offdiagonal_count": (C.c_int32, [P, i64p]),
     "tpa_build_hierarchy": (C.c_int32, [P, C.POINTER(MultigridOptionsC)]),
     "tpa_hierarchy_sizes": (C.c_int32, [P, i32p, i64p, C.c_int32]),

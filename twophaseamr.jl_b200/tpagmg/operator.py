@@ -1,7 +1,9 @@
 """`PoissonOperator` and the two-phase coefficient / surface-tension inputs.
 
 Mirrors (ronaldremmerswaal/TwoPhaseAMR.jl):
-  src/operators/elliptic.jl:969-980     PoissonOperator(mesh; face_coefficient)
+  src/operators/elliptic.jl:969-980     PoissonOperator(mesh; face_coefficient, velocity_boundary,
+                                        boundary_face_coefficient)
+  src/operators/elliptic.jl:76-87       `_pressure_boundary_sides` (open sides)
   src/two_phase/forces.jl:23-36, 69-84  staggered liquid fraction, mixture density
   src/two_phase/forces.jl:113-140       PoissonOperator(interface; density): kappa = 1/rho_f
   src/two_phase/forces.jl:312-314, 345-378  CGFM jumps sigma*kappa*([c+ > 1/2] - [c- > 1/2])*|f|
@@ -14,11 +16,51 @@ from __future__ import annotations
 import numpy as np
 
 
-class PoissonOperator:
-    """Positive Poisson operator `-div(kappa grad p)` on a `BlockTreeMesh`."""
+OPEN_CONDITIONS = ("outflow", "zero_gradient")
+SIDES = ("left", "right", "bottom", "top")
 
-    def __init__(self, mesh, face_coefficient=1.0):
+
+def pressure_boundary_sides(velocity_boundary):
+    """`_pressure_boundary_sides` (elliptic.jl:76-87): which sides (left, right,
+    bottom, top) are open.  None, "no_slip" or "free_slip": none.  A 4-tuple of
+    booleans is taken as it is; a dict maps side names to velocity conditions
+    ("outflow" and "zero_gradient" open a side, any other closes it)."""
+    if velocity_boundary is None or velocity_boundary in ("no_slip", "free_slip"):
+        return (False, False, False, False)
+    if isinstance(velocity_boundary, dict):
+        unknown = set(velocity_boundary) - set(SIDES)
+        if unknown:
+            raise ValueError(f"unknown sides: {sorted(unknown)}")
+        return tuple(velocity_boundary.get(side) in OPEN_CONDITIONS for side in SIDES)
+    sides = tuple(bool(v) for v in velocity_boundary)
+    if len(sides) != 4:
+        raise ValueError("velocity_boundary needs four sides (left, right, bottom, top)")
+    return sides
+
+
+class PoissonOperator:
+    """Positive Poisson operator `-div(kappa grad p)` on a `BlockTreeMesh`.
+
+    velocity_boundary: the open (pressure Dirichlet) sides, see
+    `pressure_boundary_sides`; boundary_face_coefficient: one per boundary face
+    for the open faces, or None to extend the interior coefficients."""
+
+    def __init__(self, mesh, face_coefficient=1.0, velocity_boundary=None, boundary_face_coefficient=None):
         self.mesh = mesh
+        self.open_sides = pressure_boundary_sides(velocity_boundary)
+        for a in (0, 1):
+            if mesh.periodic[a] and (self.open_sides[2 * a] or self.open_sides[2 * a + 1]):
+                raise ValueError("a periodic axis has no open sides")
+        self.boundary_face_coefficient = None
+        if boundary_face_coefficient is not None:
+            nb = mesh.nboundary_faces
+            bc = np.full(nb, float(boundary_face_coefficient)) if np.isscalar(boundary_face_coefficient) \
+                else np.array(boundary_face_coefficient, dtype=np.float64)
+            if bc.shape != (nb,):
+                raise ValueError("one coefficient and aperture are required per boundary face")
+            if not (np.all(np.isfinite(bc)) and np.all(bc >= 0)):
+                raise ValueError("boundary coefficients must be finite and nonnegative")
+            self.boundary_face_coefficient = bc
         nf = mesh.nfaces
         if np.isscalar(face_coefficient):
             kappa = np.full(nf, float(face_coefficient))

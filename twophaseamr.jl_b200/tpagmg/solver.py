@@ -87,6 +87,13 @@ class EllipticSolver:
         self.ctx = _lib.Context(device)
         self.ctx.call("tpa_set_mesh", *mesh._mesh_args())
         self._kappa = _lib.f64(operator.face_coefficient)
+        sides = getattr(operator, "open_sides", (False, False, False, False))
+        if any(sides):
+            so = np.array([1 if v else 0 for v in sides], dtype=np.int32)
+            bc = getattr(operator, "boundary_face_coefficient", None)
+            self._bcoef = None if bc is None else _lib.f64(bc)
+            self.ctx.call("tpa_set_open_boundaries", _lib.ptr(so, C.c_int32),
+                          None if self._bcoef is None else _lib.ptr(self._bcoef, C.c_double))
         self.ctx.call("tpa_set_operator", _lib.ptr(self._kappa, C.c_double))
         o = _lib.MultigridOptionsC(mg.coarse_size, mg.pre_sweeps, mg.post_sweeps, mg.max_levels,
                                    1 if mg.smoother == "red_black" else 0)
