@@ -24,7 +24,12 @@ struct CgState {
     double gamma, pAp, alpha, beta, pnorm2, strong_max, target, rsum, rnorm;
     int flags;  // 1 user exit, 2 zero curvature, 4 machine stop, 8 zero initial residual
     int iter, itmax;
+    int fresh;  // the next r'z starts the run (gamma = r'z, p = z)
 };
+
+// flags that end a run in the middle of a loop body: the direction and the
+// update of that body do nothing
+constexpr int kCgHalt = 2 | 4 | 8;
 
 enum Counter { kRestrictSum = 0, kPostMean = 1, kCgAp = 2, kCgUpdate = 3, kCgZ = 4, kCgRes = 5, kRsum = 6 };
 
@@ -121,6 +126,22 @@ __device__ __forceinline__ void alpha_from(double pAp, CgState* s) {
     }
 }
 
+// End of a loop body (Krylov.jl `cg!`: iter += 1, `tired`, then the callback):
+// the iteration count, the strong-residual callback max|r_i|/V_i <= target on
+// the updated residual, and the loop condition.  A body that halted (zero
+// curvature, machine stop, zero initial residual) ends the run uncounted, as
+// `cg!` leaves its loop before counting.  One thread.
+__device__ __forceinline__ void cg_after_update(CgState* s, bool halted, cudaGraphConditionalHandle handle,
+                                                int set_cond) {
+    bool stop = halted;
+    if (!halted) {
+        s->iter += 1;
+        if (s->strong_max <= s->target) s->flags |= 1;
+        stop = (s->flags & 1) || s->iter >= s->itmax;
+    }
+    if (set_cond) cudaGraphSetConditional(handle, stop ? 0u : 1u);
+}
+
 // Ap = A p and alpha = gamma / p'Ap with the zero-curvature guard: the CG
 // operator product alone, as time_fused times it (the CG loop runs the
 // *_cg_dir_ap kernels, which also form p)
@@ -154,11 +175,12 @@ __device__ __forceinline__ double* dir_new(double* pa, double* pb, int iter) { r
 // max|r_i|/V_i and sum(r).  vol null: every cell's volume is vol0.
 __global__ void k_cg_update(int n, double* __restrict__ x, double* __restrict__ r, double* pa, double* pb,
                             const double* __restrict__ ap, const double* __restrict__ vol, double vol0, double* pmax,
-                            double* psum, unsigned* counter, CgState* s) {
+                            double* psum, unsigned* counter, CgState* s, cudaGraphConditionalHandle handle,
+                            int set_cond) {
     pdl_entry();
     const double* __restrict__ p = dir_new(pa, pb, s->iter);
     __shared__ bool last;
-    const bool skip = s->flags & 2;
+    const bool skip = s->flags & kCgHalt;
     const double alpha = s->alpha;
     double m = 0, sum = 0;
     bool nan = false;
@@ -214,6 +236,7 @@ __global__ void k_cg_update(int n, double* __restrict__ x, double* __restrict__ 
             s->strong_max = mx;
             s->rsum = sm;
             *counter = 0;
+            cg_after_update(s, skip, handle, set_cond);
         }
     }
 }
@@ -303,16 +326,14 @@ void with_nxc(const SView<T>& S, F f) {
     else f(std::integral_constant<int, 0>{});
 }
 
-__device__ void cg_after_z(CgState* s, double g, int init, cudaGraphConditionalHandle handle, int set_cond);
+__device__ void cg_after_z(CgState* s, double g);
 
 // gamma_next = r'z for z = x0 - mean (the V-cycle's output, not stored: the
-// next operator product forms z and p where it reads them) and the stopping
-// rules; `init` starts a run (gamma = r'z, iter 0: the first direction is z).
-// With `set_cond`, sets the graph loop condition.
+// next operator product forms z and p where it reads them), then beta or the
+// start of a run (cg_after_z)
 template <typename T>
 __global__ void k_cg_z(int n, const T* __restrict__ xv, const double* mean, const double* __restrict__ r,
-                       double* partial, unsigned* counter, CgState* s, int init, cudaGraphConditionalHandle handle,
-                       int set_cond) {
+                       double* partial, unsigned* counter, CgState* s) {
     pdl_entry();
     const double m = mean ? *mean : 0.0;
     double v = 0;
@@ -330,42 +351,40 @@ __global__ void k_cg_z(int n, const T* __restrict__ xv, const double* mean, cons
         double g = fold_partials(partial, gridDim.x);
         if (threadIdx.x == 0) {
             *counter = 0;
-            cg_after_z(s, g, init, handle, set_cond);
+            cg_after_z(s, g);
         }
     }
 }
 
-// gamma_next = g = r'z: the stopping rules and beta (a run starts with `init`);
-// with `set_cond`, sets the graph loop condition.  One thread.
-__device__ void cg_after_z(CgState* s, double g, int init, cudaGraphConditionalHandle handle, int set_cond) {
-    bool stop;
-    if (init) {
+// gamma_next = g = r'z from the V-cycle at the start of a loop body.  The
+// loop body is Krylov.jl's iteration rotated: V-cycle z = M r and r'z, then
+// the direction, Ap and alpha, then the x / r update and the stopping rules.
+// So a run of k iterations applies k V-cycles; `cg!`'s last z, which only
+// its stopping test follows, is not formed.  The iterates and the iteration
+// count are those of `cg!`.  A fresh run takes gamma = r'z (zero: nothing to
+// solve, flag 8); a later body applies the machine stop sqrt(r'z) + 1 <= 1
+// (flag 4; the iteration that reached it was counted by its update) or forms
+// beta.  One thread.
+__device__ void cg_after_z(CgState* s, double g) {
+    if (s->fresh) {
+        s->fresh = 0;
         s->gamma = g;
         s->pnorm2 = g;
         s->rnorm = sqrt(g);
         s->beta = 0;
-        s->iter = 0;
-        s->flags = g == 0 ? 8 : 0;
-        stop = g == 0 || s->itmax <= 0;
-    } else if (s->flags & 2) {
-        stop = true;  // zero curvature: the iteration is abandoned
-    } else {
-        double rnorm = sqrt(g);
-        s->rnorm = rnorm;
-        bool solved = rnorm + 1.0 <= 1.0;
-        if (!solved) {
-            double beta = g / s->gamma;
-            s->beta = beta;
-            s->pnorm2 = g + beta * beta * s->pnorm2;
-            s->gamma = g;
-        } else {
-            s->flags |= 4;
-        }
-        s->iter += 1;
-        if (s->strong_max <= s->target) s->flags |= 1;
-        stop = solved || s->iter >= s->itmax || (s->flags & 1);
+        if (g == 0) s->flags |= 8;
+        return;
     }
-    if (set_cond) cudaGraphSetConditional(handle, stop ? 0u : 1u);
+    const double rnorm = sqrt(g);
+    s->rnorm = rnorm;
+    if (rnorm + 1.0 <= 1.0) {
+        s->flags |= 4;
+        return;
+    }
+    const double beta = g / s->gamma;
+    s->beta = beta;
+    s->pnorm2 = g + beta * beta * s->pnorm2;
+    s->gamma = g;
 }
 
 // r'z folded into the finest post-smoothing of the CG loop's V-cycle:
@@ -376,11 +395,7 @@ struct CgRz {
     const double* r;
     double* partial;
     CgState* s;
-    cudaGraphConditionalHandle handle;
-    int set_cond;
-    __device__ void operator()(double mean, double rx) const {
-        cg_after_z(s, rx - mean * s->rsum, 0, handle, set_cond);
-    }
+    __device__ void operator()(double mean, double rx) const { cg_after_z(s, rx - mean * s->rsum); }
 };
 
 // The next search direction p = z + beta p_old, formed where the
@@ -412,6 +427,7 @@ template <typename T>
 __global__ void k_cg_dir_ap(LevelView<double> A, const T* __restrict__ xv, const double* mean, double* pa,
                             double* pb, double* __restrict__ ap, double* partial, unsigned* counter, CgState* s) {
     pdl_entry();
+    if (s->flags & kCgHalt) return;  // the run ended at this body's r'z
     const NextDir<T> d = next_dir(xv, mean, pa, pb, s);
     double* __restrict__ pn = dir_new(pa, pb, s->iter);
     double v = 0;
@@ -437,6 +453,7 @@ template <typename T, int NXC>
 __global__ void s_cg_dir_ap(SView<double> L, const T* __restrict__ xv, const double* mean, double* pa, double* pb,
                             double* __restrict__ ap, double* partial, unsigned* counter, CgState* s) {
     pdl_entry();
+    if (s->flags & kCgHalt) return;  // the run ended at this body's r'z
     const NextDir<T> d = next_dir(xv, mean, pa, pb, s);
     double* __restrict__ pn = dir_new(pa, pb, s->iter);
     s_apply_dot_ld<double, NXC>(L, d, [&](int c, double v) { pn[c] = v; }, ap, partial, counter,
@@ -449,6 +466,7 @@ __global__ void __launch_bounds__(256) v_cg_dir_ap(SView<double> L, const T* __r
                                                    double* pa, double* pb, double* __restrict__ ap, double* partial,
                                                    unsigned* counter, CgState* s) {
     pdl_entry();
+    if (s->flags & kCgHalt) return;  // the run ended at this body's r'z
     const int k = s->iter;
     const double* __restrict__ po = dir_old(pa, pb, k);
     double* __restrict__ pn = dir_new(pa, pb, k);
@@ -474,6 +492,7 @@ __global__ void k_cg_set(CgState* s, double target, int itmax) {
     s->itmax = itmax;
     s->flags = 0;
     s->iter = 0;
+    s->fresh = 1;
 }
 
 __global__ void k_z_out(int n, const float* __restrict__ xf, const double* __restrict__ xd, const double* mean,
@@ -928,25 +947,28 @@ void DeviceSolver::enqueue_cg_body(int precision, cudaGraphConditionalHandle han
             go(k_cg_dir_ap<T>, fold_grid(k_cg_dir_ap<T>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, A, xv, mean, pa,
                pb, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
     };
-    if (precision == 0) dir_ap(vd_[0].x);
-    else dir_ap(vf_[0].x);
-    const DevLevel& L0 = levels_[0];
-    go(k_cg_update, fold_grid(k_cg_update, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, xw_.p, r_.p, pa, pb,
-       ap_.p, L0.const_vol ? nullptr : A.vol, L0.vol0, fpartial_.p, fpartial2_.p, counters_.p + kCgUpdate, s);
+    // z = M r and r'z (beta, or the start of a run)
     if (rz_foldable()) {
-        // r'z and the stopping rules in the V-cycle's last kernel
-        const CgRz epi{r_.p, fpartial2_.p, s, handle, set_cond};
+        // r'z in the V-cycle's last kernel
+        const CgRz epi{r_.p, fpartial2_.p, s};
         if (precision == 0) enqueue_vcycle_epi<double>(r_.p, &s->rsum, mean, epi);
         else enqueue_vcycle_epi<float>(r_.p, &s->rsum, mean, epi);
     } else if (precision == 0) {
         enqueue_vcycle<double>(r_.p, &s->rsum, mean);
         go(k_cg_z<double>, fold_grid(k_cg_z<double>, kThreads, blocks_for((n + 3) / 4), kMaxGrid), kThreads, 0, n,
-           vd_[0].x, mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 0, handle, set_cond);
+           vd_[0].x, mean, r_.p, fpartial_.p, counters_.p + kCgZ, s);
     } else {
         enqueue_vcycle<float>(r_.p, &s->rsum, mean);
         go(k_cg_z<float>, fold_grid(k_cg_z<float>, kThreads, blocks_for((n + 3) / 4), kMaxGrid), kThreads, 0, n,
-           vf_[0].x, mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 0, handle, set_cond);
+           vf_[0].x, mean, r_.p, fpartial_.p, counters_.p + kCgZ, s);
     }
+    // p = z + beta p_old, Ap and alpha; then x, r, the callback and the loop condition
+    if (precision == 0) dir_ap(vd_[0].x);
+    else dir_ap(vf_[0].x);
+    const DevLevel& L0 = levels_[0];
+    go(k_cg_update, fold_grid(k_cg_update, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, xw_.p, r_.p, pa, pb,
+       ap_.p, L0.const_vol ? nullptr : A.vol, L0.vol0, fpartial_.p, fpartial2_.p, counters_.p + kCgUpdate, s, handle,
+       set_cond);
     TPA_CUDA(cudaGetLastError());
 }
 
@@ -1005,10 +1027,9 @@ cudaGraphExec_t DeviceSolver::cg_graph(int precision) {
 void DeviceSolver::cg_fused(int precision, double target, int itmax, int& niter, int& flags) {
     const int n = levels_[0].n;
     const Launch go{stream_, pdl_};
-    const int nl = int(levels_.size());
     CgState* s = reinterpret_cast<CgState*>(cgs_.p);
-    double* mean = lsum_.p + nl;
     cudaGraphExec_t exec = cg_graph(precision);
+    // a run: the state, r = b - A x and sum(r); the loop bodies follow
     go(k_cg_set, 1, 1, 0, s, target, itmax);
     if (sdev_[0].vec)
         go(v_cg_residual, fold_grid(v_cg_residual, 256, (sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0, sd_[0], b_.p, xw_.p, r_.p,
@@ -1023,20 +1044,9 @@ void DeviceSolver::cg_fused(int precision, double target, int itmax, int& niter,
         go(k_cg_residual, fold_grid(k_cg_residual, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, vd_[0], b_.p, xw_.p, r_.p, fpartial_.p,
                                                                 counters_.p + kCgRes, s);
     launches_ += 2;
-    if (precision == 0) {
-        enqueue_vcycle<double>(r_.p, &s->rsum, mean);
-        go(k_cg_z<double>, fold_grid(k_cg_z<double>, kThreads, blocks_for((n + 3) / 4), kMaxGrid), kThreads, 0, n,
-           vd_[0].x, mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(), 0);
-    } else {
-        enqueue_vcycle<float>(r_.p, &s->rsum, mean);
-        go(k_cg_z<float>, fold_grid(k_cg_z<float>, kThreads, blocks_for((n + 3) / 4), kMaxGrid), kThreads, 0, n,
-           vf_[0].x, mean, r_.p, fpartial_.p, counters_.p + kCgZ, s, 1, cudaGraphConditionalHandle(), 0);
-    }
-    ++launches_;
     CgState hs;
-    TPA_CUDA(cudaMemcpyAsync(&hs, s, sizeof(CgState), cudaMemcpyDeviceToHost, stream_));
-    TPA_CUDA(cudaStreamSynchronize(stream_));
-    if (!(hs.flags & 8) && itmax > 0 && std::getenv("TPAGMG_NO_GRAPH")) {
+    std::memset(&hs, 0, sizeof(hs));
+    if (itmax > 0 && std::getenv("TPAGMG_NO_GRAPH")) {
         // the same iteration launched kernel by kernel, stopping rules read on
         // the host after each one (profiling and diagnosis)
         bool stop = false;
@@ -1046,14 +1056,14 @@ void DeviceSolver::cg_fused(int precision, double target, int itmax, int& niter,
             launches_ = before + graph_body_launches_[precision];
             TPA_CUDA(cudaMemcpyAsync(&hs, s, sizeof(CgState), cudaMemcpyDeviceToHost, stream_));
             TPA_CUDA(cudaStreamSynchronize(stream_));
-            stop = (hs.flags & 7) || hs.iter >= hs.itmax;
+            stop = (hs.flags & (kCgHalt | 1)) || hs.iter >= hs.itmax;
         }
-    } else if (!(hs.flags & 8) && itmax > 0) {
+    } else if (itmax > 0) {
         TPA_CUDA(cudaGraphLaunch(exec, stream_));
         TPA_CUDA(cudaMemcpyAsync(&hs, s, sizeof(CgState), cudaMemcpyDeviceToHost, stream_));
         TPA_CUDA(cudaStreamSynchronize(stream_));
-        // every started body ran its kernels; zero curvature ends one early
-        int bodies = hs.iter + ((hs.flags & 2) ? 1 : 0);
+        // every body ran its kernels; a body that halted is not counted
+        const int bodies = hs.iter + ((hs.flags & kCgHalt) ? 1 : 0);
         launches_ += bodies * graph_body_launches_[precision];
     }
     TPA_CUDA(cudaGetLastError());
