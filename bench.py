@@ -379,11 +379,20 @@ def main():
     solver = EllipticSolver(PoissonOperator(mesh, kappa), device=local)
     stream = torch.cuda.current_stream()
     solver.ctx.call("tpa_set_stream", C.c_void_p(stream.cuda_stream))
-    layout, tune_s = solver.tuning(), 0.0
+    # each precision runs on the layout the autotuner found fastest for its own
+    # V-cycle (the refinement solve runs the FP32 cycle: the mixed layout)
+    layout, tune_s, layouts = solver.tuning(), 0.0, {}
     if not (args.no_autotune or args.profile):
         t0 = time.perf_counter()
-        layout, _ = solver.autotune(precision="mixed", vcycles=20)
+        layouts["fp64"], _ = solver.autotune(precision="fp64", vcycles=20)
+        layouts["mixed"], _ = solver.autotune(precision="mixed", vcycles=20)
+        layout = layouts["mixed"]
         tune_s = time.perf_counter() - t0
+
+    def use_layout(precision):
+        lay = layouts.get("fp64" if precision == "fp64" else "mixed")
+        if lay is not None:
+            solver.set_tuning(**{k: v for k, v in lay.items() if k != "ms_per_vcycle"})
     if args.workload == "droplet_amr":
         rhs_h = W.droplet_rhs(mesh, solver.apply(psi))
     else:
@@ -409,12 +418,6 @@ def main():
         print(json.dumps({"profile": "droplet_amr mixed", "solves": args.steps, "kernel_launches": launches}))
         return
 
-    clk = ClockSampler(local).__enter__()
-    for _ in range(args.warmup):
-        device_solve("mixed")
-        device_solve("fp64")
-    barrier()
-
     def timed(precision, steps):
         ms, its, launches = [], [], 0
         for _ in range(steps):
@@ -432,19 +435,32 @@ def main():
             launches += st.kernel_launches
         return float(np.mean(ms)), float(np.mean(its)), launches, ms
 
-    barrier()
-    mixed_ms, mixed_it, mixed_launches, _ = timed("mixed", args.steps)
-    barrier()
-    fp64_ms, fp64_it, _, _ = timed("fp64", args.steps)
+    # each precision on its layout: W warm-up solves, then K timed ones
+    clk = ClockSampler(local).__enter__()
+    res = {}
+    for precision in ("mixed", "fp64", "mixed_ir"):
+        use_layout(precision)
+        for _ in range(args.warmup):
+            device_solve(precision)
+        barrier()
+        res[precision] = timed(precision, args.steps)
     clk.__exit__(None, None, None)
-    device_solve("mixed")
-    x_mixed = x_d.clone()
+    mixed_ms, mixed_it, mixed_launches, _ = res["mixed"]
+    fp64_ms, fp64_it, _, _ = res["fp64"]
+    ir_ms, ir_it, _, _ = res["mixed_ir"]
+    use_layout("fp64")
     device_solve("fp64")
     x_ref = x_d.clone()
+    use_layout("mixed")  # left in effect for the measurements below
+    device_solve("mixed_ir")
+    x_ir = x_d.clone()
+    device_solve("mixed")
+    x_mixed = x_d.clone()
     mixed_err = float((x_mixed - x_ref).abs().max() / x_ref.abs().max())
+    ir_err = float((x_ir - x_ref).abs().max() / x_ref.abs().max())
 
     # max over ranks (each rank solves its own replica: no work to sum)
-    (mixed_ms, fp64_ms), _ = combine_over_ranks([mixed_ms, fp64_ms], [], world, "cuda")
+    (mixed_ms, fp64_ms, ir_ms), _ = combine_over_ranks([mixed_ms, fp64_ms, ir_ms], [], world, "cuda")
 
     # end to end through the public C-ABI with pinned host buffers
     rhs_pin = torch.from_numpy(rhs_h).pin_memory()
@@ -606,6 +622,7 @@ def main():
         ref_max = float(np.max(np.abs(x_oracle)))
         oracle_err = {"mixed": float(np.max(np.abs(x_mixed.cpu().numpy() - x_oracle)) / ref_max),
                       "fp64": float(np.max(np.abs(x_ref.cpu().numpy() - x_oracle)) / ref_max),
+                      "mixed_ir": float(np.max(np.abs(x_ir.cpu().numpy() - x_oracle)) / ref_max),
                       "norm": "max |x_gpu - x_oracle| / max |x_oracle|",
                       "oracle": f"C restatement solved to rtol 1e-12 ({ost.cycles} CG iterations) on the same RHS"}
     # DRAM bytes per launch of the roofline kernel from a committed ncu capture
@@ -632,9 +649,15 @@ def main():
         "config": {"workload": wname,
                    "fine_cells": n, "levels": solver.level_sizes(), "parallelism": "replicas" if world > 1 else "1 GPU",
                    "l2": "flushed between steps (256 MiB write)", "device_layout": dict(solver.device_info(), tiled_levels=solver.tiled_levels()),
-                   "autotuned_layout": layout, "autotune_s": tune_s},
-        "time_to_tolerance_ms": {"mixed": mixed_ms, "fp64": fp64_ms, "speedup_mixed_over_fp64": fp64_ms / mixed_ms},
-        "cg_iterations": {"mixed": mixed_it, "fp64": fp64_it},
+                   "autotuned_layout": layout, "autotuned_layout_fp64": layouts.get("fp64"), "autotune_s": tune_s},
+        "time_to_tolerance_ms": {"mixed": mixed_ms, "fp64": fp64_ms, "speedup_mixed_over_fp64": fp64_ms / mixed_ms,
+                                 "mixed_ir": ir_ms, "speedup_mixed_ir_over_fp64": fp64_ms / ir_ms},
+        "cg_iterations": {"mixed": mixed_it, "fp64": fp64_it, "mixed_ir": ir_it},
+        "precisions": {"mixed": "FP32 V-cycle, FP64 Krylov vectors",
+                       "fp64": "FP64 V-cycle and Krylov vectors",
+                       "mixed_ir": "FP32 V-cycle and Krylov vectors (r, p, Ap, z) inside FP64 iterative refinement: "
+                                   "FP64 iterate, true residual and inner products"},
+        "mixed_ir_error_vs_fp64": ir_err,
         "fp64_value": world * n * fp64_it / (fp64_ms * 1e-3),
         "mixed_error_vs_fp64": mixed_err,
         "error_vs_fp64_oracle": oracle_err,

@@ -160,7 +160,13 @@ tpa_status tpa_last_refresh(const tpa_context* ctx, int32_t* path, double* ms);
 /* solve!(solution, solver, rhs; rtol, atol, max_cycles, compatibility)
  * (src/solvers/multigrid/elliptic_solver.jl:628-675).  rhs is the strong-form
  * right-hand side, x the initial guess on entry and the solution on return,
- * both host arrays in cell order. */
+ * both host arrays in cell order.  precision 0: FP64 V-cycle and Krylov
+ * vectors; 1: FP32 V-cycle, FP64 Krylov vectors; 2: FP64 iterative
+ * refinement around CG runs whose r, p, Ap and z are stored in FP32 (the
+ * iterate, the true residual that starts each run and every inner product
+ * stay FP64; a run stops at 1e-5 of the true residual it started from, or at
+ * the target).  2 has no counterpart in the reference and needs the default
+ * cycle; stats->cycles sums the CG iterations of all runs. */
 tpa_status tpa_solve(tpa_context* ctx, const double* rhs, double* x, double rtol, double atol, int32_t max_cycles,
                      int32_t compatibility, int32_t precision, tpa_stats* stats);
 /* Same with device pointers (cell order, on the context's device). */
@@ -237,13 +243,15 @@ tpa_status tpa_batch_solve_device(tpa_batch* batch, const double* rhs, double* x
  * CSR level of the multi-CTA part as two launches on haloed block tiles (both
  * pre-sweeps, the residual and the restriction in one, the prolongation and
  * both post-sweeps in the other; the halo is recomputed in each tile), 2 also
- * the constant-coefficient 16x16 levels (on 22 x 22 stencil tiles), 0 none.
+ * the constant-coefficient 16x16 levels (on 22 x 22 stencil tiles), 3 the
+ * constant-coefficient levels of at most 2^19 cells only (larger ones keep
+ * the vectorized kernels), 0 none.
  * Every layout gives the same V-cycle to rounding. */
 typedef struct {
     int32_t tail_cells, tail_ctas, structured, vectorized, pdl, fuse_restrict, persistent, tiles;
     double ms_per_vcycle; /* measured time (tpa_autotune), else 0 */
 } tpa_tune_config;
-/* Autotuner: times `vcycles` V-cycles (precision 0 FP64, 1 mixed) of every
+/* Autotuner: times `vcycles` V-cycles (precision 0 FP64, 1 or 2 FP32) of every
  * candidate layout on the uploaded hierarchy (tail size x tail CTAs x stencil
  * policy, then the best without vectorized kernels, without PDL, with the
  * fused restriction, as one cooperative launch and on block tiles), keeps the
@@ -375,7 +383,7 @@ typedef struct {
     const double* inherited_divergence; /* NULL, or the `_inherited_divergence` cell array */
     int32_t max_cycles;                 /* default 100 */
     int32_t compatibility;              /* 0 :project, 1 :error */
-    int32_t precision;                  /* 0 FP64 V-cycle, 1 FP32 V-cycle */
+    int32_t precision;                  /* 0 FP64, 1 mixed, 2 mixed refinement (tpa_solve) */
     int32_t prepared;                   /* 0: `project!` (walls made impermeable first),
                                            1: `_project_prepared!` (boundary velocity as given) */
 } tpa_projection_options;

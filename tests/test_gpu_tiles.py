@@ -135,3 +135,35 @@ def test_stencil_tiles_match_vectorized_kernels(name):
     assert solve(xm, s, rhs, rtol=1e-10, precision="mixed").converged
     assert np.max(np.abs(x - po)) <= 1e-10 * np.max(np.abs(po))
     assert np.max(np.abs(xm - po)) <= 1e-9 * np.max(np.abs(po))
+
+
+def test_stencil_tiles_on_small_levels_only():
+    """tiles = 3: stencil tiles on the constant-coefficient levels of at most
+    2^19 cells; the 1024^2 finest level keeps the vectorized kernels.  The
+    V-cycle equals the six-launch one to rounding, and the solve reaches the
+    tolerance in the same number of iterations."""
+    m = BlockTreeMesh(base_mesh=(1024, 1024), block_size=(16, 16), periodic=(True, True))
+    s = EllipticSolver(PoissonOperator(m))
+    s0 = EllipticSolver(PoissonOperator(m))
+    s2 = EllipticSolver(PoissonOperator(m))
+    s.set_tuning(tiles=3, tail_cells=1024)
+    s0.set_tuning(tiles=0, tail_cells=1024)
+    s2.set_tuning(tiles=2, tail_cells=1024)
+    multi = [n for n in s.level_sizes()[:-1] if n > 1024]  # the levels outside the one-CTA tail
+    assert s0.device_info()["structured_levels"] >= len(multi)
+    assert s2.tiled_levels() == len(multi)
+    assert s.tiled_levels() == sum(1 for n in multi if n <= 1 << 19) == len(multi) - 1
+    rng = np.random.default_rng(11)
+    r = rng.standard_normal(m.ncells)
+    r -= r.mean()
+    r *= m.cell_volumes()
+    for precision, tol in (("fp64", 1e-13), ("mixed", 1e-5)):
+        z, z0 = s.vcycle(r, precision=precision), s0.vcycle(r, precision=precision)
+        assert np.max(np.abs(z - z0)) <= tol * np.max(np.abs(z0)), precision
+    rhs = r / m.cell_volumes()
+    for precision in ("fp64", "mixed"):
+        x, x0 = np.zeros(m.ncells), np.zeros(m.ncells)
+        st = solve(x, s, rhs, rtol=1e-10, precision=precision)
+        st0 = solve(x0, s0, rhs, rtol=1e-10, precision=precision)
+        assert st.converged and st0.converged and st.cycles == st0.cycles
+        assert np.max(np.abs(x - x0)) <= 1e-9 * np.max(np.abs(x0))

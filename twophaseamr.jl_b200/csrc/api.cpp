@@ -809,7 +809,7 @@ void project_body(tpa_context* ctx, double* u_int, double* u_bnd, double* p, con
     if (!o) throw tpa::Error(TPA_ERR_INVALID_ARG, "null options");
     if (o->compatibility != 0 && o->compatibility != 1)
         throw tpa::Error(TPA_ERR_INVALID_ARG, "compatibility must be :project or :error");
-    if (o->precision != 0 && o->precision != 1) throw tpa::Error(TPA_ERR_INVALID_ARG, "bad precision");
+    if (o->precision < 0 || o->precision > 2) throw tpa::Error(TPA_ERR_INVALID_ARG, "bad precision");
     if (o->max_cycles < 0) throw tpa::Error(TPA_ERR_INVALID_ARG, "max_cycles must be nonnegative");
     // 0 stands for "not given"; any other value (negative, inf, nan) is checked
     const double reference_dt = o->reference_dt == 0.0 ? o->dt : o->reference_dt;
@@ -1080,8 +1080,9 @@ extern "C" {
 tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tpa_tune_config* best,
                         tpa_tune_config* tried, int32_t capacity, int32_t* ntried) {
     return guard(ctx, [&] {
-        if (precision != 0 && precision != 1) throw tpa::Error(TPA_ERR_INVALID_ARG, "bad precision");
+        if (precision < 0 || precision > 2) throw tpa::Error(TPA_ERR_INVALID_ARG, "bad precision");
         if (vcycles <= 0) throw tpa::Error(TPA_ERR_INVALID_ARG, "vcycles must be positive");
+        precision = std::min(precision, 1);  // the refinement solve runs the FP32 V-cycle
         ensure_device(ctx);
         ensure_host_fresh(ctx);  // stencil copies come from the host levels
         tpa::DeviceSolver& d = *ctx->dev;
@@ -1132,7 +1133,7 @@ tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tp
         run(pe);
         // the CSR levels on haloed block tiles (two launches per level), with
         // the tail sizes around the best one
-        for (int tiles : {1, 2})
+        for (int tiles : {1, 2, 3})
             for (int cells : {1024, 2048, 4096}) {
                 tpa::TuneConfig tl = b0;
                 tl.tiles = tiles;
@@ -1151,7 +1152,7 @@ tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tp
 tpa_status tpa_set_tuning(tpa_context* ctx, const tpa_tune_config* cfg) {
     return guard(ctx, [&] {
         if (!cfg) throw tpa::Error(TPA_ERR_INVALID_ARG, "null configuration");
-        if (cfg->tail_ctas > 8 || cfg->structured > 2 || cfg->tiles > 2)
+        if (cfg->tail_ctas > 8 || cfg->structured > 2 || cfg->tiles > 3)
             throw tpa::Error(TPA_ERR_INVALID_ARG, "bad configuration");
         ensure_device(ctx);
         ensure_host_fresh(ctx);  // stencil copies come from the host levels

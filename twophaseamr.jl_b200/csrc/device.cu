@@ -834,7 +834,10 @@ void DeviceSolver::solve(const double* rhs, double* x_user, double rtol, double 
     if (!(atol >= 0)) throw Error(1, "atol must be nonnegative");
     if (max_cycles < 0) throw Error(1, "max_cycles must be nonnegative");
     if (compatibility != 0 && compatibility != 1) throw Error(1, "compatibility must be :project or :error");
-    if (precision != 0 && precision != 1) throw Error(1, "precision must be 0 (FP64) or 1 (mixed)");
+    if (precision < 0 || precision > 2)
+        throw Error(1, "precision must be 0 (FP64), 1 (mixed) or 2 (mixed with FP32 Krylov vectors)");
+    if (precision == 2 && (!fused_ok_ || std::getenv("TPAGMG_PLAIN_SOLVE")))
+        throw Error(5, "the refinement solve needs the fused cycle (two pre- and two post-sweeps, one component)");
     if (fused_ok_ && !std::getenv("TPAGMG_PLAIN_SOLVE")) {
         solve_fast(rhs, x_user, rtol, atol, max_cycles, compatibility, precision, st);
         return;

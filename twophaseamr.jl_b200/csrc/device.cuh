@@ -207,9 +207,9 @@ public:
 
 private:
     void build_views();
-    template <typename T> void enqueue_vcycle(const double* r, const double* rsum, double* mean_out);
-    template <typename T, typename Epi>
-    void enqueue_vcycle_epi(const double* r, const double* rsum, double* mean_out, const Epi& epi);
+    template <typename T, typename R> void enqueue_vcycle(const R* r, const double* rsum, double* mean_out);
+    template <typename T, typename Epi, typename R>
+    void enqueue_vcycle_epi(const R* r, const double* rsum, double* mean_out, const Epi& epi);
     bool rz_foldable() const;
     // CG from the current xw_/b_: returns iterations and flags (Krylov.jl cg! loop)
     void cg_fused(int precision, double target, int itmax, int& niter, int& flags);
@@ -263,8 +263,15 @@ private:
     DevArray<double> fpartial_, fpartial2_, lsum_, xw_;
     DevArray<unsigned> counters_;
     DevArray<char> cgs_;  // CgState
-    cudaGraphExec_t cg_exec_[2] = {nullptr, nullptr};
-    int graph_body_launches_[2] = {0, 0};
+    // one captured CG loop per precision: 0 FP64, 1 mixed, 2 the refinement
+    // solve's inner runs (FP32 r, directions and Ap)
+    cudaGraphExec_t cg_exec_[3] = {nullptr, nullptr, nullptr};
+    int graph_body_launches_[3] = {0, 0, 0};
+    // FP32 r, pa, pb, Ap of the refinement solve, each ir_stride() floats
+    // (16-byte aligned sections); allocated by its first solve
+    DevArray<float> ir_;
+    size_t ir_stride() const { return (size_t(levels_[0].n) + 3) & ~size_t(3); }
+    double ir_eta_ = 1e-5;  // inner-run reduction of the refinement solve
 
     // block-structured level data (stencil + exception rows)
     struct StructDev {

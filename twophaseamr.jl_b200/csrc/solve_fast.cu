@@ -274,7 +274,14 @@ void DeviceSolver::solve_fast(const double* rhs, double* x_user, double rtol, do
     if (init.linf > target) {
         while (total < max_cycles) {
             int niter = 0, flags = 0;
-            cg_fused(precision, target, max_cycles - total, niter, flags);
+            // precision 2, FP64 iterative refinement: each run is a CG on the
+            // correction with FP32 r, directions and Ap (x and every inner
+            // product stay FP64), started from the FP32 rounding of the true
+            // residual and stopped at a fixed reduction of it or at the target;
+            // its recurrence residual follows the true one to about the FP32
+            // unit roundoff per iteration
+            const double inner = precision == 2 ? std::max(target, ir_eta_ * fin.linf) : target;
+            cg_fused(precision, inner, max_cycles - total, niter, flags);
             total += niter;
             // gauge of the iterate, then the true residual and its norms
             k_xmean<<<fold_grid(k_xmean, kThreads, want, kGrid), kThreads, 0, stream_>>>(n, xw_.p, L.const_vol ? nullptr : A.vol, L.vol0, tmp_.p, spartial_.p, counters_.p + kCMean,

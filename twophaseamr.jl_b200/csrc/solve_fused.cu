@@ -38,7 +38,12 @@ inline int blocks_for(int64_t n) {
     return int(g < 1 ? 1 : g);
 }
 
-constexpr int kMaxGrid = 1184;  // 8 CTAs on each of 148 SMs: bounds the partials every fold reads
+constexpr int kMaxGrid = 1184;
+// tiles = 3: the largest constant-coefficient level on stencil tiles.  A level
+// of 2^19 cells is 2048 tiles, under two resident waves of 256-thread CTAs;
+// the next level up streams HBM at a rate the tiles' index arithmetic cannot
+// keep.
+constexpr int kStencilTileCells = 1 << 19;  // 8 CTAs on each of 148 SMs: bounds the partials every fold reads
 #define TPA_GRID_STRIDE(i, n) for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += gridDim.x * blockDim.x)
 
 // Kernel launch on `s`, with programmatic dependent launch when `pdl`: the
@@ -166,30 +171,37 @@ __global__ void k_cg_ap(LevelView<double> A, const double* __restrict__ p, doubl
 // Search directions of iteration `iter` in the ping-pong pair (pa, pb): the
 // previous one (read by the operator product) and the new one (written by it,
 // read by the update).
-__device__ __forceinline__ const double* dir_old(const double* pa, const double* pb, int iter) {
+template <typename P>
+__device__ __forceinline__ const P* dir_old(const P* pa, const P* pb, int iter) {
     return (iter & 1) ? pb : pa;
 }
-__device__ __forceinline__ double* dir_new(double* pa, double* pb, int iter) { return (iter & 1) ? pa : pb; }
+template <typename P>
+__device__ __forceinline__ P* dir_new(P* pa, P* pb, int iter) {
+    return (iter & 1) ? pa : pb;
+}
 
 // x += alpha p, r -= alpha Ap (p: this iteration's direction); folds
-// max|r_i|/V_i and sum(r).  vol null: every cell's volume is vol0.
-__global__ void k_cg_update(int n, double* __restrict__ x, double* __restrict__ r, double* pa, double* pb,
-                            const double* __restrict__ ap, const double* __restrict__ vol, double vol0, double* pmax,
-                            double* psum, unsigned* counter, CgState* s, cudaGraphConditionalHandle handle,
-                            int set_cond) {
+// max|r_i|/V_i and sum(r).  vol null: every cell's volume is vol0.  P is the
+// storage type of r, p and Ap (FP32 in the refinement solve's inner runs);
+// x and the arithmetic stay FP64, and the norms are those of the stored r.
+template <typename P>
+__global__ void k_cg_update(int n, double* __restrict__ x, P* __restrict__ r, P* pa, P* pb, const P* __restrict__ ap,
+                            const double* __restrict__ vol, double vol0, double* pmax, double* psum,
+                            unsigned* counter, CgState* s, cudaGraphConditionalHandle handle, int set_cond) {
     pdl_entry();
-    const double* __restrict__ p = dir_new(pa, pb, s->iter);
+    const P* __restrict__ p = dir_new(pa, pb, s->iter);
     __shared__ bool last;
     const bool skip = s->flags & kCgHalt;
     const double alpha = s->alpha;
     double m = 0, sum = 0;
     bool nan = false;
     TPA_GRID_STRIDE(i, n) {
-        double ri = r[i];
+        double ri = double(r[i]);
         if (!skip) {
-            x[i] += alpha * p[i];
-            ri -= alpha * ap[i];
-            r[i] = ri;
+            x[i] += alpha * double(p[i]);
+            const P rs = P(ri - alpha * double(ap[i]));
+            r[i] = rs;
+            ri = double(rs);
         }
         double V = vol ? vol[i] : vol0;
         if (V > 0) {
@@ -331,8 +343,8 @@ __device__ void cg_after_z(CgState* s, double g);
 // gamma_next = r'z for z = x0 - mean (the V-cycle's output, not stored: the
 // next operator product forms z and p where it reads them), then beta or the
 // start of a run (cg_after_z)
-template <typename T>
-__global__ void k_cg_z(int n, const T* __restrict__ xv, const double* mean, const double* __restrict__ r,
+template <typename T, typename R>
+__global__ void k_cg_z(int n, const T* __restrict__ xv, const double* mean, const R* __restrict__ r,
                        double* partial, unsigned* counter, CgState* s) {
     pdl_entry();
     const double m = mean ? *mean : 0.0;
@@ -342,11 +354,11 @@ __global__ void k_cg_z(int n, const T* __restrict__ xv, const double* mean, cons
     const int nq = n >> 2;
     TPA_GRID_STRIDE(k, nq) {
         const Quad<T> xq = q_ldv(xv + 4 * k);
-        const Quad<double> rq = q_ldv(r + 4 * k);
-        for (int c = 0; c < 4; ++c) v += rq.v[c] * (double(xq.v[c]) - m);
+        const Quad<R> rq = q_ldv(r + 4 * k);
+        for (int c = 0; c < 4; ++c) v += double(rq.v[c]) * (double(xq.v[c]) - m);
     }
     for (int i = 4 * nq + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        v += r[i] * (double(xv[i]) - m);
+        v += double(r[i]) * (double(xv[i]) - m);
     if (publish_partial(v, partial, counter)) {
         double g = fold_partials(partial, gridDim.x);
         if (threadIdx.x == 0) {
@@ -403,40 +415,43 @@ struct CgRz {
 // output (FP32 or FP64) and p_old from the other buffer of the ping-pong pair;
 // the first iteration of a run (iter 0) takes p = z.  So neither z nor a
 // separate p pass goes through memory, and no launch of its own is needed.
-template <typename T>
+// P: the storage type of the directions.  The value is rounded to P where it
+// is formed, so the operator product below is that of the stored direction
+// (the x update adds the stored one).
+template <typename T, typename P>
 struct NextDir {
     const T* __restrict__ x;
-    const double* __restrict__ pold;
+    const P* __restrict__ pold;
     double mean, beta;
     bool first;
     __device__ __forceinline__ double operator()(int j) const {
         const double z = double(x[j]) - mean;
-        return first ? z : z + beta * pold[j];
+        return double(P(first ? z : z + beta * double(pold[j])));
     }
 };
 
-template <typename T>
-__device__ __forceinline__ NextDir<T> next_dir(const T* xv, const double* mean, const double* pa, const double* pb,
-                                               const CgState* s) {
+template <typename T, typename P>
+__device__ __forceinline__ NextDir<T, P> next_dir(const T* xv, const double* mean, const P* pa, const P* pb,
+                                                  const CgState* s) {
     const int k = s->iter;
-    return NextDir<T>{xv, dir_old(pa, pb, k), *mean, s->beta, k == 0};
+    return NextDir<T, P>{xv, dir_old(pa, pb, k), *mean, s->beta, k == 0};
 }
 
 // p = z + beta p_old, Ap and alpha = gamma / p'Ap (CSR finest level)
-template <typename T>
-__global__ void k_cg_dir_ap(LevelView<double> A, const T* __restrict__ xv, const double* mean, double* pa,
-                            double* pb, double* __restrict__ ap, double* partial, unsigned* counter, CgState* s) {
+template <typename T, typename P>
+__global__ void k_cg_dir_ap(LevelView<double> A, const T* __restrict__ xv, const double* mean, P* pa, P* pb,
+                            P* __restrict__ ap, double* partial, unsigned* counter, CgState* s) {
     pdl_entry();
     if (s->flags & kCgHalt) return;  // the run ended at this body's r'z
-    const NextDir<T> d = next_dir(xv, mean, pa, pb, s);
-    double* __restrict__ pn = dir_new(pa, pb, s->iter);
+    const NextDir<T, P> d = next_dir(xv, mean, pa, pb, s);
+    P* __restrict__ pn = dir_new(pa, pb, s->iter);
     double v = 0;
     TPA_GRID_STRIDE(i, A.n) {
         double y = 0;
         for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) y += A.val[k] * d(A.ci[k]);
         const double pi = d(i);
-        pn[i] = pi;
-        ap[i] = y;
+        pn[i] = P(pi);
+        ap[i] = P(y);
         v += pi * y;
     }
     if (publish_partial(v, partial, counter)) {
@@ -449,27 +464,27 @@ __global__ void k_cg_dir_ap(LevelView<double> A, const T* __restrict__ xv, const
 }
 
 // the same on a block-structured finest level
-template <typename T, int NXC>
-__global__ void s_cg_dir_ap(SView<double> L, const T* __restrict__ xv, const double* mean, double* pa, double* pb,
-                            double* __restrict__ ap, double* partial, unsigned* counter, CgState* s) {
+template <typename T, typename P, int NXC>
+__global__ void s_cg_dir_ap(SView<double> L, const T* __restrict__ xv, const double* mean, P* pa, P* pb,
+                            P* __restrict__ ap, double* partial, unsigned* counter, CgState* s) {
     pdl_entry();
     if (s->flags & kCgHalt) return;  // the run ended at this body's r'z
-    const NextDir<T> d = next_dir(xv, mean, pa, pb, s);
-    double* __restrict__ pn = dir_new(pa, pb, s->iter);
-    s_apply_dot_ld<double, NXC>(L, d, [&](int c, double v) { pn[c] = v; }, ap, partial, counter,
+    const NextDir<T, P> d = next_dir(xv, mean, pa, pb, s);
+    P* __restrict__ pn = dir_new(pa, pb, s->iter);
+    s_apply_dot_ld<double, NXC>(L, d, [&](int c, double v) { pn[c] = P(v); }, ap, partial, counter,
                                 [&](double pAp) { alpha_from(pAp, s); });
 }
 
 // the same on a constant-coefficient 16x16 finest level (vectorized quads)
-template <typename T>
+template <typename T, typename P>
 __global__ void __launch_bounds__(256) v_cg_dir_ap(SView<double> L, const T* __restrict__ xv, const double* mean,
-                                                   double* pa, double* pb, double* __restrict__ ap, double* partial,
+                                                   P* pa, P* pb, P* __restrict__ ap, double* partial,
                                                    unsigned* counter, CgState* s) {
     pdl_entry();
     if (s->flags & kCgHalt) return;  // the run ended at this body's r'z
     const int k = s->iter;
-    const double* __restrict__ po = dir_old(pa, pb, k);
-    double* __restrict__ pn = dir_new(pa, pb, k);
+    const P* __restrict__ po = dir_old(pa, pb, k);
+    P* __restrict__ pn = dir_new(pa, pb, k);
     const double mu = *mean, beta = s->beta;
     const bool first = k == 0;
     auto ld = [&](int c) {
@@ -478,12 +493,34 @@ __global__ void __launch_bounds__(256) v_cg_dir_ap(SView<double> L, const T* __r
         if (first) {
             for (int m = 0; m < 4; ++m) q.v[m] = double(xq.v[m]) - mu;
         } else {
-            const Quad<double> pq = q_ldv(po + c);
-            for (int m = 0; m < 4; ++m) q.v[m] = (double(xq.v[m]) - mu) + beta * pq.v[m];
+            const Quad<P> pq = q_ldv(po + c);
+            for (int m = 0; m < 4; ++m) q.v[m] = (double(xq.v[m]) - mu) + beta * double(pq.v[m]);
         }
+        for (int m = 0; m < 4; ++m) q.v[m] = double(P(q.v[m]));  // the stored direction
         return q;
     };
     v_apply_dot_ld(L, ld, pn, ap, partial, counter, [&](double pAp) { alpha_from(pAp, s); });
+}
+
+// Start of an inner run of the refinement solve: the FP64 true residual
+// rounded to the FP32 recurrence residual, and the sum of the stored values
+// (the V-cycle's right-hand-side projection uses it)
+__global__ void k_ir_start(int n, const double* __restrict__ r, float* __restrict__ r32, double* partial,
+                           unsigned* counter, CgState* s) {
+    pdl_entry();
+    double v = 0;
+    TPA_GRID_STRIDE(i, n) {
+        const float ri = float(r[i]);
+        r32[i] = ri;
+        v += double(ri);
+    }
+    if (publish_partial(v, partial, counter)) {
+        const double t = fold_partials(partial, gridDim.x);
+        if (threadIdx.x == 0) {
+            s->rsum = t;
+            *counter = 0;
+        }
+    }
 }
 
 __global__ void k_cg_set(CgState* s, double target, int itmax) {
@@ -530,10 +567,13 @@ TuneConfig DeviceSolver::effective_tuning() const {
     if (tune_.persistent >= 0) c.persistent = tune_.persistent ? 1 : 0;
     // 1: CSR levels on tiles (the default: measured faster on the droplet),
     // 2: the constant-coefficient 16x16 levels on stencil tiles as well
-    // (measured slower than the vectorized kernels on uniform 2048^2), 0: none
+    // (measured slower than the vectorized kernels on uniform 2048^2, whose
+    // finest level makes the tile kernel instruction-bound), 3: stencil tiles
+    // on the constant-coefficient levels of at most kStencilTileCells cells
+    // only, where the six vectorized launches are latency-bound, 0: none
     c.tiles = 1;
-    if (const char* e = std::getenv("TPAGMG_TILES")) c.tiles = std::min(2, std::max(0, std::atoi(e)));
-    if (tune_.tiles >= 0) c.tiles = std::min(2, tune_.tiles);
+    if (const char* e = std::getenv("TPAGMG_TILES")) c.tiles = std::min(3, std::max(0, std::atoi(e)));
+    if (tune_.tiles >= 0) c.tiles = std::min(3, tune_.tiles);
     if (rb_) {  // the red-black sweeps exist for the CSR levels and the tail only
         c.structured = 0;
         c.persistent = 0;
@@ -562,6 +602,9 @@ void DeviceSolver::build_views() {
     // lowers it; 0 makes every barrier that has to wait give up)
     barrier_spins_ = kBarrierSpins;
     if (const char* e = std::getenv("TPAGMG_BARRIER_SPINS")) barrier_spins_ = std::strtoull(e, nullptr, 10);
+    // reduction of the true residual per inner run of the refinement solve
+    ir_eta_ = 1e-5;
+    if (const char* e = std::getenv("TPAGMG_IR_ETA")) ir_eta_ = std::min(0.5, std::max(1e-7, std::atof(e)));
     // 1: every CSR level; above 1: levels of at most that many cells
     rr_cells_ = cfg.fuse_restrict == 1 ? INT32_MAX : cfg.fuse_restrict;
     fused_ok_ = (pre_ == 2 && post_ == 2);
@@ -672,18 +715,19 @@ void DeviceSolver::destroy_graphs() {
         }
 }
 
-// V-cycle on r (FP64, integrated residual) with level-0 RHS sum `rsum`
-// (device pointer); result in view 0's x, level-0 mean in *mean_out.
-template <typename T>
-void DeviceSolver::enqueue_vcycle(const double* r, const double* rsum, double* mean_out) {
+// V-cycle on r (integrated residual, FP64 or FP32 storage R) with level-0
+// RHS sum `rsum` (device pointer); result in view 0's x, level-0 mean in
+// *mean_out.
+template <typename T, typename R>
+void DeviceSolver::enqueue_vcycle(const R* r, const double* rsum, double* mean_out) {
     enqueue_vcycle_epi<T>(r, rsum, mean_out, MeanOnly());
 }
 
 // The same, with `epi` run by the finest level's last post-smoothing after it
 // folds the mean (see MeanOnly).  The caller checks rz_foldable() first when
 // the epilogue must run.
-template <typename T, typename Epi>
-void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, double* mean_out, const Epi& epi) {
+template <typename T, typename Epi, typename R>
+void DeviceSolver::enqueue_vcycle_epi(const R* r, const double* rsum, double* mean_out, const Epi& epi) {
     const Launch go{stream_, pdl_};
     const int nl = int(levels_.size());
     const int t = tail_first_;
@@ -699,10 +743,14 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
     const std::vector<LevelView<T>>& V = *Vp;
     if (coop_grid_ > 0) {
         // the whole cycle in one cooperative launch (persistent.cuh)
-        const Launch gc{stream_, false, 1, true};
-        gc(k_vcycle_grid<T>, coop_grid_, kTailThreads, 0, Vdev, t, nl, r, rsum, mean_out, coarse_inv_.p, coarse_n_,
-           fpartial_.p, bar_.p, lsum_.p, err_.p, barrier_spins_);
-        ++launches_;
+        if constexpr (std::is_same<R, double>::value) {
+            const Launch gc{stream_, false, 1, true};
+            gc(k_vcycle_grid<T>, coop_grid_, kTailThreads, 0, Vdev, t, nl, r, rsum, mean_out, coarse_inv_.p,
+               coarse_n_, fpartial_.p, bar_.p, lsum_.p, err_.p, barrier_spins_);
+            ++launches_;
+        } else {
+            throw Error(5, "the cooperative V-cycle takes an FP64 right-hand side");
+        }
         if (!V[0].singular) TPA_CUDA(cudaMemsetAsync(mean_out, 0, sizeof(double), stream_));
         return;
     }
@@ -718,7 +766,7 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
             if (tdev_.size() > size_t(l) && tdev_[size_t(l)].vec) {
                 // both pre-sweeps, the residual and the restriction on 22 x 22 tiles
                 if (l == 0)
-                    go(v_tile_down<T, double>, S.nblocks, kTileThreads, 0, S, r, rsum, V[size_t(l + 1)].b, fpartial_.p,
+                    go(v_tile_down<T, R>, S.nblocks, kTileThreads, 0, S, r, rsum, V[size_t(l + 1)].b, fpartial_.p,
                        counters_.p + kRestrictSum, next_sum ? lsum_.p + l + 1 : nullptr);
                 else
                     go(v_tile_down<T, T>, S.nblocks, kTileThreads, 0, S, (const T*)S.b,
@@ -727,7 +775,7 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
                 ++launches_;
                 continue;
             }
-            if (l == 0) go(v_pre2<T, double>, groups, 256, 0, S, r, rsum);
+            if (l == 0) go(v_pre2<T, R>, groups, 256, 0, S, r, rsum);
             else go(v_pre2<T, T>, groups, 256, 0, S, S.b, lsum_.p + l);
             go(v_residual<T>, groups, 256, 0, S);
             go(v_restrict<T>, next_sum ? fold_grid(v_restrict<T>, 256, groups, kMaxGrid) : groups, 256, 0, S,
@@ -742,7 +790,7 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
             const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
             with_nxc(S, [&](auto nxc) {
                 constexpr int N = decltype(nxc)::value;
-                if (l == 0) go(s_pre2<T, double, N>, g, th, 0, S, r, rsum);
+                if (l == 0) go(s_pre2<T, R, N>, g, th, 0, S, r, rsum);
                 else go(s_pre2<T, T, N>, g, th, 0, S, S.b, lsum_.p + l);
                 go(s_residual<T, N>, g, th, 0, S);
                 go(s_restrict<T, N>, next_sum ? fold_grid(s_restrict<T, N>, th, g, kMaxGrid, th * sizeof(T)) : g,
@@ -762,7 +810,7 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
             with_tile_threads(D.nt, [&](auto nt) {
                 constexpr int NT = decltype(nt)::value;
                 if (l == 0)
-                    go(k_tile_down<T, double, NT>, D.ntiles, NT, sm, L, TV, r, rsum, V[size_t(l + 1)].b, fpartial_.p,
+                    go(k_tile_down<T, R, NT>, D.ntiles, NT, sm, L, TV, r, rsum, V[size_t(l + 1)].b, fpartial_.p,
                        counters_.p + kRestrictSum, next_sum ? lsum_.p + l + 1 : nullptr);
                 else
                     go(k_tile_down<T, T, NT>, D.ntiles, NT, sm, L, TV, (const T*)L.b, (const double*)(lsum_.p + l),
@@ -777,7 +825,7 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
             // two half-sweeps on a large one
             const bool pair = L.n <= rb_pair_cells_;
             T* first = pair ? L.y : L.x;
-            if (l == 0) go(k_rb_pre<T, double>, blocks_for(L.n), kThreads, 0, L, r, rsum, first);
+            if (l == 0) go(k_rb_pre<T, R>, blocks_for(L.n), kThreads, 0, L, r, rsum, first);
             else go(k_rb_pre<T, T>, blocks_for(L.n), kThreads, 0, L, L.b, lsum_.p + l, first);
             if (pair) {
                 go(k_rb_pair<T>, blocks_for(L.n), kThreads, 0, L, (const T*)L.y, L.x, 0, nullptr, nullptr, nullptr);
@@ -788,7 +836,7 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
                 launches_ += 2;
             }
         } else if (l == 0) {
-            go(k_pre2<T, double>, blocks_for(L.n), kThreads, 0, L, r, rsum);
+            go(k_pre2<T, R>, blocks_for(L.n), kThreads, 0, L, r, rsum);
         } else {
             go(k_pre2<T, T>, blocks_for(L.n), kThreads, 0, L, L.b, lsum_.p + l);
         }
@@ -811,12 +859,12 @@ void DeviceSolver::enqueue_vcycle_epi(const double* r, const double* rsum, doubl
     const size_t tsm = tail_smem_[std::is_same<T, double>::value ? 0 : 1];
     if (tsm > 0) {
         // the tail's levels staged in shared memory (tail_smem.cuh)
-        go(k_tail_smem<T, double>, 1, kTailThreads, tsm, Vdev, t, nl, t == 0 ? r : nullptr, coarse_inv_.p, coarse_n_,
+        go(k_tail_smem<T, R>, 1, kTailThreads, tsm, Vdev, t, nl, t == 0 ? r : nullptr, coarse_inv_.p, coarse_n_,
            t == 0 && V[0].singular ? mean_out : nullptr);
         ++launches_;
     } else {
     const Launch gt{stream_, pdl_, tail_ctas_};
-    gt(k_tail<T, double>, tail_ctas_, kTailThreads, 0, Vdev, t, nl, t == 0 ? r : nullptr, coarse_inv_.p, coarse_n_,
+    gt(k_tail<T, R>, tail_ctas_, kTailThreads, 0, Vdev, t, nl, t == 0 ? r : nullptr, coarse_inv_.p, coarse_n_,
                                                          t == 0 && V[0].singular ? mean_out : nullptr);
     ++launches_;
     }
@@ -929,46 +977,50 @@ void DeviceSolver::enqueue_cg_body(int precision, cudaGraphConditionalHandle han
     CgState* s = reinterpret_cast<CgState*>(cgs_.p);
     double* mean = lsum_.p + nl;
     const LevelView<double>& A = vd_[0];
-    double* const pa = p_.p;  // the ping-pong pair of search directions
-    double* const pb = z_.p;
-    // p = z + beta p_old from the last V-cycle's output, Ap and alpha
-    auto dir_ap = [&](auto* xv) {
+    const DevLevel& L0 = levels_[0];
+    // xv: the V-cycle's finest-level output (z = xv - mean); r, the ping-pong
+    // pair (pa, pb) of search directions and ap in the storage type P
+    auto body = [&](auto* xv, auto* r, auto* pa, auto* pb, auto* ap) {
         using T = std::remove_pointer_t<decltype(xv)>;
+        using P = std::remove_pointer_t<decltype(r)>;
+        // z = M r and r'z (beta, or the start of a run)
+        if (std::is_same<P, double>::value && rz_foldable()) {
+            // r'z in the V-cycle's last kernel
+            const CgRz epi{r_.p, fpartial2_.p, s};
+            enqueue_vcycle_epi<T>(r_.p, &s->rsum, mean, epi);
+        } else {
+            enqueue_vcycle<T>((const P*)r, &s->rsum, mean);
+            go(k_cg_z<T, P>, fold_grid(k_cg_z<T, P>, kThreads, blocks_for((n + 3) / 4), kMaxGrid), kThreads, 0, n,
+               (const T*)xv, mean, (const P*)r, fpartial_.p, counters_.p + kCgZ, s);
+        }
+        // p = z + beta p_old, Ap and alpha = gamma / p'Ap
         if (sdev_[0].vec)
-            go(v_cg_dir_ap<T>, fold_grid(v_cg_dir_ap<T>, 256, (sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0, sd_[0], xv,
-               mean, pa, pb, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
+            go(v_cg_dir_ap<T, P>, fold_grid(v_cg_dir_ap<T, P>, 256, (sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0,
+               sd_[0], (const T*)xv, mean, pa, pb, ap, fpartial_.p, counters_.p + kCgAp, s);
         else if (sdev_[0].on)
             with_nxc(sd_[0], [&](auto nxc) {
                 constexpr int N = decltype(nxc)::value;
-                go(s_cg_dir_ap<T, N>, fold_grid(s_cg_dir_ap<T, N>, sd_[0].cpb, sd_[0].nblocks, kMaxGrid), sd_[0].cpb, 0,
-                   sd_[0], xv, mean, pa, pb, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
+                go(s_cg_dir_ap<T, P, N>, fold_grid(s_cg_dir_ap<T, P, N>, sd_[0].cpb, sd_[0].nblocks, kMaxGrid),
+                   sd_[0].cpb, 0, sd_[0], (const T*)xv, mean, pa, pb, ap, fpartial_.p, counters_.p + kCgAp, s);
             });
         else
-            go(k_cg_dir_ap<T>, fold_grid(k_cg_dir_ap<T>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, A, xv, mean, pa,
-               pb, ap_.p, fpartial_.p, counters_.p + kCgAp, s);
+            go(k_cg_dir_ap<T, P>, fold_grid(k_cg_dir_ap<T, P>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, A,
+               (const T*)xv, mean, pa, pb, ap, fpartial_.p, counters_.p + kCgAp, s);
+        // x, r, the callback and the loop condition
+        go(k_cg_update<P>, fold_grid(k_cg_update<P>, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, xw_.p, r, pa,
+           pb, (const P*)ap, L0.const_vol ? nullptr : A.vol, L0.vol0, fpartial_.p, fpartial2_.p,
+           counters_.p + kCgUpdate, s, handle, set_cond);
     };
-    // z = M r and r'z (beta, or the start of a run)
-    if (rz_foldable()) {
-        // r'z in the V-cycle's last kernel
-        const CgRz epi{r_.p, fpartial2_.p, s};
-        if (precision == 0) enqueue_vcycle_epi<double>(r_.p, &s->rsum, mean, epi);
-        else enqueue_vcycle_epi<float>(r_.p, &s->rsum, mean, epi);
-    } else if (precision == 0) {
-        enqueue_vcycle<double>(r_.p, &s->rsum, mean);
-        go(k_cg_z<double>, fold_grid(k_cg_z<double>, kThreads, blocks_for((n + 3) / 4), kMaxGrid), kThreads, 0, n,
-           vd_[0].x, mean, r_.p, fpartial_.p, counters_.p + kCgZ, s);
+    if (precision == 0) {
+        body(vd_[0].x, r_.p, p_.p, z_.p, ap_.p);
+    } else if (precision == 1) {
+        body(vf_[0].x, r_.p, p_.p, z_.p, ap_.p);
     } else {
-        enqueue_vcycle<float>(r_.p, &s->rsum, mean);
-        go(k_cg_z<float>, fold_grid(k_cg_z<float>, kThreads, blocks_for((n + 3) / 4), kMaxGrid), kThreads, 0, n,
-           vf_[0].x, mean, r_.p, fpartial_.p, counters_.p + kCgZ, s);
+        // the refinement solve's inner runs: FP32 r, directions and Ap
+        float* w = ir_.p;
+        const size_t n4 = ir_stride();
+        body(vf_[0].x, w, w + n4, w + 2 * n4, w + 3 * n4);
     }
-    // p = z + beta p_old, Ap and alpha; then x, r, the callback and the loop condition
-    if (precision == 0) dir_ap(vd_[0].x);
-    else dir_ap(vf_[0].x);
-    const DevLevel& L0 = levels_[0];
-    go(k_cg_update, fold_grid(k_cg_update, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, xw_.p, r_.p, pa, pb,
-       ap_.p, L0.const_vol ? nullptr : A.vol, L0.vol0, fpartial_.p, fpartial2_.p, counters_.p + kCgUpdate, s, handle,
-       set_cond);
     TPA_CUDA(cudaGetLastError());
 }
 
@@ -1010,7 +1062,7 @@ cudaGraphExec_t DeviceSolver::cg_graph(int precision) {
     cudaError_t ce = cudaStreamEndCapture(stream_, &captured);
     stream_ = saved;
     // + direction/Ap, update and (unless folded) z
-    graph_body_launches_[precision] = launches_ - saved_launches + (rz_foldable() ? 2 : 3);
+    graph_body_launches_[precision] = launches_ - saved_launches + (precision < 2 && rz_foldable() ? 2 : 3);
     launches_ = saved_launches;
     if (ce != cudaSuccess) {
         cudaGraphDestroy(g);
@@ -1028,10 +1080,22 @@ void DeviceSolver::cg_fused(int precision, double target, int itmax, int& niter,
     const int n = levels_[0].n;
     const Launch go{stream_, pdl_};
     CgState* s = reinterpret_cast<CgState*>(cgs_.p);
+    if (precision == 2) {
+        if (coop_grid_ > 0) throw Error(5, "the refinement solve runs the multi-launch V-cycle, not the cooperative one");
+        if (ir_.n != 4 * ir_stride()) {
+            destroy_graphs();  // a captured body holds the old addresses
+            ir_.alloc(4 * ir_stride());
+            TPA_CUDA(cudaMemsetAsync(ir_.p, 0, ir_.n * sizeof(float), stream_));
+        }
+    }
     cudaGraphExec_t exec = cg_graph(precision);
     // a run: the state, r = b - A x and sum(r); the loop bodies follow
     go(k_cg_set, 1, 1, 0, s, target, itmax);
-    if (sdev_[0].vec)
+    if (precision == 2)
+        // an inner run of the refinement solve starts from the true residual
+        go(k_ir_start, fold_grid(k_ir_start, kThreads, blocks_for(n), kMaxGrid), kThreads, 0, n, (const double*)r_.p,
+           ir_.p, fpartial_.p, counters_.p + kCgRes, s);
+    else if (sdev_[0].vec)
         go(v_cg_residual, fold_grid(v_cg_residual, 256, (sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0, sd_[0], b_.p, xw_.p, r_.p,
            fpartial_.p, counters_.p + kCgRes, s);
     else if (sdev_[0].on)
@@ -1228,8 +1292,8 @@ void DeviceSolver::upload_tiles(const Hierarchy& h) {
     TPA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
     size_t down_d = 0, up_d = 0;
     for (int l = 0; l < tail_first_ && l + 1 < nl; ++l) {
-        if (sdev_[size_t(l)].vec) {
-            tdev_[size_t(l)].vec = cfg.tiles >= 2;  // stencil tiles need no lists
+        if (sdev_[size_t(l)].vec) {  // stencil tiles need no lists
+            tdev_[size_t(l)].vec = cfg.tiles == 2 || (cfg.tiles == 3 && levels_[size_t(l)].n <= kStencilTileCells);
             continue;
         }
         if (sdev_[size_t(l)].on) continue;

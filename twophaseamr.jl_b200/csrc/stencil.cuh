@@ -241,9 +241,10 @@ __device__ __forceinline__ void s_apply_dot(const SView<T>& L, const T* x, T* y,
 }
 
 // s_apply_dot with the operand formed where it is read: ld(q) = x_q, and
-// keep(c, x_c) stores the operand of the CTA's own cells
-template <typename T, int NXC, typename Ld, typename Keep, typename Fold>
-__device__ __forceinline__ void s_apply_dot_ld(const SView<T>& L, Ld ld, Keep keep, T* y, double* partial,
+// keep(c, x_c) stores the operand of the CTA's own cells; y has the storage
+// type P of the product
+template <typename T, int NXC, typename Ld, typename Keep, typename P, typename Fold>
+__device__ __forceinline__ void s_apply_dot_ld(const SView<T>& L, Ld ld, Keep keep, P* y, double* partial,
                                                unsigned* counter, Fold fold) {
     double part = 0;
     for (int b = blockIdx.x; b < L.nblocks; b += gridDim.x) {
@@ -251,7 +252,7 @@ __device__ __forceinline__ void s_apply_dot_ld(const SView<T>& L, Ld ld, Keep ke
         const T v = s_apply<NXC>(L, b, i, j, c, ld);
         const T xc = ld(c);
         keep(c, xc);
-        y[c] = v;
+        y[c] = P(v);
         part += double(xc) * double(v);
     }
     if (publish_partial(part, partial, counter)) {

@@ -51,6 +51,10 @@ __device__ __forceinline__ void q_st(double* p, const Quad<double>& q) {
     reinterpret_cast<double2*>(p)[0] = make_double2(q.v[0], q.v[1]);
     reinterpret_cast<double2*>(p)[1] = make_double2(q.v[2], q.v[3]);
 }
+// FP64 values stored as FP32 (round to nearest)
+__device__ __forceinline__ void q_st(float* p, const Quad<double>& q) {
+    *reinterpret_cast<float4*>(p) = make_float4(float(q.v[0]), float(q.v[1]), float(q.v[2]), float(q.v[3]));
+}
 
 // Position of a thread's quad.
 struct QPos {
@@ -426,9 +430,12 @@ __device__ __forceinline__ void v_apply_dot(const SView<double>& L, const double
 
 // v_apply_dot with the operand formed where it is read: ld(c) is the quad of
 // the operand at cells c .. c+3, and the CTA's own quads are stored to `keep`
-template <typename Ld, typename Fold>
-__device__ __forceinline__ void v_apply_dot_ld(const SView<double>& L, Ld ld, double* keep, double* y,
-                                               double* partial, unsigned* counter, Fold fold) {
+// (P: the storage type of the operand and the product; FP32 storage takes an
+// operand that ld has already rounded to FP32, so the product is that of the
+// stored operand)
+template <typename P, typename Ld, typename Fold>
+__device__ __forceinline__ void v_apply_dot_ld(const SView<double>& L, Ld ld, P* keep, P* y, double* partial,
+                                               unsigned* counter, Fold fold) {
     const int groups = (L.nblocks + 3) / 4;
     double part = 0;
     TPA_Q_LOOP(groups) {

@@ -20,7 +20,10 @@ import numpy as np
 from . import _lib
 from .options import LinearSolverOptions, MultigridOptions
 
-_PRECISION = {"fp64": 0, "mixed": 1}
+# "fp64": FP64 V-cycle and Krylov vectors; "mixed": FP32 V-cycle, FP64 Krylov
+# vectors; "mixed_ir": FP32 V-cycle and Krylov vectors (r, p, Ap, z) in an FP64
+# iterative-refinement loop (FP64 iterate, true residual and inner products)
+_PRECISION = {"fp64": 0, "mixed": 1, "mixed_ir": 2}
 
 
 @dataclass
@@ -76,7 +79,7 @@ class EllipticSolver:
         popts = dict(preconditioner_options or {})
         precision = popts.pop("precision", "fp64")
         if precision not in _PRECISION:
-            raise ValueError("precision must be 'fp64' or 'mixed'")
+            raise ValueError("precision must be 'fp64', 'mixed' or 'mixed_ir'")
         if popts:
             raise ValueError(f"unsupported preconditioner_options: {sorted(popts)}")
         self.operator = operator
@@ -205,8 +208,9 @@ class EllipticSolver:
     def vcycle(self, r, precision=None):
         r = _lib.f64(r)
         z = np.empty_like(r)
+        # the refinement solve preconditions with the FP32 cycle
         self.ctx.call("tpa_vcycle", _lib.ptr(r, C.c_double), _lib.ptr(z, C.c_double),
-                      _PRECISION[precision or self.precision])
+                      min(_PRECISION[precision or self.precision], 1))
         return z
 
     def _stats_from(self, st):
