@@ -342,7 +342,9 @@ def main():
     ap.add_argument("--size", type=int, default=2048, help="cells per side of the uniform workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default device layout")
-    ap.add_argument("--profile", action="store_true", help="only W warm-up and K mixed solves (for ncu)")
+    ap.add_argument("--profile", action="store_true", help="only W warm-up and K solves (for ncu)")
+    ap.add_argument("--profile-precision", default="mixed", choices=["mixed", "fp64", "mixed_ir"],
+                    help="precision of the --profile solves")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -407,15 +409,16 @@ def main():
         return solver.solve_device(rhs_d.data_ptr(), x_d.data_ptr(), rtol=RTOL, precision=precision)
 
     if args.profile:
-        # profiling pass: W warm-up solves, then K mixed solves and nothing else
+        # profiling pass: W warm-up solves, then K solves and nothing else
+        prec = args.profile_precision
         for _ in range(args.warmup):
-            device_solve("mixed")
+            device_solve(prec)
         torch.cuda.synchronize()
         launches = 0
         for _ in range(args.steps):
-            launches += device_solve("mixed").kernel_launches
+            launches += device_solve(prec).kernel_launches
         torch.cuda.synchronize()
-        print(json.dumps({"profile": "droplet_amr mixed", "solves": args.steps, "kernel_launches": launches}))
+        print(json.dumps({"profile": f"{args.workload} {prec}", "solves": args.steps, "kernel_launches": launches}))
         return
 
     def timed(precision, steps):
