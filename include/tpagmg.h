@@ -139,6 +139,14 @@ tpa_status tpa_level_info(const tpa_context* ctx, int32_t level, double* smoothe
 tpa_status tpa_level_red_black(const tpa_context* ctx, int32_t level, uint8_t* colours, double* weight);
 /* Restricted face coefficients of level `level` (tree_coarsening.jl:538-555). */
 tpa_status tpa_level_face_coefficients(const tpa_context* ctx, int32_t level, double* kappa);
+/* The assembled operator of level `level`, the stiffness (A + A')/2 with any
+ * open-face conductances on its diagonal (operators/elliptic.jl:175-257), as
+ * CSR with sorted columns: *nnz receives the entry count; row_ptr (n + 1),
+ * col and val (*nnz each) may be NULL to ask for the count first.  Host
+ * set-up data, for parity checks and for callers that assemble a larger
+ * system around the pressure operator (the CMDGFM system below). */
+tpa_status tpa_level_matrix(const tpa_context* ctx, int32_t level, int64_t* nnz, int64_t* row_ptr, int32_t* col,
+                            double* val);
 
 /* `_refresh_geometric_multigrid!` (geometric_preconditioner.jl:483-594): new
  * fine face coefficients on the fixed topology; refreshes every level.  Once
@@ -399,6 +407,72 @@ tpa_status tpa_project(tpa_context* ctx, double* u_interior, double* u_boundary,
                        const tpa_projection_options* options, tpa_stats* stats);
 tpa_status tpa_project_device(tpa_context* ctx, double* u_interior, double* u_boundary, double* pressure,
                               const tpa_projection_options* options, tpa_stats* stats);
+
+/* The assembled CMDGFM two-velocity projection system
+ * (`_assemble_cmdgfm_system!`, src/two_phase/projection/cmdgfm_projection.jl:
+ * 1484-1592): n = np + nx unknowns, the pressure increments of the retained
+ * cells of the gauge partition (two_phase/projection/common.jl:89-112), then
+ * one jump per mixed face; [A B; C J], nonsymmetric.  Host arrays, 0-based;
+ * the pressure unknowns index the context's mesh cells, whose operator (set by
+ * tpa_set_operator and tpa_build_hierarchy) is the pressure block's. */
+typedef struct {
+    int64_t np, nx;
+    const int64_t* row_ptr;          /* n + 1 */
+    const int32_t* col;              /* row_ptr[n] entries, sorted within a row */
+    const double* val;
+    const double* rhs;               /* n */
+    const int32_t* pressure_cell;    /* np: the cell of each pressure unknown */
+    const int32_t* pressure_anchor;  /* np: the anchor cell of its component */
+    const double* defect_weight;     /* n: a row's defect is weight |residual| (dt^2 / V for
+                                        pressure rows, dt^2 / h for jump rows: `_cmdgfm_residual_defects`) */
+    int64_t na;                      /* omitted gauge (anchor) rows, may be 0 */
+    const int64_t* extra_row_ptr;    /* na + 1, over the same n unknowns */
+    const int32_t* extra_col;
+    const double* extra_val;
+    const double* extra_rhs;         /* na */
+    const double* extra_weight;      /* na (`_cmdgfm_anchor_residual_defect`) */
+    const double* row_scale;         /* n: D_r of `_cmdgfm_krylov_scaling!` */
+    const double* col_scale;         /* n: D_c */
+    double drop_tolerance;           /* incomplete-LU drop tolerance (reference default 1e-3) */
+    double tolerance;                /* defect tolerance (reference default sqrt(eps)) */
+    int32_t max_iterations;          /* BiCGSTAB iteration budget (reference default 500) */
+    int32_t precision;               /* V-cycle: 0 FP64, 1 FP32 */
+} tpa_cmdgfm_system;
+
+typedef struct {
+    int32_t converged;      /* every defect at or below the tolerance */
+    int32_t iterations;     /* BiCGSTAB iterations of all runs */
+    int32_t attempts;       /* BiCGSTAB runs */
+    int32_t kernel_launches;
+    double initial_residual, final_residual;  /* ||rhs||, ||rhs - M x|| */
+    double pressure_defect, jump_defect, anchor_defect;
+    double setup_ms;        /* host: blocks, Schur complement, incomplete LU, schedules */
+    double device_ms;       /* CUDA-event time of the device solve, copies included */
+    int64_t factor_entries; /* entries of L and U */
+    int32_t lower_levels, upper_levels;  /* depth of the triangular solves */
+} tpa_cmdgfm_stats;
+
+/* The linear solve of the CMDGFM projection (`_project_cmdgfm_assembled!`,
+ * cmdgfm_projection.jl:2201-2291, without its warm start): residual
+ * replacement around BiCGSTAB (Krylov.jl 0.10 `bicgstab!`) on the scaled
+ * system D_r M D_c, preconditioned by the block-lower preconditioner of
+ * cmdgfm_projection.jl:374-441 -- one V-cycle of the context's pressure
+ * hierarchy on the reduced pressure block, then the incomplete LU
+ * (IncompleteLU.jl 0.2 `ilu(S; tau)`) of S = J - C D^-1 B
+ * (cmdgfm_cache.jl:550-610) on the jump block.  solution: n host doubles.
+ * The jump block is limited to 25,600 unknowns (its triangular solves keep
+ * the vector in one CTA's shared memory). */
+tpa_status tpa_cmdgfm_solve(tpa_context* ctx, const tpa_cmdgfm_system* system, double* solution,
+                            tpa_cmdgfm_stats* stats);
+
+/* The host set-up of tpa_cmdgfm_solve alone (no context, no GPU): the Schur
+ * complement S (nx x nx) and its incomplete LU, L strictly lower (unit
+ * diagonal implied) and U with its diagonal, all CSR with sorted columns.
+ * Pass NULL arrays to receive the entry counts (s_nnz, l_nnz, u_nnz) first.
+ * Parity checks. */
+tpa_status tpa_cmdgfm_factor(const tpa_cmdgfm_system* system, int64_t* s_nnz, int64_t* s_ptr, int32_t* s_col,
+                             double* s_val, int64_t* l_nnz, int64_t* l_ptr, int32_t* l_col, double* l_val,
+                             int64_t* u_nnz, int64_t* u_ptr, int32_t* u_col, double* u_val);
 
 #ifdef __cplusplus
 }

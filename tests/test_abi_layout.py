@@ -23,6 +23,13 @@ STRUCTS = {
                         "persistent", "tiles", "ms_per_vcycle"],
     "tpa_projection_options": ["dt", "tolerance", "reference_dt", "inherited_divergence", "max_cycles",
                                "compatibility", "precision", "prepared"],
+    "tpa_cmdgfm_system": ["np", "nx", "row_ptr", "col", "val", "rhs", "pressure_cell", "pressure_anchor",
+                          "defect_weight", "na", "extra_row_ptr", "extra_col", "extra_val", "extra_rhs",
+                          "extra_weight", "row_scale", "col_scale", "drop_tolerance", "tolerance",
+                          "max_iterations", "precision"],
+    "tpa_cmdgfm_stats": ["converged", "iterations", "attempts", "kernel_launches", "initial_residual",
+                         "final_residual", "pressure_defect", "jump_defect", "anchor_defect", "setup_ms",
+                         "device_ms", "factor_entries", "lower_levels", "upper_levels"],
 }
 
 
@@ -55,7 +62,8 @@ def test_ctypes_structs_match_header(c_layout):
     from tpagmg import _lib
     from tpagmg.projection import ProjectionOptions
     for s, cls in (("tpa_stats", _lib.StatsC), ("tpa_multigrid_options", _lib.MultigridOptionsC),
-                   ("tpa_tune_config", _lib.TuneC), ("tpa_projection_options", ProjectionOptions)):
+                   ("tpa_tune_config", _lib.TuneC), ("tpa_projection_options", ProjectionOptions),
+                   ("tpa_cmdgfm_system", _lib.CmdgfmSystemC), ("tpa_cmdgfm_stats", _lib.CmdgfmStatsC)):
         import ctypes
         assert ctypes.sizeof(cls) == c_layout[(s, "size")], s
         assert [f[0] for f in cls._fields_] == STRUCTS[s], s

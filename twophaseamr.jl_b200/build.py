@@ -16,8 +16,8 @@ OUT = HERE / "tpagmg" / "_lib"
 BUILD = HERE / "_build"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-HOST_SRC = ["mesh.cpp", "metric.cpp", "hierarchy.cpp", "structure.cpp", "tiles.cpp"]
-DEVICE_SRC = ["device.cu", "solve_fused.cu", "solve_fast.cu", "noalloc.cu", "adjoint.cu", "batch.cu", "autotune.cu", "refresh.cu", "projection.cu", "api.cpp"]
+HOST_SRC = ["mesh.cpp", "metric.cpp", "hierarchy.cpp", "structure.cpp", "tiles.cpp", "cmdgfm.cpp"]
+DEVICE_SRC = ["device.cu", "solve_fused.cu", "solve_fast.cu", "noalloc.cu", "adjoint.cu", "batch.cu", "autotune.cu", "refresh.cu", "projection.cu", "cmdgfm.cu", "api.cpp"]
 
 
 def _stale(target, deps):

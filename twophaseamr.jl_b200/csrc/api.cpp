@@ -12,6 +12,7 @@
 
 #include "../../include/tpagmg.h"
 #include "batch.hpp"
+#include "cmdgfm.cuh"
 #include "device.cuh"
 #include "host.hpp"
 
@@ -34,6 +35,7 @@ struct tpa_context {
     // coefficients (empty: extended from the interior ones)
     bool open[4] = {false, false, false, false};
     std::vector<double> bcoef;
+    std::unique_ptr<tpa::CmdgfmDevice> cmdgfm;  // vectors of the CMDGFM solve, kept between calls
 };
 
 namespace tpa {
@@ -513,6 +515,20 @@ tpa_status tpa_level_face_coefficients(const tpa_context* cctx, int32_t level, d
         ensure_host_fresh(ctx);
         const tpa::HostLevel& l = level_of(ctx, level);
         std::memcpy(kappa, l.op.kappa.data(), l.op.kappa.size() * sizeof(double));
+    });
+}
+
+tpa_status tpa_level_matrix(const tpa_context* cctx, int32_t level, int64_t* nnz, int64_t* row_ptr, int32_t* col,
+                            double* val) {
+    auto* ctx = const_cast<tpa_context*>(cctx);
+    return guard(ctx, [&] {
+        if (!nnz) throw tpa::Error(TPA_ERR_INVALID_ARG, "null output");
+        ensure_host_fresh(ctx);
+        const tpa::Csr& a = level_of(ctx, level).op.A;
+        *nnz = int64_t(a.col.size());
+        if (row_ptr) std::memcpy(row_ptr, a.ptr.data(), a.ptr.size() * sizeof(int64_t));
+        if (col) std::memcpy(col, a.col.data(), a.col.size() * sizeof(int32_t));
+        if (val) std::memcpy(val, a.val.data(), a.val.size() * sizeof(double));
     });
 }
 
@@ -1187,3 +1203,162 @@ tpa_status tpa_synchronize(tpa_context* ctx) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- CMDGFM
+
+namespace {
+
+// CSR rows from the C-ABI arrays, checked: row pointers from 0, nondecreasing,
+// columns in [0, ncol) and increasing within a row, finite values
+tpa::CsrRows csr_from(int64_t nrow, int64_t ncol, const int64_t* ptr, const int32_t* col, const double* val,
+                      const char* what) {
+    tpa::CsrRows m;
+    m.n = nrow;
+    if (nrow == 0) {
+        m.ptr.assign(1, 0);
+        return m;
+    }
+    if (!ptr || (ptr[nrow] > 0 && (!col || !val)))
+        throw tpa::Error(TPA_ERR_INVALID_ARG, std::string(what) + ": null array");
+    if (ptr[0] != 0) throw tpa::Error(TPA_ERR_INVALID_ARG, std::string(what) + ": row_ptr[0] must be 0");
+    m.ptr.assign(ptr, ptr + nrow + 1);
+    for (int64_t r = 0; r < nrow; ++r) {
+        if (ptr[r + 1] < ptr[r]) throw tpa::Error(TPA_ERR_INVALID_ARG, std::string(what) + ": decreasing row_ptr");
+        for (int64_t k = ptr[r]; k < ptr[r + 1]; ++k) {
+            if (col[k] < 0 || col[k] >= ncol)
+                throw tpa::Error(TPA_ERR_INVALID_ARG, std::string(what) + ": column out of range");
+            if (k > ptr[r] && col[k] <= col[k - 1])
+                throw tpa::Error(TPA_ERR_INVALID_ARG, std::string(what) + ": columns not increasing within a row");
+            if (!std::isfinite(val[k])) throw tpa::Error(TPA_ERR_NONFINITE, std::string(what) + ": non-finite entry");
+        }
+    }
+    m.col.assign(col, col + ptr[nrow]);
+    m.val.assign(val, val + ptr[nrow]);
+    return m;
+}
+
+template <typename T>
+std::vector<T> host_vector(const T* p, int64_t n, const char* what) {
+    if (n > 0 && !p) throw tpa::Error(TPA_ERR_INVALID_ARG, std::string("null ") + what);
+    return n > 0 ? std::vector<T>(p, p + n) : std::vector<T>();
+}
+
+// the system as the library takes it, every argument checked; ncells < 0
+// skips the cell-range check (no context)
+tpa::CmdgfmInput cmdgfm_input(const tpa_cmdgfm_system* sys, int64_t ncells) {
+    if (!sys) throw tpa::Error(TPA_ERR_INVALID_ARG, "null system");
+    if (sys->np < 0 || sys->nx < 0 || sys->na < 0) throw tpa::Error(TPA_ERR_INVALID_ARG, "negative size");
+    const int64_t n = sys->np + sys->nx;
+    if (n >= (int64_t(1) << 31)) throw tpa::Error(TPA_ERR_INVALID_ARG, "the system has 2^31 or more unknowns");
+    tpa::CmdgfmInput in;
+    in.np = sys->np;
+    in.m = csr_from(n, n, sys->row_ptr, sys->col, sys->val, "system");
+    in.rhs = host_vector(sys->rhs, n, "rhs");
+    in.cell = host_vector(sys->pressure_cell, sys->np, "pressure_cell");
+    in.anchor = host_vector(sys->pressure_anchor, sys->np, "pressure_anchor");
+    in.weight = host_vector(sys->defect_weight, n, "defect_weight");
+    in.extra = csr_from(sys->na, n, sys->extra_row_ptr, sys->extra_col, sys->extra_val, "anchor rows");
+    in.extra_rhs = host_vector(sys->extra_rhs, sys->na, "extra_rhs");
+    in.extra_weight = host_vector(sys->extra_weight, sys->na, "extra_weight");
+    in.row_scale = host_vector(sys->row_scale, n, "row_scale");
+    in.col_scale = host_vector(sys->col_scale, n, "col_scale");
+    for (int64_t i = 0; i < sys->np; ++i) {
+        const int32_t c = in.cell[size_t(i)], a = in.anchor[size_t(i)];
+        if (c < 0 || a < 0 || (ncells >= 0 && (c >= ncells || a >= ncells)))
+            throw tpa::Error(TPA_ERR_INVALID_ARG, "pressure cell or anchor out of the mesh");
+        if (c == a) throw tpa::Error(TPA_ERR_INVALID_ARG, "a retained cell is its own anchor");
+    }
+    for (double v : in.rhs)
+        if (!std::isfinite(v)) throw tpa::Error(TPA_ERR_NONFINITE, "right-hand side must be finite");
+    for (const auto* w : {&in.weight, &in.extra_weight})
+        for (double v : *w)
+            if (!(v >= 0 && std::isfinite(v))) throw tpa::Error(TPA_ERR_INVALID_ARG, "defect weights must be finite and nonnegative");
+    for (double v : in.extra_rhs)
+        if (!std::isfinite(v)) throw tpa::Error(TPA_ERR_NONFINITE, "anchor right-hand side must be finite");
+    for (const auto* w : {&in.row_scale, &in.col_scale})
+        for (double v : *w)
+            if (!(v > 0 && std::isfinite(v))) throw tpa::Error(TPA_ERR_INVALID_ARG, "scalings must be finite and positive");
+    if (!(sys->drop_tolerance >= 0 && std::isfinite(sys->drop_tolerance)))
+        throw tpa::Error(TPA_ERR_INVALID_ARG, "drop_tolerance must be nonnegative");
+    if (!(sys->tolerance > 0 && std::isfinite(sys->tolerance)))
+        throw tpa::Error(TPA_ERR_INVALID_ARG, "tolerance must be strictly positive");
+    if (sys->max_iterations <= 0) throw tpa::Error(TPA_ERR_INVALID_ARG, "max_iterations must be strictly positive");
+    if (sys->precision != 0 && sys->precision != 1) throw tpa::Error(TPA_ERR_INVALID_ARG, "bad precision");
+    in.tolerance = sys->tolerance;
+    in.max_iterations = sys->max_iterations;
+    in.precision = sys->precision;
+    return in;
+}
+
+void copy_csr(const tpa::CsrRows& m, int64_t* nnz, int64_t* ptr, int32_t* col, double* val) {
+    if (nnz) *nnz = int64_t(m.col.size());
+    if (ptr) std::memcpy(ptr, m.ptr.data(), m.ptr.size() * sizeof(int64_t));
+    if (col) std::memcpy(col, m.col.data(), m.col.size() * sizeof(int32_t));
+    if (val) std::memcpy(val, m.val.data(), m.val.size() * sizeof(double));
+}
+
+}  // namespace
+
+tpa_status tpa_cmdgfm_solve(tpa_context* ctx, const tpa_cmdgfm_system* system, double* solution,
+                            tpa_cmdgfm_stats* stats) {
+    return guard(ctx, [&] {
+        if (!solution && system && system->np + system->nx > 0)
+            throw tpa::Error(TPA_ERR_INVALID_ARG, "null solution");
+        ensure_device(ctx);
+        const tpa::CmdgfmInput in = cmdgfm_input(system, ctx->dev->ncells());
+        const auto t0 = std::chrono::steady_clock::now();
+        const tpa::CmdgfmFactor f = tpa::cmdgfm_factor(in.m, in.np, system->drop_tolerance);
+        const double setup_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (!ctx->cmdgfm) ctx->cmdgfm.reset(new tpa::CmdgfmDevice());
+        tpa::CmdgfmStats st;
+        ctx->cmdgfm->solve(*ctx->dev, in, f, solution, st);
+        if (stats) {
+            std::memset(stats, 0, sizeof(*stats));
+            stats->converged = st.converged ? 1 : 0;
+            stats->iterations = st.iterations;
+            stats->attempts = st.attempts;
+            stats->kernel_launches = st.launches;
+            stats->initial_residual = st.initial_residual;
+            stats->final_residual = st.final_residual;
+            stats->pressure_defect = st.pressure_defect;
+            stats->jump_defect = st.jump_defect;
+            stats->anchor_defect = st.anchor_defect;
+            stats->setup_ms = setup_ms;
+            stats->device_ms = st.device_ms;
+            stats->factor_entries = int64_t(f.lower.col.size() + f.upper.col.size() + f.pivot.size());
+            stats->lower_levels = f.nx ? f.lsched.levels() : 0;
+            stats->upper_levels = f.nx ? f.usched.levels() : 0;
+        }
+    });
+}
+
+tpa_status tpa_cmdgfm_factor(const tpa_cmdgfm_system* system, int64_t* s_nnz, int64_t* s_ptr, int32_t* s_col,
+                             double* s_val, int64_t* l_nnz, int64_t* l_ptr, int32_t* l_col, double* l_val,
+                             int64_t* u_nnz, int64_t* u_ptr, int32_t* u_col, double* u_val) {
+    try {
+        const tpa::CmdgfmInput in = cmdgfm_input(system, -1);
+        const tpa::CmdgfmFactor f = tpa::cmdgfm_factor(in.m, in.np, system->drop_tolerance);
+        copy_csr(f.schur, s_nnz, s_ptr, s_col, s_val);
+        copy_csr(f.lower, l_nnz, l_ptr, l_col, l_val);
+        // U with its pivot first in each row, the rest in column order
+        tpa::CsrRows u;
+        u.n = f.upper.n;
+        u.ptr.assign(1, 0);
+        for (int64_t r = 0; r < f.upper.n; ++r) {
+            u.col.push_back(int32_t(r));
+            u.val.push_back(f.pivot[size_t(r)]);
+            for (int64_t k = f.upper.ptr[size_t(r)]; k < f.upper.ptr[size_t(r) + 1]; ++k) {
+                u.col.push_back(f.upper.col[size_t(k)]);
+                u.val.push_back(f.upper.val[size_t(k)]);
+            }
+            u.ptr.push_back(int64_t(u.col.size()));
+        }
+        copy_csr(u, u_nnz, u_ptr, u_col, u_val);
+        return TPA_OK;
+    } catch (const tpa::Error& e) {
+        return e.code;
+    } catch (const std::exception&) {
+        return TPA_ERR_INVALID_ARG;
+    }
+}

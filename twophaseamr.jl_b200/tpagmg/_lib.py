@@ -51,6 +51,24 @@ class TuneC(C.Structure):
                 ("ms_per_vcycle", C.c_double)]
 
 
+class CmdgfmSystemC(C.Structure):
+    _fields_ = [("np", C.c_int64), ("nx", C.c_int64), ("row_ptr", C.c_void_p), ("col", C.c_void_p),
+                ("val", C.c_void_p), ("rhs", C.c_void_p), ("pressure_cell", C.c_void_p),
+                ("pressure_anchor", C.c_void_p), ("defect_weight", C.c_void_p), ("na", C.c_int64),
+                ("extra_row_ptr", C.c_void_p), ("extra_col", C.c_void_p), ("extra_val", C.c_void_p),
+                ("extra_rhs", C.c_void_p), ("extra_weight", C.c_void_p), ("row_scale", C.c_void_p),
+                ("col_scale", C.c_void_p), ("drop_tolerance", C.c_double), ("tolerance", C.c_double),
+                ("max_iterations", C.c_int32), ("precision", C.c_int32)]
+
+
+class CmdgfmStatsC(C.Structure):
+    _fields_ = [("converged", C.c_int32), ("iterations", C.c_int32), ("attempts", C.c_int32),
+                ("kernel_launches", C.c_int32), ("initial_residual", C.c_double), ("final_residual", C.c_double),
+                ("pressure_defect", C.c_double), ("jump_defect", C.c_double), ("anchor_defect", C.c_double),
+                ("setup_ms", C.c_double), ("device_ms", C.c_double), ("factor_entries", C.c_int64),
+                ("lower_levels", C.c_int32), ("upper_levels", C.c_int32)]
+
+
 P = C.c_void_p
 i32p = C.POINTER(C.c_int32)
 i64p = C.POINTER(C.c_int64)
@@ -122,6 +140,10 @@ SIGNATURES = {
     "tpa_divergence_device": (C.c_int32, [P, P, P, P]),
     "tpa_project": (C.c_int32, [P, f64p, f64p, f64p, P, C.POINTER(StatsC)]),
     "tpa_project_device": (C.c_int32, [P, P, P, P, P, C.POINTER(StatsC)]),
+    "tpa_level_matrix": (C.c_int32, [P, C.c_int32, i64p, i64p, i32p, f64p]),
+    "tpa_cmdgfm_solve": (C.c_int32, [P, C.POINTER(CmdgfmSystemC), f64p, C.POINTER(CmdgfmStatsC)]),
+    "tpa_cmdgfm_factor": (C.c_int32, [C.POINTER(CmdgfmSystemC), i64p, i64p, i32p, f64p, i64p, i64p, i32p, f64p,
+                                      i64p, i64p, i32p, f64p]),
 }
 
 _lib = None

@@ -116,6 +116,19 @@ class EllipticSolver:
         self.ctx.call("tpa_level_owners", int(level), _lib.ptr(out, C.c_int32))
         return out
 
+    def level_matrix(self, level=0):
+        """The assembled operator of a level as (row_ptr, col, val) CSR arrays
+        (int64, int32, float64) with sorted columns."""
+        nnz = C.c_int64()
+        self.ctx.call("tpa_level_matrix", int(level), C.byref(nnz), None, None, None)
+        n = self.level_sizes()[level]
+        row_ptr = np.empty(n + 1, dtype=np.int64)
+        col = np.empty(nnz.value, dtype=np.int32)
+        val = np.empty(nnz.value, dtype=np.float64)
+        self.ctx.call("tpa_level_matrix", int(level), C.byref(nnz), _lib.ptr(row_ptr, C.c_int64),
+                      _lib.ptr(col, C.c_int32), _lib.ptr(val, C.c_double))
+        return row_ptr, col, val
+
     def level_info(self, level):
         sw, tw, nc = C.c_double(), C.c_double(), C.c_int32()
         self.ctx.call("tpa_level_info", int(level), C.byref(sw), C.byref(tw), C.byref(nc))
