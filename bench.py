@@ -327,6 +327,68 @@ def batch_main(args):
         dist.destroy_process_group()
 
 
+def cmdgfm_measure(level, steps, warmup, profile=False, cpu=True):
+    """The CMDGFM two-block solve (tpa_cmdgfm_solve) on the synthetic
+    capillary-wave system of `level` refinement levels: median wall and device
+    time of `steps` solves after `warmup`, with the FP32 V-cycle in the
+    pressure block; beside it, the oracle's restatement (numpy/SciPy, one
+    thread) on the same system when `cpu`."""
+    import time as _t
+    from tpagmg import BlockTreeMesh, EllipticSolver, PoissonOperator
+    from tpagmg import workloads as W
+    from tpagmg.cmdgfm import solve_cmdgfm
+    from tpagmg.operator import mixture_density
+    spec = W.capillary_wave_spec(level)
+    m = BlockTreeMesh(**spec)
+    fr = W.wave_fractions(m)
+    kappa = 1.0 / mixture_density(m, fr, (1.0, 1e-3))
+    s = EllipticSolver(PoissonOperator(m, kappa))
+    system, exact = W.cmdgfm_system(m, s.level_matrix(0), kappa, fr)
+    for _ in range(warmup):
+        solve_cmdgfm(s, system, precision="mixed")
+    wall, dev, st, x = [], [], None, None
+    for _ in range(steps):
+        t0 = _t.perf_counter()
+        x, st = solve_cmdgfm(s, system, precision="mixed")
+        wall.append((_t.perf_counter() - t0) * 1e3)
+        dev.append(st.device_ms)
+    if profile:
+        return {"profile": f"cmdgfm capillary_wave L{level}", "solves": steps}
+    npr = system.np_
+    err = max(float(np.max(np.abs(x[:npr] - exact[:npr])) / np.max(np.abs(exact[:npr]))),
+              float(np.max(np.abs(x[npr:] - exact[npr:])) / np.max(np.abs(exact[npr:]))))
+    out = {"workload": f"capillary_wave L{level} (examples/07_capillary_wave mesh, {m.ncells} cells), "
+                       f"synthetic CMDGFM system: {system.np_} pressures + {system.nx} jumps",
+           "iterations": st.iterations, "converged": st.converged,
+           "wall_ms": float(np.median(wall)), "device_ms": float(np.median(dev)), "setup_ms": st.setup_ms,
+           "kernel_launches": st.kernel_launches, "factor_levels": [st.lower_levels, st.upper_levels],
+           "error_vs_exact": err,
+           "what": "tpa_cmdgfm_solve: residual replacement around BiCGSTAB with the FP32 GMG V-cycle on the reduced "
+                   "pressure block and the Crout ILU of J - C D^-1 B on the jump block; host arrays in and out"}
+    if cpu:
+        import scipy.sparse as sp
+        from oracle import cmdgfm as O  # the checker, timed as the CPU port
+        from oracle.mesh import block_tree_mesh
+        from oracle.multigrid import MultigridOptions, TreeGeometricMultigrid
+        from oracle.operator import PoissonOperator as OOp
+        M = sp.csr_matrix((system.val, system.col, system.row_ptr), shape=(system.n, system.n))
+        E = sp.csr_matrix((system.extra_val, system.extra_col, system.extra_row_ptr), shape=(1, system.n))
+        osys = O.CMDGFMSystem(matrix=M, rhs=system.rhs, np_=npr, pressure_cell=system.pressure_cell,
+                              pressure_anchor=system.pressure_anchor, defect_weight=system.defect_weight, extra=E,
+                              extra_rhs=system.extra_rhs, extra_weight=system.extra_weight,
+                              row_scale=system.row_scale, col_scale=system.col_scale)
+        mg = TreeGeometricMultigrid(OOp(block_tree_mesh(**spec), kappa), MultigridOptions())
+        times = []
+        for _ in range(3):
+            t0 = _t.perf_counter()
+            _, ost = O.solve(osys, mg)
+            times.append((_t.perf_counter() - t0) * 1e3)
+        out["cpu_port"] = {"ms": float(np.median(times)), "iterations": ost.iterations, "cores": 1,
+                           "kind": "port", "sample": "median of 3 solves of the same system by the oracle "
+                                                     "(numpy/SciPy restatement, hierarchy built once)"}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -334,7 +396,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--levels", type=int, default=4)
-    ap.add_argument("--workload", default="droplet_amr", choices=["droplet_amr", "uniform_2048", "batch"])
+    ap.add_argument("--workload", default="droplet_amr", choices=["droplet_amr", "uniform_2048", "batch", "cmdgfm"])
+    ap.add_argument("--cmdgfm-level", type=int, default=6, help="refinement levels of the capillary-wave CMDGFM system")
     ap.add_argument("--batch", type=int, default=256, help="problems of the batch workload")
     ap.add_argument("--workers", type=int, default=32, help="host threads of the per-problem-stream batch")
     ap.add_argument("--batch-mode", default="merged", choices=["merged", "streams"],
@@ -350,6 +413,17 @@ def main():
         return reference_arm(args)
     if args.workload == "batch":
         return batch_main(args)
+    if args.workload == "cmdgfm":
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        res = cmdgfm_measure(args.cmdgfm_level, args.steps, args.warmup, profile=args.profile,
+                             cpu=not args.no_cpu_baseline)
+        if not args.profile:
+            res = {"metric": f"CMDGFM two-block solve time (capillary wave L{args.cmdgfm_level})",
+                   "value": res["wall_ms"], "unit": "ms", "higher_is_better": False, "n_gpus": 1,
+                   "steps": args.steps, "warmup": args.warmup, **res}
+        print(json.dumps(res), flush=True)
+        return
 
     import ctypes as C
     import torch
@@ -609,6 +683,11 @@ def main():
                              "(all fields on the device; dt 1e-3, tolerance sqrt(eps))"}
         solver.refresh(kappa)
 
+    # the CMDGFM two-block solve on the capillary wave (not timed with the solves above)
+    cmdgfm = None
+    if args.workload == "droplet_amr" and rank == 0:
+        cmdgfm = cmdgfm_measure(args.cmdgfm_level, args.steps, args.warmup, cpu=world == 1 and not args.no_cpu_baseline)
+
     cpu, oracle_err = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "droplet_amr":
         # the C/OpenMP restatement on this host's cores: the same measurement as
@@ -678,6 +757,7 @@ def main():
         "refresh": refresh,
         "two_phase_step": two_phase,
         "red_black_smoother": red_black,
+        "cmdgfm": cmdgfm,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -450,6 +450,8 @@ typedef struct {
     double device_ms;       /* CUDA-event time of the device solve, copies included */
     int64_t factor_entries; /* entries of L and U */
     int32_t lower_levels, upper_levels;  /* depth of the triangular solves */
+    int64_t inverse_entries; /* entries of L^-1 and U^-1 when the jump block is applied through
+                                them (two parallel products), 0 when the factors are walked row by row */
 } tpa_cmdgfm_stats;
 
 /* The linear solve of the CMDGFM projection (`_project_cmdgfm_assembled!`,

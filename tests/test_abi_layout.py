@@ -29,7 +29,7 @@ STRUCTS = {
                           "max_iterations", "precision"],
     "tpa_cmdgfm_stats": ["converged", "iterations", "attempts", "kernel_launches", "initial_residual",
                          "final_residual", "pressure_defect", "jump_defect", "anchor_defect", "setup_ms",
-                         "device_ms", "factor_entries", "lower_levels", "upper_levels"],
+                         "device_ms", "factor_entries", "lower_levels", "upper_levels", "inverse_entries"],
 }
 
 

@@ -68,6 +68,18 @@ def test_cmdgfm_matches_oracle(level, precision):
           f"factor levels {st.lower_levels}/{st.upper_levels}")
 
 
+def test_jump_block_paths_agree(monkeypatch):
+    """The jump block through the factors' inverses (the default here) and
+    by the row walk of the factors give the same iterates to rounding."""
+    s, system, exact, xo, so = case(4)
+    x_inv, st_inv = solve_cmdgfm(s, system)
+    monkeypatch.setenv("TPAGMG_CMDGFM_WALK", "1")
+    x_walk, st_walk = solve_cmdgfm(s, system)
+    assert st_inv.inverse_entries > 0 and st_walk.inverse_entries == 0
+    assert st_inv.iterations == st_walk.iterations
+    assert np.max(np.abs(x_inv - x_walk)) <= 1e-9 * np.max(np.abs(x_walk))
+
+
 def test_cmdgfm_repeats_bit_for_bit():
     s, system, _, _, _ = case(4)
     x1, st1 = solve_cmdgfm(s, system)

@@ -1329,6 +1329,7 @@ tpa_status tpa_cmdgfm_solve(tpa_context* ctx, const tpa_cmdgfm_system* system, d
             stats->factor_entries = int64_t(f.lower.col.size() + f.upper.col.size() + f.pivot.size());
             stats->lower_levels = f.nx ? f.lsched.levels() : 0;
             stats->upper_levels = f.nx ? f.usched.levels() : 0;
+            stats->inverse_entries = st.inverse ? int64_t(f.linv.col.size() + f.uinv.col.size()) : 0;
         }
     });
 }

@@ -202,6 +202,93 @@ LevelSchedule backward_levels(const CsrRows& upper) {
     return s;
 }
 
+namespace {
+
+// column j of a triangular inverse into `out` (index, value), increasing index
+template <bool Upper>
+void inverse_column(const std::vector<std::vector<std::pair<int32_t, double>>>& cols, const std::vector<double>& pivot,
+                    int32_t j, std::vector<double>& acc, std::vector<char>& mark,
+                    std::vector<std::pair<int32_t, double>>& out) {
+    // min-heap (L: increasing index) or max-heap (U: decreasing) of touched rows
+    std::vector<int32_t> heap;
+    auto before = [](int32_t a, int32_t b) { return Upper ? a < b : a > b; };
+    auto touch = [&](int32_t i) {
+        if (!mark[size_t(i)]) {
+            mark[size_t(i)] = 1;
+            acc[size_t(i)] = 0.0;
+            heap.push_back(i);
+            std::push_heap(heap.begin(), heap.end(), before);
+        }
+    };
+    touch(j);
+    acc[size_t(j)] = 1.0;
+    double biggest = 0.0;
+    out.clear();
+    const double rel = std::ldexp(1.0, -60);
+    while (!heap.empty()) {
+        std::pop_heap(heap.begin(), heap.end(), before);
+        const int32_t i = heap.back();
+        heap.pop_back();
+        mark[size_t(i)] = 0;
+        double x = acc[size_t(i)];
+        if (Upper) x = x / pivot[size_t(i)];
+        biggest = std::max(biggest, std::fabs(x));
+        if (!(std::fabs(x) >= rel * biggest)) continue;  // dropped, not propagated
+        out.emplace_back(i, x);
+        // propagate to the rows that column i of the factor reaches
+        for (const auto& e : cols[size_t(i)]) {
+            touch(e.first);
+            acc[size_t(e.first)] -= e.second * x;
+        }
+    }
+    std::sort(out.begin(), out.end());
+}
+
+}  // namespace
+
+bool triangular_inverses(const CsrRows& lower, const CsrRows& upper, const std::vector<double>& pivot, int64_t cap,
+                         CsrRows& linv, CsrRows& uinv) {
+    const int64_t n = lower.n;
+    const size_t nn = static_cast<size_t>(n);
+    // the factors by columns
+    std::vector<std::vector<std::pair<int32_t, double>>> lcols(nn), ucols(nn);
+    for (int64_t r = 0; r < n; ++r) {
+        for (int64_t k = lower.ptr[size_t(r)]; k < lower.ptr[size_t(r) + 1]; ++k)
+            lcols[size_t(lower.col[size_t(k)])].emplace_back(int32_t(r), lower.val[size_t(k)]);
+        for (int64_t k = upper.ptr[size_t(r)]; k < upper.ptr[size_t(r) + 1]; ++k)
+            ucols[size_t(upper.col[size_t(k)])].emplace_back(int32_t(r), upper.val[size_t(k)]);
+    }
+    // columns of the inverses, gathered into rows afterwards
+    std::vector<std::vector<std::pair<int32_t, double>>> lrows(nn), urows(nn);
+    std::vector<double> acc(nn, 0.0);
+    std::vector<char> mark(nn, 0);
+    std::vector<std::pair<int32_t, double>> col;
+    int64_t total = 0;
+    for (int64_t j = 0; j < n; ++j) {
+        inverse_column<false>(lcols, pivot, int32_t(j), acc, mark, col);
+        total += int64_t(col.size());
+        for (const auto& e : col) lrows[size_t(e.first)].emplace_back(int32_t(j), e.second);
+        inverse_column<true>(ucols, pivot, int32_t(j), acc, mark, col);
+        total += int64_t(col.size());
+        for (const auto& e : col) urows[size_t(e.first)].emplace_back(int32_t(j), e.second);
+        if (total > cap) {
+            linv = CsrRows();
+            uinv = CsrRows();
+            return false;
+        }
+    }
+    for (auto* out : {&linv, &uinv}) {
+        *out = CsrRows();
+        out->n = n;
+        out->ptr.assign(1, 0);
+    }
+    for (int64_t r = 0; r < n; ++r) {
+        push_row(linv, lrows[size_t(r)]);  // columns increasing: j runs upwards
+        push_row(uinv, urows[size_t(r)]);
+    }
+    return true;
+}
+
 CmdgfmFactor cmdgfm_factor(const CsrRows& m, int64_t np, double tau) {
     CmdgfmFactor f;
     f.np = np;
@@ -221,6 +308,8 @@ CmdgfmFactor cmdgfm_factor(const CsrRows& m, int64_t np, double tau) {
     crout_ilu(f.schur, tau, f.lower, f.upper, f.pivot);
     f.lsched = forward_levels(f.lower);
     f.usched = backward_levels(f.upper);
+    // the inverses, when they stay below 64 entries a row on average
+    triangular_inverses(f.lower, f.upper, f.pivot, 64 * f.nx + 1024, f.linv, f.uinv);
     return f;
 }
 

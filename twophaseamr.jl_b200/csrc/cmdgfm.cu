@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "cmdgfm.cuh"
@@ -88,89 +89,200 @@ __global__ void k_cm_gather(int64_t np, const double* __restrict__ z, const int3
     }
 }
 
-// jr_f = src_(np+f) / rows_(np+f) - sum_c C[f,c] zp_c
-__global__ void k_cm_jump_rhs(int64_t nx, int64_t np, const double* __restrict__ src, const double* __restrict__ rows,
-                              const int64_t* __restrict__ cptr, const int32_t* __restrict__ ccol,
-                              const double* __restrict__ cval, const double* __restrict__ zp,
-                              double* __restrict__ jr) {
-    CM_LOOP(f, nx) {
-        double acc = 0;
-        for (int64_t e = cptr[f]; e < cptr[f + 1]; ++e) acc += cval[e] * zp[ccol[e]];
-        jr[f] = src[np + f] / rows[np + f] - acc;
+// One factor of the jump block laid out for its triangular solve: position i
+// holds row rows[i], its entries (col, val)[ptr[i] .. ptr[i+1]) in column
+// order and, for U, the reciprocal of its pivot inv[i].  `seq`: the positions
+// are the rows in solve order (increasing for L, decreasing for U) and one
+// thread walks them; otherwise the rows of level v are positions lev[v] ..
+// lev[v+1], independent of each other, and the CTA takes each level between
+// barriers.  A schedule whose levels hold few rows each -- the chains along
+// the interface -- runs faster on one thread than with a barrier per level.
+
+// copy a factor's arrays into shared memory at `at`; returns the view of the
+// copy and advances `at` (8-byte aligned: doubles first)
+template <bool Upper>
+__device__ TriView stage(const TriView& g, int nx, char*& at) {
+    TriView t = g;
+    double* val = reinterpret_cast<double*>(at);
+    double* inv = val + g.nnz;
+    int32_t* lev = reinterpret_cast<int32_t*>(inv + (Upper ? nx : 0));
+    int32_t* rows = lev + g.nlev + 1;
+    int32_t* ptr = rows + nx;
+    int32_t* col = ptr + nx + 1;
+    for (int e = threadIdx.x; e < g.nnz; e += blockDim.x) {
+        val[e] = g.val[e];
+        col[e] = g.col[e];
+    }
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        rows[i] = g.rows[i];
+        if (Upper) inv[i] = g.inv[i];
+    }
+    for (int i = threadIdx.x; i <= nx; i += blockDim.x) ptr[i] = g.ptr[i];
+    for (int i = threadIdx.x; i <= g.nlev; i += blockDim.x) lev[i] = g.lev[i];
+    t.val = val;
+    t.inv = inv;
+    t.lev = lev;
+    t.rows = rows;
+    t.ptr = ptr;
+    t.col = col;
+    at = reinterpret_cast<char*>(col + g.nnz);
+    at += (8 - (reinterpret_cast<size_t>(at) & 7)) & 7;
+    return t;
+}
+
+// The rows in solve order on one thread.  The next row's index, extent and
+// first kPre entries are loaded into registers while the current row is
+// summed, and the value just computed stays in a register for the next row,
+// which in a chain along the interface usually needs it: the critical path
+// per row is then one multiply-add and the reads of older values.
+template <bool Upper>
+__device__ __forceinline__ void walk_rows(double* __restrict__ y, const double* __restrict__ val,
+                                          const double* __restrict__ inv, const int32_t* __restrict__ rows,
+                                          const int32_t* __restrict__ ptr, const int32_t* __restrict__ col, int nx) {
+    constexpr int kPre = 4;
+    if (nx <= 0) return;
+    int k = rows[0], e0 = ptr[0], e1 = ptr[1];
+    int c[kPre];
+    double v[kPre];
+    for (int q = 0; q < kPre; ++q) {
+        c[q] = e0 + q < e1 ? col[e0 + q] : 0;
+        v[q] = e0 + q < e1 ? val[e0 + q] : 0.0;
+    }
+    double w = Upper ? inv[0] : 1.0;
+    int klast = -1;
+    double ylast = 0.0;
+    for (int i = 0; i < nx; ++i) {
+        const bool more = i + 1 < nx;
+        const int nk = more ? rows[i + 1] : 0;
+        const int ne1 = more ? ptr[i + 2] : e1;
+        const double nw = (Upper && more) ? inv[i + 1] : 1.0;
+        int nc[kPre];
+        double nv[kPre];
+        for (int q = 0; q < kPre; ++q) {
+            nc[q] = e1 + q < ne1 ? col[e1 + q] : 0;
+            nv[q] = e1 + q < ne1 ? val[e1 + q] : 0.0;
+        }
+        double acc = y[k];
+        for (int q = 0; q < kPre; ++q)
+            if (e0 + q < e1) {
+                double yc;
+                if (c[q] == klast) yc = ylast;
+                else yc = y[c[q]];
+                acc -= v[q] * yc;
+            }
+        for (int e = e0 + kPre; e < e1; ++e) acc -= val[e] * (col[e] == klast ? ylast : y[col[e]]);
+        const double yk = Upper ? acc * w : acc;
+        y[k] = yk;
+        klast = k;
+        ylast = yk;
+        k = nk;
+        e0 = e1;
+        e1 = ne1;
+        w = nw;
+        for (int q = 0; q < kPre; ++q) {
+            c[q] = nc[q];
+            v[q] = nv[q];
+        }
     }
 }
 
-// One triangular solve of the jump block's factor in one CTA, rows in the
-// order of a level schedule: position i holds row rows[i], its entries
-// (col, val)[ptr[i] .. ptr[i+1]) in column order and, for U, its pivot
-// piv[i]; the rows of level v are positions lev[v] .. lev[v+1] and depend
-// only on earlier levels.  The vector lives in shared memory and, when
-// `staged`, so does the whole schedule (it is read once per solve).  A thin
-// schedule (few rows per level) runs in the first warp alone, with a warp
-// barrier between levels instead of a CTA barrier.  Upper: x = U^-1 in,
-// written as dst[np + k] = x_k / cols[np + k]; else y = L^-1 in (unit
-// diagonal) into out.
 template <bool Upper>
-__global__ void __launch_bounds__(kIluThreads)
-    k_cm_trisolve(int nx, int nlev, const int32_t* __restrict__ glev, const int32_t* __restrict__ grows,
-                  const int32_t* __restrict__ gptr, const int32_t* __restrict__ gcol, const double* __restrict__ gval,
-                  const double* __restrict__ gpiv, int staged, int thin, const double* __restrict__ in,
-                  double* __restrict__ out, int64_t np, const double* __restrict__ cols) {
-    extern __shared__ double sm[];
-    double* y = sm;
-    const int nnz = gptr[nx];
-    const double* val = gval;
-    const double* piv = gpiv;
-    const int32_t *lev = glev, *rows = grows, *ptr = gptr, *col = gcol;
-    for (int f = threadIdx.x; f < nx; f += blockDim.x) y[f] = in[f];
-    if (staged) {
-        double* sval = y + nx;
-        double* spiv = sval + nnz;
-        int32_t* slev = reinterpret_cast<int32_t*>(spiv + (Upper ? nx : 0));
-        int32_t* srows = slev + nlev + 1;
-        int32_t* sptr = srows + nx;
-        int32_t* scol = sptr + nx + 1;
-        for (int e = threadIdx.x; e < nnz; e += blockDim.x) {
-            sval[e] = gval[e];
-            scol[e] = gcol[e];
-        }
-        for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-            srows[i] = grows[i];
-            if (Upper) spiv[i] = gpiv[i];
-        }
-        for (int i = threadIdx.x; i <= nx; i += blockDim.x) sptr[i] = gptr[i];
-        for (int i = threadIdx.x; i <= nlev; i += blockDim.x) slev[i] = glev[i];
-        val = sval;
-        piv = spiv;
-        lev = slev;
-        rows = srows;
-        ptr = sptr;
-        col = scol;
-    }
-    __syncthreads();
+__device__ void tri_solve(const TriView& t, double* __restrict__ y, int nx) {
     auto row = [&](int i) {
-        const int k = rows[i];
+        const int k = t.rows[i];
         double acc = y[k];
-        for (int e = ptr[i]; e < ptr[i + 1]; ++e) acc -= val[e] * y[col[e]];
-        y[k] = Upper ? acc / piv[i] : acc;
+        for (int e = t.ptr[i]; e < t.ptr[i + 1]; ++e) acc -= t.val[e] * y[t.col[e]];
+        y[k] = Upper ? acc * t.inv[i] : acc;
     };
-    if (thin) {
-        if (threadIdx.x < 32) {
-            for (int v = 0; v < nlev; ++v) {
-                for (int i = lev[v] + int(threadIdx.x); i < lev[v + 1]; i += 32) row(i);
-                __syncwarp();
-            }
-        }
+    if (t.seq) {
+        if (threadIdx.x == 0) walk_rows<Upper>(y, t.val, t.inv, t.rows, t.ptr, t.col, nx);
     } else {
-        for (int v = 0; v < nlev; ++v) {
-            for (int i = lev[v] + int(threadIdx.x); i < lev[v + 1]; i += blockDim.x) row(i);
+        for (int v = 0; v < t.nlev; ++v) {
+            for (int i = t.lev[v] + int(threadIdx.x); i < t.lev[v + 1]; i += blockDim.x) row(i);
             __syncthreads();
         }
     }
     __syncthreads();
+}
+
+// The jump block of the block preconditioner in one CTA: jr = src_xi / D_r -
+// C zp, y = (L U)^-1 jr, dst_xi = y / D_c.  The vector lives in shared
+// memory, and the factors too when `staged`.
+__global__ void __launch_bounds__(kIluThreads)
+    k_cm_jump_solve(int nx, int64_t np, const double* __restrict__ src, const double* __restrict__ rows,
+                    const int64_t* __restrict__ cptr, const int32_t* __restrict__ ccol,
+                    const double* __restrict__ cval, const double* __restrict__ zp, TriView L, TriView U,
+                    int staged, const double* __restrict__ cols, double* __restrict__ dst) {
+    extern __shared__ double sm[];
+    double* y = sm;
     for (int f = threadIdx.x; f < nx; f += blockDim.x) {
-        if (Upper) out[np + f] = y[f] / cols[np + f];
-        else out[f] = y[f];
+        double acc = 0;
+        for (int64_t e = cptr[f]; e < cptr[f + 1]; ++e) acc += cval[e] * zp[ccol[e]];
+        y[f] = src[np + f] / rows[np + f] - acc;
+    }
+    if (staged) {
+        char* at = reinterpret_cast<char*>(y + nx);
+        L = stage<false>(L, nx, at);
+        U = stage<true>(U, nx, at);
+    }
+    __syncthreads();
+    if (staged && L.seq && U.seq) {
+        // both factors walked on one thread, every array in shared memory
+        if (threadIdx.x == 0) {
+            const double* lval = reinterpret_cast<const double*>(y + nx);
+            const int32_t* llev = reinterpret_cast<const int32_t*>(lval + L.nnz);
+            const int32_t* lrows = llev + L.nlev + 1;
+            const int32_t* lptr = lrows + nx;
+            const int32_t* lcol = lptr + nx + 1;
+            walk_rows<false>(y, lval, nullptr, lrows, lptr, lcol, nx);
+            const char* at = reinterpret_cast<const char*>(lcol + L.nnz);
+            at += (8 - (reinterpret_cast<size_t>(at) & 7)) & 7;
+            const double* uval = reinterpret_cast<const double*>(at);
+            const double* uinv = uval + U.nnz;
+            const int32_t* ulev = reinterpret_cast<const int32_t*>(uinv + nx);
+            const int32_t* urows = ulev + U.nlev + 1;
+            const int32_t* uptr = urows + nx;
+            const int32_t* ucol = uptr + nx + 1;
+            walk_rows<true>(y, uval, uinv, urows, uptr, ucol, nx);
+        }
+        __syncthreads();
+    } else {
+        tri_solve<false>(L, y, nx);
+        tri_solve<true>(U, y, nx);
+    }
+    for (int f = threadIdx.x; f < nx; f += blockDim.x) dst[np + f] = y[f] / cols[np + f];
+}
+
+// The jump block through the factors' inverses (triangular_inverses): jr =
+// src_xi / D_r - C zp, y = L^-1 jr, x = U^-1 y, dst_xi = x / D_c, each a
+// row-parallel product; one CTA, jr and y in shared memory.
+__global__ void __launch_bounds__(kIluThreads)
+    k_cm_jump_inverse(int nx, int64_t np, const double* __restrict__ src, const double* __restrict__ rows,
+                      const int64_t* __restrict__ cptr, const int32_t* __restrict__ ccol,
+                      const double* __restrict__ cval, const double* __restrict__ zp,
+                      const int64_t* __restrict__ lptr, const int32_t* __restrict__ lcol,
+                      const double* __restrict__ lval, const int64_t* __restrict__ uptr,
+                      const int32_t* __restrict__ ucol, const double* __restrict__ uval,
+                      const double* __restrict__ cols, double* __restrict__ dst) {
+    extern __shared__ double sm[];
+    double* a = sm;
+    double* b = sm + nx;
+    for (int f = threadIdx.x; f < nx; f += blockDim.x) {
+        double acc = 0;
+        for (int64_t e = cptr[f]; e < cptr[f + 1]; ++e) acc += cval[e] * zp[ccol[e]];
+        a[f] = src[np + f] / rows[np + f] - acc;
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < nx; f += blockDim.x) {
+        double acc = 0;
+        for (int64_t e = lptr[f]; e < lptr[f + 1]; ++e) acc += lval[e] * a[lcol[e]];
+        b[f] = acc;
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < nx; f += blockDim.x) {
+        double acc = 0;
+        for (int64_t e = uptr[f]; e < uptr[f + 1]; ++e) acc += uval[e] * b[ucol[e]];
+        dst[np + f] = acc / cols[np + f];
     }
 }
 
@@ -481,15 +593,15 @@ void CmdgfmDevice::precondition(DeviceSolver& ds, const CmdgfmFactor& f, const d
         k_cm_gather<<<grid_of(np_), kT, 0, s>>>(np_, zfull_.p, cell_.p, anchor_.p, cols_.p, zp_.p, dst);
         ++launches_;
     }
-    if (nx_ > 0) {
-        k_cm_jump_rhs<<<grid_of(nx_), kT, 0, s>>>(nx_, np_, src, rows_.p, cptr_.p, ccol_.p, cval_.p, zp_.p, jr_.p);
-        k_cm_trisolve<false><<<1, kIluThreads, lsmem_, s>>>(int(nx_), llevels_, lsched_.p, lrows_.p, lptr_.p, lcol_.p,
-                                                            lval_.p, nullptr, lstaged_, lthin_, jr_.p, zp2_.p, 0,
-                                                            nullptr);
-        k_cm_trisolve<true><<<1, kIluThreads, usmem_, s>>>(int(nx_), ulevels_, usched_.p, urows_.p, uptr_.p, ucol_.p,
-                                                           uval_.p, piv_.p, ustaged_, uthin_, zp2_.p, dst, np_,
-                                                           cols_.p);
-        launches_ += 3;
+    if (nx_ > 0 && inverse_) {
+        k_cm_jump_inverse<<<1, kIluThreads, 2 * size_t(nx_) * sizeof(double), s>>>(
+            int(nx_), np_, src, rows_.p, cptr_.p, ccol_.p, cval_.p, zp_.p, liptr_.p, licol_.p, lival_.p, uiptr_.p,
+            uicol_.p, uival_.p, cols_.p, dst);
+        ++launches_;
+    } else if (nx_ > 0) {
+        k_cm_jump_solve<<<1, kIluThreads, jsmem_, s>>>(int(nx_), np_, src, rows_.p, cptr_.p, ccol_.p, cval_.p, zp_.p,
+                                                       lview_, uview_, jstaged_, cols_.p, dst);
+        ++launches_;
     }
     (void)f;
 }
@@ -598,50 +710,80 @@ void CmdgfmDevice::solve(DeviceSolver& ds, const CmdgfmInput& in, const CmdgfmFa
     ccol_.upload(f.coupling.col.data(), f.coupling.col.size(), s);
     cval_.upload(f.coupling.val.data(), f.coupling.val.size(), s);
     if (nx_ > 0) {
-        // each factor's rows in schedule order, entries contiguous per position
-        auto lay_out = [&](const CsrRows& m, const LevelSchedule& sc, const std::vector<double>* pv,
-                           DevBuf<int32_t>& dptr, DevBuf<int32_t>& dcol, DevBuf<double>& dval,
-                           DevBuf<int32_t>& dlev, DevBuf<int32_t>& drows, DevBuf<double>* dpiv, size_t& smem,
-                           int& staged, int& thin, int& levels) {
+        // each factor's rows in solve order, entries contiguous per position: the
+        // level schedule, or -- when its levels average fewer than 16 rows --
+        // plain row order for one thread
+        auto lay_out = [&](const CsrRows& m, const LevelSchedule& sc, bool upper, DevBuf<int32_t>& dptr,
+                           DevBuf<int32_t>& dcol, DevBuf<double>& dval, DevBuf<int32_t>& dlev,
+                           DevBuf<int32_t>& drows, DevBuf<double>* dinv, TriView& view, size_t& bytes) {
+            const int levels = sc.levels();
+            const bool seq = double(nx_) < 16.0 * double(std::max(levels, 1));
+            std::vector<int32_t> order, lev;
+            if (seq) {
+                for (int64_t i = 0; i < nx_; ++i) order.push_back(int32_t(upper ? nx_ - 1 - i : i));
+                lev = {0, int32_t(nx_)};
+            } else {
+                order = sc.rows;
+                lev = sc.level_ptr;
+            }
             std::vector<int32_t> ptr(1, 0), col;
-            std::vector<double> val, piv;
-            for (int32_t k : sc.rows) {
+            std::vector<double> val, inv;
+            for (int32_t k : order) {
                 for (int64_t e = m.ptr[size_t(k)]; e < m.ptr[size_t(k) + 1]; ++e) {
                     col.push_back(m.col[size_t(e)]);
                     val.push_back(m.val[size_t(e)]);
                 }
                 ptr.push_back(int32_t(col.size()));
-                if (pv) piv.push_back((*pv)[size_t(k)]);
+                if (upper) inv.push_back(1.0 / f.pivot[size_t(k)]);
             }
             dptr.upload(ptr.data(), ptr.size(), s);
             dcol.upload(col.data(), col.size(), s);
             dval.upload(val.data(), val.size(), s);
-            dlev.upload(sc.level_ptr.data(), sc.level_ptr.size(), s);
-            drows.upload(sc.rows.data(), sc.rows.size(), s);
-            if (dpiv) dpiv->upload(piv.data(), piv.size(), s);
-            levels = sc.levels();
-            thin = double(nx_) < 64.0 * double(std::max(levels, 1)) ? 1 : 0;
-            const size_t nnz = col.size();
-            const size_t full = size_t(nx_) * 8 + nnz * 8 + (pv ? size_t(nx_) * 8 : 0) +
-                                (size_t(levels) + 1 + size_t(nx_) + size_t(nx_) + 1 + nnz) * 4;
-            staged = full <= size_t(200) * 1024 ? 1 : 0;
-            smem = staged ? full : size_t(nx_) * 8;
+            dlev.upload(lev.data(), lev.size(), s);
+            drows.upload(order.data(), order.size(), s);
+            if (dinv) dinv->upload(inv.data(), inv.size(), s);
+            view.nlev = int(lev.size()) - 1;
+            view.nnz = int(col.size());
+            view.seq = seq ? 1 : 0;
+            view.lev = dlev.p;
+            view.rows = drows.p;
+            view.ptr = dptr.p;
+            view.col = dcol.p;
+            view.val = dval.p;
+            view.inv = dinv ? dinv->p : nullptr;
+            bytes = col.size() * 8 + (upper ? size_t(nx_) * 8 : 0) +
+                    (lev.size() + size_t(nx_) + size_t(nx_) + 1 + col.size()) * 4 + 8;
+            llevels_ = upper ? llevels_ : levels;
+            ulevels_ = upper ? levels : ulevels_;
         };
-        lay_out(f.lower, f.lsched, nullptr, lptr_, lcol_, lval_, lsched_, lrows_, nullptr, lsmem_, lstaged_, lthin_,
-                llevels_);
-        lay_out(f.upper, f.usched, &f.pivot, uptr_, ucol_, uval_, usched_, urows_, &piv_, usmem_, ustaged_, uthin_,
-                ulevels_);
-        TPA_CUDA(cudaFuncSetAttribute(k_cm_trisolve<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(std::max<size_t>(lsmem_, 1))));
-        TPA_CUDA(cudaFuncSetAttribute(k_cm_trisolve<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(std::max<size_t>(usmem_, 1))));
+        size_t lb = 0, ub = 0;
+        lay_out(f.lower, f.lsched, false, lptr_, lcol_, lval_, lsched_, lrows_, nullptr, lview_, lb);
+        lay_out(f.upper, f.usched, true, uptr_, ucol_, uval_, usched_, urows_, &piv_, uview_, ub);
+        const size_t full = size_t(nx_) * 8 + lb + ub;
+        jstaged_ = full <= size_t(200) * 1024 ? 1 : 0;
+        jsmem_ = jstaged_ ? full : size_t(nx_) * 8;
+        TPA_CUDA(cudaFuncSetAttribute(k_cm_jump_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(std::max<size_t>(jsmem_, 1))));
+        // the inverses, when the host formed them and two vectors fit in shared memory
+        // (TPAGMG_CMDGFM_WALK keeps the row walk, to compare the two paths)
+        inverse_ = !f.linv.ptr.empty() && 2 * size_t(nx_) * sizeof(double) <= size_t(200) * 1024 &&
+                   !std::getenv("TPAGMG_CMDGFM_WALK");
+        if (inverse_) {
+            liptr_.upload(f.linv.ptr.data(), f.linv.ptr.size(), s);
+            licol_.upload(f.linv.col.data(), f.linv.col.size(), s);
+            lival_.upload(f.linv.val.data(), f.linv.val.size(), s);
+            uiptr_.upload(f.uinv.ptr.data(), f.uinv.ptr.size(), s);
+            uicol_.upload(f.uinv.col.data(), f.uinv.col.size(), s);
+            uival_.upload(f.uinv.val.data(), f.uinv.val.size(), s);
+            TPA_CUDA(cudaFuncSetAttribute(k_cm_jump_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(2 * size_t(nx_) * sizeof(double))));
+        }
     }
     for (auto* b : {&sol_, &corr_, &x_, &r_, &c_, &p_, &v_, &s_, &t_, &y_, &z_}) b->alloc(size_t(std::max<int64_t>(n_, 1)));
     full_.alloc(size_t(std::max<int64_t>(ncells_, 1)));
     zfull_.alloc(size_t(std::max<int64_t>(ncells_, 1)));
     zp_.alloc(size_t(std::max<int64_t>(np_, 1)));
     jr_.alloc(size_t(std::max<int64_t>(nx_, 1)));
-    zp2_.alloc(size_t(std::max<int64_t>(nx_, 1)));
     partial_.alloc(4 * size_t(kG));
     state_.alloc(kStateSize);
     TPA_CUDA(cudaMemsetAsync(sol_.p, 0, sizeof(double) * size_t(n_), s));
@@ -730,6 +872,7 @@ void CmdgfmDevice::solve(DeviceSolver& ds, const CmdgfmInput& in, const CmdgfmFa
     cudaEventDestroy(e1);
     st.device_ms = ms;
     st.launches = launches_;
+    st.inverse = inverse_;
     TPA_CUDA(cudaGetLastError());
 }
 

@@ -36,6 +36,18 @@ struct CmdgfmStats {
     double pressure_defect = 0, jump_defect = 0, anchor_defect = 0;
     double device_ms = 0;
     int launches = 0;
+    bool inverse = false;  // the jump block went through the factors' inverses
+};
+
+// a triangular factor laid out for its solve on the device (cmdgfm.cu)
+struct TriView {
+    int nlev, nnz, seq;
+    const int32_t* lev;
+    const int32_t* rows;
+    const int32_t* ptr;
+    const int32_t* col;
+    const double* val;
+    const double* inv;
 };
 
 template <typename T>
@@ -83,10 +95,16 @@ private:
     DevBuf<int64_t> cptr_;
     DevBuf<int32_t> ccol_, lptr_, lcol_, uptr_, ucol_, lrows_, lsched_, urows_, usched_;
     DevBuf<double> cval_, lval_, uval_, piv_;
-    int llevels_ = 0, ulevels_ = 0, lstaged_ = 0, ustaged_ = 0, lthin_ = 0, uthin_ = 0;
-    size_t lsmem_ = 0, usmem_ = 0;
+    int llevels_ = 0, ulevels_ = 0, jstaged_ = 0;
+    size_t jsmem_ = 0;
+    TriView lview_{}, uview_{};
+    // the factors' inverses by rows (used when `inverse_`)
+    bool inverse_ = false;
+    DevBuf<int64_t> liptr_, uiptr_;
+    DevBuf<int32_t> licol_, uicol_;
+    DevBuf<double> lival_, uival_;
     // vectors
-    DevBuf<double> sol_, corr_, x_, r_, c_, p_, v_, s_, t_, y_, z_, full_, zfull_, zp_, jr_, zp2_, partial_;
+    DevBuf<double> sol_, corr_, x_, r_, c_, p_, v_, s_, t_, y_, z_, full_, zfull_, zp_, jr_, partial_;
     DevBuf<double> state_;
 };
 

@@ -38,7 +38,20 @@ struct CmdgfmFactor {
     std::vector<double> pivot;  // U's diagonal
     CsrRows coupling;  // C: jump rows over pressure columns, nx x np
     LevelSchedule lsched, usched;
+    // L^-1 and U^-1 by rows (empty when they outgrew the cap; the device then
+    // walks the factors row by row)
+    CsrRows linv, uinv;
 };
+
+// The inverses of the unit lower `lower` and of `upper` with its pivots, by
+// rows.  Column j of an inverse is the solution of L x = e_j (U x = e_j),
+// formed by propagating each entry along the factor's columns in solve order;
+// an entry smaller than 2^-60 of its column's largest is dropped and not
+// propagated, so applying the inverse gives the triangular solve to within
+// rounding.  Returns false, with both left empty, when together they would
+// exceed `cap` entries.
+bool triangular_inverses(const CsrRows& lower, const CsrRows& upper, const std::vector<double>& pivot, int64_t cap,
+                         CsrRows& linv, CsrRows& uinv);
 
 // S = J - C D^-1 B (two_phase/projection/cmdgfm_cache.jl:550-610): row f is
 // J's entries of row f in column order, then for each C entry (f, c) in

@@ -66,7 +66,7 @@ class CmdgfmStatsC(C.Structure):
                 ("kernel_launches", C.c_int32), ("initial_residual", C.c_double), ("final_residual", C.c_double),
                 ("pressure_defect", C.c_double), ("jump_defect", C.c_double), ("anchor_defect", C.c_double),
                 ("setup_ms", C.c_double), ("device_ms", C.c_double), ("factor_entries", C.c_int64),
-                ("lower_levels", C.c_int32), ("upper_levels", C.c_int32)]
+                ("lower_levels", C.c_int32), ("upper_levels", C.c_int32), ("inverse_entries", C.c_int64)]
 
 
 P = C.c_void_p

@@ -99,6 +99,7 @@ class CMDGFMStats:
     factor_entries: int
     lower_levels: int
     upper_levels: int
+    inverse_entries: int
 
 
 _PRECISION = {"fp64": 0, "mixed": 1}
@@ -117,7 +118,8 @@ def solve_cmdgfm(solver, system: CMDGFMSystem, precision="fp64"):
     del keep
     return x, CMDGFMStats(bool(st.converged), st.iterations, st.attempts, st.initial_residual, st.final_residual,
                           st.pressure_defect, st.jump_defect, st.anchor_defect, st.setup_ms, st.device_ms,
-                          st.kernel_launches, st.factor_entries, st.lower_levels, st.upper_levels)
+                          st.kernel_launches, st.factor_entries, st.lower_levels, st.upper_levels,
+                          st.inverse_entries)
 
 
 def cmdgfm_factor(system: CMDGFMSystem):
