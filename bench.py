@@ -343,6 +343,8 @@ def cmdgfm_measure(level, steps, warmup, profile=False, cpu=True):
     fr = W.wave_fractions(m)
     kappa = 1.0 / mixture_density(m, fr, (1.0, 1e-3))
     s = EllipticSolver(PoissonOperator(m, kappa))
+    if not profile:
+        s.autotune(precision="mixed", vcycles=20)  # the pressure block's V-cycle layout
     system, exact = W.cmdgfm_system(m, s.level_matrix(0), kappa, fr)
     for _ in range(warmup):
         solve_cmdgfm(s, system, precision="mixed")

@@ -58,10 +58,26 @@ __device__ __forceinline__ double nan_max(double a, double b) { return (a != a |
 
 // ---------------------------------------------------------------- preconditioner
 
-// full[cell_i] = src_i / rows_i (the reduced right-hand side scattered)
+// full[cell_i] = src_i / rows_i (the reduced right-hand side scattered); with
+// one component (anchor >= 0) the last block also writes full[anchor] = -(the
+// sum of the values), folded from per-block partials in block order
 __global__ void k_cm_scatter(int64_t np, const double* __restrict__ src, const double* __restrict__ rows,
-                             const int32_t* __restrict__ cell, double* __restrict__ full) {
-    CM_LOOP(i, np) full[cell[i]] = src[i] / rows[i];
+                             const int32_t* __restrict__ cell, double* __restrict__ full, int anchor,
+                             double* partial, unsigned* counter) {
+    double v = 0;
+    CM_LOOP(i, np) {
+        const double q = src[i] / rows[i];
+        full[cell[i]] = q;
+        v += q;
+    }
+    if (anchor < 0) return;
+    if (publish_partial(v, partial, counter)) {
+        const double t = fold_partials(partial, gridDim.x);
+        if (threadIdx.x == 0) {
+            full[anchor] = 0.0 - t;
+            *counter = 0;
+        }
+    }
 }
 
 // one block per anchor: full[anchor] = -(sum of its component's values)
@@ -584,9 +600,14 @@ void CmdgfmDevice::precondition(DeviceSolver& ds, const CmdgfmFactor& f, const d
                                 int precision, cudaStream_t s) {
     if (np_ > 0) {
         TPA_CUDA(cudaMemsetAsync(full_.p, 0, sizeof(double) * size_t(ncells_), s));
-        k_cm_scatter<<<grid_of(np_), kT, 0, s>>>(np_, src, rows_.p, cell_.p, full_.p);
-        k_cm_anchor<<<ngroups_, 1024, 0, s>>>(gptr_.p, gidx_.p, ganchor_.p, src, rows_.p, full_.p);
-        launches_ += 2;
+        // one component: the anchor's value folds in the scatter; several: one block each
+        k_cm_scatter<<<grid_of(np_), kT, 0, s>>>(np_, src, rows_.p, cell_.p, full_.p, ngroups_ == 1 ? anchor1_ : -1,
+                                                 partial_.p + 2 * kG, counter_.p);
+        ++launches_;
+        if (ngroups_ > 1) {
+            k_cm_anchor<<<ngroups_, 1024, 0, s>>>(gptr_.p, gidx_.p, ganchor_.p, src, rows_.p, full_.p);
+            ++launches_;
+        }
         const int before = ds.kernel_launches();
         ds.vcycle(full_.p, zfull_.p, precision);
         launches_ += ds.kernel_launches() - before;
@@ -702,6 +723,11 @@ void CmdgfmDevice::solve(DeviceSolver& ds, const CmdgfmInput& in, const CmdgfmFa
             const int g = int(std::lower_bound(anchors.begin(), anchors.end(), in.anchor[size_t(i)]) - anchors.begin());
             gidx[size_t(cur[size_t(g)]++)] = int32_t(i);
         }
+    }
+    anchor1_ = ngroups_ == 1 ? anchors[0] : -1;
+    if (!counter_.p) {
+        counter_.alloc(1);
+        TPA_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned), s));
     }
     gptr_.upload(gptr.data(), gptr.size(), s);
     gidx_.upload(gidx.data(), gidx.size(), s);

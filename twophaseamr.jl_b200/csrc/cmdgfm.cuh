@@ -90,7 +90,8 @@ private:
     DevBuf<int64_t> mptr_, eptr_;
     DevBuf<int32_t> mcol_, ecol_, cell_, anchor_, gptr_, gidx_, ganchor_;
     DevBuf<double> mval_, eval_, rhs_, weight_, erhs_, eweight_, rows_, cols_;
-    int ngroups_ = 0;
+    int ngroups_ = 0, anchor1_ = -1;
+    DevBuf<unsigned> counter_;  // fold counter of the scatter (reset by its last block)
     // jump block: C, and the factors in the order of their level schedules
     DevBuf<int64_t> cptr_;
     DevBuf<int32_t> ccol_, lptr_, lcol_, uptr_, ucol_, lrows_, lsched_, urows_, usched_;
