@@ -71,7 +71,8 @@ def test_ctypes_structs_match_header(c_layout):
             assert getattr(cls, f).offset == c_layout[(s, f)], (s, f)
 
 
-JULIA_SIZES = {"Int32": 4, "Float64": 8, "Ptr{Float64}": 8, "Ptr{Cvoid}": 8, "Int64": 8}
+JULIA_SIZES = {"Int32": 4, "Float64": 8, "Ptr{Float64}": 8, "Ptr{Cvoid}": 8, "Int64": 8, "Ptr{Int64}": 8,
+               "Ptr{Int32}": 8}
 
 
 def _julia_structs():
@@ -93,7 +94,8 @@ def test_julia_stub_matches_header(c_layout):
     size, the struct to its largest field) equal the header's."""
     julia = _julia_structs()
     for jname, cname in (("TpaStats", "tpa_stats"), ("TpaMultigridOptions", "tpa_multigrid_options"),
-                         ("TpaProjectionOptions", "tpa_projection_options")):
+                         ("TpaProjectionOptions", "tpa_projection_options"),
+                         ("TpaCmdgfmSystem", "tpa_cmdgfm_system"), ("TpaCmdgfmStats", "tpa_cmdgfm_stats")):
         fields = julia[jname]
         assert [f for f, _ in fields] == STRUCTS[cname], jname
         off, align = 0, 1
