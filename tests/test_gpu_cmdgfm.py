@@ -80,11 +80,16 @@ def test_jump_block_paths_agree(monkeypatch):
     assert np.max(np.abs(x_inv - x_walk)) <= 1e-9 * np.max(np.abs(x_walk))
 
 
-def test_cmdgfm_repeats_bit_for_bit():
+def test_cmdgfm_repeats_bit_for_bit(monkeypatch):
+    """A repeated solve, and the BiCGSTAB loop launched kernel by kernel
+    instead of as one captured graph, give the same bits."""
     s, system, _, _, _ = case(4)
     x1, st1 = solve_cmdgfm(s, system)
     x2, st2 = solve_cmdgfm(s, system)
     assert np.array_equal(x1, x2) and st1.iterations == st2.iterations
+    monkeypatch.setenv("TPAGMG_NO_GRAPH", "1")
+    x3, st3 = solve_cmdgfm(s, system)
+    assert np.array_equal(x1, x3) and st1.iterations == st3.iterations
 
 
 def test_cmdgfm_pressure_block_alone_and_bad_cells():

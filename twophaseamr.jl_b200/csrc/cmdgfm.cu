@@ -434,7 +434,8 @@ __global__ void k_cm_update2(int64_t n, const double* __restrict__ s, const doub
 }
 
 // next_rho, beta, rNorm and the stopping rules of the iteration
-__global__ void k_cm_rho(const double* p1, const double* p2, int count, double* st) {
+__global__ void k_cm_rho(const double* p1, const double* p2, int count, double* st,
+                         cudaGraphConditionalHandle handle, int set_cond) {
     const double cr = fold_partials(p1, count);
     const double rr = fold_partials(p2, count);
     if (threadIdx.x == 0) {
@@ -450,6 +451,7 @@ __global__ void k_cm_rho(const double* p1, const double* p2, int count, double* 
         const double a = st[kAlpha];
         if (a == 0.0 || a != a) flags |= kBreakdown;
         st[kFlags] = flags;
+        if (set_cond) cudaGraphSetConditional(handle, (flags & (kSolved | kTired | kBreakdown)) ? 0u : 1u);
     }
 }
 
@@ -627,11 +629,111 @@ void CmdgfmDevice::precondition(DeviceSolver& ds, const CmdgfmFactor& f, const d
     (void)f;
 }
 
+// One BiCGSTAB iteration (Krylov.jl 0.10 `bicgstab!` with the right
+// preconditioner N): y = N^-1 p, v = A y, alpha; s = r - alpha v, x += alpha y;
+// z = N^-1 s, t = A z, omega; x += omega z, r = s - omega t; next rho, beta,
+// rNorm and the stopping rules (which set the loop condition when `set_cond`);
+// p = r + beta (p - omega v).
+void CmdgfmDevice::enqueue_iteration(DeviceSolver& ds, const CmdgfmFactor& f, bool preconditioned, int precision,
+                                     cudaStream_t s, cudaGraphConditionalHandle handle, int set_cond) {
+    const int g = grid_of(n_);
+    double* p1 = partial_.p;
+    double* p2 = partial_.p + kG;
+    double* st = state_.p;
+    const double* y = p_.p;
+    if (preconditioned) {
+        precondition(ds, f, p_.p, y_.p, precision, s);
+        y = y_.p;
+    }
+    spmv(y, v_.p, 1, s);
+    k_cm_dot2<<<g, kT, 0, s>>>(n_, c_.p, v_.p, nullptr, nullptr, p1, nullptr);
+    k_cm_alpha<<<1, kT, 0, s>>>(p1, g, st);
+    k_cm_update1<<<g, kT, 0, s>>>(n_, r_.p, v_.p, y, s_.p, x_.p, st);
+    launches_ += 3;
+    const double* z = s_.p;
+    if (preconditioned) {
+        precondition(ds, f, s_.p, z_.p, precision, s);
+        z = z_.p;
+    }
+    spmv(z, t_.p, 1, s);
+    k_cm_dot2<<<g, kT, 0, s>>>(n_, t_.p, s_.p, t_.p, t_.p, p1, p2);
+    k_cm_omega<<<1, kT, 0, s>>>(p1, p2, g, st);
+    k_cm_update2<<<g, kT, 0, s>>>(n_, s_.p, t_.p, z, c_.p, x_.p, r_.p, st, p1, p2);
+    k_cm_rho<<<1, kT, 0, s>>>(p1, p2, g, st, handle, set_cond);
+    k_cm_pupdate<<<g, kT, 0, s>>>(n_, r_.p, v_.p, p_.p, st);
+    launches_ += 5;
+}
+
+// The iteration captured as the body of a graph WHILE node, kept while every
+// argument it captured is unchanged: the sizes, the jump-block layout, the
+// buffers and the pressure hierarchy's graph generation.
+cudaGraphExec_t CmdgfmDevice::loop_graph(DeviceSolver& ds, const CmdgfmFactor& f, bool preconditioned, int precision,
+                                         cudaStream_t s) {
+    std::vector<uintptr_t> key = {
+        uintptr_t(n_), uintptr_t(np_), uintptr_t(nx_), uintptr_t(ncells_), uintptr_t(ngroups_),
+        uintptr_t(int64_t(anchor1_)), uintptr_t(precision), uintptr_t(inverse_), uintptr_t(jstaged_),
+        uintptr_t(jsmem_), uintptr_t(ds.graph_generation()), uintptr_t(s)};
+    for (const void* q : {(const void*)mptr_.p, (const void*)mcol_.p, (const void*)mval_.p, (const void*)rows_.p,
+                          (const void*)cols_.p, (const void*)cell_.p, (const void*)anchor_.p, (const void*)gptr_.p,
+                          (const void*)gidx_.p, (const void*)ganchor_.p, (const void*)cptr_.p, (const void*)ccol_.p,
+                          (const void*)cval_.p, (const void*)liptr_.p, (const void*)licol_.p, (const void*)lival_.p,
+                          (const void*)uiptr_.p, (const void*)uicol_.p, (const void*)uival_.p, (const void*)x_.p,
+                          (const void*)r_.p, (const void*)c_.p, (const void*)p_.p, (const void*)v_.p,
+                          (const void*)s_.p, (const void*)t_.p, (const void*)y_.p, (const void*)z_.p,
+                          (const void*)full_.p, (const void*)zfull_.p, (const void*)zp_.p, (const void*)partial_.p,
+                          (const void*)state_.p, (const void*)counter_.p})
+        key.push_back(reinterpret_cast<uintptr_t>(q));
+    for (const TriView* v : {&lview_, &uview_}) {
+        const unsigned char* b = reinterpret_cast<const unsigned char*>(v);
+        for (size_t i = 0; i < sizeof(TriView); i += sizeof(uintptr_t)) {
+            uintptr_t w = 0;
+            std::memcpy(&w, b + i, std::min(sizeof(uintptr_t), sizeof(TriView) - i));
+            key.push_back(w);
+        }
+    }
+    const int slot = preconditioned ? 1 : 0;
+    if (exec_[slot] && key == key_[slot]) return exec_[slot];
+    if (exec_[slot]) cudaGraphExecDestroy(exec_[slot]);
+    exec_[slot] = nullptr;
+    cudaGraph_t graph;
+    TPA_CUDA(cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle handle;
+    TPA_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+    alignas(cudaGraphNodeParams) unsigned char cp_storage[sizeof(cudaGraphNodeParams)];
+    std::memset(cp_storage, 0, sizeof(cp_storage));
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_storage);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    TPA_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    const int before = launches_, ds_before = ds.kernel_launches();
+    TPA_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    enqueue_iteration(ds, f, preconditioned, precision, s, handle, 1);
+    cudaGraph_t captured;
+    const cudaError_t ce = cudaStreamEndCapture(s, &captured);
+    body_launches_[slot] = (launches_ - before);
+    launches_ = before;
+    ds.add_launches(ds_before - ds.kernel_launches());  // the capture launched nothing
+    if (ce != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        throw Error(2, std::string("graph capture failed: ") + cudaGetErrorString(ce));
+    }
+    cudaGraphExec_t exec;
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) throw Error(2, std::string("graph instantiation failed: ") + cudaGetErrorString(ie));
+    exec_[slot] = exec;
+    key_[slot] = key;
+    return exec;
+}
+
 int CmdgfmDevice::bicgstab(DeviceSolver& ds, const CmdgfmInput& in, const CmdgfmFactor& f, bool preconditioned,
                            double rtol, int itmax, cudaStream_t s) {
     const int g = grid_of(n_);
     double* p1 = partial_.p;
-    double* p2 = partial_.p + kG;
     double* st = state_.p;
     double hs[kStateSize];
     auto read = [&] {
@@ -644,31 +746,18 @@ int CmdgfmDevice::bicgstab(DeviceSolver& ds, const CmdgfmInput& in, const Cmdgfm
     launches_ += 2;
     read();
     if (int(hs[kFlags]) & (kZeroRhs | kZeroRho | kSolved | kTired)) return 0;
-    for (;;) {
-        const double* y = p_.p;
-        if (preconditioned) {
-            precondition(ds, f, p_.p, y_.p, in.precision, s);
-            y = y_.p;
-        }
-        spmv(y, v_.p, 1, s);
-        k_cm_dot2<<<g, kT, 0, s>>>(n_, c_.p, v_.p, nullptr, nullptr, p1, nullptr);
-        k_cm_alpha<<<1, kT, 0, s>>>(p1, g, st);
-        k_cm_update1<<<g, kT, 0, s>>>(n_, r_.p, v_.p, y, s_.p, x_.p, st);
-        launches_ += 3;
-        const double* z = s_.p;
-        if (preconditioned) {
-            precondition(ds, f, s_.p, z_.p, in.precision, s);
-            z = z_.p;
-        }
-        spmv(z, t_.p, 1, s);
-        k_cm_dot2<<<g, kT, 0, s>>>(n_, t_.p, s_.p, t_.p, t_.p, p1, p2);
-        k_cm_omega<<<1, kT, 0, s>>>(p1, p2, g, st);
-        k_cm_update2<<<g, kT, 0, s>>>(n_, s_.p, t_.p, z, c_.p, x_.p, r_.p, st, p1, p2);
-        k_cm_rho<<<1, kT, 0, s>>>(p1, p2, g, st);
-        k_cm_pupdate<<<g, kT, 0, s>>>(n_, r_.p, v_.p, p_.p, st);
-        launches_ += 5;
+    if (s && !std::getenv("TPAGMG_NO_GRAPH")) {
+        // the whole run as one graph launch; the host reads the state at its end
+        cudaGraphExec_t exec = loop_graph(ds, f, preconditioned, in.precision, s);
+        TPA_CUDA(cudaGraphLaunch(exec, s));
         read();
-        if (int(hs[kFlags]) & (kSolved | kTired | kBreakdown)) break;
+        launches_ += int(hs[kIter]) * body_launches_[preconditioned ? 1 : 0];
+    } else {
+        for (;;) {
+            enqueue_iteration(ds, f, preconditioned, in.precision, s, cudaGraphConditionalHandle(), 0);
+            read();
+            if (int(hs[kFlags]) & (kSolved | kTired | kBreakdown)) break;
+        }
     }
     TPA_CUDA(cudaGetLastError());
     return int(hs[kIter]);

@@ -72,6 +72,13 @@ struct DevBuf {
 
 class CmdgfmDevice {
 public:
+    CmdgfmDevice() = default;
+    CmdgfmDevice(const CmdgfmDevice&) = delete;
+    CmdgfmDevice& operator=(const CmdgfmDevice&) = delete;
+    ~CmdgfmDevice() {
+        for (auto& g : exec_)
+            if (g) cudaGraphExecDestroy(g);
+    }
     // Solves in place of `_project_cmdgfm_assembled!`'s linear part; the
     // solution (n) is a host array.  `ds` carries the pressure hierarchy.
     void solve(DeviceSolver& ds, const CmdgfmInput& in, const CmdgfmFactor& f, double* solution, CmdgfmStats& st);
@@ -83,6 +90,14 @@ private:
     void precondition(DeviceSolver& ds, const CmdgfmFactor& f, const double* src, double* dst, int precision,
                       cudaStream_t s);
     void spmv(const double* x, double* y, int mode, cudaStream_t s);
+    void enqueue_iteration(DeviceSolver& ds, const CmdgfmFactor& f, bool preconditioned, int precision,
+                           cudaStream_t s, cudaGraphConditionalHandle handle, int set_cond);
+    cudaGraphExec_t loop_graph(DeviceSolver& ds, const CmdgfmFactor& f, bool preconditioned, int precision,
+                               cudaStream_t s);
+    // captured BiCGSTAB loops (without / with the preconditioner) and what they captured
+    cudaGraphExec_t exec_[2] = {nullptr, nullptr};
+    std::vector<uintptr_t> key_[2];
+    int body_launches_[2] = {0, 0};
     int64_t n_ = 0, np_ = 0, nx_ = 0, na_ = 0, ncells_ = 0;
     int launches_ = 0;
     int precision_ = 0;

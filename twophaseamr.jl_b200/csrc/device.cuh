@@ -167,8 +167,12 @@ public:
     void residual_norms(const double* r, double out[2]);
 
     int kernel_launches() const { return launches_; }
+    // changes whenever captured graphs of this solver's kernels go stale (a new
+    // upload, a layout, a refresh): callers caching graphs of V-cycles key on it
+    unsigned graph_generation() const { return graph_gen_; }
     bool red_black() const { return rb_; }
     void reset_launches() { launches_ = 0; }
+    void add_launches(int k) { launches_ += k; }
 
 private:
     template <typename T> DevLevelT<T>& lv(int l);
@@ -199,6 +203,7 @@ private:
     CgScalars* host_sc_ = nullptr;
     double* host_d_ = nullptr;
     int launches_ = 0;
+    unsigned graph_gen_ = 0;
 
     // ---- fused cycle (default options) and the graph-captured CG loop ----
 public:

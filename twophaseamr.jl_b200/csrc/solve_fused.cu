@@ -708,6 +708,7 @@ void DeviceSolver::build_views() {
 }
 
 void DeviceSolver::destroy_graphs() {
+    ++graph_gen_;
     for (auto& g : cg_exec_)
         if (g) {
             cudaGraphExecDestroy(g);
