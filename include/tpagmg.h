@@ -437,6 +437,11 @@ typedef struct {
     double tolerance;                /* defect tolerance (reference default sqrt(eps)) */
     int32_t max_iterations;          /* BiCGSTAB iteration budget (reference default 500) */
     int32_t precision;               /* V-cycle: 0 FP64, 1 FP32 */
+    const double* initial_pressure;  /* np or NULL: the previous increment in the reduced
+                                        unknowns, x[cell] - x[anchor] (`_cmdgfm_initial_solution!`) */
+    int32_t warm_start;              /* 1: try zero pressure and then initial_pressure, each with
+                                        its jumps from the jump factor, before the Krylov loop
+                                        (the reference's default); 0: start from zero */
 } tpa_cmdgfm_system;
 
 typedef struct {
@@ -452,6 +457,7 @@ typedef struct {
     int32_t lower_levels, upper_levels;  /* depth of the triangular solves */
     int64_t inverse_entries; /* entries of L^-1 and U^-1 when the jump block is applied through
                                 them (two parallel products), 0 when the factors are walked row by row */
+    int32_t initial_guess_used;  /* the warm start replaced x = 0 */
 } tpa_cmdgfm_stats;
 
 /* The linear solve of the CMDGFM projection (`_project_cmdgfm_assembled!`,

@@ -16,8 +16,10 @@ Reference (ronaldremmerswaal/TwoPhaseAMR.jl):
   src/two_phase/projection/cmdgfm_projection.jl:1831-1917 residual defects, the omitted
       gauge (anchor) rows' defect, the scaled residual norm
   src/two_phase/projection/cmdgfm_projection.jl:1951-1971 `_cmdgfm_apply_increment!`
+  src/two_phase/projection/cmdgfm_projection.jl:1973-2040 `_cmdgfm_initial_solution!`
+      (the warm start; the previous increment is given in the reduced unknowns)
   src/two_phase/projection/cmdgfm_projection.jl:2201-2300 the residual-replacement loop of
-      `_project_cmdgfm_assembled!` (warm start off)
+      `_project_cmdgfm_assembled!`
   src/solvers/multigrid/cycles.jl:390-396                `incomplete_lu_preconditioner`
 
 Third-party algorithms, absent from the reference tree and restated from their
@@ -66,6 +68,8 @@ class CMDGFMSystem:
     drop_tolerance: float = 1e-3
     tolerance: float = np.sqrt(EPS)
     max_iterations: int = 500
+    warm_start: bool = False
+    initial_pressure: np.ndarray = None  # np: the previous increment, reduced (x[cell] - x[anchor])
 
     @property
     def n(self):
@@ -286,9 +290,50 @@ def bicgstab(apply_a, apply_n, b, atol, rtol, itmax):
     return x, it, status
 
 
+def initial_solution(system, M, pre):
+    """`_cmdgfm_initial_solution!` (cmdgfm_projection.jl:1973-2040): two
+    candidates, zero pressure and then the previous increment (when given and
+    not all zero), each with its jumps from the jump factor,
+    (L U)^-1 (rhs_xi - C p); a candidate replaces the best so far when its
+    defect is below 0.95 of the best and its scaled residual norm below the
+    best's.  Returns (solution, used)."""
+    n, npr = system.n, system.np_
+    rhs = system.rhs
+    best_defect = max(residual_defects(system, rhs))
+    best_l2 = float(np.linalg.norm(system.row_scale * rhs))
+    solution = np.zeros(n)
+    used = False
+    for use_previous in (False, True):
+        cand = np.zeros(n)
+        if use_previous:
+            if system.initial_pressure is None:
+                continue
+            cand[:npr] = system.initial_pressure
+            if not np.any(cand[:npr] != 0):
+                continue
+        if not np.all(np.isfinite(cand[:npr])):
+            continue
+        if system.nx > 0:
+            if pre is None:
+                continue
+            jr = np.array(rhs[npr:], dtype=np.float64, copy=True) - pre.C @ cand[:npr]
+            cand[npr:] = ilu_solve(pre.L, pre.U, jr)
+        if not np.all(np.isfinite(cand)):
+            continue
+        res = rhs - M @ cand
+        defect = max(residual_defects(system, res))
+        l2 = float(np.linalg.norm(system.row_scale * res))
+        if np.isfinite(defect) and np.isfinite(l2) and defect < 0.95 * best_defect and l2 < best_l2:
+            solution = cand
+            best_defect, best_l2 = defect, l2
+            used = True
+    return solution, used
+
+
 @dataclass
 class CMDGFMStats:
     converged: bool = False
+    initial_guess_used: bool = False
     iterations: int = 0
     attempts: int = 0
     initial_residual: float = 0.0
@@ -318,7 +363,7 @@ def anchor_defect(system, solution):
 
 def solve(system: CMDGFMSystem, mg, *, preconditioned=True):
     """The linear solve of `_project_cmdgfm_assembled!` (cmdgfm_projection.jl:
-    2201-2291) with warm_start = false: residual replacement around scaled,
+    2201-2291), with its warm start when `system.warm_start`: residual replacement around scaled,
     block-preconditioned BiCGSTAB runs.  `mg` is the full-cell hierarchy of the
     pressure operator (its `ldiv` is one V-cycle).  Returns (solution, stats)."""
     M = sp.csr_matrix(system.matrix)
@@ -343,6 +388,9 @@ def solve(system: CMDGFMSystem, mg, *, preconditioned=True):
     apply_n = None if pre is None else (lambda v: pre.ldiv(v / rows) / cols)
     correction = np.array(system.rhs, dtype=np.float64, copy=True)
     if n > 0 and st.initial_residual > 0:
+        if system.warm_start:
+            solution, st.initial_guess_used = initial_solution(system, M, pre)
+            correction = system.rhs - M @ solution
         while st.iterations < system.max_iterations:
             pd, jd = residual_defects(system, correction)
             defect = max(pd, jd, anchor_defect(system, solution))

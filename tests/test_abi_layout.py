@@ -26,10 +26,11 @@ STRUCTS = {
     "tpa_cmdgfm_system": ["np", "nx", "row_ptr", "col", "val", "rhs", "pressure_cell", "pressure_anchor",
                           "defect_weight", "na", "extra_row_ptr", "extra_col", "extra_val", "extra_rhs",
                           "extra_weight", "row_scale", "col_scale", "drop_tolerance", "tolerance",
-                          "max_iterations", "precision"],
+                          "max_iterations", "precision", "initial_pressure", "warm_start"],
     "tpa_cmdgfm_stats": ["converged", "iterations", "attempts", "kernel_launches", "initial_residual",
                          "final_residual", "pressure_defect", "jump_defect", "anchor_defect", "setup_ms",
-                         "device_ms", "factor_entries", "lower_levels", "upper_levels", "inverse_entries"],
+                         "device_ms", "factor_entries", "lower_levels", "upper_levels", "inverse_entries",
+                         "initial_guess_used"],
 }
 
 

@@ -40,10 +40,15 @@ def case(level):
         s = EllipticSolver(PoissonOperator(m, kappa))
         system, exact = W.cmdgfm_system(m, s.level_matrix(0), kappa, fr)
         oop = OOp(block_tree_mesh(**spec), kappa)
-        xo, so = O.solve(oracle_system(system), TreeGeometricMultigrid(oop, MultigridOptions()))
+        mg = TreeGeometricMultigrid(oop, MultigridOptions())
+        xo, so = O.solve(oracle_system(system), mg)
         assert so.converged
         CASES[level] = (s, system, exact, xo, so)
+        ORACLE_MG[level] = mg
     return CASES[level]
+
+
+ORACLE_MG = {}
 
 
 def rel(a, b, sl):
@@ -116,3 +121,23 @@ def test_cmdgfm_pressure_block_alone_and_bad_cells():
     with pytest.raises(TpaError) as e:
         solve_cmdgfm(s, CMDGFMSystem(**kw))
     assert e.value.code == TPA_ERR_INVALID_ARG
+
+
+def test_warm_start_matches_oracle():
+    """The warm start (`_cmdgfm_initial_solution!`): the GPU takes the same
+    decision as the oracle, saves the same iterations (within two) and ends at
+    the same solution, for a guess near the solution and for none."""
+    s, system, exact, xo, so = case(4)
+    npr = system.np_
+    rng = np.random.default_rng(4)
+    for guess in (exact[:npr] * (1 + 1e-4 * rng.standard_normal(npr)), None):
+        kw = dict(system.__dict__)
+        kw.update(warm_start=True, initial_pressure=guess)
+        warm = CMDGFMSystem(**kw)
+        xw_o, so_w = O.solve(oracle_system(warm), ORACLE_MG[4])
+        x, st = solve_cmdgfm(s, warm)
+        assert st.converged and st.initial_guess_used == so_w.initial_guess_used
+        assert abs(st.iterations - so_w.iterations) <= 2, (st.iterations, so_w.iterations)
+        assert rel(x, exact, slice(0, npr)) <= 1e-6 and rel(x, xw_o, slice(0, npr)) <= 1e-6
+        if guess is not None:
+            assert st.initial_guess_used and st.iterations < so.iterations

@@ -51,7 +51,8 @@ def oracle_system(system):
                           extra_rhs=system.extra_rhs, extra_weight=system.extra_weight,
                           row_scale=system.row_scale, col_scale=system.col_scale,
                           drop_tolerance=system.drop_tolerance, tolerance=system.tolerance,
-                          max_iterations=system.max_iterations)
+                          max_iterations=system.max_iterations, warm_start=system.warm_start,
+                          initial_pressure=system.initial_pressure)
 
 
 def rows_to_csr(rows, n):
@@ -184,3 +185,25 @@ def test_empty_jump_block_and_argument_checks():
     for b in bad:
         with pytest.raises(TpaError):
             cmdgfm_factor(b)
+
+
+def test_warm_start_takes_a_good_guess_and_refuses_a_bad_one():
+    """`_cmdgfm_initial_solution!` restated (cmdgfm_projection.jl:1973-2040):
+    a previous increment near the solution is taken and saves iterations; one
+    far from it is refused, and the solve ends at the same solution."""
+    spec, m, kappa, system, exact = wave_case(3)
+    oop = OOp(block_tree_mesh(**spec), kappa)
+    mg = TreeGeometricMultigrid(oop, MultigridOptions())
+    npr = system.np_
+    _, cold = O.solve(oracle_system(system), mg)
+    kw = dict(system.__dict__)
+    rng = np.random.default_rng(4)
+    kw.update(warm_start=True, initial_pressure=exact[:npr] * (1 + 1e-4 * rng.standard_normal(npr)))
+    good = CMDGFMSystem(**kw)
+    x, warm = O.solve(oracle_system(good), mg)
+    assert warm.initial_guess_used and warm.converged and warm.iterations < cold.iterations
+    assert np.max(np.abs(x[:npr] - exact[:npr])) <= 1e-6 * np.max(np.abs(exact[:npr]))
+    kw.update(initial_pressure=exact[:npr] * 50.0)
+    x, bad = O.solve(oracle_system(CMDGFMSystem(**kw)), mg)
+    assert bad.converged
+    assert np.max(np.abs(x[:npr] - exact[:npr])) <= 1e-6 * np.max(np.abs(exact[:npr]))

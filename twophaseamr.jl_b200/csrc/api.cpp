@@ -1287,6 +1287,9 @@ tpa::CmdgfmInput cmdgfm_input(const tpa_cmdgfm_system* sys, int64_t ncells) {
     in.tolerance = sys->tolerance;
     in.max_iterations = sys->max_iterations;
     in.precision = sys->precision;
+    if (sys->warm_start != 0 && sys->warm_start != 1) throw tpa::Error(TPA_ERR_INVALID_ARG, "warm_start must be 0 or 1");
+    in.warm_start = sys->warm_start != 0;
+    if (sys->initial_pressure) in.initial.assign(sys->initial_pressure, sys->initial_pressure + sys->np);
     return in;
 }
 
@@ -1330,6 +1333,7 @@ tpa_status tpa_cmdgfm_solve(tpa_context* ctx, const tpa_cmdgfm_system* system, d
             stats->lower_levels = f.nx ? f.lsched.levels() : 0;
             stats->upper_levels = f.nx ? f.usched.levels() : 0;
             stats->inverse_entries = st.inverse ? int64_t(f.linv.col.size() + f.uinv.col.size()) : 0;
+            stats->initial_guess_used = st.initial_guess_used ? 1 : 0;
         }
     });
 }

@@ -616,16 +616,7 @@ void CmdgfmDevice::precondition(DeviceSolver& ds, const CmdgfmFactor& f, const d
         k_cm_gather<<<grid_of(np_), kT, 0, s>>>(np_, zfull_.p, cell_.p, anchor_.p, cols_.p, zp_.p, dst);
         ++launches_;
     }
-    if (nx_ > 0 && inverse_) {
-        k_cm_jump_inverse<<<1, kIluThreads, 2 * size_t(nx_) * sizeof(double), s>>>(
-            int(nx_), np_, src, rows_.p, cptr_.p, ccol_.p, cval_.p, zp_.p, liptr_.p, licol_.p, lival_.p, uiptr_.p,
-            uicol_.p, uival_.p, cols_.p, dst);
-        ++launches_;
-    } else if (nx_ > 0) {
-        k_cm_jump_solve<<<1, kIluThreads, jsmem_, s>>>(int(nx_), np_, src, rows_.p, cptr_.p, ccol_.p, cval_.p, zp_.p,
-                                                       lview_, uview_, jstaged_, cols_.p, dst);
-        ++launches_;
-    }
+    if (nx_ > 0) jump_apply(src, rows_.p, cols_.p, zp_.p, dst, s);
     (void)f;
 }
 
@@ -728,6 +719,20 @@ cudaGraphExec_t CmdgfmDevice::loop_graph(DeviceSolver& ds, const CmdgfmFactor& f
     exec_[slot] = exec;
     key_[slot] = key;
     return exec;
+}
+
+// dst_xi = (L U)^-1 (src_xi / rows_xi - C zp) / cols_xi: the jump block of the
+// block preconditioner (rows, cols: D_r, D_c) or of the warm start (ones)
+void CmdgfmDevice::jump_apply(const double* src, const double* rows, const double* cols, const double* zp,
+                              double* dst, cudaStream_t s) {
+    if (inverse_)
+        k_cm_jump_inverse<<<1, kIluThreads, 2 * size_t(nx_) * sizeof(double), s>>>(
+            int(nx_), np_, src, rows, cptr_.p, ccol_.p, cval_.p, zp, liptr_.p, licol_.p, lival_.p, uiptr_.p, uicol_.p,
+            uival_.p, cols, dst);
+    else
+        k_cm_jump_solve<<<1, kIluThreads, jsmem_, s>>>(int(nx_), np_, src, rows, cptr_.p, ccol_.p, cval_.p, zp,
+                                                       lview_, uview_, jstaged_, cols, dst);
+    ++launches_;
 }
 
 int CmdgfmDevice::bicgstab(DeviceSolver& ds, const CmdgfmInput& in, const CmdgfmFactor& f, bool preconditioned,
@@ -934,6 +939,54 @@ void CmdgfmDevice::solve(DeviceSolver& ds, const CmdgfmInput& in, const CmdgfmFa
     st.initial_residual = std::sqrt(rr);
     const double tol = in.tolerance;
     int iterations = 0;
+    if (n_ > 0 && st.initial_residual > 0 && in.warm_start) {
+        // `_cmdgfm_initial_solution!` (cmdgfm_projection.jl:1973-2040): zero
+        // pressure, then the given previous increment, each with its jumps
+        // from the jump factor; the best one that lowers the defect below 0.95
+        // of the best so far and the scaled residual norm replaces x = 0
+        auto row_defects = [&](const double* res) {
+            k_cm_defects<<<g, kT, 0, s>>>(n_, np_, res, weight_.p, rows_.p, p1, p2, p3);
+            k_cm_defects_fold<<<1, kT, 0, s>>>(p1, p2, p3, g, p4, 0, state_.p);
+            launches_ += 2;
+            read();
+            const double pd = hs[kPressureDefect], jd = hs[kJumpDefect];
+            return std::make_pair((pd != pd || jd != jd) ? NAN : std::max(pd, jd), std::sqrt(hs[kRhsNorm2]));
+        };
+        if (!ones_.p || ones_.n < size_t(n_)) {
+            ones_.alloc(size_t(n_));
+            const std::vector<double> one(size_t(n_), 1.0);
+            TPA_CUDA(cudaMemcpyAsync(ones_.p, one.data(), sizeof(double) * size_t(n_), cudaMemcpyHostToDevice, s));
+            TPA_CUDA(cudaStreamSynchronize(s));
+        }
+        auto best = row_defects(corr_.p);
+        for (int use_previous = 0; use_previous < 2; ++use_previous) {
+            TPA_CUDA(cudaMemsetAsync(y_.p, 0, sizeof(double) * size_t(n_), s));
+            if (use_previous) {
+                if (in.initial.empty()) continue;
+                bool any = false, finite = true;
+                for (double v : in.initial) {
+                    any = any || v != 0.0;
+                    finite = finite && std::isfinite(v);
+                }
+                if (!any || !finite) continue;
+                TPA_CUDA(cudaMemcpyAsync(y_.p, in.initial.data(), sizeof(double) * size_t(np_),
+                                         cudaMemcpyHostToDevice, s));
+            }
+            if (nx_ > 0) jump_apply(rhs_.p, ones_.p, ones_.p, y_.p, y_.p, s);
+            if (count([&] { k_cm_nonfinite<<<g, kT, 0, s>>>(n_, y_.p, p1); }) != 0.0) continue;
+            k_cm_residual<<<g, kT, 0, s>>>(n_, mptr_.p, mcol_.p, mval_.p, rhs_.p, y_.p, t_.p);
+            ++launches_;
+            const auto cand = row_defects(t_.p);
+            if (std::isfinite(cand.first) && std::isfinite(cand.second) && cand.first < 0.95 * best.first &&
+                cand.second < best.second) {
+                TPA_CUDA(cudaMemcpyAsync(sol_.p, y_.p, sizeof(double) * size_t(n_), cudaMemcpyDeviceToDevice, s));
+                best = cand;
+                st.initial_guess_used = true;
+            }
+        }
+        k_cm_residual<<<g, kT, 0, s>>>(n_, mptr_.p, mcol_.p, mval_.p, rhs_.p, sol_.p, corr_.p);
+        ++launches_;
+    }
     if (n_ > 0 && st.initial_residual > 0) {
         while (iterations < in.max_iterations) {
             defects();

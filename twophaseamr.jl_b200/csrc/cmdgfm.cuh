@@ -27,6 +27,8 @@ struct CmdgfmInput {
     double tolerance = 1.4901161193847656e-08;
     int max_iterations = 500;
     int precision = 0;                // V-cycle: 0 FP64, 1 FP32
+    bool warm_start = false;          // `_cmdgfm_initial_solution!` before the loop
+    std::vector<double> initial;      // np: the previous increment, reduced (may be empty)
 };
 
 struct CmdgfmStats {
@@ -37,6 +39,7 @@ struct CmdgfmStats {
     double device_ms = 0;
     int launches = 0;
     bool inverse = false;  // the jump block went through the factors' inverses
+    bool initial_guess_used = false;
 };
 
 // a triangular factor laid out for its solve on the device (cmdgfm.cu)
@@ -90,6 +93,9 @@ private:
     void precondition(DeviceSolver& ds, const CmdgfmFactor& f, const double* src, double* dst, int precision,
                       cudaStream_t s);
     void spmv(const double* x, double* y, int mode, cudaStream_t s);
+    void jump_apply(const double* src, const double* rows, const double* cols, const double* zp, double* dst,
+                    cudaStream_t s);
+    DevBuf<double> ones_;
     void enqueue_iteration(DeviceSolver& ds, const CmdgfmFactor& f, bool preconditioned, int precision,
                            cudaStream_t s, cudaGraphConditionalHandle handle, int set_cond);
     cudaGraphExec_t loop_graph(DeviceSolver& ds, const CmdgfmFactor& f, bool preconditioned, int precision,

@@ -58,7 +58,8 @@ class CmdgfmSystemC(C.Structure):
                 ("extra_row_ptr", C.c_void_p), ("extra_col", C.c_void_p), ("extra_val", C.c_void_p),
                 ("extra_rhs", C.c_void_p), ("extra_weight", C.c_void_p), ("row_scale", C.c_void_p),
                 ("col_scale", C.c_void_p), ("drop_tolerance", C.c_double), ("tolerance", C.c_double),
-                ("max_iterations", C.c_int32), ("precision", C.c_int32)]
+                ("max_iterations", C.c_int32), ("precision", C.c_int32), ("initial_pressure", C.c_void_p),
+                ("warm_start", C.c_int32)]
 
 
 class CmdgfmStatsC(C.Structure):
@@ -66,7 +67,8 @@ class CmdgfmStatsC(C.Structure):
                 ("kernel_launches", C.c_int32), ("initial_residual", C.c_double), ("final_residual", C.c_double),
                 ("pressure_defect", C.c_double), ("jump_defect", C.c_double), ("anchor_defect", C.c_double),
                 ("setup_ms", C.c_double), ("device_ms", C.c_double), ("factor_entries", C.c_int64),
-                ("lower_levels", C.c_int32), ("upper_levels", C.c_int32), ("inverse_entries", C.c_int64)]
+                ("lower_levels", C.c_int32), ("upper_levels", C.c_int32), ("inverse_entries", C.c_int64),
+                ("initial_guess_used", C.c_int32)]
 
 
 P = C.c_void_p

@@ -50,6 +50,8 @@ class CMDGFMSystem:
     drop_tolerance: float = 1e-3
     tolerance: float = float(np.sqrt(np.finfo(np.float64).eps))
     max_iterations: int = 500
+    warm_start: bool = False          # `_cmdgfm_initial_solution!` (the reference's default is on)
+    initial_pressure: np.ndarray = None  # np: the previous increment, reduced (x[cell] - x[anchor])
 
     @property
     def n(self):
@@ -72,13 +74,16 @@ class CMDGFMSystem:
             extra_col=np.ascontiguousarray(self.extra_col, dtype=np.int32),
             extra_val=_lib.f64(self.extra_val), extra_rhs=_lib.f64(self.extra_rhs),
             extra_weight=_lib.f64(self.extra_weight),
-            row_scale=_lib.f64(self.row_scale), col_scale=_lib.f64(self.col_scale))
+            row_scale=_lib.f64(self.row_scale), col_scale=_lib.f64(self.col_scale),
+            initial_pressure=(_lib.f64(self.initial_pressure) if self.initial_pressure is not None
+                              else np.zeros(0)))
         c = _lib.CmdgfmSystemC()
         c.np, c.nx, c.na = int(self.np_), int(self.nx), int(len(keep["extra_row_ptr"]) - 1)
         for name, arr in keep.items():
             setattr(c, name, arr.ctypes.data if arr.size else None)
         c.drop_tolerance, c.tolerance = float(self.drop_tolerance), float(self.tolerance)
         c.max_iterations, c.precision = int(self.max_iterations), int(precision)
+        c.warm_start = 1 if self.warm_start else 0
         return c, keep
 
 
@@ -100,6 +105,7 @@ class CMDGFMStats:
     lower_levels: int
     upper_levels: int
     inverse_entries: int
+    initial_guess_used: bool
 
 
 _PRECISION = {"fp64": 0, "mixed": 1}
@@ -119,7 +125,7 @@ def solve_cmdgfm(solver, system: CMDGFMSystem, precision="fp64"):
     return x, CMDGFMStats(bool(st.converged), st.iterations, st.attempts, st.initial_residual, st.final_residual,
                           st.pressure_defect, st.jump_defect, st.anchor_defect, st.setup_ms, st.device_ms,
                           st.kernel_launches, st.factor_entries, st.lower_levels, st.upper_levels,
-                          st.inverse_entries)
+                          st.inverse_entries, bool(st.initial_guess_used))
 
 
 def cmdgfm_factor(system: CMDGFMSystem):
