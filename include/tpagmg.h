@@ -114,8 +114,9 @@ tpa_status tpa_set_operator(tpa_context* ctx, const double* face_coefficient);
  * before or after tpa_set_operator; an existing operator is assembled again
  * and the hierarchy must be rebuilt.  A coefficient refresh keeps the boundary
  * coefficients (`_replace_face_coefficient`, elliptic.jl:809-824) and runs on
- * the host.  The merged batch and the adjoint reject operators with open
- * sides (TPA_ERR_UNSUPPORTED). */
+ * the host.  The adjoint's face-coefficient gradient holds the boundary
+ * coefficients fixed, as a refresh does.  The merged batch rejects operators
+ * with open sides (TPA_ERR_UNSUPPORTED). */
 tpa_status tpa_set_open_boundaries(tpa_context* ctx, const int32_t open_sides[4], const double* boundary_coefficient);
 /* Number of stored off-diagonal inverse-metric entries (0 when K is diagonal),
  * operators/gradient.jl:369-393. */

@@ -131,12 +131,54 @@ def test_projection_keeps_open_face_velocity():
     assert np.max(np.abs(div)) <= 1e-8 * scale / m.spacing.min()
 
 
-def test_batch_and_adjoint_reject_open_sides():
+def test_batch_rejects_open_sides():
     from tpagmg import BatchedSolver
     m, s, oo, v, material = build(False, (False, False))
     with pytest.raises(TpaError) as e:
         BatchedSolver([s])
     assert e.value.code == TPA_ERR_UNSUPPORTED
-    with pytest.raises(TpaError) as e:
-        s.adjoint(v, v)
-    assert e.value.code == TPA_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("explicit", [True, False], ids=["explicit_boundary", "extended_boundary"])
+def test_adjoint_with_open_sides_matches_finite_differences(explicit):
+    """The adjoint with open sides: dJ/drhs and dJ/dkappa (boundary
+    coefficients held fixed, as a refresh keeps them) against central
+    differences (step 1e-6) of refreshed solves along 8 seeded directions, to
+    1e-6 relative plus the floor of the difference quotient."""
+    from test_gpu_adjoint import fd_floor
+    spec = spec_935(True, (False, False))
+    m = BlockTreeMesh(**spec)
+    om = block_tree_mesh(**spec)
+    kappa = 1.2 * np.exp(0.3 * np.sin(1.3 * np.arange(m.nfaces)))
+    material = 0.8 + 0.2 * om.bface_center[:, 1]
+    op = PoissonOperator(m, kappa, velocity_boundary=BOUNDARY,
+                         boundary_face_coefficient=material if explicit else None)
+    s = EllipticSolver(op, multigrid=MultigridOptions(coarse_size=8))
+    x, y = m.cell_centers()
+    rhs = np.cos(3 * x) * np.sin(2 * y) + 0.3
+    target = np.sin(5 * x + y)
+
+    def J(rhs_, kap):
+        s.refresh(kap)
+        p_ = np.zeros(m.ncells)
+        st = solve(p_, s, rhs_, rtol=1e-13, compatibility="error")
+        assert st.converged
+        return 0.5 * np.sum((p_ - target) ** 2), p_, st.target_linf
+
+    J0, p0, _ = J(rhs, kappa)
+    rb, kb, st = s.adjoint(p0, p0 - target, rtol=1e-13)
+    assert st.converged
+    rng = np.random.default_rng(77)
+    h = 1e-6
+    for _ in range(8):
+        d = rng.standard_normal(m.ncells)
+        jp, _, tp = J(rhs + h * d, kappa)
+        jm, _, tm = J(rhs - h * d, kappa)
+        fd = (jp - jm) / (2 * h)
+        assert abs(fd - rb @ d) <= 1e-6 * abs(fd) + fd_floor(J0, h, (tp, tm), rb), (fd, rb @ d)
+        dk = rng.standard_normal(m.nfaces) * kappa
+        jp, _, tp = J(rhs, kappa + h * dk)
+        jm, _, tm = J(rhs, kappa - h * dk)
+        fd = (jp - jm) / (2 * h)
+        assert abs(fd - kb @ dk) <= 1e-6 * abs(fd) + fd_floor(J0, h, (tp, tm), rb), (fd, kb @ dk)
+    s.refresh(kappa)

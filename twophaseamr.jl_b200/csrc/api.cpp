@@ -691,8 +691,12 @@ tpa_status tpa_face_coefficient_gradient(tpa_context* ctx, const double* p, cons
 static void adjoint_on_device(tpa_context* ctx, const double* p, const double* pbar, double* rhs_bar,
                               double* kappa_bar, double rtol, double atol, int32_t max_cycles, int32_t precision,
                               tpa_stats* stats) {
-    if (ctx->have_hierarchy && ctx->hier.levels[0].op.any_open())
-        throw tpa::Error(TPA_ERR_UNSUPPORTED, "the adjoint takes closed sides only (no open pressure sides)");
+    // Open sides: the operator stays symmetric and an anchored component has
+    // no projection and no gauge, so the adjoint solve is the solve.  The
+    // gradient is taken at fixed boundary coefficients, as a coefficient
+    // refresh keeps them (`_replace_face_coefficient`, elliptic.jl:809-824):
+    // the open-face conductances then do not depend on kappa, and the face
+    // kernel's -lam' (dS/dkappa_f) p is the whole derivative.
     ensure_faces(ctx);
     tpa::DeviceSolver& d = *ctx->dev;
     size_t n = size_t(d.ncells());
