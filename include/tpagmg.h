@@ -254,7 +254,12 @@ tpa_status tpa_batch_solve_device(tpa_batch* batch, const double* rhs, double* x
  * both post-sweeps in the other; the halo is recomputed in each tile), 2 also
  * the constant-coefficient 16x16 levels (on 22 x 22 stencil tiles), 3 the
  * constant-coefficient levels of at most 2^19 cells only (larger ones keep
- * the vectorized kernels), 0 none.
+ * the vectorized kernels), 4 as 3 with the larger levels of a periodic block
+ * lattice (one tree level of 16x16 blocks filling the domain, constant
+ * diagonal and volumes) on row-streaming kernels (two launches per level: a
+ * warp walks a strip 26 cells wide up the level with the phases one row
+ * apart), 5 every periodic lattice level on row-streaming kernels and the
+ * other constant-coefficient levels as 3, 0 none.
  * Every layout gives the same V-cycle to rounding. */
 typedef struct {
     int32_t tail_cells, tail_ctas, structured, vectorized, pdl, fuse_restrict, persistent, tiles;
@@ -337,6 +342,10 @@ tpa_status tpa_device_info(tpa_context* ctx, int64_t out[4]);
  * when its tiles do not fit).  Uploads the hierarchy if needed.  Measurement
  * support; no reference counterpart. */
 tpa_status tpa_tiled_levels(tpa_context* ctx, int32_t* count);
+/* Of those, the levels on the row-streaming kernels (tpa_tune_config.tiles 4
+ * or 5).  Uploads the hierarchy if needed.  Measurement support; no
+ * reference counterpart. */
+tpa_status tpa_streamed_levels(tpa_context* ctx, int32_t* count);
 /* Run subsequent device work on the caller's CUDA stream (a cudaStream_t
  * passed as void*; NULL restores the context's own stream).  Replaces nothing
  * in the reference (it has no device); it lets a caller order the solve with

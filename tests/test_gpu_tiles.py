@@ -167,3 +167,75 @@ def test_stencil_tiles_on_small_levels_only():
         st0 = solve(x0, s0, rhs, rtol=1e-10, precision=precision)
         assert st.converged and st0.converged and st.cycles == st0.cycles
         assert np.max(np.abs(x - x0)) <= 1e-9 * np.max(np.abs(x0))
+
+
+STREAM_CASES = {
+    # (mesh, levels expected on the row-streaming kernels with tiles = 5)
+    "periodic_256": (dict(base_mesh=(256, 256), block_size=(16, 16), periodic=(True, True)), 3),
+    "periodic_256x128": (dict(base_mesh=(256, 128), block_size=(16, 16), extent=(2.0, 1.0),
+                              periodic=(True, True)), 3),
+    "channel_256x128": (dict(base_mesh=(256, 128), block_size=(16, 16), extent=(2.0, 1.0),
+                             periodic=(True, False)), 0),  # walls: no level qualifies
+}
+
+
+@pytest.mark.parametrize("name", list(STREAM_CASES))
+def test_row_streaming_matches_vectorized_kernels(name):
+    """Periodic lattice levels on the row-streaming kernels (tiles = 5): every
+    multi-CTA level of the periodic meshes (down to 2 x 2 blocks, strips
+    wrapping around both axes), none of the channel's.  The V-cycle equals
+    the six-launch one to rounding (the same row arithmetic; only the coarse
+    sums fold in another order), twice (buffers reused), and the solves match
+    the oracle with the untiled layout's iteration counts."""
+    spec, nstream = STREAM_CASES[name]
+    m = BlockTreeMesh(**spec)
+    s = EllipticSolver(PoissonOperator(m), multigrid=MultigridOptions(coarse_size=64))
+    s0 = EllipticSolver(PoissonOperator(m), multigrid=MultigridOptions(coarse_size=64))
+    s.set_tuning(tiles=5, tail_cells=1024)
+    s0.set_tuning(tiles=0, tail_cells=1024)
+    assert s.streamed_levels() == nstream and s0.streamed_levels() == 0
+    rng = np.random.default_rng(6)
+    vol = m.cell_volumes()
+    for trial in range(2):
+        r = rng.standard_normal(m.ncells) * vol
+        r -= vol * np.sum(r) / np.sum(vol)
+        for precision, tol in (("fp64", 1e-13), ("mixed", 1e-5)):
+            z, z0 = s.vcycle(r, precision=precision), s0.vcycle(r, precision=precision)
+            assert np.max(np.abs(z - z0)) <= tol * np.max(np.abs(z0)), (precision, trial)
+    oo = OOp(block_tree_mesh(**spec), np.ones(m.nfaces))
+    rhs = W.gaussian_rhs(m, 8)
+    po, _ = osolve(oo, TreeGeometricMultigrid(oo, OMG(coarse_size=64)), rhs, rtol=1e-12)
+    for precision, rtol, tol in (("fp64", 1e-12, 1e-10), ("mixed", 1e-10, 1e-9)):
+        x, x0 = np.zeros(m.ncells), np.zeros(m.ncells)
+        st = solve(x, s, rhs, rtol=rtol, precision=precision)
+        st0 = solve(x0, s0, rhs, rtol=rtol, precision=precision)
+        assert st.converged and st.cycles == st0.cycles, (precision, st.cycles, st0.cycles)
+        assert np.max(np.abs(x - po)) <= tol * np.max(np.abs(po)), precision
+
+
+def test_row_streaming_on_the_large_levels_only():
+    """tiles = 4 on 1024^2: the 1M-cell finest level on the row-streaming
+    kernels, the levels of at most 2^19 cells on stencil tiles.  The V-cycle
+    equals the six-launch one to rounding, and the solves take the same number
+    of iterations to the same solution, in every precision."""
+    m = BlockTreeMesh(base_mesh=(1024, 1024), block_size=(16, 16), periodic=(True, True))
+    s = EllipticSolver(PoissonOperator(m))
+    s0 = EllipticSolver(PoissonOperator(m))
+    s.set_tuning(tiles=4, tail_cells=1024)
+    s0.set_tuning(tiles=0, tail_cells=1024)
+    multi = [n for n in s.level_sizes()[:-1] if n > 1024]
+    assert s.streamed_levels() == 1 and s.tiled_levels() == len(multi)
+    rng = np.random.default_rng(12)
+    r = rng.standard_normal(m.ncells)
+    r -= r.mean()
+    r *= m.cell_volumes()
+    for precision, tol in (("fp64", 1e-13), ("mixed", 1e-5)):
+        z, z0 = s.vcycle(r, precision=precision), s0.vcycle(r, precision=precision)
+        assert np.max(np.abs(z - z0)) <= tol * np.max(np.abs(z0)), precision
+    rhs = r / m.cell_volumes()
+    for precision in ("fp64", "mixed", "mixed_ir"):
+        x, x0 = np.zeros(m.ncells), np.zeros(m.ncells)
+        st = solve(x, s, rhs, rtol=1e-10, precision=precision)
+        st0 = solve(x0, s0, rhs, rtol=1e-10, precision=precision)
+        assert st.converged and st0.converged and st.cycles == st0.cycles, precision
+        assert np.max(np.abs(x - x0)) <= 1e-9 * np.max(np.abs(x0)), precision

@@ -1160,6 +1160,15 @@ tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tp
                 tl.tail_cells = cells;
                 run(tl);
             }
+        // the periodic lattice levels on the row-streaming kernels: the larger
+        // ones (4) or all (5), each with the best tail size of the tiled runs
+        const tpa::TuneConfig tb = res[best_of()].first;
+        for (int tiles : {4, 5}) {
+            tpa::TuneConfig tl = b0;
+            tl.tiles = tiles;
+            tl.tail_cells = tb.tiles ? tb.tail_cells : b0.tail_cells;
+            run(tl);
+        }
         const size_t b = best_of();
         d.reconfigure(ctx->hier, res[b].first);
         if (best) *best = to_c(res[b].first, res[b].second);
@@ -1172,7 +1181,7 @@ tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tp
 tpa_status tpa_set_tuning(tpa_context* ctx, const tpa_tune_config* cfg) {
     return guard(ctx, [&] {
         if (!cfg) throw tpa::Error(TPA_ERR_INVALID_ARG, "null configuration");
-        if (cfg->tail_ctas > 8 || cfg->structured > 2 || cfg->tiles > 3)
+        if (cfg->tail_ctas > 8 || cfg->structured > 2 || cfg->tiles > 5)
             throw tpa::Error(TPA_ERR_INVALID_ARG, "bad configuration");
         ensure_device(ctx);
         ensure_host_fresh(ctx);  // stencil copies come from the host levels
@@ -1185,6 +1194,14 @@ tpa_status tpa_tiled_levels(tpa_context* ctx, int32_t* count) {
         if (!count) throw tpa::Error(TPA_ERR_INVALID_ARG, "null output");
         ensure_device(ctx);
         *count = ctx->dev->tiled_levels();
+    });
+}
+
+tpa_status tpa_streamed_levels(tpa_context* ctx, int32_t* count) {
+    return guard(ctx, [&] {
+        if (!count) throw tpa::Error(TPA_ERR_INVALID_ARG, "null output");
+        ensure_device(ctx);
+        *count = ctx->dev->streamed_levels();
     });
 }
 

@@ -12,6 +12,7 @@
 #include "host.hpp"
 #include "stencil.cuh"
 #include "stencil4.cuh"
+#include "stream.cuh"
 #include "structure.hpp"
 #include "tiles.cuh"
 #include "tiles.hpp"
@@ -287,6 +288,7 @@ private:
         DevArray<float> cx_f, cy_f, exv_f;
         int64_t nex = 0;
         bool const_coef = false, const_diag = false;
+        int snbx = 0, snby = 0;  // periodic block lattice for the row-streaming kernels (0: none)
     };
     std::vector<StructDev> sdev_;
     std::vector<SView<double>> sd_;
@@ -297,6 +299,7 @@ private:
     struct TileDev {
         bool on = false;   // CSR tiles (k_tile_*)
         bool vec = false;  // constant-coefficient 16x16 level: stencil tiles (v_tile_*)
+        bool stream = false;  // periodic lattice level: row-streaming kernels (v_stream_*)
         int ntiles = 0, n3max = 0, n2max = 0, n1max = 0, emax = 0, nent = 0;
         int nt = 256;  // threads per CTA
         DevArray<int> cell, own, cell_off, ring, lrp, lrp_off, ent_off, pos, co, co_off;
@@ -305,6 +308,7 @@ private:
         DevArray<float> val_f;
     };
     std::vector<TileDev> tdev_;
+    StreamGeom stream_geom(int l) const;  // strips of a row-streamed level (stream.cuh)
     std::vector<TileView<double>> td_;
     std::vector<TileView<float>> tf_;
     void upload_tiles(const Hierarchy& h);
@@ -316,6 +320,8 @@ public:
     int structured_levels() const;
     // Levels whose V-cycle phases run on haloed block tiles.
     int tiled_levels() const;
+    // Of those, the levels on the row-streaming kernels.
+    int streamed_levels() const;
     int64_t exception_rows() const;
 
     // ---- coefficient refresh on the device (csrc/refresh.cu) ----

@@ -15,6 +15,7 @@
 
 #include "device.cuh"
 #include "persistent.cuh"
+#include "stream.cuh"
 #include "tail_smem.cuh"
 
 namespace tpa {
@@ -570,10 +571,13 @@ TuneConfig DeviceSolver::effective_tuning() const {
     // (measured slower than the vectorized kernels on uniform 2048^2, whose
     // finest level makes the tile kernel instruction-bound), 3: stencil tiles
     // on the constant-coefficient levels of at most kStencilTileCells cells
-    // only, where the six vectorized launches are latency-bound, 0: none
+    // only, where the six vectorized launches are latency-bound, 4: as 3, with
+    // the larger periodic lattice levels on the row-streaming kernels
+    // (stream.cuh), 5: every periodic lattice level on the row-streaming
+    // kernels, the other constant-coefficient levels as 3, 0: none
     c.tiles = 1;
-    if (const char* e = std::getenv("TPAGMG_TILES")) c.tiles = std::min(3, std::max(0, std::atoi(e)));
-    if (tune_.tiles >= 0) c.tiles = std::min(3, tune_.tiles);
+    if (const char* e = std::getenv("TPAGMG_TILES")) c.tiles = std::min(5, std::max(0, std::atoi(e)));
+    if (tune_.tiles >= 0) c.tiles = std::min(5, tune_.tiles);
     if (rb_) {  // the red-black sweeps exist for the CSR levels and the tail only
         c.structured = 0;
         c.persistent = 0;
@@ -764,6 +768,20 @@ void DeviceSolver::enqueue_vcycle_epi(const R* r, const double* rsum, double* me
             const SView<T>& S = (*Sp)[size_t(l)];
             const int groups = (S.nblocks + 3) / 4;
             const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
+            if (tdev_.size() > size_t(l) && tdev_[size_t(l)].stream) {
+                // both pre-sweeps, the residual and the restriction, streamed by rows
+                const StreamGeom g = stream_geom(l);
+                const int grid = (g.nsx * g.nsy + kStreamWarps - 1) / kStreamWarps;
+                if (l == 0)
+                    go(v_stream_down<T, R>, grid, kStreamWarps * 32, 0, S, g, r, rsum, V[size_t(l + 1)].b,
+                       fpartial_.p, counters_.p + kRestrictSum, next_sum ? lsum_.p + l + 1 : nullptr);
+                else
+                    go(v_stream_down<T, T>, grid, kStreamWarps * 32, 0, S, g, (const T*)S.b,
+                       (const double*)(lsum_.p + l), V[size_t(l + 1)].b, fpartial_.p, counters_.p + kRestrictSum,
+                       next_sum ? lsum_.p + l + 1 : nullptr);
+                ++launches_;
+                continue;
+            }
             if (tdev_.size() > size_t(l) && tdev_[size_t(l)].vec) {
                 // both pre-sweeps, the residual and the restriction on 22 x 22 tiles
                 if (l == 0)
@@ -875,6 +893,15 @@ void DeviceSolver::enqueue_vcycle_epi(const R* r, const double* rsum, double* me
             const SView<T>& S = (*Sp)[size_t(l)];
             const int groups = (S.nblocks + 3) / 4;
             const bool want_mean = (l == 0) && L.singular;
+            if (tdev_.size() > size_t(l) && tdev_[size_t(l)].stream) {
+                // prolongation and both post-sweeps, streamed by rows
+                const StreamGeom g = stream_geom(l);
+                const int grid = (g.nsx * g.nsy + kStreamWarps - 1) / kStreamWarps;
+                go(v_stream_up<T, Epi>, grid, kStreamWarps * 32, 0, S, g, (const T*)V[size_t(l + 1)].x, fpartial_.p,
+                   counters_.p + kPostMean, want_mean ? mean_out : nullptr, epi);
+                ++launches_;
+                continue;
+            }
             if (tdev_.size() > size_t(l) && tdev_[size_t(l)].vec) {
                 // prolongation and both post-sweeps on 22 x 22 tiles
                 go(v_tile_up<T, Epi>, S.nblocks, kTileThreads, 0, S, (const T*)V[size_t(l + 1)].x, fpartial_.p,
@@ -1293,8 +1320,11 @@ void DeviceSolver::upload_tiles(const Hierarchy& h) {
     TPA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
     size_t down_d = 0, up_d = 0;
     for (int l = 0; l < tail_first_ && l + 1 < nl; ++l) {
-        if (sdev_[size_t(l)].vec) {  // stencil tiles need no lists
-            tdev_[size_t(l)].vec = cfg.tiles == 2 || (cfg.tiles == 3 && levels_[size_t(l)].n <= kStencilTileCells);
+        if (sdev_[size_t(l)].vec) {  // stencil tiles and row streaming need no lists
+            const bool small = levels_[size_t(l)].n <= kStencilTileCells;
+            TileDev& D = tdev_[size_t(l)];
+            D.stream = sdev_[size_t(l)].snbx > 0 && (cfg.tiles == 5 || (cfg.tiles == 4 && !small));
+            D.vec = !D.stream && (cfg.tiles == 2 || (cfg.tiles >= 3 && small));
             continue;
         }
         if (sdev_[size_t(l)].on) continue;
@@ -1389,10 +1419,61 @@ void DeviceSolver::gather_tile_values() {
     TPA_CUDA(cudaStreamSynchronize(stream_));
 }
 
+int DeviceSolver::streamed_levels() const {
+    int k = 0;
+    for (const auto& d : tdev_) k += d.stream ? 1 : 0;
+    return k;
+}
+
 int DeviceSolver::tiled_levels() const {
     int k = 0;
-    for (const auto& d : tdev_) k += (d.on || d.vec) ? 1 : 0;
+    for (const auto& d : tdev_) k += (d.on || d.vec || d.stream) ? 1 : 0;
     return k;
+}
+
+// The block lattice of a level for the row-streaming kernels (stream.cuh):
+// returns its width nbx in blocks (height in `nby`), or 0 when the level does not
+// qualify.  It qualifies when both axes are periodic and its 16 x 16 blocks are
+// one tree level filling an nbx x nby rectangle in row-major order (the
+// (level, j, i) sort), with the same-size neighbours of the periodic lattice.
+// The next level must be the lattice halved in both directions: block map with
+// coarse block (j / 2) (nbx / 2) + i / 2, offsets 8 (i mod 2) and 8 (j mod 2),
+// scale 2.
+static int stream_lattice(const Mesh& m, const Mesh& mc, const StructLevel& st, int& nby) {
+    nby = 0;
+    if (!m.periodic[0] || !m.periodic[1] || m.bs[0] != 16 || m.bs[1] != 16 || m.keys.empty()) return 0;
+    const int lev = key_level(m.keys[0]);
+    int64_t nbx = 0, ny = 0;
+    for (uint64_t k : m.keys) {
+        if (key_level(k) != lev) return 0;
+        nbx = std::max<int64_t>(nbx, key_i(k) + 1);
+        ny = std::max<int64_t>(ny, key_j(k) + 1);
+    }
+    const int64_t nb = m.nblocks();
+    if (nbx * ny != nb || nbx < 2 || ny < 2 || nbx % 2 || ny % 2 || nb * 256 > int64_t(INT32_MAX)) return 0;
+    if (mc.nblocks() * 4 != nb || int64_t(st.nbr.size()) != 4 * nb || int64_t(st.map.size()) != 4 * nb) return 0;
+    for (int64_t b = 0; b < nb; ++b) {
+        const int64_t i = b % nbx, j = b / nbx;
+        if (m.keys[size_t(b)] != pack_key(lev, i, j)) return 0;
+        const int32_t* q = &st.nbr[size_t(4 * b)];
+        if (q[0] != j * nbx + (i + nbx - 1) % nbx || q[1] != j * nbx + (i + 1) % nbx ||
+            q[2] != ((j + ny - 1) % ny) * nbx + i || q[3] != ((j + 1) % ny) * nbx + i)
+            return 0;
+        const int32_t* mp = &st.map[size_t(4 * b)];
+        if (mp[0] != (j / 2) * (nbx / 2) + i / 2 || mp[1] != (i % 2) * 8 || mp[2] != (j % 2) * 8 || mp[3] != 2) return 0;
+    }
+    nby = int(ny);
+    return int(nbx);
+}
+
+StreamGeom DeviceSolver::stream_geom(int l) const {
+    const StructDev& D = sdev_[size_t(l)];
+    StreamGeom g;
+    g.nbx = D.snbx;
+    g.nby = D.snby;
+    g.nsx = (16 * D.snbx + kStreamCols - 1) / kStreamCols;
+    g.nsy = 16 * D.snby / kStreamRows;
+    return g;
 }
 
 // Block-structured copies of every level that qualifies: 16x16-style blocks
@@ -1453,6 +1534,8 @@ void DeviceSolver::upload_structured(const Hierarchy& h) {
         DevLevel& L = levels_[size_t(l)];
         const std::vector<double>& hv = hl.op.volumes;
         const bool const_vol = !hv.empty() && std::all_of(hv.begin(), hv.end(), [&](double v) { return v == hv[0]; });
+        if (D.vec && st.const_diag && const_vol)
+            D.snbx = stream_lattice(hl.op.mesh, h.levels[size_t(l + 1)].op.mesh, st, D.snby);
         auto fill = [&](auto& v, auto& DL, auto* cx, auto* cy, auto* exv, auto cast) {
             v.nx = hl.op.mesh.bs[0];
             v.ny = hl.op.mesh.bs[1];

@@ -1,0 +1,226 @@
+// Row-streaming halves of the V-cycle for periodic constant-coefficient 16x16
+// levels (tpa_tune_config.tiles = 4 or 5).
+//
+// The level is a full rectangle of nbx x nby blocks in row-major order (the
+// mesh's (level, j, i) sort of a single-level leaf set), periodic on both axes,
+// with one stencil coefficient c0, one inverse diagonal dinv0 and one cell
+// volume, and the next level is the same lattice halved.  A cell is then
+// addressed by its lattice position alone.
+//
+// A warp owns a strip of kStreamCols interior columns with a three-cell frame on
+// each side (32 lanes, lane l at column x0 + l - 3) and kStreamRows interior
+// rows, and walks up the strip one row at a time, frame rows included.  The
+// phases of a half run one row apart in registers: the west / east neighbours
+// come from the adjacent lanes by shuffles, the south / north ones from the
+// rows the lane already holds.  Each phase is valid on a frame one cell
+// narrower than the last, so the interior is exact.  Input rows are staged
+// kStreamDepth rows ahead in shared memory by cp.async, each lane copying the
+// cells of its own column.
+//
+// The arithmetic is that of the vectorized kernels (stencil4.cuh: q_apply's
+// neighbour order west, east, south, north, v_pre2, v_residual, v_restrict,
+// v_prolong, v_sweep), which follow the default V-cycle of
+// src/solvers/multigrid/cycles.jl:46-77 (ronaldremmerswaal/TwoPhaseAMR.jl).
+// Only the order of the coarse right-hand-side and mean sums differs.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "stencil4.cuh"
+
+namespace tpa {
+
+struct StreamGeom {
+    int nbx, nby;  // blocks across / up the level
+    int nsx, nsy;  // strips across / up the level
+};
+
+constexpr int kStreamWarps = 4;                // strips per CTA
+constexpr int kStreamCols = 26;                // interior columns of a strip
+constexpr int kStreamRows = 32;                // interior rows of a strip
+constexpr int kStreamSteps = kStreamRows + 6;  // rows walked: the interior and a three-row frame each side
+constexpr int kStreamDepth = 8;                // rows staged ahead
+
+template <int B>
+__device__ __forceinline__ void st_cp_async(void* dst, const void* src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(B) : "memory");
+}
+__device__ __forceinline__ void st_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void st_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// cell of lattice position (gx, gy), both inside the level
+__device__ __forceinline__ int st_cell(const StreamGeom& g, int gx, int gy) {
+    return (((gy >> 4) * g.nbx + (gx >> 4)) << 8) + ((gy & 15) << 4) + (gx & 15);
+}
+// the next level's cell holding fine position (gx, gy) (2 x 2 aggregation)
+__device__ __forceinline__ int st_coarse(const StreamGeom& g, int gx, int gy) {
+    const int cx = gx >> 1, cy = gy >> 1;
+    return (((cy >> 4) * (g.nbx >> 1) + (cx >> 4)) << 8) + ((cy & 15) << 4) + (cx & 15);
+}
+__device__ __forceinline__ int st_wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+// c0 (4 v - (w + e + s + n)) at this lane's cell of a row; every lane of the
+// warp calls it (shuffles).  The lanes at the strip's edges get their own
+// value as a neighbour; their results lie outside the frame that is used.
+template <typename T>
+__device__ __forceinline__ T st_apply(const SView<T>& L, T s, T c, T n) {
+    const T w = __shfl_up_sync(0xffffffffu, c, 1);
+    const T e = __shfl_down_sync(0xffffffffu, c, 1);
+    T off = w;
+    off += e;
+    off += s;
+    off += n;
+    return L.c0 * (T(4) * c - off);
+}
+
+// Both pre-sweeps from x = 0 with the level's RHS projection, the residual, and
+// the restriction b_c = P_tent'(r - wt A D^-1 r) with the optional coarse RHS sum.
+// The pre-smoothed iterate goes to L.y and the projected RHS to L.bp (read by
+// v_stream_up); the residual stays in registers.
+template <typename T, typename TB>
+__global__ void __launch_bounds__(kStreamWarps * 32)
+    v_stream_down(SView<T> L, StreamGeom g, const TB* __restrict__ bin, const double* level_sum,
+                  T* __restrict__ bc, double* partial, unsigned* counter, double* coarse_sum) {
+    pdl_entry();
+    constexpr int S = kStreamSteps, D = kStreamDepth;
+    __shared__ TB stage[kStreamWarps][D][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int strip = blockIdx.x * kStreamWarps + wid;
+    double part = 0;
+    if (strip < g.nsx * g.nsy) {
+        const int W = g.nbx * 16, H = g.nby * 16;
+        const int x0 = (strip % g.nsx) * kStreamCols, y0 = (strip / g.nsx) * kStreamRows;
+        const int gx0 = x0 + lane - 3;
+        const bool out_col = lane >= 3 && lane < 3 + kStreamCols && gx0 < W;
+        const int gx = st_wrap(gx0, W);
+        const double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
+        const double vol0 = double(L.vol0);
+        const T wd = L.w * L.dinv0;
+        auto cell = [&](int k) { return st_cell(g, gx, st_wrap(y0 - 3 + k, H)); };
+#pragma unroll
+        for (int k = 0; k < D - 1; ++k) {
+            st_cp_async<sizeof(TB)>(&stage[wid][k][lane], bin + cell(k));
+            st_commit();
+        }
+        T bp[S], x1[S], x2[S], r[S], s[S], t[S];
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+            if (k + D - 1 < S) st_cp_async<sizeof(TB)>(&stage[wid][(k + D - 1) % D][lane], bin + cell(k + D - 1));
+            st_commit();
+            st_wait<D - 1>();
+            const TB a = stage[wid][k % D][lane];
+            bp[k] = mean != 0.0 ? T(double(a) - vol0 * mean) : T(a);
+            x1[k] = wd * bp[k];  // the first sweep from zero, pointwise
+            if (k >= 2) {  // rows 1 .. S - 2
+                const int j = k - 1;
+                x2[j] = x1[j] + wd * (bp[j] - st_apply(L, x1[j - 1], x1[j], x1[j + 1]));
+                if (j >= 3 && j < 3 + kStreamRows && out_col) {
+                    const int c = cell(j);
+                    L.y[c] = x2[j];
+                    L.bp[c] = bp[j];
+                }
+            }
+            if (k >= 4) {  // rows 2 .. S - 3: their x2 neighbours exist
+                const int j = k - 2;
+                r[j] = bp[j] - st_apply(L, x2[j - 1], x2[j], x2[j + 1]);
+                s[j] = L.dinv0 * r[j];
+            }
+            if (k >= 6) {  // rows 3 .. S - 4: the interior
+                const int j = k - 3;
+                t[j] = r[j] - L.tw * st_apply(L, s[j - 1], s[j], s[j + 1]);
+                // rows j - 1 and j of the interior are a coarse row: horizontal pairs,
+                // then the row above, as v_restrict sums them
+                if (j >= 4 && j < 3 + kStreamRows && (j & 1) == 0) {
+                    const T h0 = t[j - 1] + __shfl_down_sync(0xffffffffu, t[j - 1], 1);
+                    const T d0 = t[j] + __shfl_down_sync(0xffffffffu, t[j], 1);
+                    const T v = h0 + d0;
+                    if (out_col && ((lane - 3) & 1) == 0) {
+                        bc[st_coarse(g, gx, y0 + j - 4)] = v;
+                        part += double(v);
+                    }
+                }
+            }
+        }
+    }
+    if (coarse_sum) {
+        if (publish_partial(part, partial, counter)) {
+            const double sum = fold_partials(partial, gridDim.x);
+            if (threadIdx.x == 0) {
+                *coarse_sum = sum;
+                *counter = 0;
+            }
+        }
+    }
+}
+
+// The prolongation x = y + e - wt D^-1 A e with e = P_tent x_c (y: the
+// pre-smoothed iterate of v_stream_down) and both post-sweeps into L.x; with
+// `mean_out`, the volume mean of L.x (and the epilogue's sums) folded.
+template <typename T, typename Epi>
+__global__ void __launch_bounds__(kStreamWarps * 32)
+    v_stream_up(SView<T> L, StreamGeom g, const T* __restrict__ xc, double* partial, unsigned* counter,
+                double* mean_out, Epi epi) {
+    pdl_entry();
+    constexpr int S = kStreamSteps, D = kStreamDepth;
+    __shared__ T se[kStreamWarps][D][32], sy[kStreamWarps][D][32], sb[kStreamWarps][D][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int strip = blockIdx.x * kStreamWarps + wid;
+    double v = 0, w = 0;
+    if (strip < g.nsx * g.nsy) {
+        const int W = g.nbx * 16, H = g.nby * 16;
+        const int x0 = (strip % g.nsx) * kStreamCols, y0 = (strip / g.nsx) * kStreamRows;
+        const int gx0 = x0 + lane - 3;
+        const bool out_col = lane >= 3 && lane < 3 + kStreamCols && gx0 < W;
+        const int gx = st_wrap(gx0, W);
+        const T wd = L.w * L.dinv0;
+        auto stage_row = [&](int k) {
+            const int gy = st_wrap(y0 - 3 + k, H);
+            const int c = st_cell(g, gx, gy);
+            st_cp_async<sizeof(T)>(&se[wid][k % D][lane], xc + st_coarse(g, gx, gy));
+            st_cp_async<sizeof(T)>(&sy[wid][k % D][lane], L.y + c);
+            st_cp_async<sizeof(T)>(&sb[wid][k % D][lane], L.bp + c);
+        };
+#pragma unroll
+        for (int k = 0; k < D - 1; ++k) {
+            stage_row(k);
+            st_commit();
+        }
+        T e[S], y[S], b[S], p[S], q[S];
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+            if (k + D - 1 < S) stage_row(k + D - 1);
+            st_commit();
+            st_wait<D - 1>();
+            e[k] = se[wid][k % D][lane];
+            y[k] = sy[wid][k % D][lane];
+            b[k] = sb[wid][k % D][lane];
+            if (k >= 2) {  // rows 1 .. S - 2
+                const int j = k - 1;
+                p[j] = y[j] + (e[j] - L.tw * L.dinv0 * st_apply(L, e[j - 1], e[j], e[j + 1]));
+            }
+            if (k >= 4) {  // rows 2 .. S - 3
+                const int j = k - 2;
+                q[j] = p[j] + wd * (b[j] - st_apply(L, p[j - 1], p[j], p[j + 1]));
+            }
+            if (k >= 6) {  // rows 3 .. S - 4: the interior
+                const int j = k - 3;
+                const T o = q[j] + wd * (b[j] - st_apply(L, q[j - 1], q[j], q[j + 1]));
+                if (j >= 3 && j < 3 + kStreamRows && out_col) {
+                    const int c = st_cell(g, gx, y0 + j - 3);
+                    L.x[c] = o;
+                    if (mean_out) {
+                        v += double(L.vol0) * double(o);
+                        if constexpr (Epi::kRz) w += epi.r[c] * double(o);
+                    }
+                }
+            }
+        }
+    }
+    if (mean_out) fold_mean(v, w, partial, counter, mean_out, L.cvol_inv, epi);
+}
+
+}  // namespace tpa

@@ -130,6 +130,7 @@ SIGNATURES = {
     "tpa_set_stream": (C.c_int32, [P, P]),
     "tpa_device_info": (C.c_int32, [P, i64p]),
     "tpa_tiled_levels": (C.c_int32, [P, i32p]),
+    "tpa_streamed_levels": (C.c_int32, [P, i32p]),
     "tpa_residual_norms": (C.c_int32, [P, P, f64p]),
     "tpa_residual_norms_noalloc": (C.c_int32, [P, P, P, C.c_int64, f64p]),
     "tpa_time_kernel": (C.c_int32, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, f64p]),

@@ -181,6 +181,12 @@ class EllipticSolver:
         self.ctx.call("tpa_tiled_levels", C.byref(n))
         return int(n.value)
 
+    def streamed_levels(self):
+        """Of the tiled levels, those on the row-streaming kernels (tiles 4, 5)."""
+        n = C.c_int32()
+        self.ctx.call("tpa_streamed_levels", C.byref(n))
+        return int(n.value)
+
     def set_tuning(self, **fields):
         """Apply a layout (tail_cells, tail_ctas, structured, vectorized, pdl,
         fuse_restrict, persistent, tiles; omitted fields: default)."""
