@@ -300,6 +300,7 @@ private:
         bool on = false;   // CSR tiles (k_tile_*)
         bool vec = false;  // constant-coefficient 16x16 level: stencil tiles (v_tile_*)
         bool stream = false;  // periodic lattice level: row-streaming kernels (v_stream_*)
+        int srows[2] = {0, 0}, sgrid[2] = {0, 0};  // their strip height and grid (FP64, FP32 kernels)
         int ntiles = 0, n3max = 0, n2max = 0, n1max = 0, emax = 0, nent = 0;
         int nt = 256;  // threads per CTA
         DevArray<int> cell, own, cell_off, ring, lrp, lrp_off, ent_off, pos, co, co_off;
@@ -308,7 +309,7 @@ private:
         DevArray<float> val_f;
     };
     std::vector<TileDev> tdev_;
-    StreamGeom stream_geom(int l) const;  // strips of a row-streamed level (stream.cuh)
+    StreamGeom stream_geom(int l, bool fp32) const;  // strips of a row-streamed level (stream.cuh)
     std::vector<TileView<double>> td_;
     std::vector<TileView<float>> tf_;
     void upload_tiles(const Hierarchy& h);

@@ -19,6 +19,30 @@
 #include "tail_smem.cuh"
 
 namespace tpa {
+
+// the strip height of a row-streamed level: the one whose rounds of resident
+// warps (ctas CTAs per SM) walk the fewest rows, the taller on a tie
+static int stream_rows(int nbx, int nby, int sms, int ctas) {
+    const int64_t slots = int64_t(ctas) * kStreamWarps * sms;
+    int best = 0;
+    int64_t cost = 0;
+    for (int rows : {36, 16}) {
+        const int64_t strips = int64_t((16 * nbx + kStreamCols - 1) / kStreamCols) * ((16 * nby + rows - 1) / rows);
+        const int64_t c = (strips + slots - 1) / slots * (rows + 6);
+        if (!best || c < cost) {
+            best = rows;
+            cost = c;
+        }
+    }
+    return best;
+}
+
+template <typename F>
+static void with_stream_rows(int rows, F f) {
+    if (rows == 16) f(std::integral_constant<int, 16>{});
+    else f(std::integral_constant<int, 36>{});
+}
+
 namespace {
 
 struct CgState {
@@ -770,15 +794,19 @@ void DeviceSolver::enqueue_vcycle_epi(const R* r, const double* rsum, double* me
             const bool next_sum = (l + 1 < t) && V[size_t(l + 1)].singular;
             if (tdev_.size() > size_t(l) && tdev_[size_t(l)].stream) {
                 // both pre-sweeps, the residual and the restriction, streamed by rows
-                const StreamGeom g = stream_geom(l);
-                const int grid = (g.nsx * g.nsy + kStreamWarps - 1) / kStreamWarps;
-                if (l == 0)
-                    go(v_stream_down<T, R>, grid, kStreamWarps * 32, 0, S, g, r, rsum, V[size_t(l + 1)].b,
-                       fpartial_.p, counters_.p + kRestrictSum, next_sum ? lsum_.p + l + 1 : nullptr);
-                else
-                    go(v_stream_down<T, T>, grid, kStreamWarps * 32, 0, S, g, (const T*)S.b,
-                       (const double*)(lsum_.p + l), V[size_t(l + 1)].b, fpartial_.p, counters_.p + kRestrictSum,
-                       next_sum ? lsum_.p + l + 1 : nullptr);
+                constexpr bool fp32 = std::is_same<T, float>::value;
+                const StreamGeom g = stream_geom(l, fp32);
+                const int grid = tdev_[size_t(l)].sgrid[fp32 ? 1 : 0];
+                with_stream_rows(g.rows, [&](auto rows) {
+                    constexpr int RW = decltype(rows)::value;
+                    if (l == 0)
+                        go(v_stream_down<T, R, RW>, grid, kStreamWarps * 32, 0, S, g, r, rsum, V[size_t(l + 1)].b,
+                           fpartial_.p, counters_.p + kRestrictSum, next_sum ? lsum_.p + l + 1 : nullptr);
+                    else
+                        go(v_stream_down<T, T, RW>, grid, kStreamWarps * 32, 0, S, g, (const T*)S.b,
+                           (const double*)(lsum_.p + l), V[size_t(l + 1)].b, fpartial_.p,
+                           counters_.p + kRestrictSum, next_sum ? lsum_.p + l + 1 : nullptr);
+                });
                 ++launches_;
                 continue;
             }
@@ -895,10 +923,14 @@ void DeviceSolver::enqueue_vcycle_epi(const R* r, const double* rsum, double* me
             const bool want_mean = (l == 0) && L.singular;
             if (tdev_.size() > size_t(l) && tdev_[size_t(l)].stream) {
                 // prolongation and both post-sweeps, streamed by rows
-                const StreamGeom g = stream_geom(l);
-                const int grid = (g.nsx * g.nsy + kStreamWarps - 1) / kStreamWarps;
-                go(v_stream_up<T, Epi>, grid, kStreamWarps * 32, 0, S, g, (const T*)V[size_t(l + 1)].x, fpartial_.p,
-                   counters_.p + kPostMean, want_mean ? mean_out : nullptr, epi);
+                constexpr bool fp32 = std::is_same<T, float>::value;
+                const StreamGeom g = stream_geom(l, fp32);
+                const int grid = tdev_[size_t(l)].sgrid[fp32 ? 1 : 0];
+                with_stream_rows(g.rows, [&](auto rows) {
+                    constexpr int RW = decltype(rows)::value;
+                    go(v_stream_up<T, Epi, RW>, grid, kStreamWarps * 32, 0, S, g, (const T*)V[size_t(l + 1)].x,
+                       fpartial_.p, counters_.p + kPostMean, want_mean ? mean_out : nullptr, epi);
+                });
                 ++launches_;
                 continue;
             }
@@ -1325,6 +1357,14 @@ void DeviceSolver::upload_tiles(const Hierarchy& h) {
             TileDev& D = tdev_[size_t(l)];
             D.stream = sdev_[size_t(l)].snbx > 0 && (cfg.tiles == 5 || (cfg.tiles == 4 && !small));
             D.vec = !D.stream && (cfg.tiles == 2 || (cfg.tiles >= 3 && small));
+            if (D.stream)
+                for (int fp32 = 0; fp32 < 2; ++fp32) {
+                    const int ctas = fp32 ? stream_ctas_per_sm<float>() : stream_ctas_per_sm<double>();
+                    D.srows[fp32] = stream_rows(sdev_[size_t(l)].snbx, sdev_[size_t(l)].snby, sms, ctas);
+                    const StreamGeom g = stream_geom(l, fp32 != 0);
+                    D.sgrid[fp32] = int(std::min<int64_t>((int64_t(g.nsx) * g.nsy + kStreamWarps - 1) / kStreamWarps,
+                                                          int64_t(ctas) * sms));
+                }
             continue;
         }
         if (sdev_[size_t(l)].on) continue;
@@ -1466,13 +1506,14 @@ static int stream_lattice(const Mesh& m, const Mesh& mc, const StructLevel& st, 
     return int(nbx);
 }
 
-StreamGeom DeviceSolver::stream_geom(int l) const {
+StreamGeom DeviceSolver::stream_geom(int l, bool fp32) const {
     const StructDev& D = sdev_[size_t(l)];
     StreamGeom g;
     g.nbx = D.snbx;
     g.nby = D.snby;
+    g.rows = tdev_[size_t(l)].srows[fp32 ? 1 : 0];
     g.nsx = (16 * D.snbx + kStreamCols - 1) / kStreamCols;
-    g.nsy = 16 * D.snby / kStreamRows;
+    g.nsy = (16 * D.snby + g.rows - 1) / g.rows;
     return g;
 }
 

@@ -8,8 +8,9 @@
 // addressed by its lattice position alone.
 //
 // A warp owns a strip of kStreamCols interior columns with a three-cell frame on
-// each side (32 lanes, lane l at column x0 + l - 3) and kStreamRows interior
-// rows, and walks up the strip one row at a time, frame rows included.  The
+// each side (32 lanes, lane l at column x0 + l - 3) and ROWS interior rows
+// (a template parameter, chosen per level), and walks up the strip one row at a
+// time, frame rows included.  The
 // phases of a half run one row apart in registers: the west / east neighbours
 // come from the adjacent lanes by shuffles, the south / north ones from the
 // rows the lane already holds.  Each phase is valid on a frame one cell
@@ -33,13 +34,18 @@ namespace tpa {
 struct StreamGeom {
     int nbx, nby;  // blocks across / up the level
     int nsx, nsy;  // strips across / up the level
+    int rows;      // interior rows of a strip (the kernel's ROWS)
 };
 
-constexpr int kStreamWarps = 4;                // strips per CTA
-constexpr int kStreamCols = 26;                // interior columns of a strip
-constexpr int kStreamRows = 32;                // interior rows of a strip
-constexpr int kStreamSteps = kStreamRows + 6;  // rows walked: the interior and a three-row frame each side
-constexpr int kStreamDepth = 8;                // rows staged ahead
+constexpr int kStreamWarps = 4;   // warps per CTA
+constexpr int kStreamCols = 26;   // interior columns of a strip (32 lanes, a 3-cell frame each side)
+constexpr int kStreamDepth = 8;   // rows staged ahead
+// resident CTAs per SM the kernels are built for: 8 in FP32 (64 registers),
+// 6 in FP64 (85 registers, which the FP64 kernels need without spilling)
+template <typename T>
+constexpr int stream_ctas_per_sm() {
+    return sizeof(T) == 8 ? 6 : 8;
+}
 
 template <int B>
 __device__ __forceinline__ void st_cp_async(void* dst, const void* src) {
@@ -80,27 +86,30 @@ __device__ __forceinline__ T st_apply(const SView<T>& L, T s, T c, T n) {
 // Both pre-sweeps from x = 0 with the level's RHS projection, the residual, and
 // the restriction b_c = P_tent'(r - wt A D^-1 r) with the optional coarse RHS sum.
 // The pre-smoothed iterate goes to L.y and the projected RHS to L.bp (read by
-// v_stream_up); the residual stays in registers.
-template <typename T, typename TB>
-__global__ void __launch_bounds__(kStreamWarps * 32)
+// v_stream_up); the residual stays in registers.  The warps of the grid take the
+// strips in turn (ROWS interior rows each; the last strip up the level may be
+// cut short, its rows past the top are walked but not written).
+template <typename T, typename TB, int ROWS>
+__global__ void __launch_bounds__(kStreamWarps * 32, stream_ctas_per_sm<T>())
     v_stream_down(SView<T> L, StreamGeom g, const TB* __restrict__ bin, const double* level_sum,
                   T* __restrict__ bc, double* partial, unsigned* counter, double* coarse_sum) {
     pdl_entry();
-    constexpr int S = kStreamSteps, D = kStreamDepth;
+    constexpr int S = ROWS + 6, D = kStreamDepth;
     __shared__ TB stage[kStreamWarps][D][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int strip = blockIdx.x * kStreamWarps + wid;
+    const int W = g.nbx * 16, H = g.nby * 16;
+    const double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
+    const double vol0 = double(L.vol0);
+    const T wd = L.w * L.dinv0;
     double part = 0;
-    if (strip < g.nsx * g.nsy) {
-        const int W = g.nbx * 16, H = g.nby * 16;
-        const int x0 = (strip % g.nsx) * kStreamCols, y0 = (strip / g.nsx) * kStreamRows;
+    for (int strip = blockIdx.x * kStreamWarps + wid; strip < g.nsx * g.nsy; strip += gridDim.x * kStreamWarps) {
+        const int x0 = (strip % g.nsx) * kStreamCols, y0 = (strip / g.nsx) * ROWS;
         const int gx0 = x0 + lane - 3;
         const bool out_col = lane >= 3 && lane < 3 + kStreamCols && gx0 < W;
         const int gx = st_wrap(gx0, W);
-        const double mean = (L.singular && level_sum) ? *level_sum * L.cvol_inv : 0.0;
-        const double vol0 = double(L.vol0);
-        const T wd = L.w * L.dinv0;
         auto cell = [&](int k) { return st_cell(g, gx, st_wrap(y0 - 3 + k, H)); };
+        // interior row j (3 <= j < ROWS + 3) lies inside the level
+        auto in_row = [&](int j) { return y0 + j - 3 < H; };
 #pragma unroll
         for (int k = 0; k < D - 1; ++k) {
             st_cp_async<sizeof(TB)>(&stage[wid][k][lane], bin + cell(k));
@@ -118,7 +127,7 @@ __global__ void __launch_bounds__(kStreamWarps * 32)
             if (k >= 2) {  // rows 1 .. S - 2
                 const int j = k - 1;
                 x2[j] = x1[j] + wd * (bp[j] - st_apply(L, x1[j - 1], x1[j], x1[j + 1]));
-                if (j >= 3 && j < 3 + kStreamRows && out_col) {
+                if (j >= 3 && j < 3 + ROWS && out_col && in_row(j)) {
                     const int c = cell(j);
                     L.y[c] = x2[j];
                     L.bp[c] = bp[j];
@@ -134,11 +143,11 @@ __global__ void __launch_bounds__(kStreamWarps * 32)
                 t[j] = r[j] - L.tw * st_apply(L, s[j - 1], s[j], s[j + 1]);
                 // rows j - 1 and j of the interior are a coarse row: horizontal pairs,
                 // then the row above, as v_restrict sums them
-                if (j >= 4 && j < 3 + kStreamRows && (j & 1) == 0) {
+                if (j >= 4 && j < 3 + ROWS && (j & 1) == 0) {
                     const T h0 = t[j - 1] + __shfl_down_sync(0xffffffffu, t[j - 1], 1);
                     const T d0 = t[j] + __shfl_down_sync(0xffffffffu, t[j], 1);
                     const T v = h0 + d0;
-                    if (out_col && ((lane - 3) & 1) == 0) {
+                    if (out_col && ((lane - 3) & 1) == 0 && in_row(j)) {
                         bc[st_coarse(g, gx, y0 + j - 4)] = v;
                         part += double(v);
                     }
@@ -160,23 +169,22 @@ __global__ void __launch_bounds__(kStreamWarps * 32)
 // The prolongation x = y + e - wt D^-1 A e with e = P_tent x_c (y: the
 // pre-smoothed iterate of v_stream_down) and both post-sweeps into L.x; with
 // `mean_out`, the volume mean of L.x (and the epilogue's sums) folded.
-template <typename T, typename Epi>
-__global__ void __launch_bounds__(kStreamWarps * 32)
+template <typename T, typename Epi, int ROWS>
+__global__ void __launch_bounds__(kStreamWarps * 32, stream_ctas_per_sm<T>())
     v_stream_up(SView<T> L, StreamGeom g, const T* __restrict__ xc, double* partial, unsigned* counter,
                 double* mean_out, Epi epi) {
     pdl_entry();
-    constexpr int S = kStreamSteps, D = kStreamDepth;
+    constexpr int S = ROWS + 6, D = kStreamDepth;
     __shared__ T se[kStreamWarps][D][32], sy[kStreamWarps][D][32], sb[kStreamWarps][D][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int strip = blockIdx.x * kStreamWarps + wid;
+    const int W = g.nbx * 16, H = g.nby * 16;
+    const T wd = L.w * L.dinv0;
     double v = 0, w = 0;
-    if (strip < g.nsx * g.nsy) {
-        const int W = g.nbx * 16, H = g.nby * 16;
-        const int x0 = (strip % g.nsx) * kStreamCols, y0 = (strip / g.nsx) * kStreamRows;
+    for (int strip = blockIdx.x * kStreamWarps + wid; strip < g.nsx * g.nsy; strip += gridDim.x * kStreamWarps) {
+        const int x0 = (strip % g.nsx) * kStreamCols, y0 = (strip / g.nsx) * ROWS;
         const int gx0 = x0 + lane - 3;
         const bool out_col = lane >= 3 && lane < 3 + kStreamCols && gx0 < W;
         const int gx = st_wrap(gx0, W);
-        const T wd = L.w * L.dinv0;
         auto stage_row = [&](int k) {
             const int gy = st_wrap(y0 - 3 + k, H);
             const int c = st_cell(g, gx, gy);
@@ -209,7 +217,7 @@ __global__ void __launch_bounds__(kStreamWarps * 32)
             if (k >= 6) {  // rows 3 .. S - 4: the interior
                 const int j = k - 3;
                 const T o = q[j] + wd * (b[j] - st_apply(L, q[j - 1], q[j], q[j + 1]));
-                if (j >= 3 && j < 3 + kStreamRows && out_col) {
+                if (j >= 3 && j < 3 + ROWS && out_col && y0 + j - 3 < H) {
                     const int c = st_cell(g, gx, y0 + j - 3);
                     L.x[c] = o;
                     if (mean_out) {
