@@ -26,7 +26,7 @@ static int stream_rows(int nbx, int nby, int sms, int ctas) {
     const int64_t slots = int64_t(ctas) * kStreamWarps * sms;
     int best = 0;
     int64_t cost = 0;
-    for (int rows : {36, 16}) {
+    for (int rows : {36, 24, 16}) {
         const int64_t strips = int64_t((16 * nbx + kStreamCols - 1) / kStreamCols) * ((16 * nby + rows - 1) / rows);
         const int64_t c = (strips + slots - 1) / slots * (rows + 6);
         if (!best || c < cost) {
@@ -40,6 +40,7 @@ static int stream_rows(int nbx, int nby, int sms, int ctas) {
 template <typename F>
 static void with_stream_rows(int rows, F f) {
     if (rows == 16) f(std::integral_constant<int, 16>{});
+    else if (rows == 24) f(std::integral_constant<int, 24>{});
     else f(std::integral_constant<int, 36>{});
 }
 
