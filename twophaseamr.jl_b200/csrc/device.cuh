@@ -301,6 +301,7 @@ private:
         bool vec = false;  // constant-coefficient 16x16 level: stencil tiles (v_tile_*)
         bool stream = false;  // periodic lattice level: row-streaming kernels (v_stream_*)
         int srows[2] = {0, 0}, sgrid[2] = {0, 0};  // their strip height and grid (FP64, FP32 kernels)
+        int cg_rows = 0, cg_grid = 0;              // the same for the CG direction kernel (finest level)
         int ntiles = 0, n3max = 0, n2max = 0, n1max = 0, emax = 0, nent = 0;
         int nt = 256;  // threads per CTA
         DevArray<int> cell, own, cell_off, ring, lrp, lrp_off, ent_off, pos, co, co_off;
@@ -310,6 +311,7 @@ private:
     };
     std::vector<TileDev> tdev_;
     StreamGeom stream_geom(int l, bool fp32) const;  // strips of a row-streamed level (stream.cuh)
+    StreamGeom stream_cg_geom() const;                // strips of the streamed CG direction kernel
     std::vector<TileView<double>> td_;
     std::vector<TileView<float>> tf_;
     void upload_tiles(const Hierarchy& h);

@@ -22,13 +22,18 @@ namespace tpa {
 
 // the strip height of a row-streamed level: the one whose rounds of resident
 // warps (ctas CTAs per SM) walk the fewest rows, the taller on a tie
-static int stream_rows(int nbx, int nby, int sms, int ctas) {
+// (strips of `cols` interior columns; `frame` rows walked besides the interior)
+// (`shallow`: the short strips of 8 and 4 rows too, for the small levels,
+// where a strip's walk is the kernel's time)
+static int stream_rows(int nbx, int nby, int sms, int ctas, int cols = kStreamCols, int frame = 6,
+                       bool shallow = true) {
     const int64_t slots = int64_t(ctas) * kStreamWarps * sms;
     int best = 0;
     int64_t cost = 0;
-    for (int rows : {36, 24, 16}) {
-        const int64_t strips = int64_t((16 * nbx + kStreamCols - 1) / kStreamCols) * ((16 * nby + rows - 1) / rows);
-        const int64_t c = (strips + slots - 1) / slots * (rows + 6);
+    for (int rows : {36, 24, 16, 8, 4}) {
+        if (!shallow && rows < 16) break;
+        const int64_t strips = int64_t((16 * nbx + cols - 1) / cols) * ((16 * nby + rows - 1) / rows);
+        const int64_t c = (strips + slots - 1) / slots * (rows + frame);
         if (!best || c < cost) {
             best = rows;
             cost = c;
@@ -39,6 +44,16 @@ static int stream_rows(int nbx, int nby, int sms, int ctas) {
 
 template <typename F>
 static void with_stream_rows(int rows, F f) {
+    if (rows == 4) f(std::integral_constant<int, 4>{});
+    else if (rows == 8) f(std::integral_constant<int, 8>{});
+    else if (rows == 16) f(std::integral_constant<int, 16>{});
+    else if (rows == 24) f(std::integral_constant<int, 24>{});
+    else f(std::integral_constant<int, 36>{});
+}
+
+// the strip heights of the streamed CG direction kernel (finest level)
+template <typename F>
+static void with_cg_rows(int rows, F f) {
     if (rows == 16) f(std::integral_constant<int, 16>{});
     else if (rows == 24) f(std::integral_constant<int, 24>{});
     else f(std::integral_constant<int, 36>{});
@@ -526,6 +541,83 @@ __global__ void __launch_bounds__(256) v_cg_dir_ap(SView<double> L, const T* __r
         return q;
     };
     v_apply_dot_ld(L, ld, pn, ap, partial, counter, [&](double pAp) { alpha_from(pAp, s); });
+}
+
+// The same on a periodic lattice finest level, streamed by rows (stream.cuh):
+// a warp walks a strip of kStreamCgCols interior columns (a column pair per
+// lane, a one-pair frame each side) and ROWS rows with a frame row each side;
+// the direction of a row is formed where the row is loaded, and A p one row
+// behind it.
+constexpr int kStreamCgCols = 60;
+constexpr int kStreamCgCtas = 6;  // resident CTAs per SM the kernel is built for
+
+template <typename T, typename P, int ROWS>
+__global__ void __launch_bounds__(kStreamWarps * 32, kStreamCgCtas)
+    v_stream_dir_ap(SView<double> L, StreamGeom g, const T* __restrict__ xv, const double* mean, P* pa, P* pb,
+                    P* __restrict__ ap, double* partial, unsigned* counter, CgState* s) {
+    pdl_entry();
+    if (s->flags & kCgHalt) return;  // the run ended at this body's r'z
+    constexpr int S = ROWS + 2, D = kStreamDepth;
+    __shared__ P2<T> sz[kStreamWarps][D][32];
+    __shared__ P2<P> sp[kStreamWarps][D][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int it = s->iter;
+    const P* __restrict__ po = dir_old(pa, pb, it);
+    P* __restrict__ pn = dir_new(pa, pb, it);
+    const double mu = *mean, beta = s->beta;
+    const bool first = it == 0;
+    const int W = g.nbx * 16, H = g.nby * 16;
+    double part = 0;
+    for (int strip = blockIdx.x * kStreamWarps + wid; strip < g.nsx * g.nsy; strip += gridDim.x * kStreamWarps) {
+        const int x0 = (strip % g.nsx) * kStreamCgCols, y0 = (strip / g.nsx) * ROWS;
+        const int gx0 = x0 - 2 + 2 * lane;
+        const bool out_col = lane >= 1 && lane < 1 + kStreamCgCols / 2 && gx0 < W;
+        const int gx = st_wrap(gx0, W);
+        auto cell = [&](int k) { return st_cell(g, gx, st_wrap(y0 - 1 + k, H)); };
+        auto stage = [&](int k) {
+            const int c = cell(k);
+            st_cp_async<sizeof(P2<T>)>(&sz[wid][k % D][lane], xv + c);
+            if (!first) st_cp_async<sizeof(P2<P>)>(&sp[wid][k % D][lane], po + c);
+        };
+#pragma unroll
+        for (int k = 0; k < D - 1; ++k) {
+            stage(k);
+            st_commit();
+        }
+        P2<double> q[S];
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+            if (k + D - 1 < S) stage(k + D - 1);
+            st_commit();
+            st_wait<D - 1>();
+            const P2<T> z = sz[wid][k % D][lane];
+            double ql = double(z.l) - mu, qr = double(z.r) - mu;
+            if (!first) {
+                const P2<P> pq = sp[wid][k % D][lane];
+                ql = (double(z.l) - mu) + beta * double(pq.l);
+                qr = (double(z.r) - mu) + beta * double(pq.r);
+            }
+            q[k] = P2<double>{double(P(ql)), double(P(qr))};  // the stored direction
+            if (k >= 2) {  // rows 1 .. ROWS: the interior
+                const int j = k - 1;
+                const P2<double> ax = st_apply(L, q[j - 1], q[j], q[j + 1]);
+                if (out_col && y0 + j - 1 < H) {
+                    const int c = cell(j);
+                    *reinterpret_cast<P2<P>*>(pn + c) = P2<P>{P(q[j].l), P(q[j].r)};
+                    *reinterpret_cast<P2<P>*>(ap + c) = P2<P>{P(ax.l), P(ax.r)};
+                    part += q[j].l * ax.l;
+                    part += q[j].r * ax.r;
+                }
+            }
+        }
+    }
+    if (publish_partial(part, partial, counter)) {
+        const double sum = fold_partials(partial, gridDim.x);
+        if (threadIdx.x == 0) {
+            alpha_from(sum, s);
+            *counter = 0;
+        }
+    }
 }
 
 // Start of an inner run of the refinement solve: the FP64 true residual
@@ -1055,7 +1147,14 @@ void DeviceSolver::enqueue_cg_body(int precision, cudaGraphConditionalHandle han
                (const T*)xv, mean, (const P*)r, fpartial_.p, counters_.p + kCgZ, s);
         }
         // p = z + beta p_old, Ap and alpha = gamma / p'Ap
-        if (sdev_[0].vec)
+        if (sdev_[0].vec && tdev_.size() && tdev_[0].stream) {
+            const StreamGeom g = stream_cg_geom();
+            with_cg_rows(g.rows, [&](auto rows) {
+                constexpr int RW = decltype(rows)::value;
+                go(v_stream_dir_ap<T, P, RW>, tdev_[0].cg_grid, kStreamWarps * 32, 0, sd_[0], g, (const T*)xv, mean,
+                   pa, pb, ap, fpartial_.p, counters_.p + kCgAp, s);
+            });
+        } else if (sdev_[0].vec)
             go(v_cg_dir_ap<T, P>, fold_grid(v_cg_dir_ap<T, P>, 256, (sd_[0].nblocks + 3) / 4, kMaxGrid), 256, 0,
                sd_[0], (const T*)xv, mean, pa, pb, ap, fpartial_.p, counters_.p + kCgAp, s);
         else if (sdev_[0].on)
@@ -1094,6 +1193,10 @@ void DeviceSolver::enqueue_cg_body(int precision, cudaGraphConditionalHandle han
 // than the separate pass it replaces (3.35 -> 3.38 ms), and the structured
 // kernel, with the same capped grid, is left out with it.  The CSR
 // post-smoothing has one thread per cell and gains (droplet: 2.56 -> 2.49 ms).
+// The row-streamed finest level (v_stream_up) takes the epilogue as well, but
+// its r loads raised the kernel from 21.6 to 34-35 µs on 2048^2, plain or
+// staged by cp.async, about what the separate pass costs (12.8 µs); it is left
+// out too.
 bool DeviceSolver::rz_foldable() const {
     return tail_first_ > 0 && coop_grid_ == 0 && !rb_ && levels_[0].ncomp == 1 && !sdev_.empty() && !sdev_[0].on;
 }
@@ -1366,6 +1469,12 @@ void DeviceSolver::upload_tiles(const Hierarchy& h) {
                     D.sgrid[fp32] = int(std::min<int64_t>((int64_t(g.nsx) * g.nsy + kStreamWarps - 1) / kStreamWarps,
                                                           int64_t(ctas) * sms));
                 }
+            if (D.stream && l == 0) {  // the CG's direction and operator product on the finest level
+                D.cg_rows = stream_rows(sdev_[0].snbx, sdev_[0].snby, sms, kStreamCgCtas, kStreamCgCols, 2, false);
+                const StreamGeom g = stream_cg_geom();
+                D.cg_grid = int(std::min<int64_t>((int64_t(g.nsx) * g.nsy + kStreamWarps - 1) / kStreamWarps,
+                                                  int64_t(kStreamCgCtas) * sms));
+            }
             continue;
         }
         if (sdev_[size_t(l)].on) continue;
@@ -1470,6 +1579,17 @@ int DeviceSolver::tiled_levels() const {
     int k = 0;
     for (const auto& d : tdev_) k += (d.on || d.vec || d.stream) ? 1 : 0;
     return k;
+}
+
+StreamGeom DeviceSolver::stream_cg_geom() const {
+    const StructDev& D = sdev_[0];
+    StreamGeom g;
+    g.nbx = D.snbx;
+    g.nby = D.snby;
+    g.rows = tdev_[0].cg_rows;
+    g.nsx = (16 * D.snbx + kStreamCgCols - 1) / kStreamCgCols;
+    g.nsy = (16 * D.snby + g.rows - 1) / g.rows;
+    return g;
 }
 
 // The block lattice of a level for the row-streaming kernels (stream.cuh):
