@@ -560,18 +560,26 @@ def main():
     e2e_ms_mean = float(np.mean(e2e_ms))
 
     # roofline of the dominant kernel, timed alone (CUDA events, 200 launches):
-    # with the finest level on CSR tiles its down kernel (both pre-sweeps, the
-    # residual and the restriction), else the smoothing sweep
+    # with the finest level on CSR tiles or row-streamed its down kernel (both
+    # pre-sweeps, the residual and the restriction), else the smoothing sweep
     skappa = 0 if args.workload == "uniform_2048" else 1
     sweep, sweep64 = C.c_double(), C.c_double()
+
+    def down_kernel(which, name):
+        solver.ctx.call("tpa_time_kernel", which, 0, 1, 200, C.byref(sweep))
+        solver.ctx.call("tpa_time_kernel", which, 0, 0, 200, C.byref(sweep64))
+        # read the FP64 residual (and two face coefficients when they vary),
+        # write the pre-smoothed iterate, the projected RHS and the coarse RHS
+        # (a quarter of a value per fine cell): 8 + 2 s_kappa + 2 s + s / 4
+        return name, n * (8 + 2 * 4 * skappa + 2 * 4 + 1)
+
     try:
-        solver.ctx.call("tpa_time_kernel", 6, 0, 1, 200, C.byref(sweep))
-        solver.ctx.call("tpa_time_kernel", 6, 0, 0, 200, C.byref(sweep64))
-        # read the FP64 residual and two face coefficients, write the
-        # pre-smoothed iterate, the projected RHS and the coarse RHS (a quarter
-        # of a value per fine cell): 8 + 2 s_kappa + 2 s + s / 4
-        kname = "k_tile_down, finest level, FP32 cycle (both pre-sweeps, residual, restriction)"
-        alg32 = n * (8 + 2 * 4 * skappa + 2 * 4 + 1)
+        try:
+            kname, alg32 = down_kernel(6, "k_tile_down, finest level, FP32 cycle (both pre-sweeps, residual, "
+                                          "restriction)")
+        except _lib.TpaError:
+            kname, alg32 = down_kernel(8, "v_stream_down, finest level, FP32 cycle (row-streamed: both "
+                                          "pre-sweeps, residual, restriction)")
     except _lib.TpaError:
         solver.ctx.call("tpa_time_kernel", 0, 0, 1, 200, C.byref(sweep))
         solver.ctx.call("tpa_time_kernel", 0, 0, 0, 200, C.byref(sweep64))

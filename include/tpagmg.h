@@ -354,7 +354,8 @@ tpa_status tpa_set_stream(tpa_context* ctx, void* stream);
 /* Average device time in ms of `iters` back-to-back launches of one kernel on
  * level `level`: which = 0 smoothing sweep, 1 restriction, 4 first two
  * sweeps, 5 residual (default cycle), 6 / 7 the down / up kernel of a level on
- * CSR tiles; on the plain cycle 1 is residual + restriction;
+ * CSR tiles, 8 / 9 those of a row-streamed level (tiles 4, 5); on the plain
+ * cycle 1 is residual + restriction;
  * 2 prolongation, 3 CG operator product (finest level, FP64).  Measurement
  * support for the roofline; it overwrites the level's work vectors. */
 tpa_status tpa_time_kernel(tpa_context* ctx, int32_t which, int32_t level, int32_t precision, int32_t iters,

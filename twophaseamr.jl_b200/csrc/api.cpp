@@ -755,7 +755,7 @@ tpa_status tpa_set_stream(tpa_context* ctx, void* stream) {
 tpa_status tpa_time_kernel(tpa_context* ctx, int32_t which, int32_t level, int32_t precision, int32_t iters,
                            double* ms) {
     return guard(ctx, [&] {
-        if (which < 0 || which > 7 || iters <= 0 || !ms || (precision != 0 && precision != 1))
+        if (which < 0 || which > 9 || iters <= 0 || !ms || (precision != 0 && precision != 1))
             throw tpa::Error(TPA_ERR_INVALID_ARG, "bad kernel timing request");
         ensure_device(ctx);
         *ms = ctx->dev->time_kernel(which, level, precision, iters);

@@ -1372,7 +1372,34 @@ double DeviceSolver::time_fused(int which, int level, int precision, int iters) 
                                                        counters_.p, nullptr, MeanOnly());
         });
     };
+    // 8 / 9: the down / up row-streaming kernel of a streamed lattice level
+    auto one_stream = [&](const auto& S, const auto& V, auto tag) {
+        using T = decltype(tag);
+        constexpr bool fp32 = std::is_same<T, float>::value;
+        const SView<T>& L = S[size_t(level)];
+        const StreamGeom g = stream_geom(level, fp32);
+        const int grid = tdev_[size_t(level)].sgrid[fp32 ? 1 : 0];
+        with_stream_rows(g.rows, [&](auto rows) {
+            constexpr int RW = decltype(rows)::value;
+            if (which == 8 && level == 0)  // the finest level reads the FP64 residual, as in the cycle
+                v_stream_down<T, double, RW><<<grid, kStreamWarps * 32, 0, stream_>>>(
+                    L, g, (const double*)r_.p, nullptr, V[size_t(level + 1)].b, fpartial_.p, counters_.p, nullptr);
+            else if (which == 8)
+                v_stream_down<T, T, RW><<<grid, kStreamWarps * 32, 0, stream_>>>(
+                    L, g, (const T*)L.b, nullptr, V[size_t(level + 1)].b, fpartial_.p, counters_.p, nullptr);
+            else
+                v_stream_up<T, MeanOnly, RW><<<grid, kStreamWarps * 32, 0, stream_>>>(
+                    L, g, (const T*)V[size_t(level + 1)].x, fpartial_.p, counters_.p, nullptr, MeanOnly());
+        });
+    };
     auto launch = [&]() {
+        if (which == 8 || which == 9) {
+            if (size_t(level) >= tdev_.size() || !tdev_[size_t(level)].stream)
+                throw Error(1, "level does not run on the row-streaming kernels");
+            if (precision == 0) one_stream(sd_, vd_, double(0));
+            else one_stream(sf_, vf_, float(0));
+            return;
+        }
         if (which == 6 || which == 7) {
             if (size_t(level) >= tdev_.size() || !tdev_[size_t(level)].on)
                 throw Error(1, "level does not run on CSR tiles");
