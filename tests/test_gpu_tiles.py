@@ -170,12 +170,15 @@ def test_stencil_tiles_on_small_levels_only():
 
 
 STREAM_CASES = {
-    # (mesh, levels expected on the row-streaming kernels with tiles = 5)
-    "periodic_256": (dict(base_mesh=(256, 256), block_size=(16, 16), periodic=(True, True)), 3),
+    # (mesh, levels expected on the row-streaming kernels with tiles = 5, tail cells)
+    "periodic_256": (dict(base_mesh=(256, 256), block_size=(16, 16), periodic=(True, True)), 3, 1024),
     "periodic_256x128": (dict(base_mesh=(256, 128), block_size=(16, 16), extent=(2.0, 1.0),
-                              periodic=(True, True)), 3),
+                              periodic=(True, True)), 3, 1024),
+    # down to the 32 x 32 level (2 x 2 blocks, one strip wrapping across it), only
+    # the 16 x 16 level in the tail
+    "periodic_128_tail256": (dict(base_mesh=(128, 128), block_size=(16, 16), periodic=(True, True)), 3, 256),
     "channel_256x128": (dict(base_mesh=(256, 128), block_size=(16, 16), extent=(2.0, 1.0),
-                             periodic=(True, False)), 0),  # walls: no level qualifies
+                             periodic=(True, False)), 0, 1024),  # walls: no level qualifies
 }
 
 
@@ -187,12 +190,12 @@ def test_row_streaming_matches_vectorized_kernels(name):
     the six-launch one to rounding (the same row arithmetic; only the coarse
     sums fold in another order), twice (buffers reused), and the solves match
     the oracle with the untiled layout's iteration counts."""
-    spec, nstream = STREAM_CASES[name]
+    spec, nstream, tail = STREAM_CASES[name]
     m = BlockTreeMesh(**spec)
     s = EllipticSolver(PoissonOperator(m), multigrid=MultigridOptions(coarse_size=64))
     s0 = EllipticSolver(PoissonOperator(m), multigrid=MultigridOptions(coarse_size=64))
-    s.set_tuning(tiles=5, tail_cells=1024)
-    s0.set_tuning(tiles=0, tail_cells=1024)
+    s.set_tuning(tiles=5, tail_cells=tail)
+    s0.set_tuning(tiles=0, tail_cells=tail)
     assert s.streamed_levels() == nstream and s0.streamed_levels() == 0
     rng = np.random.default_rng(6)
     vol = m.cell_volumes()

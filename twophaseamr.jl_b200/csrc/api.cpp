@@ -1154,21 +1154,22 @@ tpa_status tpa_autotune(tpa_context* ctx, int32_t precision, int32_t vcycles, tp
         // the CSR levels on haloed block tiles (two launches per level), with
         // the tail sizes around the best one
         for (int tiles : {1, 2, 3})
-            for (int cells : {1024, 2048, 4096}) {
+            for (int cells : {256, 1024, 2048, 4096}) {
                 tpa::TuneConfig tl = b0;
                 tl.tiles = tiles;
                 tl.tail_cells = cells;
                 run(tl);
             }
         // the periodic lattice levels on the row-streaming kernels: the larger
-        // ones (4) or all (5), each with the best tail size of the tiled runs
-        const tpa::TuneConfig tb = res[best_of()].first;
-        for (int tiles : {4, 5}) {
-            tpa::TuneConfig tl = b0;
-            tl.tiles = tiles;
-            tl.tail_cells = tb.tiles ? tb.tail_cells : b0.tail_cells;
-            run(tl);
-        }
+        // ones (4) or all (5), with the small tails (the streamed levels reach
+        // down to 32 x 32 cells)
+        for (int tiles : {4, 5})
+            for (int cells : {256, 1024, 2048}) {
+                tpa::TuneConfig tl = b0;
+                tl.tiles = tiles;
+                tl.tail_cells = cells;
+                run(tl);
+            }
         const size_t b = best_of();
         d.reconfigure(ctx->hier, res[b].first);
         if (best) *best = to_c(res[b].first, res[b].second);
